@@ -1,0 +1,352 @@
+"""Benchmark of the Hush denoise path on synthetic 1080p G-buffer sequences.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--mlp fp32|bf16|f16]
+
+A step is one denoised 1920x1080 frame of the seeded 64-frame sequence (3 independently moving objects, camera pan
+U[0,4] px/frame with 0.2 deg/frame yaw, a camera cut and reset() at frame 32). Inputs are generated on the device
+before timing, so the timed region starts with them resident in HBM; every frame reads its own 83 MB of inputs plus
+~230 MB of state, more than the 126 MB L2, so no L2 flush is needed between frames.
+
+Prints one JSON line (rank 0). For N > 1 (torchrun), every rank denoises its own independent sequence on its own GPU
+(replicas: the path has no cross-GPU exchange); value = total frames / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "1080p ms/frame + %HBM roofline, BF16-MLP vs FP32 plain; train-step ms at equal error"
+W, H, SEQ = 1920, 1080, 64
+
+# Algorithmic bytes per launch of each fused stage at this build's formats (8 B per rgba16float texel), per
+# full-res pixel (P), half-res pixel (h) and quarter-res pixel (q): unique global reads + writes.
+STAGE_BYTES = {
+    "temporal+mlp": lambda P, h, q: P * (32 + 24 + 24) + h * (8 + 40),  # 4 inputs, 3 history gathers, A0/mom/key;
+                                                                        # prev par0, par0..2 + Ah + Gh
+    "mid1+coarse1": lambda P, h, q: h * (32 + 8) + q * 16,               # Ah Gh par1 par2 -> Bh0; -> C1, CG
+    "mid2+coarse2": lambda P, h, q: h * (32 + 8) + q * 24,               # Bh0 Gh par1 par2 -> Bh1; C1 CG -> C0
+    "mid3": lambda P, h, q: h * (32 + 8),                                # Bh1 Gh par1 par2 -> Bh0
+    "fine+final": lambda P, h, q: P * (32 + 16) + h * 48 + q * 16,       # A0 key mat emi -> hist X; 6 half, 2 quarter
+    "taa": lambda P, h, q: P * 32,                                       # X motion prevTaa -> taa
+}
+
+
+def _env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic():
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary (profiles/traffic.json)."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p))
+        except Exception:
+            return {}
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _cpu_baseline_sample(frames: int = 3):
+    """The oracle (f32 restatement of the reference's passes, OpenMP over rows) on 1080p frames: ms/frame over the
+    frames after the first, all host threads."""
+    import numpy as np  # noqa: F401
+
+    import oracle
+    from hush_b200 import builtin_weights, scene
+
+    oracle.set_threads(0)
+    cores = os.cpu_count() or 1
+    cfg = scene.CONFIG_1080P
+    o = oracle.OracleHush(W, H, builtin_weights())
+    times = []
+    for i in range(frames):
+        f = scene.frame_host(cfg, i)
+        t = time.perf_counter()
+        o.denoise(f)
+        times.append(time.perf_counter() - t)
+    ms = 1000.0 * statistics.mean(times[1:] if len(times) > 1 else times)
+    return {"value": round(ms, 3), "unit": "ms/frame", "cores": cores, "kind": "port",
+            "sample": f"{frames} frames of the 1920x1080 sequence (frame 0 untimed), oracle f32, {cores} threads"}
+
+
+def run_reference(args):
+    rank, _, world = _env_rank()
+    if rank != 0:
+        return 0
+    import oracle
+    from hush_b200 import builtin_weights, scene
+
+    oracle.set_threads(0)
+    cores = os.cpu_count() or 1
+    cfg = scene.CONFIG_1080P
+    o = oracle.OracleHush(W, H, builtin_weights())
+    n = args.warmup + args.steps
+    frames = {}
+    times = []
+    for i in range(n):
+        k = i % SEQ
+        if k not in frames:
+            frames[k] = scene.frame_host(cfg, k)
+        if k == 32 or (k == 0 and i > 0):
+            o.reset()
+        t = time.perf_counter()
+        o.denoise(frames[k])
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t)
+        if len(frames) > 4:
+            frames.pop(min(frames))
+    ms = 1000.0 * sum(times) / max(len(times), 1)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(ms, 3), "unit": "ms/frame", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "1920x1080 64-frame sequence, 3 moving objects, pan U[0,4] px/frame, cut at 32",
+                   "width": W, "height": H, "mlp": "fp32"},
+        "cpu_baseline": {"value": round(ms, 3), "unit": "ms/frame", "cores": cores, "kind": "port",
+                         "sample": "one full 1920x1080 frame per step; the reference's WGSL cannot run here (no "
+                                   "WebGPU / Dawn / node), its scalar restatement (oracle/) stands in"},
+        "e2e": {"value": round(ms, 3), "unit": "ms/frame", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from hush_b200 import Hush, scene
+
+    rank, local, world = _env_rank()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    cfg = scene.CONFIG_1080P.with_(seed=1 + rank)
+    nseq = min(SEQ, args.warmup + args.steps)
+    # the sequence, generated on the device (untimed)
+    frames = [scene.frame_device(cfg, i) for i in range(nseq)]
+    torch.cuda.synchronize()
+    hush = Hush(local, {"width": W, "height": H, "mlp": args.mlp, "schedule": args.schedule,
+                        "graph": args.graph})
+    stream = torch.cuda.current_stream()
+
+    def step(i):
+        k = i % nseq
+        if k == 32 or (k == 0 and i > 0):
+            hush.reset()
+        return hush.denoise(frames[k], stream=stream)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world > 1:
+            t = torch.tensor([x], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    # ---- headline: device-resident inputs
+    for i in range(args.warmup):
+        step(i)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for i in range(args.warmup, args.warmup + args.steps):
+            step(i)
+        e1.record(stream)
+        barrier()
+    ms_total = max_over_ranks(e0.elapsed_time(e1))
+    ms_frame = ms_total / args.steps
+    clocks = clk.summary()
+
+    # ---- per-kernel breakdown: the same frames with CUDA events between the stages
+    stage_ms = {}
+    hush_timer_frames = min(args.steps, 16)
+    from hush_b200 import HushTimer
+
+    for i in range(args.warmup + args.steps, args.warmup + args.steps + hush_timer_frames):
+        k = i % nseq
+        if k == 32 or k == 0:
+            hush.reset()
+        t = HushTimer()
+        hush.denoise(frames[k], timer=t, stream=stream)
+        for label, ms in t.last:
+            stage_ms.setdefault(label, []).append(ms)
+    stage_avg = {k: statistics.mean(v) for k, v in stage_ms.items()}
+
+    # ---- end to end through the public API with host buffers (pinned), H2D inputs + D2H output every step
+    host = []
+    for k in range(min(nseq, 8)):
+        host.append({n: frames[k][n].cpu().pin_memory() for n in scene.NAMES})
+    dev_in = {n: torch.empty_like(frames[0][n]) for n in scene.NAMES}
+    out_host = torch.empty((H, W, 4), dtype=torch.float16).pin_memory()
+    hush.reset()
+    e2e_steps = min(args.steps, 32)
+    for i in range(3):
+        for n in scene.NAMES:
+            dev_in[n].copy_(host[i % len(host)][n], non_blocking=True)
+        out_host.copy_(hush.denoise(dev_in, stream=stream), non_blocking=True)
+    barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for i in range(e2e_steps):
+        for n in scene.NAMES:
+            dev_in[n].copy_(host[i % len(host)][n], non_blocking=True)
+        out_host.copy_(hush.denoise(dev_in, stream=stream), non_blocking=True)
+    f1.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1)) / e2e_steps
+    h2d = sum(host[0][n].numel() * 2 for n in scene.NAMES)
+    d2h = out_host.numel() * 2
+
+    if rank != 0:
+        hush.destroy()
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+
+    P, h, q = W * H, ((W + 1) // 2) * ((H + 1) // 2), ((W + 3) // 4) * ((H + 3) // 4)
+    peak, peak_kind = _peaks()
+    per_stage = {}
+    for label, ms in stage_avg.items():
+        nbytes = STAGE_BYTES[label](P, h, q) if label in STAGE_BYTES else None
+        per_stage[label] = {"ms": round(ms, 4),
+                            "gbs": round(nbytes / (ms * 1e-3) / 1e9, 1) if nbytes else None,
+                            "bytes": nbytes}
+    dominant = max(stage_avg, key=stage_avg.get) if stage_avg else None
+    tr = _traffic().get(dominant) if dominant else None
+    roof = None
+    if dominant and dominant in STAGE_BYTES:
+        ach = per_stage[dominant]["gbs"]
+        roof = {"kernel": dominant, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": round(ach / peak, 4), "peak_source": peak_kind,
+                "traffic": (tr or {}).get("bytes_per_launch"),
+                "algorithmic_bytes_per_launch": per_stage[dominant]["bytes"]}
+    filt_bytes = sum(v["bytes"] for v in per_stage.values() if v["bytes"])
+    filt_ms = sum(v["ms"] for v in per_stage.values())
+    n_kernels = 6 if args.schedule == "fused" and args.mlp == "fp32" else 8
+    line = {
+        "metric": METRIC, "value": round(ms_frame / world, 4), "unit": "ms/frame", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_frame, 4), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "1920x1080 64-frame sequence, 3 moving objects, pan U[0,4] px/frame, cut at 32 "
+                               "(reset); inputs generated on the device",
+                   "width": W, "height": H, "mlp": args.mlp, "schedule": args.schedule, "graph": bool(args.graph),
+                   "l2": "no flush: each frame reads 83 MB of fresh inputs + ~230 MB of state (> 126 MB L2)",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": roof,
+        "frame_hbm": {"bytes_per_frame": filt_bytes, "sum_stage_ms": round(filt_ms, 4),
+                      "gbs": round(filt_bytes / (filt_ms * 1e-3) / 1e9, 1) if filt_ms else None,
+                      "frac": round(filt_bytes / (filt_ms * 1e-3) / 1e9 / peak, 4) if filt_ms else None,
+                      "compulsory_108B_per_px_ms": round(108 * P / (peak * 1e9) * 1e3, 4)},
+        "stages": per_stage,
+        "clocks": clocks,
+        "e2e": {"value": round(e2e_ms / world, 4), "unit": "ms/frame", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": n_kernels * args.steps,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = _cpu_baseline_sample()
+    print(json.dumps(line), flush=True)
+    hush.destroy()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--warmup", type=int, default=8)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mlp", default="fp32", choices=["fp32", "bf16", "f16"])
+    ap.add_argument("--schedule", default="fused", choices=["fused", "passes"])
+    ap.add_argument("--graph", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

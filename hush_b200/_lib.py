@@ -1,0 +1,109 @@
+"""ctypes bindings of the C ABI in include/hush.h (libhush_b200.so, built in-tree by hush_b200/build.py)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libhush_b200.so")
+
+HUSH_OK, HUSH_ERR_ARG, HUSH_ERR_DEVICE, HUSH_ERR_CUDA, HUSH_ERR_KERNEL = 0, 1, 2, 3, 4
+MLP_FP32, MLP_BF16, MLP_F16 = 0, 1, 2
+SCHED_FUSED, SCHED_PASSES = 0, 1
+PASS_NAMES = ["temporal", "infer", "mid2", "mid3", "coarse1", "coarse2", "fine_final", "taa"]
+BUF_NAMES = ["A0", "X", "BH0", "BH1", "MOM0", "MOM1", "KEY0", "KEY1", "HIST0", "HIST1", "TAA0", "TAA1",
+             "PAR0_0", "PAR0_1", "PAR1", "PAR2", "F0", "F1", "F2", "F3", "C0", "C1", "CG"]
+BUF = {n: i for i, n in enumerate(BUF_NAMES)}
+
+
+class HushDesc(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("exposure", C.c_float),
+                ("weights", C.POINTER(C.c_uint16)), ("n_weights", C.c_size_t), ("f16", C.c_int),
+                ("mlp_mode", C.c_int), ("schedule", C.c_int), ("device", C.c_int)]
+
+
+class HushInputs(C.Structure):
+    _fields_ = [("radiance", C.c_void_p), ("normal_depth", C.c_void_p), ("motion", C.c_void_p),
+                ("material", C.c_void_p), ("emission", C.c_void_p), ("width", C.c_int * 5),
+                ("height", C.c_int * 5), ("pitch", C.c_size_t * 5)]
+
+
+class HushTiming(C.Structure):
+    _fields_ = [("label", C.c_char_p), ("ms", C.c_float)]
+
+
+class SvgfOptions(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("sigma_l", C.c_float), ("sigma_n", C.c_float), ("sigma_z", C.c_float),
+                ("alpha_color", C.c_float), ("alpha_moments", C.c_float), ("taa_alpha", C.c_float),
+                ("taa", C.c_int)]
+
+
+class SvgfInputs(C.Structure):
+    _fields_ = [("radiance", C.c_void_p), ("normal_depth", C.c_void_p), ("motion", C.c_void_p),
+                ("material", C.c_void_p), ("emission", C.c_void_p), ("prev_normal_depth", C.c_void_p),
+                ("prev_motion", C.c_void_p), ("pitch", C.c_size_t * 7)]
+
+
+class HushScene(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("n_objects", C.c_int), ("n_moving", C.c_int),
+                ("sky_frac", C.c_float), ("pan_min", C.c_float), ("pan_max", C.c_float), ("yaw_deg", C.c_float),
+                ("firefly_rate", C.c_float), ("firefly_scale", C.c_float), ("cut_frame", C.c_int),
+                ("seed", C.c_uint32)]
+
+
+_P = C.c_void_p
+_SIGS = {
+    "hush_hidden_of": (C.c_int, [C.c_long]),
+    "hush_desc_default": (HushDesc, [C.c_int, C.c_int]),
+    "hush_required_limits": (None, [C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_size_t)]),
+    "hush_create": (C.c_int, [C.POINTER(HushDesc), C.POINTER(_P)]),
+    "hush_destroy": (None, [_P]),
+    "hush_resize": (C.c_int, [_P, C.c_int, C.c_int]),
+    "hush_reset": (C.c_int, [_P]),
+    "hush_set_exposure": (C.c_int, [_P, C.c_float]),
+    "hush_get_exposure": (C.c_float, [_P]),
+    "hush_set_weights": (C.c_int, [_P, C.POINTER(C.c_uint16), C.c_size_t]),
+    "hush_set_mlp_mode": (C.c_int, [_P, C.c_int]),
+    "hush_set_schedule": (C.c_int, [_P, C.c_int]),
+    "hush_get_size": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "hush_get_hidden": (C.c_int, [_P]),
+    "hush_get_frame": (C.c_int, [_P]),
+    "hush_denoise": (C.c_int, [_P, C.POINTER(HushInputs), _P, C.POINTER(_P)]),
+    "hush_output": (_P, [_P]),
+    "hush_timer_enable": (C.c_int, [_P, C.c_int]),
+    "hush_timer_read": (C.c_int, [_P, C.POINTER(HushTiming), C.c_int]),
+    "hush_set_graph": (C.c_int, [_P, C.c_int]),
+    "hush_last_error": (C.c_char_p, [_P]),
+    "hush_global_error": (C.c_char_p, []),
+    "hush_run_pass": (C.c_int, [_P, C.c_int, C.POINTER(HushInputs), _P]),
+    "hush_end_frame": (C.c_int, [_P]),
+    "hush_buffer": (C.c_int, [_P, C.c_int, C.POINTER(_P), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                              C.POINTER(C.c_int)]),
+    "svgf_options_default": (SvgfOptions, []),
+    "svgf_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(SvgfOptions), C.c_int, C.POINTER(_P)]),
+    "svgf_destroy": (None, [_P]),
+    "svgf_resize": (C.c_int, [_P, C.c_int, C.c_int]),
+    "svgf_reset": (C.c_int, [_P]),
+    "svgf_encode": (C.c_int, [_P, C.POINTER(SvgfInputs), _P, C.POINTER(_P)]),
+    "svgf_output": (_P, [_P]),
+    "svgf_last_error": (C.c_char_p, [_P]),
+    "hush_scene_frame_host": (C.c_int, [C.POINTER(HushScene), C.c_int] + [C.c_void_p] * 6),
+    "hush_scene_frame_device": (C.c_int, [C.POINTER(HushScene), C.c_int] + [C.c_void_p] * 7),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libhush_b200.so (it must have been built: python -m hush_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"hush_b200: native library missing at {LIB_PATH}; run `python -m hush_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib

@@ -1,0 +1,435 @@
+// Per-pixel device functions of the Hush passes. Each mirrors one WGSL function of the reference
+// (src/denoise/hush.js) with its operation order; the kernels around them decide the tiling and fusion.
+#pragma once
+#include "common.cuh"
+
+namespace hush {
+
+// Everything one frame's kernels need: sizes, borrowed inputs (row pitch in texels), the previous frame's history
+// and this frame's outputs. Internal images are dense (pitch = their width).
+struct HushFrame {
+  int W, H, W2, H2, W4, H4;
+  int reset;        // flags bit 1 of the reference uniform (hush.js:827)
+  float exposure;
+  const uint2 *rad, *nd, *mv, *mat, *emi;
+  int p_rad, p_nd, p_mv, p_mat, p_emi;
+  const uint2 *key_prev, *hist_prev, *mom_prev, *par0_prev, *taa_prev;
+  uint2 *A0, *X, *mom, *key, *hist, *taa, *par0, *par1, *par2, *Bh0, *Bh1, *C0, *C1, *CG;
+  uint4 *F0, *F1, *F2, *F3;
+  // half-res planes of the fused path: block means (F2.zw) and guide (F3.xy) as rgba16float
+  uint2 *Ah, *Gh;
+  const float *w_glob;  // decoded f32 weights in device memory (any hidden width)
+  int hidden;
+  unsigned int *err;    // device error word (bounded waits in the tensor-core MLP)
+};
+
+// Weights of the shipped width (h = 16) passed by value: kernel parameters live in the constant bank, so every
+// thread of a warp reads the same weight in one broadcast (the reference bakes them in as WGSL literals, hush.js:750).
+constexpr int H16_COUNT = 16 * 16 + 34 * 16 + 12;  // 812
+struct MlpW16 {
+  float w[H16_COUNT];
+};
+
+// ------------------------------------------------------------------------------------------------ MLP
+// mlpCode (hush.js:683-704): per output, bias + sum_i input_i * w_i in increasing i; ReLU on the hidden layers.
+template <int HD>
+HD_INL void mlp_fwd(const float *__restrict__ w, const float *f, float *o) {
+  constexpr int W1 = 0, B1 = HD * N_FEAT, W2 = B1 + HD, B2 = W2 + HD * HD, W3 = B2 + HD, B3 = W3 + N_OUT * HD;
+  float h1[HD], h2[HD];
+#pragma unroll
+  for (int j = 0; j < HD; j++) {
+    float a = w[B1 + j];
+#pragma unroll
+    for (int i = 0; i < N_FEAT; i++) a = a + f[i] * w[W1 + j * N_FEAT + i];
+    h1[j] = fmaxf(a, 0.0f);
+  }
+#pragma unroll
+  for (int j = 0; j < HD; j++) {
+    float a = w[B2 + j];
+#pragma unroll
+    for (int i = 0; i < HD; i++) a = a + h1[i] * w[W2 + j * HD + i];
+    h2[j] = fmaxf(a, 0.0f);
+  }
+#pragma unroll
+  for (int j = 0; j < N_OUT; j++) {
+    float a = w[B3 + j];
+#pragma unroll
+    for (int i = 0; i < HD; i++) a = a + h2[i] * w[W3 + j * HD + i];
+    o[j] = a;
+  }
+}
+
+// Any hidden width, weights in global memory.
+HD_INL void mlp_fwd_dyn(const float *__restrict__ w, int hd, const float *f, float *o) {
+  const int W1 = 0, B1 = hd * N_FEAT, W2 = B1 + hd, B2 = W2 + hd * hd, W3 = B2 + hd, B3 = W3 + N_OUT * hd;
+  float h1[256];
+  for (int j = 0; j < hd; j++) {
+    float a = __ldg(w + B1 + j);
+    for (int i = 0; i < N_FEAT; i++) a = a + f[i] * __ldg(w + W1 + j * N_FEAT + i);
+    h1[j] = fmaxf(a, 0.0f);
+  }
+  float h2[256];
+  for (int j = 0; j < hd; j++) {
+    float a = __ldg(w + B2 + j);
+    for (int i = 0; i < hd; i++) a = a + h1[i] * __ldg(w + W2 + j * hd + i);
+    h2[j] = fmaxf(a, 0.0f);
+  }
+  for (int j = 0; j < N_OUT; j++) {
+    float a = __ldg(w + B3 + j);
+    for (int i = 0; i < hd; i++) a = a + h2[i] * __ldg(w + W3 + j * hd + i);
+    o[j] = a;
+  }
+}
+
+// Output heads (hush.js:357-362): par0 = (alpha, gamma, beta, kappa), par1 = s, par2 = c.
+HD_INL void mlp_heads(const float *o, float4 &p0, float4 &p1, float4 &p2) {
+  p0.x = 1.0f / 32.0f + (31.0f / 32.0f) * sigmoidf_(o[0]);
+  p0.y = 0.5f + 7.5f * sigmoidf_(o[1]);
+  p0.z = sigmoidf_(o[2]);
+  p0.w = sigmoidf_(o[3]);
+  p1.x = 0.25f * expf(fminf(fmaxf(o[4], -5.0f), 5.0f));
+  p1.y = 0.25f * expf(fminf(fmaxf(o[5], -5.0f), 5.0f));
+  p1.z = 0.25f * expf(fminf(fmaxf(o[6], -5.0f), 5.0f));
+  p1.w = 0.25f * expf(fminf(fmaxf(o[7], -5.0f), 5.0f));
+  p2.x = expf(fminf(fmaxf(o[8], -4.0f), 4.0f));
+  p2.y = expf(fminf(fmaxf(o[9], -4.0f), 4.0f));
+  p2.z = expf(fminf(fmaxf(o[10], -4.0f), 4.0f));
+  p2.w = expf(fminf(fmaxf(o[11], -4.0f), 4.0f));
+}
+
+// ------------------------------------------------------------------------------------------------ a-trous
+// atrousFn (hush.js:431-476) over shared-memory tiles sA (colour, variance) and sG (decoded normal, depth) of row
+// stride SW. (lx, ly) is the centre's tile position, (qx, qy) its image position, (w, h) the image size for the
+// inside() test. The tiles hold clamp-to-edge loads.
+template <int R, int STEP, bool PREF, int SW>
+HD_INL float4 filt(const float4 *sA, const float4 *sG, int lx, int ly, int qx, int qy, int w, int h, float s,
+                   float c) {
+  const int ti = ly * SW + lx;
+  const float4 gp = sG[ti];
+  const float4 center = sA[ti];
+  float gv;
+  if (PREF) {
+    gv = 0.0625f * (sA[ti - SW - 1].w + sA[ti - SW + 1].w + sA[ti + SW - 1].w + sA[ti + SW + 1].w) +
+         0.125f * (sA[ti - SW].w + sA[ti - 1].w + sA[ti + 1].w + sA[ti + SW].w) + 0.25f * center.w;
+  } else {
+    gv = center.w;
+  }
+  const float lc = lum(center);
+  const float sl = s / (sqrtf(fmaxf(gv, 1e-12f)) + 1e-6f);
+  const float zl = sG[ti - 1].w, zr = sG[ti + 1].w, zu = sG[ti - SW].w, zd = sG[ti + SW].w;
+  const float gx = fminf(zr > 0.0f ? fabsf(zr - gp.w) : 1e9f, zl > 0.0f ? fabsf(zl - gp.w) : 1e9f);
+  const float gy = fminf(zd > 0.0f ? fabsf(zd - gp.w) : 1e9f, zu > 0.0f ? fabsf(zu - gp.w) : 1e9f);
+  const float zg = fminf(fmaxf(gx, gy), gp.w);
+  // 1 / (zg * sqrt(d) * step + 1e-3) per distinct squared distance d (the literal is sqrt(d) * step as f32)
+  float iz[9];
+#pragma unroll
+  for (int d = 1; d <= 2 * R * R; d++) {
+    const float k = d == 1 ? 1.0f * STEP
+                    : d == 2 ? 1.41421356237309515f * STEP
+                    : d == 4 ? 2.0f * STEP
+                    : d == 5 ? 2.23606797749978981f * STEP
+                    : d == 8 ? 2.82842712474619029f * STEP
+                             : 0.0f;
+    iz[d] = 1.0f / (zg * k + 1e-3f);
+  }
+  constexpr float hc = R == 1 ? 0.5f : 0.375f;
+  const float cw = (hc * hc) * c;
+  float sw = cw;
+  float scx = center.x * cw, scy = center.y * cw, scz = center.z * cw;
+  float sv = center.w * cw * cw;
+#pragma unroll
+  for (int dy = -R; dy <= R; dy++) {
+#pragma unroll
+    for (int dx = -R; dx <= R; dx++) {
+      if (dx == 0 && dy == 0) continue;
+      const float hx = R == 1 ? (dx == 0 ? 0.5f : 0.25f) : (dx == 0 ? 0.375f : (dx == 1 || dx == -1) ? 0.25f : 0.0625f);
+      const float hy = R == 1 ? (dy == 0 ? 0.5f : 0.25f) : (dy == 0 ? 0.375f : (dy == 1 || dy == -1) ? 0.25f : 0.0625f);
+      const int o = dy * STEP * SW + dx * STEP;
+      const float4 gq = sG[ti + o];
+      const int tx = qx + dx * STEP, ty = qy + dy * STEP;
+      if (tx >= 0 && ty >= 0 && tx < w && ty < h && gq.w >= 0.0f) {
+        const float4 cq = sA[ti + o];
+        const float wt = (hx * hy) * pow128(fmaxf(dot3(gq, gp), 0.0f)) *
+                         expf(-fabsf(gq.w - gp.w) * iz[dx * dx + dy * dy] - sl * fabsf(lum(cq) - lc));
+        sw += wt;
+        scx += wt * cq.x;
+        scy += wt * cq.y;
+        scz += wt * cq.z;
+        sv += wt * wt * cq.w;
+      }
+    }
+  }
+  return make_float4(scx / sw, scy / sw, scz / sw, sv / (sw * sw));
+}
+
+// ------------------------------------------------------------------------------------------------ TEMPORAL
+// History key test (hush.js:103-105).
+HD_INL bool check_key(float4 k, float4 n, float zPrev, float obj) {
+  return k.z >= 0.0f && k.w == obj && fabsf(k.z - zPrev) <= 0.05f * zPrev + 0.01f &&
+         dot3(oct_dec(k.x, k.y), n) >= 0.9f;
+}
+
+// Per-pixel feature inputs of pixel() (hush.js:111-223), the five vec4 P0..P4.
+struct PixP {
+  float4 P0, P1, P2, P3, P4;
+};
+HD_INL PixP pixp_default() {
+  PixP R;
+  R.P0 = R.P1 = R.P3 = R.P4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  R.P2 = make_float4(0.f, 0.f, -1.0f, 0.f);
+  return R;
+}
+
+// pixel(): temporal accumulation of one pixel at (px, py), illumination tile sI (row stride SW, centre at (lx, ly)).
+// Writes A0, mom, key and returns the feature inputs.
+template <int SW>
+HD_INL PixP temporal_pixel(const HushFrame &f, int px, int py, const float4 *sI, int lx, int ly) {
+  PixP R = pixp_default();
+  const int W = f.W, H = f.H;
+  const float4 nd = ldh(f.nd, py * f.p_nd + px);
+  const float4 mv = ldh(f.mv, py * f.p_mv + px);
+  const int oi = py * W + px;
+  if (nd.w < 0.0f) {
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    sth(f.A0, oi, z);
+    sth(f.mom, oi, z);
+    sth(f.key, oi, make_float4(0.f, 0.f, -1.0f, mv.z));
+    return R;
+  }
+  const float4 mr = ldh(f.mat, py * f.p_mat + px);
+  const int ti = ly * SW + lx;
+  const float4 illum = sI[ti];
+  const float l = lum(illum);
+  float s1x = 0.f, s1y = 0.f, s1z = 0.f, cnt = 0.f;
+#pragma unroll
+  for (int j = 0; j < 9; j++) {
+    const float4 c = sI[ti + (j / 3 - 1) * SW + (j % 3 - 1)];
+    s1x += c.x * c.w; s1y += c.y * c.w; s1z += c.z * c.w;
+    cnt += c.w;
+  }
+  cnt = fmaxf(cnt, 1.0f);
+  const float mux = s1x / cnt, muy = s1y / cnt, muz = s1z / cnt;
+  const float slm = lum3(mux, muy, muz);
+  float svx = 0.f, svy = 0.f, svz = 0.f, svar = 0.f;
+#pragma unroll
+  for (int j = 0; j < 9; j++) {
+    const float4 c = sI[ti + (j / 3 - 1) * SW + (j % 3 - 1)];
+    const float dx = c.x - mux, dy = c.y - muy, dz = c.z - muz;
+    const float dl = lum(c) - slm;
+    svx += c.w * dx * dx; svy += c.w * dy * dy; svz += c.w * dz * dz;
+    svar += c.w * dl * dl;
+  }
+  const float sdx = sqrtf(fmaxf(svx / cnt, 1e-12f)), sdy = sqrtf(fmaxf(svy / cnt, 1e-12f)),
+              sdz = sqrtf(fmaxf(svz / cnt, 1e-12f));
+  svar /= cnt;
+  bool has = false;
+  float hcx = 0.f, hcy = 0.f, hcz = 0.f;
+  float4 hm = make_float4(0.f, 0.f, 0.f, 0.f);
+  float v = 0.f, alpha = 1.0f, gamma = 1.0f;
+  if (!f.reset) {
+    const float ppx = (float)px + mv.x, ppy = (float)py + mv.y;
+    const float bx = floorf(ppx), by = floorf(ppy);
+    const float fx = ppx - bx, fy = ppy - by;
+    const int bix = __float2int_rz(bx), biy = __float2int_rz(by);
+    float sumW = 0.f;
+    const float wts[4] = {(1.0f - fx) * (1.0f - fy), fx * (1.0f - fy), (1.0f - fx) * fy, fx * fy};
+    float4 k4[4], c4[4], m4[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int q = clampi(biy + (i >> 1), 0, H - 1) * W + clampi(bix + (i & 1), 0, W - 1);
+      k4[i] = ldh(f.key_prev, q);
+      c4[i] = ldh(f.hist_prev, q);
+      m4[i] = ldh(f.mom_prev, q);
+    }
+    const int cx = __float2int_rz(floorf(ppx + 0.5f)), cy = __float2int_rz(floorf(ppy + 0.5f));
+    const float4 pq = ldh(f.par0_prev, (clampi(cy, 0, H - 1) >> 1) * f.W2 + (clampi(cx, 0, W - 1) >> 1));
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int qx = bix + (i & 1), qy = biy + (i >> 1);
+      if (wts[i] > 0.0f && qx >= 0 && qy >= 0 && qx < W && qy < H && check_key(k4[i], nd, mv.w, mv.z)) {
+        sumW += wts[i];
+        hcx += wts[i] * c4[i].x; hcy += wts[i] * c4[i].y; hcz += wts[i] * c4[i].z;
+        hm.x += wts[i] * m4[i].x; hm.y += wts[i] * m4[i].y; hm.z += wts[i] * m4[i].z; hm.w += wts[i] * m4[i].w;
+      }
+    }
+    if (sumW >= 0.01f) {
+      hcx /= sumW; hcy /= sumW; hcz /= sumW;
+      hm.x /= sumW; hm.y /= sumW; hm.z /= sumW; hm.w /= sumW;
+      v = sumW;
+      has = true;
+    } else {
+      float n3 = 0.f;
+      hcx = hcy = hcz = 0.f;
+      hm = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int j = 0; j < 9; j++) {
+        const int qx = cx + j % 3 - 1, qy = cy + j / 3 - 1;
+        if (qx >= 0 && qy >= 0 && qx < W && qy < H && check_key(ldh(f.key_prev, qy * W + qx), nd, mv.w, mv.z)) {
+          n3 += 1.0f;
+          const float4 c = ldh(f.hist_prev, qy * W + qx), m = ldh(f.mom_prev, qy * W + qx);
+          hcx += c.x; hcy += c.y; hcz += c.z;
+          hm.x += m.x; hm.y += m.y; hm.z += m.z; hm.w += m.w;
+        }
+      }
+      if (n3 > 0.0f) {
+        hcx /= n3; hcy /= n3; hcz /= n3;
+        hm.x /= n3; hm.y /= n3; hm.z /= n3; hm.w /= n3;
+        v = 0.1f;
+        has = true;
+      }
+    }
+    alpha = pq.x;
+    gamma = pq.y;
+  }
+  has = has && hm.w > 0.0f;
+  float colx = illum.x, coly = illum.y, colz = illum.z;
+  float nmx = l, nmy = l * l, nfast = l, len1 = 1.0f, lag = 0.0f;
+  if (has) {
+    const float hclx = fminf(fmaxf(hcx, mux - gamma * sdx), mux + gamma * sdx);
+    const float hcly = fminf(fmaxf(hcy, muy - gamma * sdy), muy + gamma * sdy);
+    const float hclz = fminf(fmaxf(hcz, muz - gamma * sdz), muz + gamma * sdz);
+    len1 = fminf(hm.w + 1.0f, HMAX);
+    const float a = fmaxf(alpha, 1.0f / len1);
+    colx = hclx + (illum.x - hclx) * a;
+    coly = hcly + (illum.y - hcly) * a;
+    colz = hclz + (illum.z - hclz) * a;
+    nmx = hm.x + (l - hm.x) * a;
+    nmy = hm.y + (l * l - hm.y) * a;
+    nfast = hm.z + (l - hm.z) * fmaxf(1.0f / 6.0f, 1.0f / len1);
+    const float lh = lum3(hcx, hcy, hcz);
+    lag = fabsf(slm - lh) / (sqrtf(fmaxf(svar / cnt, 1e-12f)) + 0.02f * lh + 1e-3f);
+  } else {
+    v = 0.0f;
+  }
+  const float tvar = fmaxf(nmy - nmx * nmx, 0.0f);
+  const float4 A = make_float4(colx, coly, colz, svar + (tvar - svar) * fminf(len1 / 4.0f, 1.0f));
+  const float2 oc = oct_enc(nd.x, nd.y, nd.z);
+  sth(f.A0, oi, A);
+  sth(f.mom, oi, make_float4(nmx, nmy, nfast, len1));
+  sth(f.key, oi, make_float4(oc.x, oc.y, nd.w, mv.z));
+  const float E = f.exposure;
+  const float4 Aq = make_float4(qf16(A.x), qf16(A.y), qf16(A.z), qf16(A.w));
+  const float m1 = E * qf16(nmx);
+  const float m2 = E * E * qf16(nmy);
+  R.P0 = make_float4(E * lum(Aq), E * qf16(l), fmaxf(m2 - m1 * m1, 0.0f), len1);
+  R.P1 = make_float4(qf16(v), qf16(lag), E * qf16(nfast), m1);
+  R.P2 = make_float4(qf16(oc.x), qf16(oc.y), qf16(nd.w), qf16(sqrtf(mv.x * mv.x + mv.y * mv.y)));
+  R.P3 = mr;
+  R.P4 = Aq;
+  return R;
+}
+
+// Block features of block() (hush.js:226-282) from the four pixels' P (j = 0..3 in (x, y) = (j & 1, j >> 1)) and
+// the 4x4 illumination neighbourhood of the block (tile sI, top-left of the neighbourhood at tile index t0).
+// Returns the 20 features in f[], the block mean colour AC, and the guide (oct normal, Z, count) in G; ok = nv > 0.
+template <int SW>
+HD_INL bool block_features(const PixP *P, const float4 *sI, int t0, float E, float *f, float4 &AC, float4 &G) {
+  float nv = 0.f;
+  float4 S0 = make_float4(0.f, 0.f, 0.f, 0.f), S1 = S0, S3 = S0;
+  AC = S0;
+  float Nx = 0.f, Ny = 0.f, Nz = 0.f, MV = 0.f, Z = 0.f;
+  float la[4], zs[4];
+  float4 ns[4];
+  bool ok[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    ok[j] = P[j].P2.z >= 0.0f;
+    la[j] = 0.f; zs[j] = 0.f;
+    ns[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!ok[j]) continue;
+    nv += 1.0f;
+    la[j] = P[j].P0.x;
+    ns[j] = oct_dec(P[j].P2.x, P[j].P2.y);
+    zs[j] = P[j].P2.z;
+    S0.x += P[j].P0.x; S0.y += P[j].P0.y; S0.z += P[j].P0.z; S0.w += P[j].P0.w;
+    S1.x += P[j].P1.x; S1.y += P[j].P1.y; S1.z += P[j].P1.z; S1.w += P[j].P1.w;
+    Nx += ns[j].x; Ny += ns[j].y; Nz += ns[j].z;
+    S3.x += P[j].P3.x; S3.y += P[j].P3.y; S3.z += P[j].P3.z; S3.w += P[j].P3.w;
+    AC.x += P[j].P4.x; AC.y += P[j].P4.y; AC.z += P[j].P4.z; AC.w += P[j].P4.w;
+    MV += P[j].P2.w;
+    Z += P[j].P2.z;
+  }
+  if (nv == 0.0f) {
+    G = make_float4(0.f, 0.f, -1.0f, 0.f);
+    return false;
+  }
+  const float k = 1.0f / nv;
+  S0.x *= k; S0.y *= k; S0.z *= k; S0.w *= k;
+  S1.x *= k; S1.y *= k; S1.z *= k; S1.w *= k;
+  Nx *= k; Ny *= k; Nz *= k;
+  S3.x *= k; S3.y *= k; S3.z *= k; S3.w *= k;
+  AC.x *= k; AC.y *= k; AC.z *= k; AC.w *= k;
+  MV *= k;
+  Z *= k;
+  const float Lacc = S0.x;
+  float VA = 0.f;
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+    if (ok[j]) VA += (la[j] - Lacc) * (la[j] - Lacc);
+  VA *= k;
+  float s1 = 0.f, n4 = 0.f;
+  float lq[16];
+#pragma unroll
+  for (int j = 0; j < 16; j++) {
+    const float4 t = sI[t0 + (j >> 2) * SW + (j & 3)];
+    lq[j] = E * qf16(lum(t));
+    s1 += t.w * E * qf16(lum(t));
+    n4 += t.w;
+  }
+  const float mu4 = s1 / fmaxf(n4, 1.0f);
+  float var4 = 0.f;
+#pragma unroll
+  for (int j = 0; j < 16; j++) {
+    const float w = sI[t0 + (j >> 2) * SW + (j & 3)].w;
+    const float d = lq[j] - mu4;
+    var4 += w * d * d;
+  }
+  var4 /= fmaxf(n4, 1.0f);
+  const float nl = fmaxf(sqrtf(Nx * Nx + Ny * Ny + Nz * Nz), 1e-6f);
+  const float4 Nn = make_float4(Nx / nl, Ny / nl, Nz / nl, 0.f);
+  float zmax = -1e30f, zmin = 1e30f, mind = 1e30f;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    if (ok[j]) {
+      zmax = fmaxf(zmax, zs[j]);
+      zmin = fminf(zmin, zs[j]);
+      mind = fminf(mind, dot3(ns[j], Nn));
+    }
+  }
+  const float dz = fminf(fmaxf((zmax - zmin) / fmaxf(zmin, 1e-6f), 0.0f), 1.0f);
+  const float dn = fminf(fmaxf(1.0f - mind, 0.0f), 2.0f);
+  const float2 oc = oct_enc(Nn.x, Nn.y, Nn.z);
+  f[0] = log1p_w(Lacc); f[1] = log1p_w(S0.y); f[2] = log1p_w(S0.z); f[3] = log1p_w(var4);
+  f[4] = S0.w / HMAX; f[5] = S1.x; f[6] = log1p_w(S1.y);
+  f[7] = log1p_w(fabsf(S1.z - S1.w) / (S1.w + 1e-3f));
+  f[8] = oc.x; f[9] = oc.y; f[10] = dz; f[11] = dn;
+  f[12] = S3.x; f[13] = S3.y; f[14] = S3.z; f[15] = S3.w;
+  f[16] = 1.0f - nv / 4.0f; f[17] = log1p_w(MV); f[18] = log1p_w(mu4); f[19] = log1p_w(VA);
+  G = make_float4(oc.x, oc.y, Z, nv);
+  return true;
+}
+
+// ------------------------------------------------------------------------------------------------ FINE_FINAL
+HD_INL float jbw(float frx, float fry, int j, float4 nq, float zq, float4 n, float z) {  // hush.js:552-558
+  const float wb = ((j & 1) == 1 ? frx : 1.0f - frx) * ((j >> 1) == 1 ? fry : 1.0f - fry);
+  const float dn = fmaxf(dot3(nq, n), 0.0f);
+  const float dn2 = dn * dn;
+  const float dn4 = dn2 * dn2;
+  return wb * expf(-fabsf(zq - z) / (0.05f * z + 1e-3f)) * dn4 * dn4;
+}
+
+// ------------------------------------------------------------------------------------------------ TAA
+HD_INL float3 to_ycocg(float3 c) {
+  return make_float3(c.x * 0.25f + c.y * 0.5f + c.z * 0.25f, c.x * 0.5f - c.z * 0.5f,
+                     -c.x * 0.25f + c.y * 0.5f - c.z * 0.25f);
+}
+HD_INL float3 from_ycocg(float3 c) { return make_float3(c.x + c.y - c.z, c.x + c.z, c.x - c.y - c.z); }
+HD_INL float3 tmap(float3 c) {
+  const float d = 1.0f + lum3(c.x, c.y, c.z);
+  return make_float3(c.x / d, c.y / d, c.z / d);
+}
+HD_INL float3 itmap(float3 c) {
+  const float d = fmaxf(1.0f - lum3(c.x, c.y, c.z), 1e-4f);
+  return make_float3(c.x / d, c.y / d, c.z / d);
+}
+
+}  // namespace hush

@@ -1,0 +1,174 @@
+/* hush_b200: C ABI of the B200-native Hush denoiser (and its SVGF baseline).
+ *
+ * The drop-in boundary for the reference's `Hush` / `SVGF` JavaScript classes (src/index.d.ts:36-83). Device
+ * buffers replace GPUTextures: every image is rgba16float, i.e. 4 x f16 = 8 bytes per texel, row-major, with a row
+ * pitch in bytes (0 = dense, width * 8). The WebGPU command encoder is replaced by a CUDA stream (`void *` holding a
+ * cudaStream_t; NULL = the default stream). Calls are stream-ordered and not thread-safe per instance.
+ *
+ * Every call returns HUSH_OK (0) or an error code; the message (same text as the reference's thrown Error) is
+ * available from hush_last_error(instance) or, for calls without an instance, hush_global_error().
+ */
+#ifndef HUSH_B200_H
+#define HUSH_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HUSH_OK 0
+#define HUSH_ERR_ARG 1      /* bad argument: missing input, size mismatch, bad weights, bad size */
+#define HUSH_ERR_DEVICE 2   /* device lacks a required capability (the reference's requiredLimits check) */
+#define HUSH_ERR_CUDA 3     /* a CUDA runtime call failed */
+#define HUSH_ERR_KERNEL 4   /* a kernel reported an error word (e.g. a bounded wait that gave up) */
+
+typedef struct hush_s hush_t;
+typedef struct svgf_s svgf_t;
+
+/* MLP arithmetic. FP32 is the reference's form (f32 FMA chain, hush.js:683-704); BF16 / F16 run the three layers
+ * as tcgen05 tensor-core MMAs with FP32 accumulation (operands rounded to bf16 / f16). */
+enum { HUSH_MLP_FP32 = 0, HUSH_MLP_BF16 = 1, HUSH_MLP_F16 = 2 };
+
+/* Kernel schedule: FUSED (default) = the B200 frame (fused temporal+features+MLP, half-res pyramid, fine+final+TAA);
+ * PASSES = one kernel per reference dispatch (hush.js:858-870). Both give the same results. */
+enum { HUSH_SCHED_FUSED = 0, HUSH_SCHED_PASSES = 1 };
+
+/* Constructor options: replaces HushOptions (src/index.d.ts:19-29, hush.js:728-732). */
+typedef struct {
+  int width, height;
+  float exposure;            /* default 1 when the descriptor comes from hush_desc_default() */
+  const uint16_t *weights;   /* f16 blob W1 b1 W2 b2 W3 b3 (hush.js:20-21); NULL = built-in weights */
+  size_t n_weights;          /* number of f16 values; the MLP width follows (hiddenOf) */
+  int f16;                   /* reference option `f16` (hush.js:740): selects HUSH_MLP_F16 when mlp_mode is FP32 */
+  int mlp_mode;              /* HUSH_MLP_* */
+  int schedule;              /* HUSH_SCHED_* */
+  int device;                /* CUDA device ordinal; -1 = current device */
+} hush_desc;
+
+/* Frame inputs: replaces HushInputs (src/index.d.ts:11-17). Device pointers to rgba16float images.
+ * width/height are the sizes of the images (checked against the denoiser's, hush.js:814-820); 0 = trust the
+ * caller. pitch is the row pitch in bytes, 0 = dense. */
+typedef struct {
+  const void *radiance, *normal_depth, *motion, *material, *emission;
+  int width[5], height[5];
+  size_t pitch[5];
+} hush_inputs;
+
+/* Per-pass GPU time of the last denoise(), like the reference's timer hook (hush.js:842-851, gpu.js:25-77). */
+typedef struct {
+  const char *label;
+  float ms;
+} hush_timing;
+
+/* hiddenOf (hush.js:22-25): hidden width h for n f16 weights (n = h^2 + 34 h + 12), 0 if none fits. */
+int hush_hidden_of(long n);
+
+/* Defaults for hush_desc (exposure 1, built-in weights, FP32 MLP, fused schedule, current device). */
+hush_desc hush_desc_default(int width, int height);
+
+/* Hush.requiredLimits (hush.js:721, 726): compute capability and dynamic shared memory the kernels need. */
+void hush_required_limits(int *cc_major, int *cc_minor, size_t *shared_bytes);
+
+/* new Hush(device, options) (hush.js:731-761). */
+int hush_create(const hush_desc *desc, hush_t **out);
+/* destroy() (hush.js:803-807). */
+void hush_destroy(hush_t *h);
+/* resize(width, height) (hush.js:764-794): reallocates when the size changes and resets the history. */
+int hush_resize(hush_t *h, int width, int height);
+/* reset() (hush.js:801): the next frame starts without history. */
+int hush_reset(hush_t *h);
+/* exposure property (hush.js:739, read per frame at 828). */
+int hush_set_exposure(hush_t *h, float exposure);
+float hush_get_exposure(const hush_t *h);
+/* Replaces the MLP weights (same blob format as the constructor option). */
+int hush_set_weights(hush_t *h, const uint16_t *weights, size_t n);
+int hush_set_mlp_mode(hush_t *h, int mode);
+int hush_set_schedule(hush_t *h, int schedule);
+int hush_get_size(const hush_t *h, int *width, int *height);
+int hush_get_hidden(const hush_t *h);
+int hush_get_frame(const hush_t *h);
+
+/* denoise(encoder, inputs, timer) (hush.js:813-822, encode 835-874): enqueues one frame on `stream` and returns
+ * (in *out) the instance-owned output image (rgba16float, dense, linear HDR, alpha 1). Two images alternate from
+ * frame to frame: the pointer stays valid until the next-but-one call (hush.js:796-798). */
+int hush_denoise(hush_t *h, const hush_inputs *in, void *stream, const void **out);
+/* output getter (hush.js:798): the last frame's output image. */
+const void *hush_output(const hush_t *h);
+
+/* Timer (hush.js:842-851): mode 0 off, 1 per pass, 2 whole frame as one span. hush_timer_read synchronises on
+ * the recorded events and fills up to max entries; returns the number filled (or -1 on error). */
+int hush_timer_enable(hush_t *h, int mode);
+int hush_timer_read(hush_t *h, hush_timing *out, int max);
+
+/* CUDA-graph replay of whole frames (config-5 style): capture the frame once per input-pointer set and replay it. */
+int hush_set_graph(hush_t *h, int enable);
+
+/* Last error message of the instance / of the calling thread (for hush_create failures). */
+const char *hush_last_error(const hush_t *h);
+const char *hush_global_error(void);
+
+/* ---- pass-level interface (tests, adjoint checks) ------------------------------------------------------------
+ * Pass ids follow the reference's dispatch order (hush.js:858-870). hush_run_pass runs one reference pass on the
+ * instance's state for the current frame (ping-pong by frame parity, hush.js:837); hush_end_frame does the frame++
+ * and history-reset bookkeeping (hush.js:871-872). */
+enum {
+  HUSH_PASS_TEMPORAL = 0, HUSH_PASS_INFER, HUSH_PASS_MID2, HUSH_PASS_MID3, HUSH_PASS_COARSE1, HUSH_PASS_COARSE2,
+  HUSH_PASS_FINE_FINAL, HUSH_PASS_TAA, HUSH_PASS_COUNT
+};
+/* State images (hush.js:783-793). F0..F3 are 16-byte texels (8 x f16); the rest 8-byte texels (4 x f16). */
+enum {
+  HUSH_BUF_A0 = 0, HUSH_BUF_X, HUSH_BUF_BH0, HUSH_BUF_BH1, HUSH_BUF_MOM0, HUSH_BUF_MOM1, HUSH_BUF_KEY0,
+  HUSH_BUF_KEY1, HUSH_BUF_HIST0, HUSH_BUF_HIST1, HUSH_BUF_TAA0, HUSH_BUF_TAA1, HUSH_BUF_PAR0_0, HUSH_BUF_PAR0_1,
+  HUSH_BUF_PAR1, HUSH_BUF_PAR2, HUSH_BUF_F0, HUSH_BUF_F1, HUSH_BUF_F2, HUSH_BUF_F3, HUSH_BUF_C0, HUSH_BUF_C1,
+  HUSH_BUF_CG, HUSH_BUF_COUNT
+};
+int hush_run_pass(hush_t *h, int pass, const hush_inputs *in, void *stream);
+int hush_end_frame(hush_t *h);
+/* Device pointer and geometry of a state image. */
+int hush_buffer(hush_t *h, int id, void **dptr, int *width, int *height, int *texel_bytes);
+
+/* ---- SVGF baseline (src/denoise/svgf.js) ---------------------------------------------------------------------- */
+/* SVGFOptions (src/index.d.ts:63-72, svgf.js:278-281). iterations must be 1..5 (the reference's uniform array
+ * holds 5 a-trous iterations, svgf.js:294). */
+typedef struct {
+  int iterations;
+  float sigma_l, sigma_n, sigma_z, alpha_color, alpha_moments, taa_alpha;
+  int taa;
+} svgf_options;
+/* Inputs: HushInputs plus last frame's normalDepth / motion (svgf.js:341). */
+typedef struct {
+  const void *radiance, *normal_depth, *motion, *material, *emission, *prev_normal_depth, *prev_motion;
+  size_t pitch[7];
+} svgf_inputs;
+
+svgf_options svgf_options_default(void);
+/* new SVGF(device, width, height, options) (svgf.js:273-300). */
+int svgf_create(int width, int height, const svgf_options *opts, int device, svgf_t **out);
+void svgf_destroy(svgf_t *s);
+int svgf_resize(svgf_t *s, int width, int height);
+int svgf_reset(svgf_t *s);
+/* encode(encoder, inputs) (svgf.js:343-378): one frame; *out = this frame's output image. */
+int svgf_encode(svgf_t *s, const svgf_inputs *in, void *stream, const void **out);
+const void *svgf_output(const svgf_t *s);
+const char *svgf_last_error(const svgf_t *s);
+
+/* ---- synthetic G-buffer scenes (benchmark / test / training inputs) ------------------------------------------ */
+typedef struct {
+  int width, height, n_objects, n_moving;
+  float sky_frac, pan_min, pan_max, yaw_deg, firefly_rate, firefly_scale;
+  int cut_frame;
+  uint32_t seed;
+} hush_scene;
+/* One frame on the host: five dense rgba16float images (may be NULL) and the noise-free radiance + emission as
+ * f32 rgb (may be NULL). */
+int hush_scene_frame_host(const hush_scene *sc, int frame, uint16_t *radiance, uint16_t *normal_depth,
+                          uint16_t *motion, uint16_t *material, uint16_t *emission, float *clean);
+/* The same on the device, enqueued on `stream`. */
+int hush_scene_frame_device(const hush_scene *sc, int frame, void *radiance, void *normal_depth, void *motion,
+                            void *material, void *emission, void *clean, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,180 @@
+"""CPU oracle of the Hush denoise path: TEST INFRASTRUCTURE ONLY.
+
+Loaded by the tests, by ``__graft_entry__.smoke()`` as the checker and by ``bench.py``'s CPU-baseline leg; never by
+the product path (hush_b200). See hush_oracle.h for what it restates and its parity status (unpinned by reference
+outputs: the reference ships no golden vectors and cannot run here).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle_hush.so")
+
+PASS_NAMES = ["temporal", "infer", "mid2", "mid3", "coarse1", "coarse2", "fine_final", "taa"]
+BUF_NAMES = ["A0", "X", "BH0", "BH1", "MOM0", "MOM1", "KEY0", "KEY1", "HIST0", "HIST1", "TAA0", "TAA1",
+             "PAR0_0", "PAR0_1", "PAR1", "PAR2", "F0", "F1", "F2", "F3", "C0", "C1", "CG"]
+INPUTS = ["radiance", "normalDepth", "motion", "material", "emission"]
+
+
+class _Inputs(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("radiance", "normal_depth", "motion", "material", "emission")]
+
+
+class _SvgfOpts(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("sigma_l", C.c_float), ("sigma_n", C.c_float), ("sigma_z", C.c_float),
+                ("alpha_color", C.c_float), ("alpha_moments", C.c_float), ("taa_alpha", C.c_float),
+                ("taa", C.c_int)]
+
+
+class _SvgfInputs(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("radiance", "normal_depth", "motion", "material", "emission",
+                                           "prev_normal_depth", "prev_motion")]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"oracle library missing at {LIB_PATH}; run `make -C oracle`")
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        sig = {
+            "ho_hidden_of": (C.c_int, [C.c_long]),
+            "ho_hush_create": (P, [C.c_int, C.c_int, C.c_float, P, C.c_long, C.c_int]),
+            "ho_hush_destroy": (None, [P]),
+            "ho_hush_reset": (None, [P]),
+            "ho_hush_set_exposure": (None, [P, C.c_float]),
+            "ho_hush_frame": (C.c_int, [P]),
+            "ho_hush_denoise": (P, [P, C.POINTER(_Inputs)]),
+            "ho_hush_pass": (C.c_int, [P, C.c_int, C.POINTER(_Inputs)]),
+            "ho_hush_end_frame": (None, [P]),
+            "ho_hush_buffer": (P, [P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+            "ho_set_threads": (None, [C.c_int]),
+            "ho_f2h_rz": (C.c_uint16, [C.c_float]),
+            "ho_h2f": (C.c_float, [C.c_uint16]),
+            "ho_qf16": (C.c_float, [C.c_float]),
+            "ho_mlp": (None, [P, C.c_long, P, P, C.c_int]),
+            "ho_svgf_create": (P, [C.c_int, C.c_int, C.POINTER(_SvgfOpts), C.c_int]),
+            "ho_svgf_destroy": (None, [P]),
+            "ho_svgf_reset": (None, [P]),
+            "ho_svgf_encode": (P, [P, C.POINTER(_SvgfInputs)]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def set_threads(n: int = 0):
+    lib().ho_set_threads(int(n))
+
+
+def _as_u16(a: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(a)
+    return a.view(np.uint16) if a.dtype == np.float16 else a.astype(np.uint16)
+
+
+class OracleHush:
+    """The oracle's Hush instance (mode 0: f32 like the WGSL, mode 1: f64 arithmetic)."""
+
+    def __init__(self, width, height, weights: np.ndarray, exposure=1.0, fp64=False):
+        self.w16 = np.ascontiguousarray(weights.astype(np.uint16))
+        self.W, self.H = int(width), int(height)
+        self._h = lib().ho_hush_create(self.W, self.H, float(exposure), self.w16.ctypes.data, self.w16.size,
+                                       1 if fp64 else 0)
+        if not self._h:
+            raise ValueError("oracle: bad weights or size")
+        self._keep = None
+
+    def _inputs(self, inputs: dict) -> _Inputs:
+        arrs = [np.ascontiguousarray(inputs[n]).view(np.uint16) for n in INPUTS]
+        self._keep = arrs
+        return _Inputs(*[a.ctypes.data for a in arrs])
+
+    def denoise(self, inputs: dict) -> np.ndarray:
+        inp = self._inputs(inputs)
+        p = lib().ho_hush_denoise(self._h, C.byref(inp))
+        return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint16)), (self.H, self.W, 4)).view(np.float16).copy()
+
+    def run_pass(self, name: str, inputs: dict | None = None):
+        inp = self._inputs(inputs) if inputs is not None else _Inputs()
+        lib().ho_hush_pass(self._h, PASS_NAMES.index(name), C.byref(inp))
+
+    def end_frame(self):
+        lib().ho_hush_end_frame(self._h)
+
+    def reset(self):
+        lib().ho_hush_reset(self._h)
+
+    def set_exposure(self, e):
+        lib().ho_hush_set_exposure(self._h, float(e))
+
+    @property
+    def frame(self):
+        return lib().ho_hush_frame(self._h)
+
+    def buffer(self, name: str) -> np.ndarray:
+        """Live view of a state buffer as float16 (h, w, channels)."""
+        w, h, c = C.c_int(), C.c_int(), C.c_int()
+        p = lib().ho_hush_buffer(self._h, BUF_NAMES.index(name), C.byref(w), C.byref(h), C.byref(c))
+        return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint16)), (h.value, w.value, c.value)).view(np.float16)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().ho_hush_destroy(self._h)
+            self._h = None
+
+
+class OracleSVGF:
+    def __init__(self, width, height, options: dict | None = None, fp64=False):
+        o = _SvgfOpts(5, 4.0, 128.0, 1.0, 0.2, 0.2, 0.1, 1)
+        names = {"iterations": "iterations", "sigmaL": "sigma_l", "sigmaN": "sigma_n", "sigmaZ": "sigma_z",
+                 "alphaColor": "alpha_color", "alphaMoments": "alpha_moments", "taaAlpha": "taa_alpha", "taa": "taa"}
+        for k, v in (options or {}).items():
+            setattr(o, names[k], int(v) if k in ("iterations", "taa") else float(v))
+        self.W, self.H = int(width), int(height)
+        self._h = lib().ho_svgf_create(self.W, self.H, C.byref(o), 1 if fp64 else 0)
+
+    def encode(self, inputs: dict) -> np.ndarray:
+        names = INPUTS + ["prevNormalDepth", "prevMotion"]
+        arrs = [np.ascontiguousarray(inputs[n]).view(np.uint16) for n in names]
+        inp = _SvgfInputs(*[a.ctypes.data for a in arrs])
+        p = lib().ho_svgf_encode(self._h, C.byref(inp))
+        return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint16)), (self.H, self.W, 4)).view(np.float16).copy()
+
+    def reset(self):
+        lib().ho_svgf_reset(self._h)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().ho_svgf_destroy(self._h)
+            self._h = None
+
+
+def f2h_rz(x: float) -> int:
+    return int(lib().ho_f2h_rz(float(x)))
+
+
+def h2f(h: int) -> float:
+    return float(lib().ho_h2f(int(h)))
+
+
+def qf16(x: float) -> float:
+    return float(lib().ho_qf16(float(x)))
+
+
+def mlp(weights: np.ndarray, features: np.ndarray, fp64=False) -> np.ndarray:
+    w = np.ascontiguousarray(weights.astype(np.uint16))
+    f = np.ascontiguousarray(features.astype(np.float32))
+    o = np.zeros(12, dtype=np.float32)
+    lib().ho_mlp(w.ctypes.data, w.size, f.ctypes.data, o.ctypes.data, 1 if fp64 else 0)
+    return o

@@ -1,0 +1,271 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle, on a B200.
+
+Bound (north star): |cuda - oracle| <= 2e-3 * max(|oracle|, floor) per channel with floor = 1e-2 of the frame's
+mean |value|. Pass-level tests start every pass from the oracle's exact state, so differences cannot accumulate;
+sequence tests run both sides independently over whole sequences, where the f16 history feeds rounding differences
+back frame after frame.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from hush_b200 import Hush, HushError, SVGF, builtin_weights, scene
+
+from .util import mismatch, to_f32
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# per-pass: fraction of values allowed outside the bound (f16 round-toward-zero boundary flips of a last-ulp f32
+# difference); sequences: the same differences fed back through the temporal history and TAA
+PASS_FRAC = 2e-3
+SEQ_FRAC = 1e-2
+
+PASS_OUTPUTS = {
+    "temporal": ["A0", "MOM{c}", "KEY{c}", "F0", "F1", "F2", "F3"],
+    "infer": ["PAR0_{c}", "PAR1", "PAR2", "BH0"],
+    "mid2": ["BH1"],
+    "mid3": ["BH0"],
+    "coarse1": ["C1", "CG"],
+    "coarse2": ["C0"],
+    "fine_final": ["HIST{c}", "X"],
+    "taa": ["TAA{c}"],
+}
+
+
+def _dev(frame):
+    return {k: torch.from_numpy(np.ascontiguousarray(frame[k])).cuda() for k in oracle.INPUTS}
+
+
+def _upload(o, g, names=None):
+    for name in names or oracle.BUF_NAMES:
+        src = torch.from_numpy(o.buffer(name).copy()).cuda()
+        g.buffer(name).copy_(src)
+    torch.cuda.synchronize()
+
+
+def _download(g, name):
+    return g.buffer(name).float().cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def seq_small():
+    cfg = scene.SceneConfig(128, 72, 5, n_moving=2, pan_min=1.0, pan_max=3.0, seed=5)
+    return cfg, [scene.frame_host(cfg, i) for i in range(cfg.frames)]
+
+
+@pytest.mark.parametrize("pass_name", oracle.PASS_NAMES)
+def test_pass_level_parity(seq_small, pass_name):
+    cfg, frames = seq_small
+    o = oracle.OracleHush(cfg.width, cfg.height, builtin_weights())
+    for f in frames[:3]:
+        o.denoise(f)
+    g = Hush(0, {"width": cfg.width, "height": cfg.height, "schedule": "passes"})
+    for _ in range(3):
+        g.end_frame()
+    f = frames[3]
+    fd = _dev(f)
+    c = o.frame & 1
+    for p in oracle.PASS_NAMES:
+        _upload(o, g)
+        o.run_pass(p, f)
+        g.run_pass(p, fd)
+        torch.cuda.synchronize()
+        if p != pass_name:
+            continue
+        for name in PASS_OUTPUTS[p]:
+            name = name.format(c=c)
+            ref = o.buffer(name).astype(np.float32)
+            got = _download(g, name)
+            frac, worst, _ = mismatch(got, ref)
+            assert frac <= PASS_FRAC, f"{p}/{name}: {frac:.2e} of values out of bound (worst {worst:.3g})"
+        break
+
+
+def _run_sequence(cfg, frames, sched, mlp="fp32", reset_at=(), exposure=None):
+    o = oracle.OracleHush(cfg.width, cfg.height, builtin_weights())
+    g = Hush(0, {"width": cfg.width, "height": cfg.height, "schedule": sched, "mlp": mlp})
+    stats = []
+    for i, f in enumerate(frames):
+        if i in reset_at:
+            o.reset()
+            g.reset()
+        if exposure is not None and i == 1:
+            o.set_exposure(exposure)
+            g.exposure = exposure
+        ref = o.denoise(f).astype(np.float32)
+        got = to_f32(g.denoise(_dev(f)))
+        stats.append(mismatch(got, ref))
+    return stats
+
+
+@pytest.mark.parametrize("sched", ["passes", "fused"])
+def test_sequence_parity_360p(sched):
+    cfg = scene.CONFIG_360P
+    frames = [scene.frame_host(cfg, i) for i in range(cfg.frames)]
+    stats = _run_sequence(cfg, frames, sched)
+    for i, (frac, worst, _) in enumerate(stats):
+        assert frac <= SEQ_FRAC, f"frame {i}: {frac:.2e} out of bound (worst {worst:.3g})"
+
+
+@pytest.mark.parametrize("sched", ["passes", "fused"])
+def test_committed_fixture(sched):
+    gf = np.load(os.path.join(HERE, "golden", "oracle_seq.npz"))
+    H, W = gf["out0"].shape[:2]
+    g = Hush(0, {"width": W, "height": H, "schedule": sched})
+    n = sum(1 for k in gf.files if k.startswith("out"))
+    for i in range(n):
+        inp = {k: torch.from_numpy(gf[f"in{i}_{k}"]).cuda() for k in oracle.INPUTS}
+        got = to_f32(g.denoise(inp))
+        frac, worst, _ = mismatch(got, gf[f"out{i}"].astype(np.float32))
+        assert frac <= SEQ_FRAC, f"frame {i}: {frac:.2e} (worst {worst:.3g})"
+
+
+@pytest.mark.parametrize("size", [(1, 1), (2, 2), (3, 1), (17, 9), (33, 17), (65, 3), (130, 67)])
+@pytest.mark.parametrize("sched", ["passes", "fused"])
+def test_odd_and_tiny_sizes(size, sched):
+    W, H = size
+    cfg = scene.SceneConfig(W, H, 3, n_moving=1, pan_min=2.0, pan_max=2.0, seed=9)
+    frames = [scene.frame_host(cfg, i) for i in range(cfg.frames)]
+    for i, (frac, worst, _) in enumerate(_run_sequence(cfg, frames, sched)):
+        assert frac <= max(SEQ_FRAC, 2.0 / (W * H * 4)), (size, i, frac, worst)
+
+
+def test_reset_and_exposure_mid_sequence():
+    cfg = scene.SceneConfig(96, 64, 5, n_moving=2, pan_min=3.0, pan_max=3.0, seed=4)
+    frames = [scene.frame_host(cfg, i) for i in range(cfg.frames)]
+    for sched in ("passes", "fused"):
+        for i, (frac, worst, _) in enumerate(_run_sequence(cfg, frames, sched, reset_at=(3,), exposure=2.5)):
+            assert frac <= SEQ_FRAC, (sched, i, frac, worst)
+
+
+def test_fused_matches_passes_state():
+    cfg = scene.SceneConfig(160, 96, 4, n_moving=2, pan_min=1.0, pan_max=2.0, seed=12)
+    frames = [scene.frame_host(cfg, i) for i in range(cfg.frames)]
+    a = Hush(0, {"width": cfg.width, "height": cfg.height, "schedule": "passes"})
+    b = Hush(0, {"width": cfg.width, "height": cfg.height, "schedule": "fused"})
+    for f in frames:
+        fd = _dev(f)
+        oa, ob = to_f32(a.denoise(fd)), to_f32(b.denoise(fd))
+        assert mismatch(ob, oa)[0] <= SEQ_FRAC
+    c = (a.frame - 1) & 1
+    for name in ("A0", f"MOM{c}", f"KEY{c}", f"PAR0_{c}", "PAR1", "PAR2", f"HIST{c}", "BH0", "C0", "CG"):
+        assert mismatch(_download(b, name), _download(a, name))[0] <= SEQ_FRAC, name
+
+
+def test_pitched_inputs_match_dense():
+    cfg = scene.SceneConfig(70, 40, 2, seed=13)
+    frames = [scene.frame_host(cfg, i) for i in range(cfg.frames)]
+    a = Hush(0, {"width": 70, "height": 40})
+    b = Hush(0, {"width": 70, "height": 40})
+    for f in frames:
+        dense = _dev(f)
+        pitched = {}
+        for k, t in dense.items():
+            big = torch.zeros((40, 96, 4), dtype=torch.float16, device="cuda")
+            big[:, 5:75] = t
+            pitched[k] = big[:, 5:75]
+        oa = a.denoise(dense).clone()
+        ob = b.denoise(pitched).clone()
+        assert torch.equal(oa, ob)
+
+
+def test_output_alternates_and_getter():
+    g = Hush(0, {"width": 32, "height": 16})
+    cfg = scene.SceneConfig(32, 16, 3, seed=2)
+    ptrs = []
+    for i in range(3):
+        out = g.denoise(_dev(scene.frame_host(cfg, i)))
+        assert out.data_ptr() == g.output.data_ptr()
+        ptrs.append(out.data_ptr())
+    assert ptrs[0] == ptrs[2] and ptrs[0] != ptrs[1]
+
+
+def test_graph_replay_is_bit_identical():
+    cfg = scene.SceneConfig(200, 120, 4, n_moving=2, seed=21)
+    frames = [_dev(scene.frame_host(cfg, i)) for i in range(cfg.frames)]
+    a = Hush(0, {"width": 200, "height": 120})
+    b = Hush(0, {"width": 200, "height": 120, "graph": True})
+    for f in frames:
+        oa = a.denoise(f).clone()
+        ob = b.denoise(f).clone()
+        torch.cuda.synchronize()
+        assert torch.equal(oa, ob)
+
+
+def test_other_hidden_width_uses_the_generic_mlp():
+    rng = np.random.default_rng(3)
+    h = 8
+    n = h * h + 34 * h + 12
+    w = (rng.normal(0, 0.3, n)).astype(np.float16).view(np.uint16)
+    cfg = scene.SceneConfig(64, 48, 3, seed=6)
+    o = oracle.OracleHush(64, 48, w)
+    g = Hush(0, {"width": 64, "height": 48, "weights": w.tobytes()})
+    assert g.hidden == 8
+    for i in range(cfg.frames):
+        f = scene.frame_host(cfg, i)
+        frac, worst, _ = mismatch(to_f32(g.denoise(_dev(f))), o.denoise(f).astype(np.float32))
+        assert frac <= SEQ_FRAC, (i, frac, worst)
+
+
+def test_error_messages_match_the_reference():
+    g = Hush(0, {"width": 32, "height": 16})
+    f = _dev(scene.frame_host(scene.SceneConfig(32, 16, 1), 0))
+    bad = dict(f)
+    del bad["motion"]
+    with pytest.raises(HushError, match="missing input 'motion'"):
+        g.denoise(bad)
+    small = dict(f)
+    small["material"] = f["material"][:8]
+    with pytest.raises(HushError, match=r"'material' is 32x8, the denoiser 32x16 \(call resize\)"):
+        g.denoise(small)
+    with pytest.raises(HushError, match="813 f16 values fit no MLP size"):
+        Hush(0, {"width": 8, "height": 8, "weights": np.zeros(813, np.uint16).tobytes()})
+    with pytest.raises(HushError, match="bad size 0x8"):
+        Hush(0, {"width": 0, "height": 8})
+    with pytest.raises(HushError, match="bad size"):
+        g.resize(-1, 3)
+
+
+def test_resize_resets_and_reallocates():
+    g = Hush(0, {"width": 32, "height": 16})
+    g.denoise(_dev(scene.frame_host(scene.SceneConfig(32, 16, 1), 0)))
+    g.resize(48, 20)
+    assert (g.width, g.height, g.frame) == (48, 20, 0)
+    cfg = scene.SceneConfig(48, 20, 2, seed=8)
+    o = oracle.OracleHush(48, 20, builtin_weights())
+    for i in range(2):
+        fr = scene.frame_host(cfg, i)
+        assert mismatch(to_f32(g.denoise(_dev(fr))), o.denoise(fr).astype(np.float32))[0] <= SEQ_FRAC
+
+
+def test_svgf_parity():
+    cfg = scene.SceneConfig(160, 90, 5, n_moving=2, pan_min=1.0, pan_max=2.0, seed=31)
+    frames = [scene.frame_host(cfg, i) for i in range(cfg.frames)]
+    o = oracle.OracleSVGF(cfg.width, cfg.height)
+    s = SVGF(0, cfg.width, cfg.height)
+    prev = None
+    for i, f in enumerate(frames):
+        g = dict(f)
+        g["prevNormalDepth"] = (prev or f)["normalDepth"]
+        g["prevMotion"] = (prev or f)["motion"]
+        ref = o.encode(g).astype(np.float32)
+        dev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in g.items()}
+        got = to_f32(s.encode(dev))
+        frac, worst, _ = mismatch(got, ref)
+        assert frac <= SEQ_FRAC, (i, frac, worst)
+        prev = f
+
+
+def test_device_generator_matches_host():
+    cfg = scene.SceneConfig(128, 72, 2, n_moving=2, seed=17)
+    for i in range(2):
+        h = scene.frame_host(cfg, i)
+        d = scene.frame_device(cfg, i)
+        torch.cuda.synchronize()
+        for k in scene.NAMES:
+            a, b = d[k].float().cpu().numpy(), h[k].astype(np.float32)
+            assert np.mean(np.abs(a - b) <= 1e-2 * np.maximum(np.abs(b), 1)) > 0.99, k
