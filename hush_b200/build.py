@@ -25,10 +25,16 @@ ORACLE_LIB = os.path.join(ORACLE_DIR, "liboracle_hush.so")
 WEIGHTS = os.path.join(PKG, "data", "hush-weights.bin")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# --use_fast_math: exp / log / division / sqrt as the hardware approximations. WGSL itself only promises that
+# accuracy (exp 3 + 2|x| ULP, log 2^-21 absolute on [0.5, 2], division 2.5 ULP, inverseSqrt 2 ULP), so the kernels
+# stay inside the reference's own numerical contract; the parity tests bound the effect against the exact oracle.
 NVCC_FLAGS = [
-    "-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-fopenmp",
+    "-O3", "-std=c++17", "-lineinfo", "--use_fast_math", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-fopenmp",
     "-I", os.path.join(ROOT, "include"), "-I", BUILD, "-I", CSRC,
 ] + ARCH
+# SVGF's temporal pass compares a weighted-average history length stored with round-toward-zero against 4
+# (svgf.js:94, 121): an ulp of difference flips the branch, so that file keeps IEEE arithmetic throughout.
+PER_FILE_DROP = {"svgf.cu": {"--use_fast_math"}}
 
 
 def _nvcc() -> str:
@@ -91,7 +97,8 @@ def build_cuda(force: bool = False, verbose: bool = False, extra_flags=None) -> 
         obj = os.path.join(BUILD, s[:-3] + ".o")
         objs.append(obj)
         if force or not os.path.exists(obj) or max(os.path.getmtime(src), header_time) > os.path.getmtime(obj):
-            jobs.append([nvcc, "-c", src, "-o", obj] + flags)
+            drop = PER_FILE_DROP.get(s, set())
+            jobs.append([nvcc, "-c", src, "-o", obj] + [x for x in flags if x not in drop])
     if jobs:
         with cf.ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
             list(ex.map(lambda c: _run(c, verbose), jobs))

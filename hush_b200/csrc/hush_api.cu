@@ -159,7 +159,20 @@ static int set_weights(hush_t *h, const uint16_t *weights, size_t n) {
   h->wf = wf;
   h->hidden = hd;
   std::memset(&h->w16, 0, sizeof(h->w16));
-  if (hd == 16) std::memcpy(h->w16.w, wf.data(), sizeof(h->w16.w));
+  if (hd == 16) {
+    std::memcpy(h->w16.w, wf.data(), sizeof(h->w16.w));
+    // tensor-core operands (bf16, then f16), then the FP32 weights of the 4-lane MLP
+    alignas(16) uint8_t blob[2 * MLP_TC_BLOB_BYTES + MLP_FP32_BLOB_BYTES];
+    mlp_tc_build_blob(wf.data(), 1, blob);
+    mlp_tc_build_blob(wf.data(), 0, blob + MLP_TC_BLOB_BYTES);
+    mlp_fp32_build_blob(wf.data(), reinterpret_cast<float *>(blob + 2 * MLP_TC_BLOB_BYTES));
+    if (!h->tc_blob_dev) {
+      e = cudaMalloc(&h->tc_blob_dev, sizeof(blob));
+      if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc of the tensor-core weights");
+    }
+    e = cudaMemcpy(h->tc_blob_dev, blob, sizeof(blob), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaMemcpy of the tensor-core weights");
+  }
   drop_graphs(h);  // graphs bake the weights in as kernel parameters
   return HUSH_OK;
 }
@@ -350,7 +363,8 @@ static int encode_frame(hush_t *h, const HushFrame &f, cudaStream_t st, bool tim
       n++;
     }
   };
-  if (h->schedule == HUSH_SCHED_PASSES || h->mlp_mode != HUSH_MLP_FP32 || h->hidden != 16) {
+  // the tensor-core MLP exists in the fused temporal kernel for h = 16; other widths run the reference passes
+  if (h->schedule == HUSH_SCHED_PASSES || h->hidden != 16) {
     for (int p = 0; p < PASS_COUNT && e == cudaSuccess; p++) {
       mark(PASS_LABELS[p]);
       e = launch_pass(p, f, h->w16, st);

@@ -13,8 +13,13 @@
 // Levels with a neighbourhood (the a-trous levels, TAA) stay separate launches: fusing them needs recomputed halos,
 // and on B200 these passes are bound by instruction issue rather than HBM, so recomputation costs more than the
 // L2-resident round trip of a half-res image.
+#include <cuda_bf16.h>
+
+#include <type_traits>
+
 #include "hush_device.cuh"
 #include "hush_internal.h"
+#include "umma.cuh"
 
 namespace hush {
 
@@ -26,63 +31,504 @@ HD_INL float4 gh_decode(float4 g) {  // (oct normal, depth, count) -> (normal, d
 }
 
 // ------------------------------------------------------------------------------------------------ stage 0
-// Tile 32 x 8 pixels = 16 x 4 blocks, 256 threads; the illumination tile carries an apron of 1.
+// Tile 32 x 8 pixels = 16 x 4 blocks, 256 threads. Three phases, every thread busy in each:
+//   1. illumination tile (apron 1) in shared memory as (r, g, b, L): L = luminance, or L_INVALID outside the image
+//      or on sky
+//   2. pixel(): one pixel per thread (hush.js:111-223), feature inputs P0..P4 to shared memory
+//   3. block(): a 4-lane group per 2x2 block (hush.js:226-282). Every lane forms the block sums itself in the
+//      reference's order; the MLP (FP32 form) splits each layer over the group, 4 hidden units per lane, with the
+//      transposed weights in shared memory. The tensor-core form (TC) writes the features as MMA operand rows and
+//      warps 0-1 run the three layers as tcgen05 MMAs (M = 128 with 64 rows used, N = 16, K = 32 / 16 / 16) on bf16
+//      or f16 operands with FP32 accumulation in TMEM; bias, ReLU and the heads stay FP32.
 constexpr int K1_TW = 32, K1_TH = 8;
+constexpr int K1_NB = (K1_TW / 2) * (K1_TH / 2);  // 64 blocks
+constexpr uint32_t MBAR_POLLS = 1u << 22;
+// L of a tile entry outside the image or on sky (a valid luminance is finite and far above it)
+constexpr float L_INVALID = -1e30f;
+HD_INL bool l_valid(float L) { return L > -1e29f; }
 
-template <bool TC>
+struct TcSmem {
+  alignas(128) uint8_t a1[128 * 32 * 2];  // layer-1 A: 128 rows x K 32 (features 0..19, zero padded)
+  alignas(128) uint8_t a2[128 * 16 * 2];  // layer-2 / layer-3 A: 128 rows x K 16
+  alignas(128) uint8_t b[MLP_TC_BLOB_BYTES];  // B1 (16 x 32), B2 (16 x 16), B3 (16 x 16)
+  alignas(8) uint64_t mbar;
+  uint32_t tmem;
+  uint32_t flags[K1_NB];  // bit 0: block inside the half-res image, bit 1: block has valid pixels
+};
+struct FpSmem {
+  float4 w[MLP_FP32_BLOB_BYTES / 16];  // transposed weights + biases (mlp_fp32_build_blob)
+  float4 h[K1_NB][4];                  // hidden activations of each block, exchanged within its 4-lane group
+};
+
+template <bool BF16>
+HD_INL uint16_t to_op(float v) {
+  if constexpr (BF16) return __bfloat16_as_ushort(__float2bfloat16_rn(v));
+  else return __half_as_ushort(__float2half_rn(v));
+}
+template <bool BF16>
+HD_INL uint4 pack8(const float *v) {
+  uint4 q;
+  q.x = (uint32_t)to_op<BF16>(v[0]) | ((uint32_t)to_op<BF16>(v[1]) << 16);
+  q.y = (uint32_t)to_op<BF16>(v[2]) | ((uint32_t)to_op<BF16>(v[3]) << 16);
+  q.z = (uint32_t)to_op<BF16>(v[4]) | ((uint32_t)to_op<BF16>(v[5]) << 16);
+  q.w = (uint32_t)to_op<BF16>(v[6]) | ((uint32_t)to_op<BF16>(v[7]) << 16);
+  return q;
+}
+
+// One MMA layer of the tensor-core MLP, run by warps 0-1: thread 0 issues after the 64-thread barrier and commits;
+// every thread waits for the phase and loads its row (16 columns). Returns false if the wait gave up.
+HD_INL bool tc_layer(TcSmem &S, int li, bool first, uint32_t b_off, uint32_t kcore_b, uint32_t idesc, uint32_t phase,
+                     float *d) {
+  umma::fence_before_sync();
+  umma::fence_proxy_async();
+  asm volatile("bar.sync 1, 64;" ::: "memory");
+  const uint32_t mbar = umma::smem_u32(&S.mbar);
+  if (li == 0) {
+    umma::fence_after_sync();
+    const uint32_t a = umma::smem_u32(first ? S.a1 : S.a2);
+    const uint32_t kcore_a = first ? 4u : 2u;
+    const uint32_t b = umma::smem_u32(S.b) + b_off;
+    const int kblocks = first ? 2 : 1;
+    for (int kb = 0; kb < kblocks; kb++)
+      umma::mma_f16(S.tmem, umma::sdesc(a + 256u * kb, 128, 128 * kcore_a),
+                    umma::sdesc(b + 256u * kb, 128, 128 * kcore_b), idesc, kb > 0 ? 1u : 0u);
+    umma::commit(mbar);
+  }
+  const bool ok = umma::mbar_wait_bounded(mbar, phase, MBAR_POLLS);
+  umma::fence_after_sync();
+  umma::ld16(S.tmem + ((uint32_t)(32 * (li >> 5)) << 16), d);
+  return ok;
+}
+
+// pixel() of hush.js:111-223 over the (r, g, b, L) tile; same arithmetic as temporal_pixel().
+HD_INL PixP temporal_pixel_fast(const HushFrame &f, int px, int py, const float4 *sI, int ti) {
+  constexpr int SW = K1_TW + 2;
+  PixP R = pixp_default();
+  const int W = f.W, H = f.H;
+  const uint2 ndr = __ldg(f.nd + py * f.p_nd + px), mvr = __ldg(f.mv + py * f.p_mv + px);
+  const float4 nd = h4_to_f4(ndr), mv = h4_to_f4(mvr);
+  const int oi = py * W + px;
+  if (nd.w < 0.0f) {
+    f.A0[oi] = make_uint2(0, 0);
+    f.mom[oi] = make_uint2(0, 0);
+    sth(f.key, oi, make_float4(0.f, 0.f, -1.0f, mv.z));
+    return R;
+  }
+  // reprojection gathers first (the dependent-load chain), kept packed until used
+  uint2 k4[4], c4[4], m4[4], pqr;
+  float fx = 0.f, fy = 0.f, ppx = 0.f, ppy = 0.f;
+  int bix = 0, biy = 0, cx = 0, cy = 0;
+  if (!f.reset) {
+    ppx = (float)px + mv.x;
+    ppy = (float)py + mv.y;
+    const float bx = floorf(ppx), by = floorf(ppy);
+    fx = ppx - bx;
+    fy = ppy - by;
+    bix = __float2int_rz(bx);
+    biy = __float2int_rz(by);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int q = clampi(biy + (i >> 1), 0, H - 1) * W + clampi(bix + (i & 1), 0, W - 1);
+      k4[i] = __ldg(f.key_prev + q);
+      c4[i] = __ldg(f.hist_prev + q);
+      m4[i] = __ldg(f.mom_prev + q);
+    }
+    cx = __float2int_rz(floorf(ppx + 0.5f));
+    cy = __float2int_rz(floorf(ppy + 0.5f));
+    pqr = __ldg(f.par0_prev + (clampi(cy, 0, H - 1) >> 1) * f.W2 + (clampi(cx, 0, W - 1) >> 1));
+  }
+  const uint2 mrr = __ldg(f.mat + py * f.p_mat + px);
+  // 3x3 statistics of the illumination (valid neighbours), two passes
+  const float4 illum = sI[ti];
+  const float l = illum.w;
+  float s1x = 0.f, s1y = 0.f, s1z = 0.f, cnt = 0.f;
+#pragma unroll
+  for (int j = 0; j < 9; j++) {
+    const float4 c = sI[ti + (j / 3 - 1) * SW + (j % 3 - 1)];
+    s1x += c.x; s1y += c.y; s1z += c.z;  // invalid entries hold rgb = 0
+    cnt += l_valid(c.w) ? 1.0f : 0.0f;
+  }
+  cnt = fmaxf(cnt, 1.0f);
+  const float mux = s1x / cnt, muy = s1y / cnt, muz = s1z / cnt;
+  const float slm = lum3(mux, muy, muz);
+  float svx = 0.f, svy = 0.f, svz = 0.f, svar = 0.f;
+#pragma unroll
+  for (int j = 0; j < 9; j++) {
+    const float4 c = sI[ti + (j / 3 - 1) * SW + (j % 3 - 1)];
+    if (l_valid(c.w)) {
+      const float dx = c.x - mux, dy = c.y - muy, dz = c.z - muz, dl = c.w - slm;
+      svx += dx * dx; svy += dy * dy; svz += dz * dz;
+      svar += dl * dl;
+    }
+  }
+  const float sdx = sqrtf(fmaxf(svx / cnt, 1e-12f)), sdy = sqrtf(fmaxf(svy / cnt, 1e-12f)),
+              sdz = sqrtf(fmaxf(svz / cnt, 1e-12f));
+  svar /= cnt;
+  bool has = false;
+  float hcx = 0.f, hcy = 0.f, hcz = 0.f;
+  float4 hm = make_float4(0.f, 0.f, 0.f, 0.f);
+  float v = 0.f, alpha = 1.0f, gamma = 1.0f;
+  if (!f.reset) {
+    float sumW = 0.f;
+    const float wts[4] = {(1.0f - fx) * (1.0f - fy), fx * (1.0f - fy), (1.0f - fx) * fy, fx * fy};
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int qx = bix + (i & 1), qy = biy + (i >> 1);
+      if (wts[i] > 0.0f && qx >= 0 && qy >= 0 && qx < W && qy < H && check_key(h4_to_f4(k4[i]), nd, mv.w, mv.z)) {
+        const float4 c = h4_to_f4(c4[i]), m = h4_to_f4(m4[i]);
+        sumW += wts[i];
+        hcx += wts[i] * c.x; hcy += wts[i] * c.y; hcz += wts[i] * c.z;
+        hm.x += wts[i] * m.x; hm.y += wts[i] * m.y; hm.z += wts[i] * m.z; hm.w += wts[i] * m.w;
+      }
+    }
+    if (sumW >= 0.01f) {
+      hcx /= sumW; hcy /= sumW; hcz /= sumW;
+      hm.x /= sumW; hm.y /= sumW; hm.z /= sumW; hm.w /= sumW;
+      v = sumW;
+      has = true;
+    } else {
+      float n3 = 0.f;
+      hcx = hcy = hcz = 0.f;
+      hm = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int j = 0; j < 9; j++) {
+        const int qx = cx + j % 3 - 1, qy = cy + j / 3 - 1;
+        if (qx >= 0 && qy >= 0 && qx < W && qy < H && check_key(ldh(f.key_prev, qy * W + qx), nd, mv.w, mv.z)) {
+          n3 += 1.0f;
+          const float4 c = ldh(f.hist_prev, qy * W + qx), m = ldh(f.mom_prev, qy * W + qx);
+          hcx += c.x; hcy += c.y; hcz += c.z;
+          hm.x += m.x; hm.y += m.y; hm.z += m.z; hm.w += m.w;
+        }
+      }
+      if (n3 > 0.0f) {
+        hcx /= n3; hcy /= n3; hcz /= n3;
+        hm.x /= n3; hm.y /= n3; hm.z /= n3; hm.w /= n3;
+        v = 0.1f;
+        has = true;
+      }
+    }
+    const float4 pq = h4_to_f4(pqr);
+    alpha = pq.x;
+    gamma = pq.y;
+  }
+  has = has && hm.w > 0.0f;
+  float colx = illum.x, coly = illum.y, colz = illum.z;
+  float nmx = l, nmy = l * l, nfast = l, len1 = 1.0f, lag = 0.0f;
+  if (has) {
+    const float hclx = fminf(fmaxf(hcx, mux - gamma * sdx), mux + gamma * sdx);
+    const float hcly = fminf(fmaxf(hcy, muy - gamma * sdy), muy + gamma * sdy);
+    const float hclz = fminf(fmaxf(hcz, muz - gamma * sdz), muz + gamma * sdz);
+    len1 = fminf(hm.w + 1.0f, HMAX);
+    const float a = fmaxf(alpha, 1.0f / len1);
+    colx = hclx + (illum.x - hclx) * a;
+    coly = hcly + (illum.y - hcly) * a;
+    colz = hclz + (illum.z - hclz) * a;
+    nmx = hm.x + (l - hm.x) * a;
+    nmy = hm.y + (l * l - hm.y) * a;
+    nfast = hm.z + (l - hm.z) * fmaxf(1.0f / 6.0f, 1.0f / len1);
+    const float lh = lum3(hcx, hcy, hcz);
+    lag = fabsf(slm - lh) / (sqrtf(fmaxf(svar / cnt, 1e-12f)) + 0.02f * lh + 1e-3f);
+  } else {
+    v = 0.0f;
+  }
+  const float tvar = fmaxf(nmy - nmx * nmx, 0.0f);
+  const float4 A = make_float4(colx, coly, colz, svar + (tvar - svar) * fminf(len1 / 4.0f, 1.0f));
+  const float2 oc = oct_enc(nd.x, nd.y, nd.z);
+  sth(f.A0, oi, A);
+  sth(f.mom, oi, make_float4(nmx, nmy, nfast, len1));
+  sth(f.key, oi, make_float4(oc.x, oc.y, nd.w, mv.z));
+  const float E = f.exposure;
+  const float4 Aq = make_float4(qf16(A.x), qf16(A.y), qf16(A.z), qf16(A.w));
+  const float m1 = E * qf16(nmx);
+  const float m2 = E * E * qf16(nmy);
+  R.P0 = make_float4(E * lum(Aq), E * qf16(l), fmaxf(m2 - m1 * m1, 0.0f), len1);
+  R.P1 = make_float4(qf16(v), qf16(lag), E * qf16(nfast), m1);
+  R.P2 = make_float4(qf16(oc.x), qf16(oc.y), qf16(nd.w), qf16(sqrtf(mv.x * mv.x + mv.y * mv.y)));
+  R.P3 = h4_to_f4(mrr);
+  R.P4 = Aq;
+  return R;
+}
+
+// block() features (hush.js:226-282) for block b of the tile, computed by each lane of its group. sL holds the
+// tile's L (luminance, or L_INVALID).
+HD_INL bool block_features_grp(const PixP *sP, const float *sL, int lbx, int lby, float E, float *f, float4 &AC,
+                               float4 &G) {
+  constexpr int SW = K1_TW + 2;
+  float nv = 0.f;
+  float4 S0 = make_float4(0.f, 0.f, 0.f, 0.f), S1 = S0, S3 = S0;
+  AC = S0;
+  float Nx = 0.f, Ny = 0.f, Nz = 0.f, MV = 0.f, Z = 0.f;
+  float la[4], zs[4];
+  float4 ns[4];
+  bool ok[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const PixP &P = sP[(lby * 2 + (j >> 1)) * K1_TW + lbx * 2 + (j & 1)];
+    const float4 p2 = P.P2;
+    ok[j] = p2.z >= 0.0f;
+    la[j] = 0.f; zs[j] = 0.f;
+    ns[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!ok[j]) continue;
+    const float4 p0 = P.P0, p1 = P.P1, p3 = P.P3, p4 = P.P4;
+    nv += 1.0f;
+    la[j] = p0.x;
+    ns[j] = oct_dec(p2.x, p2.y);
+    zs[j] = p2.z;
+    S0.x += p0.x; S0.y += p0.y; S0.z += p0.z; S0.w += p0.w;
+    S1.x += p1.x; S1.y += p1.y; S1.z += p1.z; S1.w += p1.w;
+    Nx += ns[j].x; Ny += ns[j].y; Nz += ns[j].z;
+    S3.x += p3.x; S3.y += p3.y; S3.z += p3.z; S3.w += p3.w;
+    AC.x += p4.x; AC.y += p4.y; AC.z += p4.z; AC.w += p4.w;
+    MV += p2.w;
+    Z += p2.z;
+  }
+  if (nv == 0.0f) {
+    G = make_float4(0.f, 0.f, -1.0f, 0.f);
+    return false;
+  }
+  const float k = 1.0f / nv;
+  S0.x *= k; S0.y *= k; S0.z *= k; S0.w *= k;
+  S1.x *= k; S1.y *= k; S1.z *= k; S1.w *= k;
+  Nx *= k; Ny *= k; Nz *= k;
+  S3.x *= k; S3.y *= k; S3.z *= k; S3.w *= k;
+  AC.x *= k; AC.y *= k; AC.z *= k; AC.w *= k;
+  MV *= k;
+  Z *= k;
+  const float Lacc = S0.x;
+  float VA = 0.f;
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+    if (ok[j]) VA += (la[j] - Lacc) * (la[j] - Lacc);
+  VA *= k;
+  // 4x4 neighbourhood (block +-1) of the tile, top-left at tile position (2 lbx, 2 lby) with the apron
+  const int t0 = (2 * lby) * SW + 2 * lbx;
+  float s1 = 0.f, n4 = 0.f, lq[16], wq[16];
+#pragma unroll
+  for (int j = 0; j < 16; j++) {
+    const float L = sL[t0 + (j >> 2) * SW + (j & 3)];
+    wq[j] = l_valid(L) ? 1.0f : 0.0f;
+    lq[j] = E * qf16(l_valid(L) ? L : 0.0f);
+    s1 += wq[j] * lq[j];
+    n4 += wq[j];
+  }
+  const float mu4 = s1 / fmaxf(n4, 1.0f);
+  float var4 = 0.f;
+#pragma unroll
+  for (int j = 0; j < 16; j++) {
+    const float d = lq[j] - mu4;
+    var4 += wq[j] * d * d;
+  }
+  var4 /= fmaxf(n4, 1.0f);
+  const float nl = fmaxf(sqrtf(Nx * Nx + Ny * Ny + Nz * Nz), 1e-6f);
+  const float4 Nn = make_float4(Nx / nl, Ny / nl, Nz / nl, 0.f);
+  float zmax = -1e30f, zmin = 1e30f, mind = 1e30f;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    if (ok[j]) {
+      zmax = fmaxf(zmax, zs[j]);
+      zmin = fminf(zmin, zs[j]);
+      mind = fminf(mind, dot3(ns[j], Nn));
+    }
+  }
+  const float dz = fminf(fmaxf((zmax - zmin) / fmaxf(zmin, 1e-6f), 0.0f), 1.0f);
+  const float dn = fminf(fmaxf(1.0f - mind, 0.0f), 2.0f);
+  const float2 oc = oct_enc(Nn.x, Nn.y, Nn.z);
+  f[0] = log1p_w(Lacc); f[1] = log1p_w(S0.y); f[2] = log1p_w(S0.z); f[3] = log1p_w(var4);
+  f[4] = S0.w / HMAX; f[5] = S1.x; f[6] = log1p_w(S1.y);
+  f[7] = log1p_w(fabsf(S1.z - S1.w) / (S1.w + 1e-3f));
+  f[8] = oc.x; f[9] = oc.y; f[10] = dz; f[11] = dn;
+  f[12] = S3.x; f[13] = S3.y; f[14] = S3.z; f[15] = S3.w;
+  f[16] = 1.0f - nv / 4.0f; f[17] = log1p_w(MV); f[18] = log1p_w(mu4); f[19] = log1p_w(VA);
+  G = make_float4(oc.x, oc.y, Z, nv);
+  return true;
+}
+
+template <bool TC, bool BF16>
 __global__ void __launch_bounds__(K1_TW *K1_TH, 3)
-    k_temporal_fused(const __grid_constant__ HushFrame f, const __grid_constant__ MlpW16 w) {
-  constexpr int SW = K1_TW + 2, SH = K1_TH + 2, NT = K1_TW * K1_TH, NB = (K1_TW / 2) * (K1_TH / 2);
+    k_temporal_fused(const __grid_constant__ HushFrame f, const __grid_constant__ MlpW16 w, const uint4 *blob) {
+  constexpr int SW = K1_TW + 2, SH = K1_TH + 2, NT = K1_TW * K1_TH;
   __shared__ float4 sI[SW * SH];
+  __shared__ float sL[SW * SH];
   __shared__ PixP sP[NT];
+  __shared__ std::conditional_t<TC, TcSmem, FpSmem> X_;
   const int li = threadIdx.x;
-  const int tx = li % K1_TW, ty = li / K1_TW;
+  if constexpr (TC) {
+    if (li < 32) {
+      umma::tmem_alloc(umma::smem_u32(&X_.tmem), 32);
+      umma::tmem_relinquish();
+    }
+    if (li == 0) umma::mbar_init(umma::smem_u32(&X_.mbar), 1);
+    if (li < MLP_TC_BLOB_BYTES / 16) reinterpret_cast<uint4 *>(X_.b)[li] = __ldg(blob + li);
+    umma::fence_proxy_async();
+    umma::fence_before_sync();
+  } else {
+    for (int i = li; i < MLP_FP32_BLOB_BYTES / 16; i += NT) reinterpret_cast<uint4 *>(X_.w)[i] = __ldg(blob + i);
+  }
+  // phase 1: illumination tile
   const int ox = blockIdx.x * K1_TW - 1, oy = blockIdx.y * K1_TH - 1;
   for (int i = li; i < SW * SH; i += NT) {
     const int qx = ox + i % SW, qy = oy + i / SW;
-    float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 e = make_float4(0.f, 0.f, 0.f, L_INVALID);
     if (qx >= 0 && qy >= 0 && qx < f.W && qy < f.H && ldh(f.nd, qy * f.p_nd + qx).w >= 0.0f) {
       const float4 r = ldh(f.rad, qy * f.p_rad + qx), m = ldh(f.mat, qy * f.p_mat + qx);
-      e = make_float4(r.x / fmaxf(m.x, 1e-3f), r.y / fmaxf(m.y, 1e-3f), r.z / fmaxf(m.z, 1e-3f), 1.0f);
+      e.x = r.x / fmaxf(m.x, 1e-3f);
+      e.y = r.y / fmaxf(m.y, 1e-3f);
+      e.z = r.z / fmaxf(m.z, 1e-3f);
+      e.w = lum3(e.x, e.y, e.z);
     }
     sI[i] = e;
+    sL[i] = e.w;
   }
   __syncthreads();
-  const int px = blockIdx.x * K1_TW + tx, py = blockIdx.y * K1_TH + ty;
-  PixP P = pixp_default();
-  if (px < f.W && py < f.H) P = temporal_pixel<SW>(f, px, py, sI, tx + 1, ty + 1);
-  sP[li] = P;
+  if constexpr (TC) umma::fence_after_sync();
+  // phase 2: one pixel per thread
+  {
+    const int tx = li % K1_TW, ty = li / K1_TW;
+    const int px = blockIdx.x * K1_TW + tx, py = blockIdx.y * K1_TH + ty;
+    PixP P = pixp_default();
+    if (px < f.W && py < f.H) P = temporal_pixel_fast(f, px, py, sI, (ty + 1) * SW + tx + 1);
+    sP[li] = P;
+  }
   __syncthreads();
-  if (li >= NB) return;
-  const int lbx = li % (K1_TW / 2), lby = li / (K1_TW / 2);
+  // phase 3: 4-lane group per block
+  const int b = li >> 2, k = li & 3;
+  const int lbx = b % (K1_TW / 2), lby = b / (K1_TW / 2);
   const int X = blockIdx.x * (K1_TW / 2) + lbx, Y = blockIdx.y * (K1_TH / 2) + lby;
-  if (X >= f.W2 || Y >= f.H2) return;
-  PixP Pj[4];
-#pragma unroll
-  for (int j = 0; j < 4; j++) Pj[j] = sP[(lby * 2 + (j >> 1)) * K1_TW + lbx * 2 + (j & 1)];
+  const bool valid = X < f.W2 && Y < f.H2;
+  const int o = Y * f.W2 + X;
   float fe[N_FEAT];
   float4 AC, G;
-  const int o = Y * f.W2 + X;
-  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (!block_features<SW>(Pj, sI, (2 * lby) * SW + 2 * lbx, f.exposure, fe, AC, G)) {
-    // INFER on a block without valid pixels (hush.js:343-346) and its packed F2/F3 (hush.js:241-244)
-    f.Ah[o] = make_uint2(0, 0);
-    f.Gh[o] = make_uint2(pk(0.f, 0.f), pk(-1.0f, 0.f));
-    sth(f.par0, o, z4); sth(f.par1, o, z4); sth(f.par2, o, z4);
-    return;
+  const bool ok = block_features_grp(sP, sL, lbx, lby, f.exposure, fe, AC, G);
+  if (valid) {
+    // the block means / guide (F2.zw, F3.xy of hush.js:280-281), by lanes 0 and 1
+    if (k == 0) f.Ah[o] = ok ? make_uint2(pk(AC.x, AC.y), pk(AC.z, AC.w)) : make_uint2(0, 0);
+    if (k == 1) f.Gh[o] = ok ? make_uint2(pk(G.x, G.y), pk(G.z, G.w)) : make_uint2(pk(0.f, 0.f), pk(-1.0f, 0.f));
   }
-  f.Ah[o] = make_uint2(pk(AC.x, AC.y), pk(AC.z, AC.w));
-  f.Gh[o] = make_uint2(pk(G.x, G.y), pk(G.z, G.w));
   // the MLP sees the features as stored (packed f16, hush.js:278-280, 348-353)
 #pragma unroll
-  for (int i = 0; i < N_FEAT; i++) fe[i] = __half2float(__ushort_as_half(f2h(qf16(fe[i]))));
-  float out[N_OUT];
-  mlp_fwd<16>(w.w, fe, out);
-  float4 p0, p1, p2;
-  mlp_heads(out, p0, p1, p2);
-  sth(f.par0, o, p0);
-  sth(f.par1, o, p1);
-  sth(f.par2, o, p2);
+  for (int i = 0; i < N_FEAT; i++) fe[i] = ok ? __half2float(__ushort_as_half(f2h(qf16(fe[i])))) : 0.0f;
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  if constexpr (!TC) {
+    // every lane runs the layers (the group exchanges through shared memory and shuffles); blocks outside the image
+    // or without valid pixels compute on zero features and store nothing / zeros
+    // layer 1: units 4k..4k+3
+    const float4 *Wt = X_.w;
+    float4 a = Wt[MLP_FP32_B1 + k];
+#pragma unroll
+    for (int i = 0; i < N_FEAT; i++) {
+      const float4 wv = Wt[MLP_FP32_W1 + i * 4 + k];
+      a.x = a.x + fe[i] * wv.x; a.y = a.y + fe[i] * wv.y; a.z = a.z + fe[i] * wv.z; a.w = a.w + fe[i] * wv.w;
+    }
+    X_.h[b][k] = make_float4(fmaxf(a.x, 0.f), fmaxf(a.y, 0.f), fmaxf(a.z, 0.f), fmaxf(a.w, 0.f));
+    __syncwarp();
+    float h[16];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const float4 t = X_.h[b][q];
+      h[4 * q] = t.x; h[4 * q + 1] = t.y; h[4 * q + 2] = t.z; h[4 * q + 3] = t.w;
+    }
+    __syncwarp();
+    a = Wt[MLP_FP32_B2 + k];
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      const float4 wv = Wt[MLP_FP32_W2 + i * 4 + k];
+      a.x = a.x + h[i] * wv.x; a.y = a.y + h[i] * wv.y; a.z = a.z + h[i] * wv.z; a.w = a.w + h[i] * wv.w;
+    }
+    X_.h[b][k] = make_float4(fmaxf(a.x, 0.f), fmaxf(a.y, 0.f), fmaxf(a.z, 0.f), fmaxf(a.w, 0.f));
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const float4 t = X_.h[b][q];
+      h[4 * q] = t.x; h[4 * q + 1] = t.y; h[4 * q + 2] = t.z; h[4 * q + 3] = t.w;
+    }
+    // layer 3: outputs k, 4 + k, 8 + k (par0.k, par1.k, par2.k)
+    a = Wt[MLP_FP32_B3 + k];
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      const float4 wv = Wt[MLP_FP32_W3 + i * 4 + k];
+      a.x = a.x + h[i] * wv.x; a.y = a.y + h[i] * wv.y; a.z = a.z + h[i] * wv.z;
+    }
+    // heads (hush.js:357-362) for component k of par0, par1, par2
+    const float p0 = k == 0 ? 1.0f / 32.0f + (31.0f / 32.0f) * sigmoidf_(a.x)
+                     : k == 1 ? 0.5f + 7.5f * sigmoidf_(a.x)
+                              : sigmoidf_(a.x);
+    const float p1 = 0.25f * expf(fminf(fmaxf(a.y, -5.0f), 5.0f));
+    const float p2 = expf(fminf(fmaxf(a.z, -4.0f), 4.0f));
+    // gather the components of each texel in the lane that stores it: lane k stores par_k (k < 3)
+    const uint32_t base = (threadIdx.x & 31) & ~3u;
+    float c0[4], c1[4], c2[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      c0[q] = __shfl_sync(0xffffffffu, p0, base + q);
+      c1[q] = __shfl_sync(0xffffffffu, p1, base + q);
+      c2[q] = __shfl_sync(0xffffffffu, p2, base + q);
+    }
+    if (valid && k < 3) {
+      // INFER on a block without valid pixels writes zeros (hush.js:343-346)
+      const float4 v = !ok ? z4
+                       : k == 0 ? make_float4(c0[0], c0[1], c0[2], c0[3])
+                       : k == 1 ? make_float4(c1[0], c1[1], c1[2], c1[3])
+                                : make_float4(c2[0], c2[1], c2[2], c2[3]);
+      sth(k == 0 ? f.par0 : k == 1 ? f.par1 : f.par2, o, v);
+    }
+  } else {
+    // operand row b: lane k writes K columns 8k .. 8k+7
+    {
+      float v8[8];
+#pragma unroll
+      for (int c = 0; c < 8; c++) {
+        const int kk = 8 * k + c;
+        v8[c] = 0.0f;
+#pragma unroll
+        for (int i = 0; i < N_FEAT; i++)
+          if (i == kk) v8[c] = fe[i];
+      }
+      *reinterpret_cast<uint4 *>(X_.a1 + umma::kmajor_off(b, 8 * k, 4)) = pack8<BF16>(v8);
+      if (k == 0) X_.flags[b] = (valid ? 1u : 0u) | (ok ? 2u : 0u);
+    }
+    umma::fence_proxy_async();
+    __syncthreads();
+    if (li >= K1_NB) return;
+    // warps 0-1: one row (block) per thread
+    constexpr int B1 = 16 * N_FEAT, B2 = B1 + 16 + 16 * 16, B3 = B2 + 16 + N_OUT * 16;
+    constexpr uint32_t ID = umma::idesc_f16(BF16 ? 1 : 0, 128, 16);
+    float row[16], d[16], out[N_OUT];
+    bool good = tc_layer(X_, li, true, 0, 4, ID, 0, d);
+#pragma unroll
+    for (int j = 0; j < 16; j++) row[j] = fmaxf(d[j] + w.w[B1 + j], 0.0f);
+    *reinterpret_cast<uint4 *>(X_.a2 + umma::kmajor_off(li, 0, 2)) = pack8<BF16>(row);
+    *reinterpret_cast<uint4 *>(X_.a2 + umma::kmajor_off(li, 8, 2)) = pack8<BF16>(row + 8);
+    good &= tc_layer(X_, li, false, 1024, 2, ID, 1, d);
+#pragma unroll
+    for (int j = 0; j < 16; j++) row[j] = fmaxf(d[j] + w.w[B2 + j], 0.0f);
+    *reinterpret_cast<uint4 *>(X_.a2 + umma::kmajor_off(li, 0, 2)) = pack8<BF16>(row);
+    *reinterpret_cast<uint4 *>(X_.a2 + umma::kmajor_off(li, 8, 2)) = pack8<BF16>(row + 8);
+    good &= tc_layer(X_, li, false, 1536, 2, ID, 0, d);
+#pragma unroll
+    for (int j = 0; j < N_OUT; j++) out[j] = d[j] + w.w[B3 + j];
+    umma::fence_before_sync();
+    asm volatile("bar.sync 1, 64;" ::: "memory");
+    if (li < 32) {
+      umma::fence_after_sync();
+      umma::tmem_dealloc(X_.tmem, 32);
+    }
+    if (!good) {
+      atomicOr(f.err, 1u);
+      return;
+    }
+    const uint32_t fl = X_.flags[li];
+    if (!(fl & 1u)) return;
+    const int Xr = blockIdx.x * (K1_TW / 2) + li % (K1_TW / 2), Yr = blockIdx.y * (K1_TH / 2) + li / (K1_TW / 2);
+    const int orow = Yr * f.W2 + Xr;
+    if (!(fl & 2u)) {
+      sth(f.par0, orow, z4); sth(f.par1, orow, z4); sth(f.par2, orow, z4);
+      return;
+    }
+    float4 p0, p1, p2;
+    mlp_heads(out, p0, p1, p2);
+    sth(f.par0, orow, p0);
+    sth(f.par1, orow, p1);
+    sth(f.par2, orow, p2);
+  }
 }
 
 // ------------------------------------------------------------------------------------------------ half / quarter
@@ -375,15 +821,19 @@ const char *fused_stage_label(int s) { return (s >= 0 && s < 6) ? STAGE_LABELS[s
 
 cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpW16 &w16, int mlp_mode, const void *mlp_tc,
                                cudaStream_t st) {
-  (void)mlp_mode;
-  (void)mlp_tc;
   const int hx = (f.W2 + HT_W - 1) / HT_W, hy = (f.H2 + HT_H - 1) / HT_H;
   const int qx = (f.W4 + HT_W - 1) / HT_W, qy = (f.H4 + HT_H - 1) / HT_H;
   switch (stage) {
-    case 0:
-      k_temporal_fused<false><<<dim3((f.W + K1_TW - 1) / K1_TW, (f.H + K1_TH - 1) / K1_TH), K1_TW * K1_TH, 0, st>>>(
-          f, w16);
+    case 0: {
+      const dim3 grid((f.W + K1_TW - 1) / K1_TW, (f.H + K1_TH - 1) / K1_TH);
+      // blob: bf16 operands, f16 operands, then the transposed FP32 weights
+      const uint4 *blob = (const uint4 *)mlp_tc;
+      if (mlp_mode == 1) k_temporal_fused<true, true><<<grid, K1_TW * K1_TH, 0, st>>>(f, w16, blob);
+      else if (mlp_mode == 2)
+        k_temporal_fused<true, false><<<grid, K1_TW * K1_TH, 0, st>>>(f, w16, blob + MLP_TC_BLOB_BYTES / 16);
+      else k_temporal_fused<false, false><<<grid, K1_TW * K1_TH, 0, st>>>(f, w16, blob + 2 * MLP_TC_BLOB_BYTES / 16);
       break;
+    }
     case 1: k_half_stage<1><<<hx * hy + qx * qy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx); break;
     case 2: k_half_stage<2><<<hx * hy + qx * qy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx); break;
     case 3: k_half_stage<3><<<hx * hy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx); break;

@@ -1,6 +1,7 @@
 // Host-side declarations shared by the kernel files and the C ABI implementation.
 #pragma once
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 #include "hush_device.cuh"
 
@@ -25,8 +26,15 @@ int fused_stage_count();
 const char *fused_stage_label(int stage);
 size_t fused_scratch_bytes(int W, int H);
 
-// Tensor-core MLP operand blob (weights in the UMMA shared-memory layout), built on the host (mlp_tc.cu).
-size_t mlp_tc_blob_bytes();
-void mlp_tc_build_blob(const float *w812, int bf16, void *host_blob);
+// Tensor-core MLP weight operands for h = 16 in the UMMA K-major no-swizzle shared-memory layout: B1 (16 x 32, W1
+// zero-padded along K), B2 (16 x 16), B3 (16 x 16, W3 zero-padded along N), in bf16 or f16 (mlp_tc.cu).
+constexpr int MLP_TC_BLOB_BYTES = 2048;
+void mlp_tc_build_blob(const float *w812, int bf16, uint8_t *blob);
+// FP32 weights of the h = 16 network for the 4-lane MLP: per input i and lane k the float4 of the units lane k owns
+// (layer 1 / 2: units 4k..4k+3; layer 3: outputs k, 4+k, 8+k), then the biases in the same grouping.
+constexpr int MLP_FP32_W1 = 0, MLP_FP32_W2 = 80, MLP_FP32_W3 = 144, MLP_FP32_B1 = 208, MLP_FP32_B2 = 212,
+              MLP_FP32_B3 = 216;  // offsets in float4
+constexpr int MLP_FP32_BLOB_BYTES = 220 * 16;
+void mlp_fp32_build_blob(const float *w812, float *blob);
 
 }  // namespace hush

@@ -1,0 +1,70 @@
+// Host side of the tensor-core MLP: the three weight matrices of the h = 16 network as UMMA B operands.
+#include <cstring>
+
+#include "hush_internal.h"
+#include "umma.cuh"
+
+namespace hush {
+
+static uint16_t f32_to_bf16_rn(float x) {
+  uint32_t u;
+  std::memcpy(&u, &x, 4);
+  if ((u & 0x7fffffffu) > 0x7f800000u) return 0x7fc0;
+  return (uint16_t)((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);
+}
+
+// f32 -> f16 round to nearest even (the weights are f16 values already, so this is exact for them).
+static uint16_t f32_to_f16_rn(float x) {
+  uint32_t u;
+  std::memcpy(&u, &x, 4);
+  const uint32_t s = (u >> 16) & 0x8000u, a = u & 0x7fffffffu;
+  if (a > 0x7f800000u) return (uint16_t)(s | 0x7e00u);
+  if (a >= 0x477ff000u) return (uint16_t)(s | 0x7c00u);  // rounds to infinity
+  if (a >= 0x38800000u) {                               // normal
+    uint32_t m = a - 0x38000000u;                       // rebias exponent
+    uint32_t r = (m + 0xfffu + ((m >> 13) & 1u)) >> 13;
+    return (uint16_t)(s | r);
+  }
+  if (a < 0x33000000u) return (uint16_t)s;  // below half the smallest subnormal
+  const uint32_t e = a >> 23, mant = (a & 0x7fffffu) | 0x800000u, shift = 126u - e;  // subnormal: mant >> shift
+  uint32_t q = mant >> shift, rem = mant & ((1u << shift) - 1u), half = 1u << (shift - 1u);
+  if (rem > half || (rem == half && (q & 1u))) q++;
+  return (uint16_t)(s | q);
+}
+
+void mlp_tc_build_blob(const float *w, int bf16, uint8_t *blob) {
+  std::memset(blob, 0, MLP_TC_BLOB_BYTES);
+  auto put = [&](uint8_t *base, int n, int k, int kcore, float v) {
+    const uint16_t h = bf16 ? f32_to_bf16_rn(v) : f32_to_f16_rn(v);
+    std::memcpy(base + umma::kmajor_off(n, k, kcore), &h, 2);
+  };
+  const int W1 = 0, B1 = 16 * 20, W2 = B1 + 16, B2 = W2 + 256, W3 = B2 + 16;
+  for (int n = 0; n < 16; n++)
+    for (int k = 0; k < 20; k++) put(blob, n, k, 4, w[W1 + n * 20 + k]);
+  for (int n = 0; n < 16; n++)
+    for (int k = 0; k < 16; k++) put(blob + 1024, n, k, 2, w[W2 + n * 16 + k]);
+  for (int n = 0; n < 12; n++)
+    for (int k = 0; k < 16; k++) put(blob + 1536, n, k, 2, w[W3 + n * 16 + k]);
+}
+
+void mlp_fp32_build_blob(const float *w, float *blob) {
+  std::memset(blob, 0, MLP_FP32_BLOB_BYTES);
+  const int W1 = 0, B1 = 16 * 20, W2 = B1 + 16, B2 = W2 + 256, W3 = B2 + 16, B3 = W3 + 12 * 16;
+  for (int i = 0; i < 20; i++)
+    for (int k = 0; k < 4; k++)
+      for (int c = 0; c < 4; c++) blob[(MLP_FP32_W1 + i * 4 + k) * 4 + c] = w[W1 + (4 * k + c) * 20 + i];
+  for (int i = 0; i < 16; i++)
+    for (int k = 0; k < 4; k++)
+      for (int c = 0; c < 4; c++) blob[(MLP_FP32_W2 + i * 4 + k) * 4 + c] = w[W2 + (4 * k + c) * 16 + i];
+  for (int i = 0; i < 16; i++)
+    for (int k = 0; k < 4; k++)
+      for (int c = 0; c < 3; c++) blob[(MLP_FP32_W3 + i * 4 + k) * 4 + c] = w[W3 + (4 * c + k) * 16 + i];
+  for (int k = 0; k < 4; k++)
+    for (int c = 0; c < 4; c++) {
+      blob[(MLP_FP32_B1 + k) * 4 + c] = w[B1 + 4 * k + c];
+      blob[(MLP_FP32_B2 + k) * 4 + c] = w[B2 + 4 * k + c];
+      if (c < 3) blob[(MLP_FP32_B3 + k) * 4 + c] = w[B3 + 4 * c + k];
+    }
+}
+
+}  // namespace hush

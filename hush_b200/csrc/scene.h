@@ -1,6 +1,6 @@
 // Analytic synthetic G-buffer scenes: a ground plane plus spheres and y-rotated boxes, ray-cast per pixel.
 //
-// Shared by the host generator (gbuffer_gen.cpp, g++) and the device generator (gbuffer_gen.cu, nvcc). Every frame
+// Shared by the host generator and the device generator (gbuffer_gen.cu). Every frame
 // buffer follows the reference's G-buffer layout (src/index.d.ts:1-17, src/denoise/hush.js:9-13):
 //   radiance     rgb noisy 1 spp radiance without the primary emission, a = 1
 //   normalDepth  world normal xyz, linear view depth w (< 0 = sky)
@@ -266,21 +266,24 @@ HS_HD void hs_shade_pixel(const hs_desc *d, const hs_scene *s, const hs_camera *
     return;
   }
   float hx = cam->px + t * dx, hy = cam->py + t * dy, hz = cam->pz + t * dz;
-  float ar, ag, ab, rough, emit = 0.0f, cellk;
+  float ar, ag, ab, rough, emit = 0.0f;
   int id;
   float vx = 0.0f, vz = 0.0f;
+  int cell;
   if (hit == -1) {
     ar = s->ground_r; ag = s->ground_g; ab = s->ground_b; rough = s->ground_rough; id = s->ground_id;
-    cellk = 1.0f;
+    cell = (int)floorf(hx + 0.25f) + (int)floorf(hz + 0.25f);  // unit cells on the plane (y = 0 is the surface)
   } else {
     const hs_object *o = &s->o[hit];
     ar = o->ar; ag = o->ag; ab = o->ab; rough = o->rough; id = o->id; emit = o->emit;
     vx = o->vx; vz = o->vz;
-    cellk = 8.0f / (2.0f * o->r);  // 8 checker cells across the object
+    // 8 cells across the object, in coordinates relative to its centre, offset by a quarter cell so that no face
+    // of a box lies on a cell boundary (host and device rounding would pick different cells there)
+    float cx, cy, cz;
+    hs_object_pos(o, frame, &cx, &cy, &cz);
+    const float k = 8.0f / (2.0f * o->r);
+    cell = (int)floorf((hx - cx) * k + 0.25f) + (int)floorf((hy - cy) * k + 0.25f) + (int)floorf((hz - cz) * k + 0.25f);
   }
-  // 8x8 checker factor 0.6 / 1.0 in object-relative coordinates
-  float ox = hx - vx * (float)frame, oz = hz - vz * (float)frame;
-  int cell = (int)floorf(ox * cellk) + (int)floorf(hy * cellk) + (int)floorf(oz * cellk);
   float chk = (cell & 1) ? 0.6f : 1.0f;
   ar *= chk; ag *= chk; ab *= chk;
   // Lambert under one directional light (hard shadow) + 0.1 ambient

@@ -48,13 +48,16 @@ __global__ void k_svgf_temporal(const SvgfFrame f) {
   const float4 alb = ldh(f.mat, y * f.p_mat + x);
   const float4 r = ldh(f.rad, y * f.p_rad + x);
   const float ix = r.x / fmaxf(alb.x, 1e-3f), iy = r.y / fmaxf(alb.y, 1e-3f), iz = r.z / fmaxf(alb.z, 1e-3f);
-  const float l = lum3(ix, iy, iz);
+  const float l = __fadd_rn(__fadd_rn(__fmul_rn(ix, 0.2126f), __fmul_rn(iy, 0.7152f)), __fmul_rn(iz, 0.0722f));
   const float ppx = (float)x + 0.5f + mv.x - 0.5f, ppy = (float)y + 0.5f + mv.y - 0.5f;
   const float flx = floorf(ppx), fly = floorf(ppy);
   const int bx = (int)flx, by = (int)fly;
   const float fx = ppx - flx, fy = ppy - fly;
+  // the history length it blends into decides the spatial / temporal variance branch (m.z >= 4), so the weighted
+  // sums are rounded product by product like an unfused shader (no FMA contraction)
   float sumW = 0.f, hcx = 0.f, hcy = 0.f, hcz = 0.f, hm0 = 0.f, hm1 = 0.f, hm2 = 0.f;
-  const float wts[4] = {(1.0f - fx) * (1.0f - fy), fx * (1.0f - fy), (1.0f - fx) * fy, fx * fy};
+  const float wts[4] = {__fmul_rn(1.0f - fx, 1.0f - fy), __fmul_rn(fx, 1.0f - fy), __fmul_rn(1.0f - fx, fy),
+                        __fmul_rn(fx, fy)};
   const bool noHistory = f.reset != 0;
   if (!noHistory) {
 #pragma unroll
@@ -63,8 +66,10 @@ __global__ void k_svgf_temporal(const SvgfFrame f) {
       if (svgf_consistent(f, qx, qy, nd, mv.w, mv.z) && wts[i] > 0.0f) {
         const float4 c = ldh(f.hist_prev, qy * f.W + qx), m = ldh(f.mom_prev, qy * f.W + qx);
         sumW += wts[i];
-        hcx += wts[i] * c.x; hcy += wts[i] * c.y; hcz += wts[i] * c.z;
-        hm0 += wts[i] * m.x; hm1 += wts[i] * m.y; hm2 += wts[i] * m.z;
+        hcx = __fadd_rn(hcx, __fmul_rn(wts[i], c.x)); hcy = __fadd_rn(hcy, __fmul_rn(wts[i], c.y));
+        hcz = __fadd_rn(hcz, __fmul_rn(wts[i], c.z));
+        hm0 = __fadd_rn(hm0, __fmul_rn(wts[i], m.x)); hm1 = __fadd_rn(hm1, __fmul_rn(wts[i], m.y));
+        hm2 = __fadd_rn(hm2, __fmul_rn(wts[i], m.z));
       }
     }
   }
@@ -82,17 +87,17 @@ __global__ void k_svgf_temporal(const SvgfFrame f) {
       }
     }
   }
-  float len, cx = ix, cy = iy, cz = iz, m0 = l, m1 = l * l;
+  float len, cx = ix, cy = iy, cz = iz, m0 = l, m1 = __fmul_rn(l, l);
   if (sumW >= 0.01f) {
     hcx /= sumW; hcy /= sumW; hcz /= sumW;
     hm0 /= sumW; hm1 /= sumW; hm2 /= sumW;
     len = fminf(hm2 + 1.0f, 64.0f);
     const float ac = fmaxf(f.alpha_color, 1.0f / len), am = fmaxf(f.alpha_moments, 1.0f / len);
-    cx = hcx * (1.0f - ac) + ix * ac;
-    cy = hcy * (1.0f - ac) + iy * ac;
-    cz = hcz * (1.0f - ac) + iz * ac;
-    m0 = hm0 * (1.0f - am) + m0 * am;
-    m1 = hm1 * (1.0f - am) + m1 * am;
+    cx = __fadd_rn(__fmul_rn(hcx, 1.0f - ac), __fmul_rn(ix, ac));
+    cy = __fadd_rn(__fmul_rn(hcy, 1.0f - ac), __fmul_rn(iy, ac));
+    cz = __fadd_rn(__fmul_rn(hcz, 1.0f - ac), __fmul_rn(iz, ac));
+    m0 = __fadd_rn(__fmul_rn(hm0, 1.0f - am), __fmul_rn(m0, am));
+    m1 = __fadd_rn(__fmul_rn(hm1, 1.0f - am), __fmul_rn(m1, am));
   } else {
     len = 1.0f;
   }
@@ -211,17 +216,22 @@ __global__ void k_svgf_resolve(const SvgfFrame f, const uint2 *il) {
     sth(f.taa, o, make_float4(r.x, r.y, r.z, 1.0f));
     return;
   }
+  // E[c^2] - E[c]^2 cancels catastrophically when the neighbourhood is flat: its products are rounded separately
+  // (no FMA contraction), as an unfused f32 shader computes them
   float3 m1 = make_float3(0.f, 0.f, 0.f), m2 = m1;
   for (int dy = -1; dy <= 1; dy++)
     for (int dx = -1; dx <= 1; dx++) {
       const float3 c = to_ycocg(tmap(svgf_remod(f, il, x + dx, y + dy)));
       m1.x += c.x; m1.y += c.y; m1.z += c.z;
-      m2.x += c.x * c.x; m2.y += c.y * c.y; m2.z += c.z * c.z;
+      m2.x = __fadd_rn(m2.x, __fmul_rn(c.x, c.x));
+      m2.y = __fadd_rn(m2.y, __fmul_rn(c.y, c.y));
+      m2.z = __fadd_rn(m2.z, __fmul_rn(c.z, c.z));
     }
   m1.x /= 9.0f; m1.y /= 9.0f; m1.z /= 9.0f;
   m2.x /= 9.0f; m2.y /= 9.0f; m2.z /= 9.0f;
-  const float sdx = sqrtf(fmaxf(m2.x - m1.x * m1.x, 0.0f)), sdy = sqrtf(fmaxf(m2.y - m1.y * m1.y, 0.0f)),
-              sdz = sqrtf(fmaxf(m2.z - m1.z * m1.z, 0.0f));
+  const float sdx = sqrtf(fmaxf(__fsub_rn(m2.x, __fmul_rn(m1.x, m1.x)), 0.0f)),
+              sdy = sqrtf(fmaxf(__fsub_rn(m2.y, __fmul_rn(m1.y, m1.y)), 0.0f)),
+              sdz = sqrtf(fmaxf(__fsub_rn(m2.z, __fmul_rn(m1.z, m1.z)), 0.0f));
   const float4 mv = ldh(f.mv, y * f.p_mv + x);
   const float uvx = ((float)x + 0.5f + mv.x) / (float)f.W, uvy = ((float)y + 0.5f + mv.y) / (float)f.H;
   const float a = f.taa_alpha;
