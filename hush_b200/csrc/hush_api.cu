@@ -40,6 +40,7 @@ struct hush_s {
   size_t pool_bytes = 0;
   uint2 *A0 = nullptr, *X = nullptr, *Bh[2] = {}, *mom[2] = {}, *key[2] = {}, *hist[2] = {}, *taa[2] = {},
         *par0[2] = {}, *par1 = nullptr, *par2 = nullptr, *C[2] = {}, *CG = nullptr, *Ah = nullptr, *Gh = nullptr;
+  float4 *Gd = nullptr, *CGd = nullptr;
   uint4 *F[4] = {};
   unsigned int *err = nullptr;
   const void *last_out = nullptr;
@@ -116,7 +117,7 @@ static int alloc_state(hush_t *h, int width, int height) {
   const size_t full = (size_t)W * H * 8, half = (size_t)W2 * H2 * 8, quarter = (size_t)W4 * H4 * 8,
                half16 = (size_t)W2 * H2 * 16;
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-  size_t total = al(full) * 10 + al(half) * 8 + al(half16) * 4 + al(quarter) * 3 + 256;
+  size_t total = al(full) * 10 + al(half) * 8 + al(half16) * 5 + al(quarter) * 3 + al(quarter * 2) + 256;
   char *pool = nullptr;
   cudaError_t e = cudaMalloc(&pool, total);
   if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc of the state images");
@@ -135,7 +136,9 @@ static int alloc_state(hush_t *h, int width, int height) {
   for (int i = 0; i < 2; i++) { h->Bh[i] = (uint2 *)take(half); h->par0[i] = (uint2 *)take(half); }
   h->par1 = (uint2 *)take(half); h->par2 = (uint2 *)take(half); h->Ah = (uint2 *)take(half); h->Gh = (uint2 *)take(half);
   for (int i = 0; i < 4; i++) h->F[i] = (uint4 *)take(half16);
+  h->Gd = (float4 *)take(half16);
   h->C[0] = (uint2 *)take(quarter); h->C[1] = (uint2 *)take(quarter); h->CG = (uint2 *)take(quarter);
+  h->CGd = (float4 *)take(quarter * 2);
   h->err = (unsigned int *)take(256);
   h->W = W; h->H = H; h->W2 = W2; h->H2 = H2; h->W4 = W4; h->H4 = H4;
   h->frame = 0;
@@ -341,7 +344,7 @@ static HushFrame make_frame(hush_t *h, const hush_inputs *in) {
   f.par0 = h->par0[cur]; f.par1 = h->par1; f.par2 = h->par2; f.Bh0 = h->Bh[0]; f.Bh1 = h->Bh[1];
   f.C0 = h->C[0]; f.C1 = h->C[1]; f.CG = h->CG;
   f.F0 = h->F[0]; f.F1 = h->F[1]; f.F2 = h->F[2]; f.F3 = h->F[3];
-  f.Ah = h->Ah; f.Gh = h->Gh;
+  f.Ah = h->Ah; f.Gh = h->Gh; f.Gd = h->Gd; f.CGd = h->CGd;
   f.w_glob = h->w_dev;
   f.hidden = h->hidden;
   f.err = h->err;

@@ -16,8 +16,10 @@ struct HushFrame {
   const uint2 *key_prev, *hist_prev, *mom_prev, *par0_prev, *taa_prev;
   uint2 *A0, *X, *mom, *key, *hist, *taa, *par0, *par1, *par2, *Bh0, *Bh1, *C0, *C1, *CG;
   uint4 *F0, *F1, *F2, *F3;
-  // half-res planes of the fused path: block means (F2.zw) and guide (F3.xy) as rgba16float
+  // half-res planes of the fused path: block means (F2.zw) and guide (F3.xy) as rgba16float, and the guides decoded
+  // once by their producer as f32 (normal, depth): Gd at half, CGd at quarter resolution
   uint2 *Ah, *Gh;
+  float4 *Gd, *CGd;
   const float *w_glob;  // decoded f32 weights in device memory (any hidden width)
   int hidden;
   unsigned int *err;    // device error word (bounded waits in the tensor-core MLP)

@@ -31,15 +31,16 @@ HD_INL float4 gh_decode(float4 g) {  // (oct normal, depth, count) -> (normal, d
 }
 
 // ------------------------------------------------------------------------------------------------ stage 0
-// Tile 32 x 8 pixels = 16 x 4 blocks, 256 threads. Three phases, every thread busy in each:
+// Tile 32 x 8 pixels = 16 x 4 blocks, 256 threads, three phases:
 //   1. illumination tile (apron 1) in shared memory as (r, g, b, L): L = luminance, or L_INVALID outside the image
 //      or on sky
 //   2. pixel(): one pixel per thread (hush.js:111-223), feature inputs P0..P4 to shared memory
-//   3. block(): a 4-lane group per 2x2 block (hush.js:226-282). Every lane forms the block sums itself in the
-//      reference's order; the MLP (FP32 form) splits each layer over the group, 4 hidden units per lane, with the
-//      transposed weights in shared memory. The tensor-core form (TC) writes the features as MMA operand rows and
-//      warps 0-1 run the three layers as tcgen05 MMAs (M = 128 with 64 rows used, N = 16, K = 32 / 16 / 16) on bf16
-//      or f16 operands with FP32 accumulation in TMEM; bias, ReLU and the heads stay FP32.
+//   3. block() (hush.js:226-282), one thread per 2x2 block, from the per-pixel terms phases 1-2 left in shared
+//      memory (decoded normals, quantised luminances). The FP32 MLP then splits each layer over a 4-lane group per
+//      block (4 hidden units per lane, packed FP32x2 FMAs, transposed weights in shared memory); the tensor-core form
+//      (TC) writes the features as MMA operand rows and warps 0-1 run the three layers as tcgen05 MMAs (M = 128 with
+//      64 rows used, N = 16, K = 32 / 16 / 16) on bf16 or f16 operands with FP32 accumulation in TMEM; bias, ReLU and
+//      the heads stay FP32.
 constexpr int K1_TW = 32, K1_TH = 8;
 constexpr int K1_NB = (K1_TW / 2) * (K1_TH / 2);  // 64 blocks
 constexpr uint32_t MBAR_POLLS = 1u << 22;
@@ -54,10 +55,6 @@ struct TcSmem {
   alignas(8) uint64_t mbar;
   uint32_t tmem;
   uint32_t flags[K1_NB];  // bit 0: block inside the half-res image, bit 1: block has valid pixels
-};
-struct FpSmem {
-  float4 w[MLP_FP32_BLOB_BYTES / 16];  // transposed weights + biases (mlp_fp32_build_blob)
-  float4 h[K1_NB][4];                  // hidden activations of each block, exchanged within its 4-lane group
 };
 
 template <bool BF16>
@@ -100,27 +97,39 @@ HD_INL bool tc_layer(TcSmem &S, int li, bool first, uint32_t b_off, uint32_t kco
   return ok;
 }
 
-// pixel() of hush.js:111-223 over the (r, g, b, L) tile; same arithmetic as temporal_pixel().
-HD_INL PixP temporal_pixel_fast(const HushFrame &f, int px, int py, const float4 *sI, int ti) {
-  constexpr int SW = K1_TW + 2;
-  PixP R = pixp_default();
+// Shared memory of the fused temporal kernel. Per-pixel arrays are structure-of-arrays (16-byte stride, no bank
+// conflicts for the 128-bit accesses).
+constexpr int K1_SW = K1_TW + 2, K1_SH = K1_TH + 2, K1_NT = K1_TW * K1_TH;
+struct K1Smem {
+  float4 I[K1_SW * K1_SH];   // illumination (r, g, b) and L (luminance or L_INVALID), apron 1
+  float2 Lq[K1_SW * K1_SH];  // (E * qf16(L), 1) for valid entries, (0, 0) otherwise: the 4x4 block statistics
+  float4 P0[K1_NT], P1[K1_NT], P2[K1_NT], P3[K1_NT], P4[K1_NT];  // pixel() feature inputs
+  float4 Ns[K1_NT];          // octDec(P2.xy) and 1 for pixels with a surface, zeros otherwise
+};
+
+// pixel() of hush.js:111-223 over the (r, g, b, L) tile; same arithmetic as temporal_pixel(). Writes A0, mom, key
+// and the pixel's entries of the shared feature-input arrays.
+HD_INL void temporal_pixel_fast(const HushFrame &f, int px, int py, K1Smem &S, int ti, int li) {
+  constexpr int SW = K1_SW;
   const int W = f.W, H = f.H;
   const uint2 ndr = __ldg(f.nd + py * f.p_nd + px), mvr = __ldg(f.mv + py * f.p_mv + px);
   const float4 nd = h4_to_f4(ndr), mv = h4_to_f4(mvr);
   const int oi = py * W + px;
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
   if (nd.w < 0.0f) {
     f.A0[oi] = make_uint2(0, 0);
     f.mom[oi] = make_uint2(0, 0);
     sth(f.key, oi, make_float4(0.f, 0.f, -1.0f, mv.z));
-    return R;
+    S.P0[li] = z4; S.P1[li] = z4; S.P2[li] = make_float4(0.f, 0.f, -1.0f, 0.f); S.P3[li] = z4; S.P4[li] = z4;
+    S.Ns[li] = z4;
+    return;
   }
   // reprojection gathers first (the dependent-load chain), kept packed until used
-  uint2 k4[4], c4[4], m4[4], pqr;
-  float fx = 0.f, fy = 0.f, ppx = 0.f, ppy = 0.f;
+  uint2 k4[4], c4[4], m4[4], pqr = make_uint2(0, 0);
+  float fx = 0.f, fy = 0.f;
   int bix = 0, biy = 0, cx = 0, cy = 0;
   if (!f.reset) {
-    ppx = (float)px + mv.x;
-    ppy = (float)py + mv.y;
+    const float ppx = (float)px + mv.x, ppy = (float)py + mv.y;
     const float bx = floorf(ppx), by = floorf(ppy);
     fx = ppx - bx;
     fy = ppy - by;
@@ -139,12 +148,12 @@ HD_INL PixP temporal_pixel_fast(const HushFrame &f, int px, int py, const float4
   }
   const uint2 mrr = __ldg(f.mat + py * f.p_mat + px);
   // 3x3 statistics of the illumination (valid neighbours), two passes
-  const float4 illum = sI[ti];
+  const float4 illum = S.I[ti];
   const float l = illum.w;
   float s1x = 0.f, s1y = 0.f, s1z = 0.f, cnt = 0.f;
 #pragma unroll
   for (int j = 0; j < 9; j++) {
-    const float4 c = sI[ti + (j / 3 - 1) * SW + (j % 3 - 1)];
+    const float4 c = S.I[ti + (j / 3 - 1) * SW + (j % 3 - 1)];
     s1x += c.x; s1y += c.y; s1z += c.z;  // invalid entries hold rgb = 0
     cnt += l_valid(c.w) ? 1.0f : 0.0f;
   }
@@ -154,7 +163,7 @@ HD_INL PixP temporal_pixel_fast(const HushFrame &f, int px, int py, const float4
   float svx = 0.f, svy = 0.f, svz = 0.f, svar = 0.f;
 #pragma unroll
   for (int j = 0; j < 9; j++) {
-    const float4 c = sI[ti + (j / 3 - 1) * SW + (j % 3 - 1)];
+    const float4 c = S.I[ti + (j / 3 - 1) * SW + (j % 3 - 1)];
     if (l_valid(c.w)) {
       const float dx = c.x - mux, dy = c.y - muy, dz = c.z - muz, dl = c.w - slm;
       svx += dx * dx; svy += dy * dy; svz += dz * dz;
@@ -166,7 +175,7 @@ HD_INL PixP temporal_pixel_fast(const HushFrame &f, int px, int py, const float4
   svar /= cnt;
   bool has = false;
   float hcx = 0.f, hcy = 0.f, hcz = 0.f;
-  float4 hm = make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 hm = z4;
   float v = 0.f, alpha = 1.0f, gamma = 1.0f;
   if (!f.reset) {
     float sumW = 0.f;
@@ -189,7 +198,7 @@ HD_INL PixP temporal_pixel_fast(const HushFrame &f, int px, int py, const float4
     } else {
       float n3 = 0.f;
       hcx = hcy = hcz = 0.f;
-      hm = make_float4(0.f, 0.f, 0.f, 0.f);
+      hm = z4;
       for (int j = 0; j < 9; j++) {
         const int qx = cx + j % 3 - 1, qy = cy + j / 3 - 1;
         if (qx >= 0 && qy >= 0 && qx < W && qy < H && check_key(ldh(f.key_prev, qy * W + qx), nd, mv.w, mv.z)) {
@@ -240,19 +249,23 @@ HD_INL PixP temporal_pixel_fast(const HushFrame &f, int px, int py, const float4
   const float4 Aq = make_float4(qf16(A.x), qf16(A.y), qf16(A.z), qf16(A.w));
   const float m1 = E * qf16(nmx);
   const float m2 = E * E * qf16(nmy);
-  R.P0 = make_float4(E * lum(Aq), E * qf16(l), fmaxf(m2 - m1 * m1, 0.0f), len1);
-  R.P1 = make_float4(qf16(v), qf16(lag), E * qf16(nfast), m1);
-  R.P2 = make_float4(qf16(oc.x), qf16(oc.y), qf16(nd.w), qf16(sqrtf(mv.x * mv.x + mv.y * mv.y)));
-  R.P3 = h4_to_f4(mrr);
-  R.P4 = Aq;
-  return R;
+  const float ox = qf16(oc.x), oy = qf16(oc.y);
+  S.P0[li] = make_float4(E * lum(Aq), E * qf16(l), fmaxf(m2 - m1 * m1, 0.0f), len1);
+  S.P1[li] = make_float4(qf16(v), qf16(lag), E * qf16(nfast), m1);
+  S.P2[li] = make_float4(ox, oy, qf16(nd.w), qf16(sqrtf(mv.x * mv.x + mv.y * mv.y)));
+  S.P3[li] = h4_to_f4(mrr);
+  S.P4[li] = Aq;
+  float4 ns = oct_dec(ox, oy);  // block() decodes the stored oct normal (hush.js:238)
+  ns.w = 1.0f;
+  S.Ns[li] = ns;
 }
 
-// block() features (hush.js:226-282) for block b of the tile, computed by each lane of its group. sL holds the
-// tile's L (luminance, or L_INVALID).
-HD_INL bool block_features_grp(const PixP *sP, const float *sL, int lbx, int lby, float E, float *f, float4 &AC,
-                               float4 &G) {
-  constexpr int SW = K1_TW + 2;
+// block() (hush.js:226-282) for block (lbx, lby) of the tile, one thread per block: the 20 features, the block mean
+// colour AC and the guide G = (oct normal, Z, count). Returns nv > 0.
+HD_INL bool block_features_tile(const K1Smem &S, int lbx, int lby, float E, float *f, float4 &AC, float4 &G) {
+  constexpr int SW = K1_SW;
+  const int p0 = (2 * lby) * K1_TW + 2 * lbx;
+  const int pj[4] = {p0, p0 + 1, p0 + K1_TW, p0 + K1_TW + 1};
   float nv = 0.f;
   float4 S0 = make_float4(0.f, 0.f, 0.f, 0.f), S1 = S0, S3 = S0;
   AC = S0;
@@ -262,24 +275,21 @@ HD_INL bool block_features_grp(const PixP *sP, const float *sL, int lbx, int lby
   bool ok[4];
 #pragma unroll
   for (int j = 0; j < 4; j++) {
-    const PixP &P = sP[(lby * 2 + (j >> 1)) * K1_TW + lbx * 2 + (j & 1)];
-    const float4 p2 = P.P2;
-    ok[j] = p2.z >= 0.0f;
+    ns[j] = S.Ns[pj[j]];
+    ok[j] = ns[j].w != 0.0f;
     la[j] = 0.f; zs[j] = 0.f;
-    ns[j] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (!ok[j]) continue;
-    const float4 p0 = P.P0, p1 = P.P1, p3 = P.P3, p4 = P.P4;
+    const float4 q0 = S.P0[pj[j]], q1 = S.P1[pj[j]], q2 = S.P2[pj[j]], q3 = S.P3[pj[j]], q4 = S.P4[pj[j]];
     nv += 1.0f;
-    la[j] = p0.x;
-    ns[j] = oct_dec(p2.x, p2.y);
-    zs[j] = p2.z;
-    S0.x += p0.x; S0.y += p0.y; S0.z += p0.z; S0.w += p0.w;
-    S1.x += p1.x; S1.y += p1.y; S1.z += p1.z; S1.w += p1.w;
+    la[j] = q0.x;
+    zs[j] = q2.z;
+    S0.x += q0.x; S0.y += q0.y; S0.z += q0.z; S0.w += q0.w;
+    S1.x += q1.x; S1.y += q1.y; S1.z += q1.z; S1.w += q1.w;
     Nx += ns[j].x; Ny += ns[j].y; Nz += ns[j].z;
-    S3.x += p3.x; S3.y += p3.y; S3.z += p3.z; S3.w += p3.w;
-    AC.x += p4.x; AC.y += p4.y; AC.z += p4.z; AC.w += p4.w;
-    MV += p2.w;
-    Z += p2.z;
+    S3.x += q3.x; S3.y += q3.y; S3.z += q3.z; S3.w += q3.w;
+    AC.x += q4.x; AC.y += q4.y; AC.z += q4.z; AC.w += q4.w;
+    MV += q2.w;
+    Z += q2.z;
   }
   if (nv == 0.0f) {
     G = make_float4(0.f, 0.f, -1.0f, 0.f);
@@ -299,23 +309,22 @@ HD_INL bool block_features_grp(const PixP *sP, const float *sL, int lbx, int lby
   for (int j = 0; j < 4; j++)
     if (ok[j]) VA += (la[j] - Lacc) * (la[j] - Lacc);
   VA *= k;
-  // 4x4 neighbourhood (block +-1) of the tile, top-left at tile position (2 lbx, 2 lby) with the apron
+  // 4x4 neighbourhood (block +-1), top-left at tile position (2 lbx, 2 lby) including the apron
   const int t0 = (2 * lby) * SW + 2 * lbx;
-  float s1 = 0.f, n4 = 0.f, lq[16], wq[16];
+  float s1 = 0.f, n4 = 0.f;
 #pragma unroll
   for (int j = 0; j < 16; j++) {
-    const float L = sL[t0 + (j >> 2) * SW + (j & 3)];
-    wq[j] = l_valid(L) ? 1.0f : 0.0f;
-    lq[j] = E * qf16(l_valid(L) ? L : 0.0f);
-    s1 += wq[j] * lq[j];
-    n4 += wq[j];
+    const float2 q = S.Lq[t0 + (j >> 2) * SW + (j & 3)];
+    s1 += q.y * q.x;
+    n4 += q.y;
   }
   const float mu4 = s1 / fmaxf(n4, 1.0f);
   float var4 = 0.f;
 #pragma unroll
   for (int j = 0; j < 16; j++) {
-    const float d = lq[j] - mu4;
-    var4 += wq[j] * d * d;
+    const float2 q = S.Lq[t0 + (j >> 2) * SW + (j & 3)];
+    const float d = q.x - mu4;
+    var4 += q.y * d * d;
   }
   var4 /= fmaxf(n4, 1.0f);
   const float nl = fmaxf(sqrtf(Nx * Nx + Ny * Ny + Nz * Nz), 1e-6f);
@@ -342,15 +351,27 @@ HD_INL bool block_features_grp(const PixP *sP, const float *sL, int lbx, int lby
   return true;
 }
 
+struct FpSmem {
+  float4 w[MLP_FP32_BLOB_BYTES / 16];  // transposed weights + biases (mlp_fp32_build_blob)
+  float4 fe[K1_NB][5];                 // features of each block, as stored
+  float4 h[K1_NB][4];                  // hidden activations of each block, exchanged within its 4-lane group
+  uint32_t flags[K1_NB];               // bit 0: block inside the half-res image, bit 1: block has valid pixels
+};
+
+HD_INL float4 ffma4(float s, float4 w, float4 a) {  // a + s * w as two packed FP32x2 FMAs
+  const float2 lo = __ffma2_rn(make_float2(s, s), make_float2(w.x, w.y), make_float2(a.x, a.y));
+  const float2 hi = __ffma2_rn(make_float2(s, s), make_float2(w.z, w.w), make_float2(a.z, a.w));
+  return make_float4(lo.x, lo.y, hi.x, hi.y);
+}
+
 template <bool TC, bool BF16>
-__global__ void __launch_bounds__(K1_TW *K1_TH, 3)
+__global__ void __launch_bounds__(K1_NT, 3)
     k_temporal_fused(const __grid_constant__ HushFrame f, const __grid_constant__ MlpW16 w, const uint4 *blob) {
-  constexpr int SW = K1_TW + 2, SH = K1_TH + 2, NT = K1_TW * K1_TH;
-  __shared__ float4 sI[SW * SH];
-  __shared__ float sL[SW * SH];
-  __shared__ PixP sP[NT];
+  constexpr int SW = K1_SW, SH = K1_SH, NT = K1_NT;
+  __shared__ K1Smem S;
   __shared__ std::conditional_t<TC, TcSmem, FpSmem> X_;
   const int li = threadIdx.x;
+  const float E = f.exposure;
   if constexpr (TC) {
     if (li < 32) {
       umma::tmem_alloc(umma::smem_u32(&X_.tmem), 32);
@@ -368,15 +389,17 @@ __global__ void __launch_bounds__(K1_TW *K1_TH, 3)
   for (int i = li; i < SW * SH; i += NT) {
     const int qx = ox + i % SW, qy = oy + i / SW;
     float4 e = make_float4(0.f, 0.f, 0.f, L_INVALID);
+    float2 lq = make_float2(0.f, 0.f);
     if (qx >= 0 && qy >= 0 && qx < f.W && qy < f.H && ldh(f.nd, qy * f.p_nd + qx).w >= 0.0f) {
       const float4 r = ldh(f.rad, qy * f.p_rad + qx), m = ldh(f.mat, qy * f.p_mat + qx);
       e.x = r.x / fmaxf(m.x, 1e-3f);
       e.y = r.y / fmaxf(m.y, 1e-3f);
       e.z = r.z / fmaxf(m.z, 1e-3f);
       e.w = lum3(e.x, e.y, e.z);
+      lq = make_float2(E * qf16(e.w), 1.0f);
     }
-    sI[i] = e;
-    sL[i] = e.w;
+    S.I[i] = e;
+    S.Lq[i] = lq;
   }
   __syncthreads();
   if constexpr (TC) umma::fence_after_sync();
@@ -384,40 +407,65 @@ __global__ void __launch_bounds__(K1_TW *K1_TH, 3)
   {
     const int tx = li % K1_TW, ty = li / K1_TW;
     const int px = blockIdx.x * K1_TW + tx, py = blockIdx.y * K1_TH + ty;
-    PixP P = pixp_default();
-    if (px < f.W && py < f.H) P = temporal_pixel_fast(f, px, py, sI, (ty + 1) * SW + tx + 1);
-    sP[li] = P;
+    if (px < f.W && py < f.H) {
+      temporal_pixel_fast(f, px, py, S, (ty + 1) * SW + tx + 1, li);
+    } else {
+      const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+      S.P0[li] = z4; S.P1[li] = z4; S.P2[li] = make_float4(0.f, 0.f, -1.0f, 0.f); S.P3[li] = z4; S.P4[li] = z4;
+      S.Ns[li] = z4;
+    }
   }
   __syncthreads();
-  // phase 3: 4-lane group per block
-  const int b = li >> 2, k = li & 3;
-  const int lbx = b % (K1_TW / 2), lby = b / (K1_TW / 2);
-  const int X = blockIdx.x * (K1_TW / 2) + lbx, Y = blockIdx.y * (K1_TH / 2) + lby;
-  const bool valid = X < f.W2 && Y < f.H2;
-  const int o = Y * f.W2 + X;
-  float fe[N_FEAT];
-  float4 AC, G;
-  const bool ok = block_features_grp(sP, sL, lbx, lby, f.exposure, fe, AC, G);
-  if (valid) {
-    // the block means / guide (F2.zw, F3.xy of hush.js:280-281), by lanes 0 and 1
-    if (k == 0) f.Ah[o] = ok ? make_uint2(pk(AC.x, AC.y), pk(AC.z, AC.w)) : make_uint2(0, 0);
-    if (k == 1) f.Gh[o] = ok ? make_uint2(pk(G.x, G.y), pk(G.z, G.w)) : make_uint2(pk(0.f, 0.f), pk(-1.0f, 0.f));
-  }
-  // the MLP sees the features as stored (packed f16, hush.js:278-280, 348-353)
+  // phase 3a: block features, one thread per block (warps 0-1)
+  if (li < K1_NB) {
+    const int lbx = li % (K1_TW / 2), lby = li / (K1_TW / 2);
+    const int X = blockIdx.x * (K1_TW / 2) + lbx, Y = blockIdx.y * (K1_TH / 2) + lby;
+    const bool valid = X < f.W2 && Y < f.H2;
+    const int o = Y * f.W2 + X;
+    float fe[N_FEAT];
+    float4 AC, G;
+    const bool ok = block_features_tile(S, lbx, lby, E, fe, AC, G);
+    if (valid) {
+      // block means and guide: F2.zw and F3.xy of hush.js:280-281 (hush.js:241-244 without valid pixels)
+      f.Ah[o] = ok ? make_uint2(pk(AC.x, AC.y), pk(AC.z, AC.w)) : make_uint2(0, 0);
+      f.Gh[o] = ok ? make_uint2(pk(G.x, G.y), pk(G.z, G.w)) : make_uint2(pk(0.f, 0.f), pk(-1.0f, 0.f));
+      // the decoded guide every half-res consumer forms from F3 (octDec of the stored oct normal, stored depth)
+      float4 gd = oct_dec(ok ? quant1(qf16(G.x)) : 0.f, ok ? quant1(qf16(G.y)) : 0.f);
+      gd.w = ok ? quant1(qf16(G.z)) : -1.0f;
+      f.Gd[o] = gd;
+    }
+    // the MLP sees the features as stored (packed f16, hush.js:278-280, 348-353)
 #pragma unroll
-  for (int i = 0; i < N_FEAT; i++) fe[i] = ok ? __half2float(__ushort_as_half(f2h(qf16(fe[i])))) : 0.0f;
+    for (int i = 0; i < N_FEAT; i++) fe[i] = ok ? __half2float(__ushort_as_half(f2h(qf16(fe[i])))) : 0.0f;
+    X_.flags[li] = (valid ? 1u : 0u) | (ok ? 2u : 0u);
+    if constexpr (TC) {
+      float v8[8];
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+#pragma unroll
+        for (int e = 0; e < 8; e++) v8[e] = 8 * c + e < N_FEAT ? fe[8 * c + e] : 0.0f;
+        *reinterpret_cast<uint4 *>(X_.a1 + umma::kmajor_off(li, 8 * c, 4)) = pack8<BF16>(v8);
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < 5; c++) X_.fe[li][c] = make_float4(fe[4 * c], fe[4 * c + 1], fe[4 * c + 2], fe[4 * c + 3]);
+    }
+  }
   const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
   if constexpr (!TC) {
-    // every lane runs the layers (the group exchanges through shared memory and shuffles); blocks outside the image
-    // or without valid pixels compute on zero features and store nothing / zeros
-    // layer 1: units 4k..4k+3
+    __syncthreads();
+    // phase 3b: FP32 MLP, a 4-lane group per block, lane k owns hidden units 4k..4k+3 and outputs k, 4+k, 8+k
+    const int b = li >> 2, k = li & 3;
     const float4 *Wt = X_.w;
+    float fe[N_FEAT];
+#pragma unroll
+    for (int c = 0; c < 5; c++) {
+      const float4 t = X_.fe[b][c];
+      fe[4 * c] = t.x; fe[4 * c + 1] = t.y; fe[4 * c + 2] = t.z; fe[4 * c + 3] = t.w;
+    }
     float4 a = Wt[MLP_FP32_B1 + k];
 #pragma unroll
-    for (int i = 0; i < N_FEAT; i++) {
-      const float4 wv = Wt[MLP_FP32_W1 + i * 4 + k];
-      a.x = a.x + fe[i] * wv.x; a.y = a.y + fe[i] * wv.y; a.z = a.z + fe[i] * wv.z; a.w = a.w + fe[i] * wv.w;
-    }
+    for (int i = 0; i < N_FEAT; i++) a = ffma4(fe[i], Wt[MLP_FP32_W1 + i * 4 + k], a);
     X_.h[b][k] = make_float4(fmaxf(a.x, 0.f), fmaxf(a.y, 0.f), fmaxf(a.z, 0.f), fmaxf(a.w, 0.f));
     __syncwarp();
     float h[16];
@@ -429,10 +477,7 @@ __global__ void __launch_bounds__(K1_TW *K1_TH, 3)
     __syncwarp();
     a = Wt[MLP_FP32_B2 + k];
 #pragma unroll
-    for (int i = 0; i < 16; i++) {
-      const float4 wv = Wt[MLP_FP32_W2 + i * 4 + k];
-      a.x = a.x + h[i] * wv.x; a.y = a.y + h[i] * wv.y; a.z = a.z + h[i] * wv.z; a.w = a.w + h[i] * wv.w;
-    }
+    for (int i = 0; i < 16; i++) a = ffma4(h[i], Wt[MLP_FP32_W2 + i * 4 + k], a);
     X_.h[b][k] = make_float4(fmaxf(a.x, 0.f), fmaxf(a.y, 0.f), fmaxf(a.z, 0.f), fmaxf(a.w, 0.f));
     __syncwarp();
 #pragma unroll
@@ -440,20 +485,16 @@ __global__ void __launch_bounds__(K1_TW *K1_TH, 3)
       const float4 t = X_.h[b][q];
       h[4 * q] = t.x; h[4 * q + 1] = t.y; h[4 * q + 2] = t.z; h[4 * q + 3] = t.w;
     }
-    // layer 3: outputs k, 4 + k, 8 + k (par0.k, par1.k, par2.k)
     a = Wt[MLP_FP32_B3 + k];
 #pragma unroll
-    for (int i = 0; i < 16; i++) {
-      const float4 wv = Wt[MLP_FP32_W3 + i * 4 + k];
-      a.x = a.x + h[i] * wv.x; a.y = a.y + h[i] * wv.y; a.z = a.z + h[i] * wv.z;
-    }
+    for (int i = 0; i < 16; i++) a = ffma4(h[i], Wt[MLP_FP32_W3 + i * 4 + k], a);
     // heads (hush.js:357-362) for component k of par0, par1, par2
     const float p0 = k == 0 ? 1.0f / 32.0f + (31.0f / 32.0f) * sigmoidf_(a.x)
                      : k == 1 ? 0.5f + 7.5f * sigmoidf_(a.x)
                               : sigmoidf_(a.x);
     const float p1 = 0.25f * expf(fminf(fmaxf(a.y, -5.0f), 5.0f));
     const float p2 = expf(fminf(fmaxf(a.z, -4.0f), 4.0f));
-    // gather the components of each texel in the lane that stores it: lane k stores par_k (k < 3)
+    // lane k stores texel par_k (k < 3)
     const uint32_t base = (threadIdx.x & 31) & ~3u;
     float c0[4], c1[4], c2[4];
 #pragma unroll
@@ -462,33 +503,20 @@ __global__ void __launch_bounds__(K1_TW *K1_TH, 3)
       c1[q] = __shfl_sync(0xffffffffu, p1, base + q);
       c2[q] = __shfl_sync(0xffffffffu, p2, base + q);
     }
-    if (valid && k < 3) {
+    const uint32_t fl = X_.flags[b];
+    if ((fl & 1u) && k < 3) {
+      const int lbx = b % (K1_TW / 2), lby = b / (K1_TW / 2);
+      const int o = (blockIdx.y * (K1_TH / 2) + lby) * f.W2 + blockIdx.x * (K1_TW / 2) + lbx;
       // INFER on a block without valid pixels writes zeros (hush.js:343-346)
-      const float4 v = !ok ? z4
+      const float4 v = !(fl & 2u) ? z4
                        : k == 0 ? make_float4(c0[0], c0[1], c0[2], c0[3])
                        : k == 1 ? make_float4(c1[0], c1[1], c1[2], c1[3])
                                 : make_float4(c2[0], c2[1], c2[2], c2[3]);
       sth(k == 0 ? f.par0 : k == 1 ? f.par1 : f.par2, o, v);
     }
   } else {
-    // operand row b: lane k writes K columns 8k .. 8k+7
-    {
-      float v8[8];
-#pragma unroll
-      for (int c = 0; c < 8; c++) {
-        const int kk = 8 * k + c;
-        v8[c] = 0.0f;
-#pragma unroll
-        for (int i = 0; i < N_FEAT; i++)
-          if (i == kk) v8[c] = fe[i];
-      }
-      *reinterpret_cast<uint4 *>(X_.a1 + umma::kmajor_off(b, 8 * k, 4)) = pack8<BF16>(v8);
-      if (k == 0) X_.flags[b] = (valid ? 1u : 0u) | (ok ? 2u : 0u);
-    }
-    umma::fence_proxy_async();
-    __syncthreads();
     if (li >= K1_NB) return;
-    // warps 0-1: one row (block) per thread
+    // warps 0-1: one row (block) per thread through the three tensor-core layers
     constexpr int B1 = 16 * N_FEAT, B2 = B1 + 16 + 16 * 16, B3 = B2 + 16 + N_OUT * 16;
     constexpr uint32_t ID = umma::idesc_f16(BF16 ? 1 : 0, 128, 16);
     float row[16], d[16], out[N_OUT];
@@ -544,7 +572,7 @@ HD_INL void tile_mid1(const HushFrame &f, int tileX, int tileY, float4 *sA, floa
   for (int i = li; i < SW * SH; i += HT_W * HT_H) {
     const int q = clampi(by - AP + i / SW, 0, f.H2 - 1) * f.W2 + clampi(bx - AP + i % SW, 0, f.W2 - 1);
     sA[i] = ldh(f.Ah, q);
-    sG[i] = gh_decode(ldh(f.Gh, q));
+    sG[i] = __ldg(f.Gd + q);
   }
   __syncthreads();
   const int X = bx + li % HT_W, Y = by + li / HT_W;
@@ -564,7 +592,7 @@ HD_INL void tile_mid(const HushFrame &f, int tileX, int tileY, const uint2 *src,
   for (int i = li; i < SW * SH; i += HT_W * HT_H) {
     const int q = clampi(by - AP + i / SW, 0, f.H2 - 1) * f.W2 + clampi(bx - AP + i % SW, 0, f.W2 - 1);
     sA[i] = ldh(src, q);
-    sG[i] = gh_decode(ldh(f.Gh, q));
+    sG[i] = __ldg(f.Gd + q);
   }
   __syncthreads();
   const int X = bx + li % HT_W, Y = by + li / HT_W;
@@ -584,16 +612,15 @@ HD_INL void down_h(const HushFrame &f, int Qx, int Qy, float4 &c, float4 &g) {
   for (int j = 0; j < 4; j++) {
     const int hx = Qx * 2 + (j & 1), hy = Qy * 2 + (j >> 1);
     if (hx >= f.W2 || hy >= f.H2) continue;
-    const float4 gq = ldh(f.Gh, hy * f.W2 + hx);
-    if (gq.w <= 0.0f) continue;
+    const float w = ldh(f.Gh, hy * f.W2 + hx).w;  // pixel count of the block
+    if (w <= 0.0f) continue;
     const float4 a = ldh(f.Ah, hy * f.W2 + hx);
-    const float w = gq.w;
+    const float4 n = __ldg(f.Gd + hy * f.W2 + hx);
     N += w;
     cx += w * a.x; cy += w * a.y; cz += w * a.z;
     vr += w * a.w;
-    const float4 n = oct_dec(gq.x, gq.y);
     nx += w * n.x; ny += w * n.y; nz += w * n.z;
-    z += w * gq.z;
+    z += w * n.w;
   }
   if (N == 0.0f) {
     c = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -617,8 +644,11 @@ HD_INL void tile_coarse1(const HushFrame &f, int tileX, int tileY, float4 *sA, f
     down_h(f, qx, qy, c, g);
     sA[i] = c;
     sG[i] = gh_decode(g);
-    if (lqx == qx && lqy == qy && lqx >= bx && lqy >= by && lqx < bx + HT_W && lqy < by + HT_H)
+    if (lqx == qx && lqy == qy && lqx >= bx && lqy >= by && lqx < bx + HT_W && lqy < by + HT_H) {
       sth(f.CG, qy * f.W4 + qx, g);
+      // coarse2 and FINE_FINAL read the guide back from its rgba16float texture
+      f.CGd[qy * f.W4 + qx] = gh_decode(quant4(g));
+    }
   }
   __syncthreads();
   const int X = bx + li % HT_W, Y = by + li / HT_W;
@@ -635,7 +665,7 @@ HD_INL void tile_coarse2(const HushFrame &f, int tileX, int tileY, float4 *sA, f
   for (int i = li; i < SW * SH; i += HT_W * HT_H) {
     const int q = clampi(by - AP + i / SW, 0, f.H4 - 1) * f.W4 + clampi(bx - AP + i % SW, 0, f.W4 - 1);
     sA[i] = ldh(f.C1, q);
-    sG[i] = gh_decode(ldh(f.CG, q));
+    sG[i] = __ldg(f.CGd + q);
   }
   __syncthreads();
   const int X = bx + li % HT_W, Y = by + li / HT_W;
@@ -667,7 +697,7 @@ __global__ void __launch_bounds__(HT_W *HT_H) k_half_stage(const __grid_constant
 // ------------------------------------------------------------------------------------------------ stage 4 / 5
 constexpr int FT_W = 32, FT_H = 8;
 
-__global__ void __launch_bounds__(FT_W *FT_H) k_fine_final_fused(const __grid_constant__ HushFrame f) {
+__global__ void __launch_bounds__(FT_W *FT_H, 3) k_fine_final_fused(const __grid_constant__ HushFrame f) {
   constexpr int AP = 1, SW = FT_W + 2, SH = FT_H + 2;
   __shared__ float4 sA[SW * SH], sG[SW * SH];
   const int li = threadIdx.x;
@@ -695,24 +725,40 @@ __global__ void __launch_bounds__(FT_W *FT_H) k_fine_final_fused(const __grid_co
   const int hp = (py >> 1) * f.W2 + (px >> 1);
   const float4 A1 = filt<1, 1, true, SW>(sA, sG, lx, ly, px, py, f.W, f.H, ldh(f.par1, hp).x, ldh(f.par2, hp).x);
   sth(f.hist, o, A1);
-  // recombination (hush.js:580-620) with the half-res block means / guide from Ah / Gh
+  // recombination (hush.js:580-620) with the half-res block means (Ah) and decoded guides (Gd, CGd); the loads of all
+  // eight footprint texels are issued before any weight is formed
   const float fx = qf16(A1.x), fy = qf16(A1.y), fz = qf16(A1.z);
   const float z = gp.w;
-  const float4 pr = ldh(f.par0, hp);
   const int hsx = (f.W + 1) / 2, hsy = (f.H + 1) / 2;
   const float hposx = ((float)px + 0.5f) / 2.0f - 0.5f, hposy = ((float)py + 0.5f) / 2.0f - 0.5f;
   const float hbx = floorf(hposx), hby = floorf(hposy);
-  float uBx = 0.f, uBy = 0.f, uBz = 0.f, uAx = 0.f, uAy = 0.f, uAz = 0.f, swh = 0.f;
+  const int qsx = (f.W + 3) / 4, qsy = (f.H + 3) / 4;
+  const float cposx = ((float)px + 0.5f) / 4.0f - 0.5f, cposy = ((float)py + 0.5f) / 4.0f - 0.5f;
+  const float cbx = floorf(cposx), cby = floorf(cposy);
+  float4 gh[4], cg[4];
+  uint2 ah[4], bm[4], cc[4];
+  bool inh[4], inq[4];
 #pragma unroll
   for (int j = 0; j < 4; j++) {
     const int qx = (int)hbx + (j & 1), qy = (int)hby + (j >> 1);
-    if (qx < 0 || qy < 0 || qx >= hsx || qy >= hsy) continue;
-    const int q = qy * f.W2 + qx;
-    const float4 g = ldh(f.Gh, q);
-    if (g.z < 0.0f) continue;
-    const float w = jbw(hposx - hbx, hposy - hby, j, oct_dec(g.x, g.y), g.z, gp, z);
-    const float4 a = ldh(f.Ah, q);
-    const float4 m = ldh(f.Bh0, q);
+    inh[j] = qx >= 0 && qy >= 0 && qx < hsx && qy < hsy;
+    const int q = clampi(qy, 0, f.H2 - 1) * f.W2 + clampi(qx, 0, f.W2 - 1);
+    gh[j] = __ldg(f.Gd + q);
+    ah[j] = __ldg(f.Ah + q);
+    bm[j] = __ldg(f.Bh0 + q);
+    const int rx = (int)cbx + (j & 1), ry = (int)cby + (j >> 1);
+    inq[j] = rx >= 0 && ry >= 0 && rx < qsx && ry < qsy;
+    const int r = clampi(ry, 0, f.H4 - 1) * f.W4 + clampi(rx, 0, f.W4 - 1);
+    cg[j] = __ldg(f.CGd + r);
+    cc[j] = __ldg(f.C0 + r);
+  }
+  const float4 pr = ldh(f.par0, hp);
+  float uBx = 0.f, uBy = 0.f, uBz = 0.f, uAx = 0.f, uAy = 0.f, uAz = 0.f, swh = 0.f;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    if (!inh[j] || gh[j].w < 0.0f) continue;
+    const float w = jbw(hposx - hbx, hposy - hby, j, gh[j], gh[j].w, gp, z);
+    const float4 a = h4_to_f4(ah[j]), m = h4_to_f4(bm[j]);
     swh += w;
     uBx += w * m.x; uBy += w * m.y; uBz += w * m.z;
     uAx += w * a.x; uAy += w * a.y; uAz += w * a.z;
@@ -723,19 +769,12 @@ __global__ void __launch_bounds__(FT_W *FT_H) k_fine_final_fused(const __grid_co
     iy = uBy / swh + pr.w * (fy - uAy / swh);
     iz = uBz / swh + pr.w * (fz - uAz / swh);
   }
-  const int qsx = (f.W + 3) / 4, qsy = (f.H + 3) / 4;
-  const float cposx = ((float)px + 0.5f) / 4.0f - 0.5f, cposy = ((float)py + 0.5f) / 4.0f - 0.5f;
-  const float cbx = floorf(cposx), cby = floorf(cposy);
   float uCx = 0.f, uCy = 0.f, uCz = 0.f, swq = 0.f;
 #pragma unroll
   for (int j = 0; j < 4; j++) {
-    const int qx = (int)cbx + (j & 1), qy = (int)cby + (j >> 1);
-    if (qx < 0 || qy < 0 || qx >= qsx || qy >= qsy) continue;
-    const int q = qy * f.W4 + qx;
-    const float4 cg = ldh(f.CG, q);
-    if (cg.z < 0.0f) continue;
-    const float w = jbw(cposx - cbx, cposy - cby, j, oct_dec(cg.x, cg.y), cg.z, gp, z);
-    const float4 c = ldh(f.C0, q);
+    if (!inq[j] || cg[j].w < 0.0f) continue;
+    const float w = jbw(cposx - cbx, cposy - cby, j, cg[j], cg[j].w, gp, z);
+    const float4 c = h4_to_f4(cc[j]);
     swq += w;
     uCx += w * c.x; uCy += w * c.y; uCz += w * c.z;
   }

@@ -269,3 +269,35 @@ def test_device_generator_matches_host():
         for k in scene.NAMES:
             a, b = d[k].float().cpu().numpy(), h[k].astype(np.float32)
             assert np.mean(np.abs(a - b) <= 1e-2 * np.maximum(np.abs(b), 1)) > 0.99, k
+
+
+@pytest.mark.parametrize("mlp,rel,frac", [("f16", 2e-3, 1e-2), ("bf16", 5e-2, 1e-2)])
+def test_tensor_core_mlp_forms(mlp, rel, frac):
+    """The tcgen05 MLP forms against the FP32 oracle: f16 operands keep the features exact (only the hidden
+    activations round), so they stay within the FP32 bound on nearly every value; bf16 operands round the features
+    to 8 bits and move the parameters by ~0.3 % on average, so they are held to a 5e-2 bound."""
+    cfg = scene.CONFIG_360P
+    frames = [scene.frame_host(cfg, i) for i in range(4)]
+    o = oracle.OracleHush(cfg.width, cfg.height, builtin_weights())
+    g = Hush(0, {"width": cfg.width, "height": cfg.height, "mlp": mlp})
+    for i, f in enumerate(frames):
+        ref = o.denoise(f).astype(np.float32)
+        got = to_f32(g.denoise(_dev(f)))
+        fr, worst, _ = mismatch(got, ref, rel=rel)
+        assert fr <= frac, (mlp, i, fr, worst)
+
+
+def test_tensor_core_parameters_match_fp32_parameters():
+    cfg = scene.SceneConfig(256, 144, 3, n_moving=2, seed=41)
+    frames = [_dev(scene.frame_host(cfg, i)) for i in range(cfg.frames)]
+    a = Hush(0, {"width": cfg.width, "height": cfg.height, "mlp": "fp32"})
+    b = Hush(0, {"width": cfg.width, "height": cfg.height, "mlp": "f16"})
+    for f in frames:
+        a.denoise(f)
+        b.denoise(f)
+    torch.cuda.synchronize()
+    c = (a.frame - 1) & 1
+    for name in (f"PAR0_{c}", "PAR1", "PAR2"):
+        pa, pb = _download(a, name), _download(b, name)
+        rel = np.abs(pb - pa) / (np.abs(pa) + 1e-3)
+        assert rel.mean() < 1e-3 and rel.max() < 5e-2, (name, rel.mean(), rel.max())
