@@ -79,6 +79,20 @@ _SIGS = {
     "hush_end_frame": (C.c_int, [_P]),
     "hush_buffer": (C.c_int, [_P, C.c_int, C.POINTER(_P), C.POINTER(C.c_int), C.POINTER(C.c_int),
                               C.POINTER(C.c_int)]),
+    "hush_trainer_create": (C.c_int, [_P, C.c_void_p, C.POINTER(_P)]),
+    "hush_trainer_destroy": (None, [_P]),
+    "hush_trainer_frame": (C.c_int, [_P, C.POINTER(HushInputs), C.c_void_p, C.c_void_p, C.c_float, C.c_int, _P,
+                                     C.POINTER(C.c_double)]),
+    "hush_trainer_end_frame": (C.c_int, [_P]),
+    "hush_trainer_reset": (C.c_int, [_P]),
+    "hush_trainer_zero_grad": (C.c_int, [_P, _P]),
+    "hush_trainer_grad": (C.c_int, [_P, C.c_void_p]),
+    "hush_trainer_theta": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
+    "hush_trainer_par": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
+    "hush_trainer_output": (C.c_int, [_P, C.c_void_p]),
+    "hush_trainer_step": (C.c_int, [_P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, _P,
+                                    C.POINTER(C.c_double)]),
+    "hush_trainer_export": (C.c_int, [_P, C.c_void_p]),
     "svgf_options_default": (SvgfOptions, []),
     "svgf_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(SvgfOptions), C.c_int, C.POINTER(_P)]),
     "svgf_destroy": (None, [_P]),

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "hush.h"
+#include "hush_instance.h"
 #include "hush_internal.h"
 #include "weights_builtin.inc"  // generated at build time from hush_b200/data/hush-weights.bin
 
@@ -22,50 +23,14 @@ static float half_to_float(uint16_t h) {  // halfToFloat (hush.js:706-711)
   return (float)(s * (1.0 + m / 1024.0) * std::ldexp(1.0, e - 15));
 }
 
-struct hush_s {
-  int dev = 0;
-  int W = 0, H = 0, W2 = 0, H2 = 0, W4 = 0, H4 = 0;
-  int frame = 0;
-  bool reset = true;
-  float exposure = 1.0f;
-  int hidden = 16;
-  int mlp_mode = HUSH_MLP_FP32;
-  int schedule = HUSH_SCHED_FUSED;
-  std::vector<float> wf;
-  MlpW16 w16;
-  float *w_dev = nullptr;
-  void *tc_blob_dev = nullptr;
-  // state images (hush.js:783-793) plus the fused path's half-res planes
-  char *pool = nullptr;
-  size_t pool_bytes = 0;
-  uint2 *A0 = nullptr, *X = nullptr, *Bh[2] = {}, *mom[2] = {}, *key[2] = {}, *hist[2] = {}, *taa[2] = {},
-        *par0[2] = {}, *par1 = nullptr, *par2 = nullptr, *C[2] = {}, *CG = nullptr, *Ah = nullptr, *Gh = nullptr;
-  float4 *Gd = nullptr, *CGd = nullptr;
-  uint4 *F[4] = {};
-  unsigned int *err = nullptr;
-  const void *last_out = nullptr;
-  std::string last_error;
-  // timer
-  int timer_mode = 0;
-  int n_events = 0;
-  cudaEvent_t ev[17] = {};
-  const char *ev_label[16] = {};
-  // graph replay
-  bool use_graph = false;
-  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
-  const void *gkey[2][5] = {};
-  int gkey_reset[2] = {-1, -1};
-  float gkey_exposure[2] = {0, 0};
-  cudaStream_t gstream[2] = {nullptr, nullptr};
-};
 
-static int fail(hush_t *h, int code, const std::string &msg) {
+int hush_fail(hush_t *h, int code, const std::string &msg) {
   if (h) h->last_error = msg;
   g_err = msg;
   return code;
 }
-static int cuda_fail(hush_t *h, cudaError_t e, const char *what) {
-  return fail(h, HUSH_ERR_CUDA, std::string("Hush: ") + what + ": " + cudaGetErrorString(e));
+int hush_cuda_fail(hush_t *h, cudaError_t e, const char *what) {
+  return hush_fail(h, HUSH_ERR_CUDA, std::string("Hush: ") + what + ": " + cudaGetErrorString(e));
 }
 
 extern "C" int hush_hidden_of(long n) {
@@ -120,9 +85,9 @@ static int alloc_state(hush_t *h, int width, int height) {
   size_t total = al(full) * 10 + al(half) * 8 + al(half16) * 5 + al(quarter) * 3 + al(quarter * 2) + 256;
   char *pool = nullptr;
   cudaError_t e = cudaMalloc(&pool, total);
-  if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc of the state images");
+  if (e != cudaSuccess) return hush_cuda_fail(h, e, "cudaMalloc of the state images");
   e = cudaMemset(pool, 0, total);
-  if (e != cudaSuccess) { cudaFree(pool); return cuda_fail(h, e, "cudaMemset"); }
+  if (e != cudaSuccess) { cudaFree(pool); return hush_cuda_fail(h, e, "cudaMemset"); }
   free_state(h);
   h->pool = pool;
   h->pool_bytes = total;
@@ -149,14 +114,14 @@ static int alloc_state(hush_t *h, int width, int height) {
 
 static int set_weights(hush_t *h, const uint16_t *weights, size_t n) {
   const int hd = hush_hidden_of((long)n);
-  if (!hd) return fail(h, HUSH_ERR_ARG, "hush weights: " + std::to_string(n) + " f16 values fit no MLP size");
+  if (!hd) return hush_fail(h, HUSH_ERR_ARG, "hush weights: " + std::to_string(n) + " f16 values fit no MLP size");
   std::vector<float> wf(n);
   for (size_t i = 0; i < n; i++) wf[i] = half_to_float(weights[i]);
   float *wd = nullptr;
   cudaError_t e = cudaMalloc(&wd, n * sizeof(float));
-  if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc of the weights");
+  if (e != cudaSuccess) return hush_cuda_fail(h, e, "cudaMalloc of the weights");
   e = cudaMemcpy(wd, wf.data(), n * sizeof(float), cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) { cudaFree(wd); return cuda_fail(h, e, "cudaMemcpy of the weights"); }
+  if (e != cudaSuccess) { cudaFree(wd); return hush_cuda_fail(h, e, "cudaMemcpy of the weights"); }
   if (h->w_dev) cudaFree(h->w_dev);
   h->w_dev = wd;
   h->wf = wf;
@@ -171,47 +136,47 @@ static int set_weights(hush_t *h, const uint16_t *weights, size_t n) {
     mlp_fp32_build_blob(wf.data(), reinterpret_cast<float *>(blob + 2 * MLP_TC_BLOB_BYTES));
     if (!h->tc_blob_dev) {
       e = cudaMalloc(&h->tc_blob_dev, sizeof(blob));
-      if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc of the tensor-core weights");
+      if (e != cudaSuccess) return hush_cuda_fail(h, e, "cudaMalloc of the tensor-core weights");
     }
     e = cudaMemcpy(h->tc_blob_dev, blob, sizeof(blob), cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) return cuda_fail(h, e, "cudaMemcpy of the tensor-core weights");
+    if (e != cudaSuccess) return hush_cuda_fail(h, e, "cudaMemcpy of the tensor-core weights");
   }
   drop_graphs(h);  // graphs bake the weights in as kernel parameters
   return HUSH_OK;
 }
 
 extern "C" int hush_create(const hush_desc *desc, hush_t **out) {
-  if (!out) return fail(nullptr, HUSH_ERR_ARG, "hush_create: out is NULL");
+  if (!out) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_create: out is NULL");
   *out = nullptr;
-  if (!desc) return fail(nullptr, HUSH_ERR_ARG, "hush_create: desc is NULL");
+  if (!desc) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_create: desc is NULL");
   int dev = desc->device;
   cudaError_t e;
   if (dev < 0) {
     e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDevice");
+    if (e != cudaSuccess) return hush_cuda_fail(nullptr, e, "cudaGetDevice");
   }
   cudaDeviceProp prop;
   e = cudaGetDeviceProperties(&prop, dev);
-  if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDeviceProperties");
+  if (e != cudaSuccess) return hush_cuda_fail(nullptr, e, "cudaGetDeviceProperties");
   int need_major, need_minor;
   size_t need_smem;
   hush_required_limits(&need_major, &need_minor, &need_smem);
   if (prop.major != need_major || prop.sharedMemPerBlockOptin < need_smem) {
-    return fail(nullptr, HUSH_ERR_DEVICE,
+    return hush_fail(nullptr, HUSH_ERR_DEVICE,
                 "Hush needs the device limit computeCapability == " + std::to_string(need_major) + "." +
                     std::to_string(need_minor) + " (sm_100a) and sharedMemPerBlockOptin >= " +
                     std::to_string(need_smem) + " (this device: " + std::to_string(prop.major) + "." +
                     std::to_string(prop.minor) + ", " + std::to_string(prop.sharedMemPerBlockOptin) + ")");
   }
   if (!(desc->width > 0 && desc->height > 0))
-    return fail(nullptr, HUSH_ERR_ARG,
+    return hush_fail(nullptr, HUSH_ERR_ARG,
                 "Hush: bad size " + std::to_string(desc->width) + "x" + std::to_string(desc->height));
   if (desc->mlp_mode < HUSH_MLP_FP32 || desc->mlp_mode > HUSH_MLP_F16)
-    return fail(nullptr, HUSH_ERR_ARG, "Hush: unknown mlp_mode " + std::to_string(desc->mlp_mode));
+    return hush_fail(nullptr, HUSH_ERR_ARG, "Hush: unknown mlp_mode " + std::to_string(desc->mlp_mode));
   if (desc->schedule != HUSH_SCHED_FUSED && desc->schedule != HUSH_SCHED_PASSES)
-    return fail(nullptr, HUSH_ERR_ARG, "Hush: unknown schedule " + std::to_string(desc->schedule));
+    return hush_fail(nullptr, HUSH_ERR_ARG, "Hush: unknown schedule " + std::to_string(desc->schedule));
   e = cudaSetDevice(dev);
-  if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaSetDevice");
+  if (e != cudaSuccess) return hush_cuda_fail(nullptr, e, "cudaSetDevice");
   hush_t *h = new hush_t();
   h->dev = dev;
   h->exposure = desc->exposure;
@@ -225,7 +190,7 @@ extern "C" int hush_create(const hush_desc *desc, hush_t **out) {
   if (rc == HUSH_OK) {
     for (int i = 0; i < 17 && rc == HUSH_OK; i++) {
       e = cudaEventCreate(&h->ev[i]);
-      if (e != cudaSuccess) rc = cuda_fail(h, e, "cudaEventCreate");
+      if (e != cudaSuccess) rc = hush_cuda_fail(h, e, "cudaEventCreate");
     }
   }
   if (rc != HUSH_OK) {
@@ -249,41 +214,41 @@ extern "C" void hush_destroy(hush_t *h) {
 }
 
 extern "C" int hush_resize(hush_t *h, int width, int height) {
-  if (!h) return fail(nullptr, HUSH_ERR_ARG, "hush_resize: NULL instance");
+  if (!h) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_resize: NULL instance");
   if (!(width > 0 && height > 0))
-    return fail(h, HUSH_ERR_ARG, "Hush: bad size " + std::to_string(width) + "x" + std::to_string(height));
+    return hush_fail(h, HUSH_ERR_ARG, "Hush: bad size " + std::to_string(width) + "x" + std::to_string(height));
   if (width == h->W && height == h->H) return HUSH_OK;
   cudaSetDevice(h->dev);
   return alloc_state(h, width, height);
 }
 
 extern "C" int hush_reset(hush_t *h) {
-  if (!h) return fail(nullptr, HUSH_ERR_ARG, "hush_reset: NULL instance");
+  if (!h) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_reset: NULL instance");
   h->reset = true;
   return HUSH_OK;
 }
 extern "C" int hush_set_exposure(hush_t *h, float e) {
-  if (!h) return fail(nullptr, HUSH_ERR_ARG, "hush_set_exposure: NULL instance");
+  if (!h) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_set_exposure: NULL instance");
   h->exposure = e;
   return HUSH_OK;
 }
 extern "C" float hush_get_exposure(const hush_t *h) { return h ? h->exposure : 0.0f; }
 extern "C" int hush_set_weights(hush_t *h, const uint16_t *w, size_t n) {
-  if (!h) return fail(nullptr, HUSH_ERR_ARG, "hush_set_weights: NULL instance");
-  if (!w) return fail(h, HUSH_ERR_ARG, "hush weights: NULL blob");
+  if (!h) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_set_weights: NULL instance");
+  if (!w) return hush_fail(h, HUSH_ERR_ARG, "hush weights: NULL blob");
   cudaSetDevice(h->dev);
   return set_weights(h, w, n);
 }
 extern "C" int hush_set_mlp_mode(hush_t *h, int mode) {
-  if (!h) return fail(nullptr, HUSH_ERR_ARG, "hush_set_mlp_mode: NULL instance");
-  if (mode < HUSH_MLP_FP32 || mode > HUSH_MLP_F16) return fail(h, HUSH_ERR_ARG, "Hush: unknown mlp_mode");
+  if (!h) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_set_mlp_mode: NULL instance");
+  if (mode < HUSH_MLP_FP32 || mode > HUSH_MLP_F16) return hush_fail(h, HUSH_ERR_ARG, "Hush: unknown mlp_mode");
   h->mlp_mode = mode;
   drop_graphs(h);
   return HUSH_OK;
 }
 extern "C" int hush_set_schedule(hush_t *h, int s) {
-  if (!h) return fail(nullptr, HUSH_ERR_ARG, "hush_set_schedule: NULL instance");
-  if (s != HUSH_SCHED_FUSED && s != HUSH_SCHED_PASSES) return fail(h, HUSH_ERR_ARG, "Hush: unknown schedule");
+  if (!h) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_set_schedule: NULL instance");
+  if (s != HUSH_SCHED_FUSED && s != HUSH_SCHED_PASSES) return hush_fail(h, HUSH_ERR_ARG, "Hush: unknown schedule");
   h->schedule = s;
   drop_graphs(h);
   return HUSH_OK;
@@ -302,28 +267,28 @@ extern "C" const char *hush_global_error(void) { return g_err.c_str(); }
 static const char *INPUT_NAMES[5] = {"radiance", "normalDepth", "motion", "material", "emission"};
 
 // Input checks of denoise() (hush.js:814-820).
-static int check_inputs(hush_t *h, const hush_inputs *in) {
-  if (!in) return fail(h, HUSH_ERR_ARG, "Hush.denoise: missing inputs");
+int hush_check_inputs(hush_t *h, const hush_inputs *in) {
+  if (!in) return hush_fail(h, HUSH_ERR_ARG, "Hush.denoise: missing inputs");
   const void *p[5] = {in->radiance, in->normal_depth, in->motion, in->material, in->emission};
   for (int k = 0; k < 5; k++) {
-    if (!p[k]) return fail(h, HUSH_ERR_ARG, std::string("Hush.denoise: missing input '") + INPUT_NAMES[k] + "'");
+    if (!p[k]) return hush_fail(h, HUSH_ERR_ARG, std::string("Hush.denoise: missing input '") + INPUT_NAMES[k] + "'");
     const int w = in->width[k], hh = in->height[k];
     if ((w || hh) && (w != h->W || hh != h->H)) {
-      return fail(h, HUSH_ERR_ARG,
+      return hush_fail(h, HUSH_ERR_ARG,
                   std::string("Hush.denoise: '") + INPUT_NAMES[k] + "' is " + std::to_string(w) + "x" +
                       std::to_string(hh) + ", the denoiser " + std::to_string(h->W) + "x" + std::to_string(h->H) +
                       " (call resize)");
     }
     const size_t pitch = in->pitch[k];
     if (pitch && (pitch % 8 || pitch < (size_t)h->W * 8))
-      return fail(h, HUSH_ERR_ARG, std::string("Hush.denoise: bad pitch for '") + INPUT_NAMES[k] + "'");
+      return hush_fail(h, HUSH_ERR_ARG, std::string("Hush.denoise: bad pitch for '") + INPUT_NAMES[k] + "'");
     if ((uintptr_t)p[k] % 8)
-      return fail(h, HUSH_ERR_ARG, std::string("Hush.denoise: '") + INPUT_NAMES[k] + "' is not 8-byte aligned");
+      return hush_fail(h, HUSH_ERR_ARG, std::string("Hush.denoise: '") + INPUT_NAMES[k] + "' is not 8-byte aligned");
   }
   return HUSH_OK;
 }
 
-static HushFrame make_frame(hush_t *h, const hush_inputs *in) {
+HushFrame hush_make_frame(hush_t *h, const hush_inputs *in) {
   const int cur = h->frame & 1, prev = cur ^ 1;
   HushFrame f;
   std::memset(&f, 0, sizeof(f));
@@ -383,18 +348,18 @@ static int encode_frame(hush_t *h, const HushFrame &f, cudaStream_t st, bool tim
     cudaEventRecord(h->ev[n], st);
     h->n_events = n + 1;
   }
-  if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
+  if (e != cudaSuccess) return hush_cuda_fail(h, e, "kernel launch");
   return HUSH_OK;
 }
 
 extern "C" int hush_denoise(hush_t *h, const hush_inputs *in, void *stream, const void **out) {
-  if (!h) return fail(nullptr, HUSH_ERR_ARG, "hush_denoise: NULL instance");
-  int rc = check_inputs(h, in);
+  if (!h) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_denoise: NULL instance");
+  int rc = hush_check_inputs(h, in);
   if (rc != HUSH_OK) return rc;
   cudaSetDevice(h->dev);
   cudaStream_t st = (cudaStream_t)stream;
   const int cur = h->frame & 1;
-  const HushFrame f = make_frame(h, in);
+  const HushFrame f = hush_make_frame(h, in);
   const bool timed = h->timer_mode != 0;
   if (h->use_graph && !timed) {
     // one graph per ping-pong parity, keyed by the input pointers, the reset flag and the exposure
@@ -406,24 +371,24 @@ extern "C" int hush_denoise(hush_t *h, const hush_inputs *in, void *stream, cons
       h->gexec[cur] = nullptr;
       cudaStream_t cs;
       cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
-      if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamCreate");
+      if (e != cudaSuccess) return hush_cuda_fail(h, e, "cudaStreamCreate");
       e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-      if (e != cudaSuccess) { cudaStreamDestroy(cs); return cuda_fail(h, e, "cudaStreamBeginCapture"); }
+      if (e != cudaSuccess) { cudaStreamDestroy(cs); return hush_cuda_fail(h, e, "cudaStreamBeginCapture"); }
       rc = encode_frame(h, f, cs, false);
       cudaGraph_t g = nullptr;
       e = cudaStreamEndCapture(cs, &g);
       cudaStreamDestroy(cs);
       if (rc != HUSH_OK) { if (g) cudaGraphDestroy(g); return rc; }
-      if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+      if (e != cudaSuccess) return hush_cuda_fail(h, e, "cudaStreamEndCapture");
       e = cudaGraphInstantiate(&h->gexec[cur], g, 0);
       cudaGraphDestroy(g);
-      if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
+      if (e != cudaSuccess) return hush_cuda_fail(h, e, "cudaGraphInstantiate");
       std::memcpy(h->gkey[cur], key, sizeof(key));
       h->gkey_reset[cur] = f.reset;
       h->gkey_exposure[cur] = f.exposure;
     }
     cudaError_t e = cudaGraphLaunch(h->gexec[cur], st);
-    if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphLaunch");
+    if (e != cudaSuccess) return hush_cuda_fail(h, e, "cudaGraphLaunch");
   } else {
     rc = encode_frame(h, f, st, timed);
     if (rc != HUSH_OK) return rc;
@@ -441,8 +406,8 @@ extern "C" const void *hush_output(const hush_t *h) {
 }
 
 extern "C" int hush_timer_enable(hush_t *h, int mode) {
-  if (!h) return fail(nullptr, HUSH_ERR_ARG, "hush_timer_enable: NULL instance");
-  if (mode < 0 || mode > 2) return fail(h, HUSH_ERR_ARG, "hush_timer_enable: mode must be 0, 1 or 2");
+  if (!h) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_timer_enable: NULL instance");
+  if (mode < 0 || mode > 2) return hush_fail(h, HUSH_ERR_ARG, "hush_timer_enable: mode must be 0, 1 or 2");
   h->timer_mode = mode;
   h->n_events = 0;
   return HUSH_OK;
@@ -452,7 +417,7 @@ extern "C" int hush_timer_read(hush_t *h, hush_timing *out, int max) {
   if (!h) return -1;
   if (h->n_events < 2) return 0;
   cudaError_t e = cudaEventSynchronize(h->ev[h->n_events - 1]);
-  if (e != cudaSuccess) { cuda_fail(h, e, "cudaEventSynchronize"); return -1; }
+  if (e != cudaSuccess) { hush_cuda_fail(h, e, "cudaEventSynchronize"); return -1; }
   int k = 0;
   if (h->timer_mode == 2) {
     float ms = 0;
@@ -471,28 +436,28 @@ extern "C" int hush_timer_read(hush_t *h, hush_timing *out, int max) {
 }
 
 extern "C" int hush_set_graph(hush_t *h, int enable) {
-  if (!h) return fail(nullptr, HUSH_ERR_ARG, "hush_set_graph: NULL instance");
+  if (!h) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_set_graph: NULL instance");
   h->use_graph = enable != 0;
   return HUSH_OK;
 }
 
 extern "C" int hush_run_pass(hush_t *h, int pass, const hush_inputs *in, void *stream) {
-  if (!h) return fail(nullptr, HUSH_ERR_ARG, "hush_run_pass: NULL instance");
-  if (pass < 0 || pass >= PASS_COUNT) return fail(h, HUSH_ERR_ARG, "hush_run_pass: bad pass id");
+  if (!h) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_run_pass: NULL instance");
+  if (pass < 0 || pass >= PASS_COUNT) return hush_fail(h, HUSH_ERR_ARG, "hush_run_pass: bad pass id");
   const bool needs_inputs = pass == PASS_TEMPORAL || pass == PASS_FINE_FINAL || pass == PASS_TAA;
   if (needs_inputs) {
-    int rc = check_inputs(h, in);
+    int rc = hush_check_inputs(h, in);
     if (rc != HUSH_OK) return rc;
   }
   cudaSetDevice(h->dev);
-  const HushFrame f = make_frame(h, needs_inputs ? in : nullptr);
+  const HushFrame f = hush_make_frame(h, needs_inputs ? in : nullptr);
   cudaError_t e = launch_pass(pass, f, h->w16, (cudaStream_t)stream);
-  if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
+  if (e != cudaSuccess) return hush_cuda_fail(h, e, "kernel launch");
   return HUSH_OK;
 }
 
 extern "C" int hush_end_frame(hush_t *h) {
-  if (!h) return fail(nullptr, HUSH_ERR_ARG, "hush_end_frame: NULL instance");
+  if (!h) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_end_frame: NULL instance");
   h->last_out = h->taa[h->frame & 1];
   h->reset = false;
   h->frame++;
@@ -500,7 +465,7 @@ extern "C" int hush_end_frame(hush_t *h) {
 }
 
 extern "C" int hush_buffer(hush_t *h, int id, void **dptr, int *width, int *height, int *texel_bytes) {
-  if (!h) return fail(nullptr, HUSH_ERR_ARG, "hush_buffer: NULL instance");
+  if (!h) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_buffer: NULL instance");
   void *p = nullptr;
   int w = h->W, hh = h->H, tb = 8;
   switch (id) {
@@ -525,7 +490,7 @@ extern "C" int hush_buffer(hush_t *h, int id, void **dptr, int *width, int *heig
     case HUSH_BUF_C0: p = h->C[0]; w = h->W4; hh = h->H4; break;
     case HUSH_BUF_C1: p = h->C[1]; w = h->W4; hh = h->H4; break;
     case HUSH_BUF_CG: p = h->CG; w = h->W4; hh = h->H4; break;
-    default: return fail(h, HUSH_ERR_ARG, "hush_buffer: bad buffer id");
+    default: return hush_fail(h, HUSH_ERR_ARG, "hush_buffer: bad buffer id");
   }
   if (dptr) *dptr = p;
   if (width) *width = w;

@@ -1,0 +1,52 @@
+// The Hush instance (the reference's `Hush` object, hush.js:725-875), shared by the C ABI and the trainer.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "hush.h"
+#include "hush_internal.h"
+
+struct hush_s {
+  int dev = 0;
+  int W = 0, H = 0, W2 = 0, H2 = 0, W4 = 0, H4 = 0;
+  int frame = 0;
+  bool reset = true;
+  float exposure = 1.0f;
+  int hidden = 16;
+  int mlp_mode = HUSH_MLP_FP32;
+  int schedule = HUSH_SCHED_FUSED;
+  std::vector<float> wf;
+  hush::MlpW16 w16;
+  float *w_dev = nullptr;
+  void *tc_blob_dev = nullptr;
+  // state images (hush.js:783-793) plus the fused path's half-res planes
+  char *pool = nullptr;
+  size_t pool_bytes = 0;
+  uint2 *A0 = nullptr, *X = nullptr, *Bh[2] = {}, *mom[2] = {}, *key[2] = {}, *hist[2] = {}, *taa[2] = {},
+        *par0[2] = {}, *par1 = nullptr, *par2 = nullptr, *C[2] = {}, *CG = nullptr, *Ah = nullptr, *Gh = nullptr;
+  float4 *Gd = nullptr, *CGd = nullptr;
+  uint4 *F[4] = {};
+  unsigned int *err = nullptr;
+  const void *last_out = nullptr;
+  std::string last_error;
+  // timer
+  int timer_mode = 0;
+  int n_events = 0;
+  cudaEvent_t ev[17] = {};
+  const char *ev_label[16] = {};
+  // graph replay
+  bool use_graph = false;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  const void *gkey[2][5] = {};
+  int gkey_reset[2] = {-1, -1};
+  float gkey_exposure[2] = {0, 0};
+  cudaStream_t gstream[2] = {nullptr, nullptr};
+};
+
+// helpers of hush_api.cu
+hush::HushFrame hush_make_frame(hush_t *h, const hush_inputs *in);
+int hush_check_inputs(hush_t *h, const hush_inputs *in);
+int hush_fail(hush_t *h, int code, const std::string &msg);
+int hush_cuda_fail(hush_t *h, cudaError_t e, const char *what);

@@ -1,0 +1,966 @@
+// Training twin of the Hush frame: hand-written forward / adjoint kernels for on-device training of the parameter MLP.
+//
+// The twin runs the frame after TEMPORAL in FP32 without the f16 storage rounding (so finite differences see a
+// smooth function): the MLP on FP32 master weights (hush.js:683-704 / 357-362), the mid levels mid1-mid3 (hush.js:366,
+// 753-754), the fine level + recombination (hush.js:578-620) and TAA (hush.js:649-676). TEMPORAL and the coarse levels
+// run as the reference passes (their outputs do not depend on the weights within a frame). The loss is the relative L1
+// of the TAA output against the noise-free image plus a temporal-gradient term.
+//
+// Gradients are exact for one frame with the temporal history held fixed (the history buffers are inputs of the
+// frame); over a window the per-frame gradients are summed (truncated backpropagation through time: the alpha / gamma
+// heads, which only act on the next frame's temporal blend, receive no gradient). The backward recomputes every
+// a-trous weight from the level's input instead of storing the weights, accumulates input gradients of the levels with
+// atomics, reduces the weight gradient per CTA in FP32 and across CTAs in FP64, and updates FP32 master weights with
+// Adam.
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "hush.h"
+#include "hush_device.cuh"
+#include "hush_instance.h"
+#include "hush_internal.h"
+
+namespace hush {
+namespace twin {
+
+constexpr int NW = H16_COUNT;  // 812 weights of the h = 16 network
+constexpr int TW = 16, TH = 8;
+constexpr int W1o = 0, B1o = 16 * 20, W2o = B1o + 16, B2o = W2o + 256, W3o = B2o + 16, B3o = W3o + 12 * 16;
+
+struct TwinFrame {
+  HushFrame f;            // instance buffers of the frame (inputs, A0, key, F0..F3, C0, CG, history)
+  const float *theta;     // FP32 master weights
+  float4 *par;            // half: 3 float4 per row (alpha gamma beta kappa | s0..s3 | c0..c3)
+  float4 *B1, *B2, *B3;   // half: mid levels
+  float4 *A1, *X, *out;   // full: fine level, pre-TAA colour, TAA output
+  const float4 *out_prev; // full: previous frame's TAA output (temporal loss term)
+  const float *clean, *clean_prev;  // full: noise-free rgb (f32, dense), previous frame's
+  float4 *gT;             // full: gradient w.r.t. the tone-mapped colour tm(X)
+  float4 *dB1, *dB2, *dB3;  // half: level gradients
+  float4 *dpar;           // half: 3 float4 per row
+  float *partials;        // per-CTA weight-gradient partials (NW floats each)
+  double *loss_partials;  // per-CTA loss partials
+  float lambda_t;         // weight of the temporal term
+  int has_prev;
+  float inv_n;            // 1 / (3 * pixels)
+};
+
+HD_INL float4 f3_guide_tw(const uint4 *F3, int i) {
+  const uint4 t = __ldg(F3 + i);
+  const float2 o = unpack2(t.x), z = unpack2(t.y);
+  float4 g = oct_dec(o.x, o.y);
+  g.w = z.x;
+  return g;
+}
+HD_INL float4 f2_ac_tw(const uint4 *F2, int i) {
+  const uint4 t = __ldg(F2 + i);
+  const float2 a = unpack2(t.z), b = unpack2(t.w);
+  return make_float4(a.x, a.y, b.x, b.y);
+}
+HD_INL void atomic_add4(float4 *p, float4 v) {
+  atomicAdd(&p->x, v.x);
+  atomicAdd(&p->y, v.y);
+  atomicAdd(&p->z, v.z);
+  atomicAdd(&p->w, v.w);
+}
+HD_INL float sgn(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }
+
+// ------------------------------------------------------------------------------------------------ MLP
+HD_INL void mlp_full(const float *th, const float *fe, float *h1, float *h2, float *o) {
+  for (int j = 0; j < 16; j++) {
+    float a = th[B1o + j];
+    for (int i = 0; i < 20; i++) a = a + fe[i] * th[W1o + j * 20 + i];
+    h1[j] = fmaxf(a, 0.0f);
+  }
+  for (int j = 0; j < 16; j++) {
+    float a = th[B2o + j];
+    for (int i = 0; i < 16; i++) a = a + h1[i] * th[W2o + j * 16 + i];
+    h2[j] = fmaxf(a, 0.0f);
+  }
+  for (int j = 0; j < 12; j++) {
+    float a = th[B3o + j];
+    for (int i = 0; i < 16; i++) a = a + h2[i] * th[W3o + j * 16 + i];
+    o[j] = a;
+  }
+}
+
+HD_INL void load_features(const HushFrame &f, int o, float *fe) {
+  const uint4 a = __ldg(f.F0 + o), b = __ldg(f.F1 + o), c = __ldg(f.F2 + o);
+  const uint32_t u[10] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y};
+  for (int i = 0; i < 10; i++) {
+    const float2 t = unpack2(u[i]);
+    fe[2 * i] = t.x;
+    fe[2 * i + 1] = t.y;
+  }
+}
+
+// MLP forward and heads per half-res pixel; also writes the instance's f16 par0..2 (the next frame's history).
+__global__ void k_mlp_fwd(const TwinFrame T) {
+  __shared__ float th[NW];
+  for (int i = threadIdx.x; i < NW; i += blockDim.x) th[i] = T.theta[i];
+  __syncthreads();
+  const HushFrame &f = T.f;
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= f.W2 * f.H2) return;
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (f3_guide_tw(f.F3, o).w < 0.0f) {
+    T.par[3 * o] = z4; T.par[3 * o + 1] = z4; T.par[3 * o + 2] = z4;
+    sth(f.par0, o, z4); sth(f.par1, o, z4); sth(f.par2, o, z4);
+    return;
+  }
+  float fe[20], h1[16], h2[16], out[12];
+  load_features(f, o, fe);
+  mlp_full(th, fe, h1, h2, out);
+  float4 p0, p1, p2;
+  mlp_heads(out, p0, p1, p2);
+  T.par[3 * o] = p0; T.par[3 * o + 1] = p1; T.par[3 * o + 2] = p2;
+  sth(f.par0, o, p0); sth(f.par1, o, p1); sth(f.par2, o, p2);
+}
+
+// ------------------------------------------------------------------------------------------------ a-trous (R = 1)
+// Forward of atrousFn with R = 1 over float4 tiles (see hush_device.cuh filt); the weight gradient helper below
+// recomputes exactly these weights.
+template <int STEP, bool PREF, int SW>
+struct Filt1 {
+  float4 gp, center;
+  float gv, lc, den, sl, cw, W;
+  float wq[8], lq[8];
+  bool ok[8];
+  float3 S;
+  float V;
+  HD_INL void run(const float4 *sA, const float4 *sG, int ti, int qx, int qy, int w, int h, float s, float c) {
+    gp = sG[ti];
+    center = sA[ti];
+    if (PREF) {
+      gv = 0.0625f * (sA[ti - SW - 1].w + sA[ti - SW + 1].w + sA[ti + SW - 1].w + sA[ti + SW + 1].w) +
+           0.125f * (sA[ti - SW].w + sA[ti - 1].w + sA[ti + 1].w + sA[ti + SW].w) + 0.25f * center.w;
+    } else {
+      gv = center.w;
+    }
+    lc = lum(center);
+    den = sqrtf(fmaxf(gv, 1e-12f)) + 1e-6f;
+    sl = s / den;
+    const float zl = sG[ti - 1].w, zr = sG[ti + 1].w, zu = sG[ti - SW].w, zd = sG[ti + SW].w;
+    const float gx = fminf(zr > 0.0f ? fabsf(zr - gp.w) : 1e9f, zl > 0.0f ? fabsf(zl - gp.w) : 1e9f);
+    const float gy = fminf(zd > 0.0f ? fabsf(zd - gp.w) : 1e9f, zu > 0.0f ? fabsf(zu - gp.w) : 1e9f);
+    const float zg = fminf(fmaxf(gx, gy), gp.w);
+    const float iz1 = 1.0f / (zg * (1.0f * STEP) + 1e-3f), iz2 = 1.0f / (zg * (1.41421356237309515f * STEP) + 1e-3f);
+    cw = 0.25f * c;
+    W = cw;
+    S = make_float3(center.x * cw, center.y * cw, center.z * cw);
+    V = center.w * cw * cw;
+    int t = 0;
+#pragma unroll
+    for (int dy = -1; dy <= 1; dy++) {
+#pragma unroll
+      for (int dx = -1; dx <= 1; dx++) {
+        if (dx == 0 && dy == 0) continue;
+        const float hh = (dx == 0 ? 0.5f : 0.25f) * (dy == 0 ? 0.5f : 0.25f);
+        const int off = dy * STEP * SW + dx * STEP;
+        const float4 gq = sG[ti + off];
+        const int tx = qx + dx * STEP, ty = qy + dy * STEP;
+        ok[t] = tx >= 0 && ty >= 0 && tx < w && ty < h && gq.w >= 0.0f;
+        wq[t] = 0.0f;
+        lq[t] = 0.0f;
+        if (ok[t]) {
+          const float4 cq = sA[ti + off];
+          lq[t] = lum(cq);
+          const float iz = (dx == 0 || dy == 0) ? iz1 : iz2;
+          wq[t] = hh * pow128(fmaxf(dot3(gq, gp), 0.0f)) * expf(-fabsf(gq.w - gp.w) * iz - sl * fabsf(lq[t] - lc));
+          W += wq[t];
+          S.x += wq[t] * cq.x; S.y += wq[t] * cq.y; S.z += wq[t] * cq.z;
+          V += wq[t] * wq[t] * cq.w;
+        }
+        t++;
+      }
+    }
+  }
+  HD_INL float4 out() const { return make_float4(S.x / W, S.y / W, S.z / W, V / (W * W)); }
+
+  // Adjoint for output gradient (g_rgb, g_v): parameter gradients ds, dc and, if dIn != nullptr, the input-level
+  // gradient scattered to the taps (image index of the tile centre pix, tap offsets STEP on a row pitch of `pitch`).
+  HD_INL void adjoint(const float4 *sA, int ti, float3 g, float g_v, float s, float &ds, float &dc, float4 *dIn,
+                      int pix, int pitch) const {
+    const float o_r = S.x / W, o_g = S.y / W, o_b = S.z / W, ov = V / (W * W);
+    const float3 gS = make_float3(g.x / W, g.y / W, g.z / W);
+    const float gV = g_v / (W * W);
+    const float gW = -(g.x * o_r + g.y * o_g + g.z * o_b) / W - 2.0f * g_v * ov / W;
+    const float dcw = gS.x * center.x + gS.y * center.y + gS.z * center.z + gV * 2.0f * cw * center.w + gW;
+    dc = dcw * 0.25f;
+    float dsl = 0.0f, dlp = 0.0f;
+    int t = 0;
+#pragma unroll
+    for (int dy = -1; dy <= 1; dy++) {
+#pragma unroll
+      for (int dx = -1; dx <= 1; dx++) {
+        if (dx == 0 && dy == 0) continue;
+        if (ok[t]) {
+          const float4 cq = sA[ti + dy * STEP * SW + dx * STEP];
+          const float dw = gS.x * cq.x + gS.y * cq.y + gS.z * cq.z + gV * 2.0f * wq[t] * cq.w + gW;
+          const float de = dw * wq[t];
+          const float sg = sgn(lq[t] - lc);
+          dsl += de * (-fabsf(lq[t] - lc));
+          dlp += de * sl * sg;
+          if (dIn) {
+            const float dlq = -de * sl * sg;
+            atomic_add4(dIn + pix + dy * STEP * pitch + dx * STEP,
+                        make_float4(gS.x * wq[t] + dlq * 0.2126f, gS.y * wq[t] + dlq * 0.7152f,
+                                    gS.z * wq[t] + dlq * 0.0722f, gV * wq[t] * wq[t]));
+          }
+        }
+        t++;
+      }
+    }
+    ds = dsl / den;
+    if (dIn) {
+      const float dgv = gv > 1e-12f ? dsl * (-s / (den * den)) * (0.5f / sqrtf(gv)) : 0.0f;
+      // centre: direct terms, luminance through every tap's weight, variance through sl (no prefilter here)
+      atomic_add4(dIn + pix, make_float4(gS.x * cw + dlp * 0.2126f, gS.y * cw + dlp * 0.7152f, gS.z * cw + dlp * 0.0722f,
+                                         gV * cw * cw + (PREF ? 0.0f : dgv)));
+    }
+  }
+};
+
+// Mid level k (1, 2, 3): B_k = filt(src; s_k, c_k). Level 1 reads the block means from F2.zw (with prefilter).
+template <int K>
+__global__ void __launch_bounds__(TW *TH) k_mid_fwd(const TwinFrame T) {
+  constexpr int STEP = K == 1 ? 1 : (K == 2 ? 2 : 4), AP = STEP, SW = TW + 2 * AP, SH = TH + 2 * AP;
+  __shared__ float4 sA[SW * SH], sG[SW * SH];
+  const HushFrame &f = T.f;
+  const float4 *src = K == 2 ? T.B1 : T.B2;
+  float4 *dst = K == 1 ? T.B1 : (K == 2 ? T.B2 : T.B3);
+  const int li = threadIdx.y * TW + threadIdx.x;
+  const int bx = blockIdx.x * TW, by = blockIdx.y * TH;
+  for (int i = li; i < SW * SH; i += TW * TH) {
+    const int q = clampi(by - AP + i / SW, 0, f.H2 - 1) * f.W2 + clampi(bx - AP + i % SW, 0, f.W2 - 1);
+    sA[i] = K == 1 ? f2_ac_tw(f.F2, q) : src[q];
+    sG[i] = f3_guide_tw(f.F3, q);
+  }
+  __syncthreads();
+  const int X = bx + threadIdx.x, Y = by + threadIdx.y;
+  if (X >= f.W2 || Y >= f.H2) return;
+  const int o = Y * f.W2 + X, ti = (threadIdx.y + AP) * SW + threadIdx.x + AP;
+  if (sG[ti].w < 0.0f) { dst[o] = make_float4(0.f, 0.f, 0.f, 0.f); return; }
+  const float4 p1 = T.par[3 * o + 1], p2 = T.par[3 * o + 2];
+  const float s = K == 1 ? p1.y : (K == 2 ? p1.z : p1.w), c = K == 1 ? p2.y : (K == 2 ? p2.z : p2.w);
+  Filt1<STEP, K == 1, SW> F;
+  F.run(sA, sG, ti, X, Y, f.W2, f.H2, s, c);
+  dst[o] = F.out();
+}
+
+template <int K>
+__global__ void __launch_bounds__(TW *TH) k_mid_bwd(const TwinFrame T) {
+  constexpr int STEP = K == 1 ? 1 : (K == 2 ? 2 : 4), AP = STEP, SW = TW + 2 * AP, SH = TH + 2 * AP;
+  __shared__ float4 sA[SW * SH], sG[SW * SH];
+  const HushFrame &f = T.f;
+  const float4 *src = K == 2 ? T.B1 : T.B2;
+  const float4 *gout = K == 1 ? T.dB1 : (K == 2 ? T.dB2 : T.dB3);
+  float4 *gin = K == 1 ? nullptr : (K == 2 ? T.dB1 : T.dB2);
+  const int li = threadIdx.y * TW + threadIdx.x;
+  const int bx = blockIdx.x * TW, by = blockIdx.y * TH;
+  for (int i = li; i < SW * SH; i += TW * TH) {
+    const int q = clampi(by - AP + i / SW, 0, f.H2 - 1) * f.W2 + clampi(bx - AP + i % SW, 0, f.W2 - 1);
+    sA[i] = K == 1 ? f2_ac_tw(f.F2, q) : src[q];
+    sG[i] = f3_guide_tw(f.F3, q);
+  }
+  __syncthreads();
+  const int X = bx + threadIdx.x, Y = by + threadIdx.y;
+  if (X >= f.W2 || Y >= f.H2) return;
+  const int o = Y * f.W2 + X, ti = (threadIdx.y + AP) * SW + threadIdx.x + AP;
+  if (sG[ti].w < 0.0f) return;
+  const float4 p1 = T.par[3 * o + 1], p2 = T.par[3 * o + 2];
+  const float s = K == 1 ? p1.y : (K == 2 ? p1.z : p1.w), c = K == 1 ? p2.y : (K == 2 ? p2.z : p2.w);
+  Filt1<STEP, K == 1, SW> F;
+  F.run(sA, sG, ti, X, Y, f.W2, f.H2, s, c);
+  const float4 g = gout[o];
+  float ds, dc;
+  F.adjoint(sA, ti, make_float3(g.x, g.y, g.z), g.w, s, ds, dc, gin, o, f.W2);
+  // s_k / c_k live in components k of par1 / par2
+  float *dp1 = &T.dpar[3 * o + 1].x, *dp2 = &T.dpar[3 * o + 2].x;
+  atomicAdd(dp1 + K, ds);
+  atomicAdd(dp2 + K, dc);
+}
+
+// ------------------------------------------------------------------------------------------------ fine + final
+struct Recomb {
+  float fx, fy, fz, swh, swq, uBx, uBy, uBz, uAx, uAy, uAz, uCx, uCy, uCz;
+  float wh[4], wqq[4];
+  int qh[4];
+  bool vh[4], vq[4];
+};
+
+HD_INL void recomb_fwd(const TwinFrame &T, int px, int py, float4 A1, float4 gp, Recomb &R) {
+  const HushFrame &f = T.f;
+  R.fx = A1.x; R.fy = A1.y; R.fz = A1.z;
+  const float z = gp.w;
+  const int hsx = (f.W + 1) / 2, hsy = (f.H + 1) / 2;
+  const float hposx = ((float)px + 0.5f) / 2.0f - 0.5f, hposy = ((float)py + 0.5f) / 2.0f - 0.5f;
+  const float hbx = floorf(hposx), hby = floorf(hposy);
+  R.uBx = R.uBy = R.uBz = R.uAx = R.uAy = R.uAz = R.swh = 0.f;
+  for (int j = 0; j < 4; j++) {
+    const int qx = (int)hbx + (j & 1), qy = (int)hby + (j >> 1);
+    R.vh[j] = false;
+    R.wh[j] = 0.f;
+    R.qh[j] = 0;
+    if (qx < 0 || qy < 0 || qx >= hsx || qy >= hsy) continue;
+    const int q = qy * f.W2 + qx;
+    const float4 g = f3_guide_tw(f.F3, q);
+    if (g.w < 0.0f) continue;
+    const float w = jbw(hposx - hbx, hposy - hby, j, g, g.w, gp, z);
+    const float4 a = f2_ac_tw(f.F2, q), m = T.B3[q];
+    R.vh[j] = true;
+    R.wh[j] = w;
+    R.qh[j] = q;
+    R.swh += w;
+    R.uBx += w * m.x; R.uBy += w * m.y; R.uBz += w * m.z;
+    R.uAx += w * a.x; R.uAy += w * a.y; R.uAz += w * a.z;
+  }
+  const int qsx = (f.W + 3) / 4, qsy = (f.H + 3) / 4;
+  const float cposx = ((float)px + 0.5f) / 4.0f - 0.5f, cposy = ((float)py + 0.5f) / 4.0f - 0.5f;
+  const float cbx = floorf(cposx), cby = floorf(cposy);
+  R.uCx = R.uCy = R.uCz = R.swq = 0.f;
+  for (int j = 0; j < 4; j++) {
+    const int qx = (int)cbx + (j & 1), qy = (int)cby + (j >> 1);
+    if (qx < 0 || qy < 0 || qx >= qsx || qy >= qsy) continue;
+    const int q = qy * f.W4 + qx;
+    const float4 cg = ldh(f.CG, q);
+    if (cg.z < 0.0f) continue;
+    const float w = jbw(cposx - cbx, cposy - cby, j, oct_dec(cg.x, cg.y), cg.z, gp, z);
+    const float4 c = ldh(f.C0, q);
+    R.swq += w;
+    R.uCx += w * c.x; R.uCy += w * c.y; R.uCz += w * c.z;
+  }
+}
+
+// fine level (A1, also the colour history) and recombination -> X
+__global__ void __launch_bounds__(TW *TH) k_fine_fwd(const TwinFrame T) {
+  constexpr int AP = 1, SW = TW + 2, SH = TH + 2;
+  __shared__ float4 sA[SW * SH], sG[SW * SH];
+  const HushFrame &f = T.f;
+  const int li = threadIdx.y * TW + threadIdx.x;
+  const int bx = blockIdx.x * TW, by = blockIdx.y * TH;
+  for (int i = li; i < SW * SH; i += TW * TH) {
+    const int q = clampi(by - AP + i / SW, 0, f.H - 1) * f.W + clampi(bx - AP + i % SW, 0, f.W - 1);
+    sA[i] = ldh(f.A0, q);
+    const float4 k = ldh(f.key, q);
+    float4 g = oct_dec(k.x, k.y);
+    g.w = k.z;
+    sG[i] = g;
+  }
+  __syncthreads();
+  const int px = bx + threadIdx.x, py = by + threadIdx.y;
+  if (px >= f.W || py >= f.H) return;
+  const int o = py * f.W + px, ti = (threadIdx.y + AP) * SW + threadIdx.x + AP;
+  const float4 alb = ldh(f.mat, py * f.p_mat + px), emi = ldh(f.emi, py * f.p_emi + px);
+  const float4 gp = sG[ti];
+  if (gp.w < 0.0f) {
+    T.A1[o] = make_float4(0.f, 0.f, 0.f, 0.f);
+    T.X[o] = make_float4(emi.x, emi.y, emi.z, 0.f);
+    sth(f.hist, o, make_float4(0.f, 0.f, 0.f, 0.f));
+    return;
+  }
+  const int hp = (py >> 1) * f.W2 + (px >> 1);
+  const float4 p0 = T.par[3 * hp], p1 = T.par[3 * hp + 1], p2 = T.par[3 * hp + 2];
+  Filt1<1, true, SW> F;
+  F.run(sA, sG, ti, px, py, f.W, f.H, p1.x, p2.x);
+  const float4 A1 = F.out();
+  T.A1[o] = A1;
+  sth(f.hist, o, A1);
+  Recomb R;
+  recomb_fwd(T, px, py, A1, gp, R);
+  float ix = R.fx, iy = R.fy, iz = R.fz;
+  if (R.swh > 1e-4f) {
+    ix = R.uBx / R.swh + p0.w * (R.fx - R.uAx / R.swh);
+    iy = R.uBy / R.swh + p0.w * (R.fy - R.uAy / R.swh);
+    iz = R.uBz / R.swh + p0.w * (R.fz - R.uAz / R.swh);
+  }
+  float upx = ix, upy = iy, upz = iz;
+  if (R.swq > 1e-4f) { upx = R.uCx / R.swq; upy = R.uCy / R.swq; upz = R.uCz / R.swq; }
+  ix = ix + (upx - ix) * p0.z;
+  iy = iy + (upy - iy) * p0.z;
+  iz = iz + (upz - iz) * p0.z;
+  T.X[o] = make_float4(ix * alb.x + emi.x, iy * alb.y + emi.y, iz * alb.z + emi.z, 0.0f);
+}
+
+// ------------------------------------------------------------------------------------------------ TAA
+HD_INL float3 tm3(float4 c) { return tmap(make_float3(c.x, c.y, c.z)); }
+
+struct TaaF {
+  float3 y[9], m1, sd, v3, cur, hh0, hh, hr, res, out;
+  int q[9];
+  bool inside, lo_act[3], hi_act[3], act_itm;
+  float d;
+};
+
+HD_INL void taa_fwd(const TwinFrame &T, int px, int py, TaaF &A) {
+  const HushFrame &f = T.f;
+  const int o = py * f.W + px;
+  A.cur = tm3(T.X[o]);
+  A.inside = false;
+  for (int j = 0; j < 9; j++) {
+    A.q[j] = clampi(py + j / 3 - 1, 0, f.H - 1) * f.W + clampi(px + j % 3 - 1, 0, f.W - 1);
+    A.y[j] = to_ycocg(tm3(T.X[A.q[j]]));
+  }
+  A.res = A.cur;
+  for (int c = 0; c < 3; c++) A.lo_act[c] = A.hi_act[c] = false;
+  if (!f.reset) {
+    float3 m1 = make_float3(0.f, 0.f, 0.f);
+    for (int j = 0; j < 9; j++) { m1.x += A.y[j].x; m1.y += A.y[j].y; m1.z += A.y[j].z; }
+    m1.x /= 9.0f; m1.y /= 9.0f; m1.z /= 9.0f;
+    float3 v3 = make_float3(0.f, 0.f, 0.f);
+    for (int j = 0; j < 9; j++) {
+      const float dx = A.y[j].x - m1.x, dy = A.y[j].y - m1.y, dz = A.y[j].z - m1.z;
+      v3.x += dx * dx; v3.y += dy * dy; v3.z += dz * dz;
+    }
+    v3.x /= 9.0f; v3.y /= 9.0f; v3.z /= 9.0f;
+    A.m1 = m1;
+    A.v3 = v3;
+    A.sd = make_float3(sqrtf(fmaxf(v3.x, 1e-12f)), sqrtf(fmaxf(v3.y, 1e-12f)), sqrtf(fmaxf(v3.z, 1e-12f)));
+    const float4 mv = ldh(f.mv, py * f.p_mv + px);
+    const float szx = (float)f.W, szy = (float)f.H;
+    const float uvx = ((float)px + 0.5f + mv.x) / szx, uvy = ((float)py + 0.5f + mv.y) / szy;
+    if (uvx >= 0.0f && uvy >= 0.0f && uvx <= 1.0f && uvy <= 1.0f) {
+      A.inside = true;
+      const float ppx = uvx * szx - 0.5f, ppy = uvy * szy - 0.5f;
+      const float bxf = floorf(ppx), byf = floorf(ppy);
+      const float fx = ppx - bxf, fy = ppy - byf;
+      float3 hist = make_float3(0.f, 0.f, 0.f);
+      for (int j = 0; j < 4; j++) {
+        const int ox = j & 1, oy = j >> 1;
+        const float wb = (ox == 1 ? fx : 1.0f - fx) * (oy == 1 ? fy : 1.0f - fy);
+        const float4 t = ldh(f.taa_prev, clampi((int)byf + oy, 0, f.H - 1) * f.W + clampi((int)bxf + ox, 0, f.W - 1));
+        hist.x += wb * t.x; hist.y += wb * t.y; hist.z += wb * t.z;
+      }
+      A.hh0 = to_ycocg(tmap(hist));
+      float h0[3] = {A.hh0.x, A.hh0.y, A.hh0.z}, mm[3] = {m1.x, m1.y, m1.z}, ss[3] = {A.sd.x, A.sd.y, A.sd.z}, hc[3];
+      for (int c = 0; c < 3; c++) {
+        const float lo = mm[c] - 1.25f * ss[c], hi = mm[c] + 1.25f * ss[c];
+        const float mx = fmaxf(h0[c], lo);
+        A.lo_act[c] = h0[c] < lo;
+        hc[c] = fminf(mx, hi);
+        A.hi_act[c] = mx > hi;
+      }
+      A.hh = make_float3(hc[0], hc[1], hc[2]);
+      A.hr = from_ycocg(A.hh);
+      A.res = make_float3(A.hr.x + (A.cur.x - A.hr.x) * 0.1f, A.hr.y + (A.cur.y - A.hr.y) * 0.1f,
+                          A.hr.z + (A.cur.z - A.hr.z) * 0.1f);
+    }
+  }
+  const float l = lum3(A.res.x, A.res.y, A.res.z);
+  A.act_itm = 1.0f - l > 1e-4f;
+  A.d = fmaxf(1.0f - l, 1e-4f);
+  A.out = make_float3(A.res.x / A.d, A.res.y / A.d, A.res.z / A.d);
+}
+
+__global__ void k_taa_fwd(const TwinFrame T) {
+  const HushFrame &f = T.f;
+  const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
+  if (px >= f.W || py >= f.H) return;
+  TaaF A;
+  taa_fwd(T, px, py, A);
+  const int o = py * f.W + px;
+  T.out[o] = make_float4(A.out.x, A.out.y, A.out.z, 1.0f);
+  sth(f.taa, o, make_float4(A.out.x, A.out.y, A.out.z, 1.0f));
+}
+
+// ------------------------------------------------------------------------------------------------ loss
+// L = (1 / 3N) sum |out - clean| / (|clean| + 1e-2) + lambda (1 / 3N) sum |d out - d clean| / (|clean| + 1e-2),
+// d = difference to the previous frame. Writes dL/dout (into gT, as the seed of the TAA adjoint) and per-CTA FP64
+// partial sums.
+__global__ void k_loss(const TwinFrame T, int backward) {
+  const HushFrame &f = T.f;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double l = 0.0;
+  if (i < f.W * f.H) {
+    const float4 o = T.out[i];
+    const float ov[3] = {o.x, o.y, o.z};
+    float g[3] = {0.f, 0.f, 0.f};
+    for (int c = 0; c < 3; c++) {
+      const float cl = T.clean[3 * i + c], den = fabsf(cl) + 1e-2f;
+      const float d = ov[c] - cl;
+      l += fabs((double)d) / den;
+      g[c] = sgn(d) / den;
+      if (T.has_prev) {
+        const float4 op = T.out_prev[i];
+        const float opv[3] = {op.x, op.y, op.z};
+        const float dd = (ov[c] - opv[c]) - (cl - T.clean_prev[3 * i + c]);
+        l += (double)T.lambda_t * fabs((double)dd) / den;
+        g[c] += T.lambda_t * sgn(dd) / den;
+      }
+    }
+    l *= T.inv_n;
+    if (backward) T.gT[i] = make_float4(g[0] * T.inv_n, g[1] * T.inv_n, g[2] * T.inv_n, 0.f);
+  }
+  // block reduction in FP64
+  for (int off = 16; off > 0; off >>= 1) l += __shfl_down_sync(0xffffffffu, l, off);
+  __shared__ double ws[32];
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = l;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if (threadIdx.x == 0) T.loss_partials[blockIdx.x] = v;
+  }
+}
+
+__global__ void k_reduce_f64(const double *partials, int n, double *out) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v += partials[i];
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  __shared__ double ws[32];
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double u = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) u += __shfl_down_sync(0xffffffffu, u, off);
+    if (threadIdx.x == 0) *out = u;
+  }
+}
+
+// ------------------------------------------------------------------------------------------------ TAA adjoint
+// Pass 1 (per pixel p): from dL/dout (in gT[p], overwritten) to the gradients of tm(X) at the 3x3 window (clip box)
+// and at p (current colour); scattered into gT2.
+HD_INL float3 itm_adjoint(const TaaF &A, float3 g) {
+  const float inv = 1.0f / A.d;
+  float3 r = make_float3(g.x * inv, g.y * inv, g.z * inv);
+  if (A.act_itm) {
+    const float k = (g.x * A.res.x + g.y * A.res.y + g.z * A.res.z) * inv * inv;
+    r.x += k * 0.2126f; r.y += k * 0.7152f; r.z += k * 0.0722f;
+  }
+  return r;
+}
+HD_INL float3 ycocg_adjoint(float3 g) {  // transpose of to_ycocg
+  return make_float3(0.25f * g.x + 0.5f * g.y - 0.25f * g.z, 0.5f * g.x + 0.5f * g.z, 0.25f * g.x - 0.5f * g.y - 0.25f * g.z);
+}
+
+__global__ void k_taa_bwd(const TwinFrame T, const float4 *gout, float4 *gT) {
+  const HushFrame &f = T.f;
+  const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
+  if (px >= f.W || py >= f.H) return;
+  const int o = py * f.W + px;
+  TaaF A;
+  taa_fwd(T, px, py, A);
+  const float4 go = gout[o];
+  const float3 gres = itm_adjoint(A, make_float3(go.x, go.y, go.z));
+  float3 gcur = gres;
+  if (A.inside) {
+    gcur = make_float3(0.1f * gres.x, 0.1f * gres.y, 0.1f * gres.z);
+    const float3 ghr = make_float3(0.9f * gres.x, 0.9f * gres.y, 0.9f * gres.z);
+    // from_ycocg transpose
+    const float gh[3] = {ghr.x + ghr.y + ghr.z, ghr.x - ghr.z, -ghr.x + ghr.y - ghr.z};
+    float gm[3], gs[3];
+    const float v3[3] = {A.v3.x, A.v3.y, A.v3.z}, sd[3] = {A.sd.x, A.sd.y, A.sd.z}, m1[3] = {A.m1.x, A.m1.y, A.m1.z};
+    for (int c = 0; c < 3; c++) {
+      const float glo = A.lo_act[c] ? gh[c] : 0.0f, ghi = A.hi_act[c] ? gh[c] : 0.0f;
+      gm[c] = glo + ghi;
+      gs[c] = 1.25f * (ghi - glo);
+      gs[c] = v3[c] > 1e-12f ? gs[c] / (2.0f * sd[c]) : 0.0f;  // d sd / d v3
+    }
+    for (int j = 0; j < 9; j++) {
+      const float yy[3] = {A.y[j].x, A.y[j].y, A.y[j].z};
+      float3 gy;
+      gy.x = gm[0] / 9.0f + gs[0] * 2.0f * (yy[0] - m1[0]) / 9.0f;
+      gy.y = gm[1] / 9.0f + gs[1] * 2.0f * (yy[1] - m1[1]) / 9.0f;
+      gy.z = gm[2] / 9.0f + gs[2] * 2.0f * (yy[2] - m1[2]) / 9.0f;
+      const float3 gt = ycocg_adjoint(gy);
+      if (gt.x != 0.f || gt.y != 0.f || gt.z != 0.f) atomic_add4(gT + A.q[j], make_float4(gt.x, gt.y, gt.z, 0.f));
+    }
+  }
+  atomic_add4(gT + o, make_float4(gcur.x, gcur.y, gcur.z, 0.f));
+}
+
+// Pass 2 (per full pixel): dL/dX from the tm gradient; then recombination, fine-level parameter and mid-level input
+// gradients.
+__global__ void __launch_bounds__(TW *TH) k_fine_bwd(const TwinFrame T, const float4 *gT) {
+  constexpr int AP = 1, SW = TW + 2, SH = TH + 2;
+  __shared__ float4 sA[SW * SH], sG[SW * SH];
+  const HushFrame &f = T.f;
+  const int li = threadIdx.y * TW + threadIdx.x;
+  const int bx = blockIdx.x * TW, by = blockIdx.y * TH;
+  for (int i = li; i < SW * SH; i += TW * TH) {
+    const int q = clampi(by - AP + i / SW, 0, f.H - 1) * f.W + clampi(bx - AP + i % SW, 0, f.W - 1);
+    sA[i] = ldh(f.A0, q);
+    const float4 k = ldh(f.key, q);
+    float4 g = oct_dec(k.x, k.y);
+    g.w = k.z;
+    sG[i] = g;
+  }
+  __syncthreads();
+  const int px = bx + threadIdx.x, py = by + threadIdx.y;
+  if (px >= f.W || py >= f.H) return;
+  const int o = py * f.W + px, ti = (threadIdx.y + AP) * SW + threadIdx.x + AP;
+  const float4 gp = sG[ti];
+  if (gp.w < 0.0f) return;  // X = emission: no dependence on the parameters
+  // tm adjoint: tm(X) = X / (1 + lum(X))
+  const float4 Xv = T.X[o], gt = gT[o];
+  const float L1 = 1.0f + lum(Xv);
+  const float k = (gt.x * Xv.x + gt.y * Xv.y + gt.z * Xv.z) / (L1 * L1);
+  const float3 gX = make_float3(gt.x / L1 - k * 0.2126f, gt.y / L1 - k * 0.7152f, gt.z / L1 - k * 0.0722f);
+  const float4 alb = ldh(f.mat, py * f.p_mat + px);
+  const int hp = (py >> 1) * f.W2 + (px >> 1);
+  const float4 p0 = T.par[3 * hp], p1 = T.par[3 * hp + 1], p2 = T.par[3 * hp + 2];
+  Filt1<1, true, SW> F;
+  F.run(sA, sG, ti, px, py, f.W, f.H, p1.x, p2.x);
+  const float4 A1 = F.out();
+  Recomb R;
+  recomb_fwd(T, px, py, A1, gp, R);
+  float ix = R.fx, iy = R.fy, iz = R.fz;
+  const bool mid = R.swh > 1e-4f;
+  if (mid) {
+    ix = R.uBx / R.swh + p0.w * (R.fx - R.uAx / R.swh);
+    iy = R.uBy / R.swh + p0.w * (R.fy - R.uAy / R.swh);
+    iz = R.uBz / R.swh + p0.w * (R.fz - R.uAz / R.swh);
+  }
+  // X = ill2 * alb + emi, ill2 = ill + (up - ill) beta
+  const float3 g2 = make_float3(gX.x * alb.x, gX.y * alb.y, gX.z * alb.z);
+  float3 gill = g2;
+  float gbeta = 0.0f;
+  if (R.swq > 1e-4f) {
+    const float upx = R.uCx / R.swq, upy = R.uCy / R.swq, upz = R.uCz / R.swq;
+    gbeta = g2.x * (upx - ix) + g2.y * (upy - iy) + g2.z * (upz - iz);
+    gill = make_float3(g2.x * (1.0f - p0.z), g2.y * (1.0f - p0.z), g2.z * (1.0f - p0.z));
+  }
+  float3 gf = gill;
+  float gkappa = 0.0f;
+  if (mid) {
+    gkappa = gill.x * (R.fx - R.uAx / R.swh) + gill.y * (R.fy - R.uAy / R.swh) + gill.z * (R.fz - R.uAz / R.swh);
+    gf = make_float3(gill.x * p0.w, gill.y * p0.w, gill.z * p0.w);
+    for (int j = 0; j < 4; j++) {
+      if (!R.vh[j]) continue;
+      const float w = R.wh[j] / R.swh;
+      atomic_add4(T.dB3 + R.qh[j], make_float4(gill.x * w, gill.y * w, gill.z * w, 0.f));
+    }
+  }
+  float ds, dc;
+  F.adjoint(sA, ti, gf, 0.0f, p1.x, ds, dc, nullptr, 0, 0);
+  float *d0 = &T.dpar[3 * hp].x, *d1 = &T.dpar[3 * hp + 1].x, *d2 = &T.dpar[3 * hp + 2].x;
+  atomicAdd(d0 + 2, gbeta);
+  atomicAdd(d0 + 3, gkappa);
+  atomicAdd(d1 + 0, ds);
+  atomicAdd(d2 + 0, dc);
+}
+
+// ------------------------------------------------------------------------------------------------ MLP adjoint
+// One row (half-res pixel) per thread: heads adjoint, then the three layers; the weight gradient of the CTA's rows is
+// reduced in shared memory (rows x activations stored transposed) and written as one partial per CTA.
+constexpr int MB_ROWS = 128;
+__global__ void __launch_bounds__(MB_ROWS) k_mlp_bwd(const TwinFrame T) {
+  extern __shared__ float sm[];
+  float *th = sm;                               // NW
+  float *sd3 = th + NW;                         // [12][ROWS]
+  float *sd2 = sd3 + 12 * MB_ROWS;              // [16][ROWS]
+  float *sd1 = sd2 + 16 * MB_ROWS;              // [16][ROWS]
+  float *sf = sd1 + 16 * MB_ROWS;               // [20][ROWS]
+  float *sh1 = sf + 20 * MB_ROWS;               // [16][ROWS]
+  float *sh2 = sh1 + 16 * MB_ROWS;              // [16][ROWS]
+  for (int i = threadIdx.x; i < NW; i += MB_ROWS) th[i] = T.theta[i];
+  __syncthreads();
+  const HushFrame &f = T.f;
+  const int r = threadIdx.x;
+  const int o = blockIdx.x * MB_ROWS + r;
+  float fe[20], h1[16], h2[16], out[12], d3[12], d2[16], d1[16];
+  for (int i = 0; i < 20; i++) fe[i] = 0.f;
+  for (int i = 0; i < 16; i++) h1[i] = h2[i] = d2[i] = d1[i] = 0.f;
+  for (int i = 0; i < 12; i++) d3[i] = 0.f;
+  if (o < f.W2 * f.H2 && f3_guide_tw(f.F3, o).w >= 0.0f) {
+    load_features(f, o, fe);
+    mlp_full(th, fe, h1, h2, out);
+    const float4 q0 = T.dpar[3 * o], q1 = T.dpar[3 * o + 1], q2 = T.dpar[3 * o + 2];
+    const float4 p0 = T.par[3 * o], p1 = T.par[3 * o + 1], p2 = T.par[3 * o + 2];
+    // heads (hush.js:357-362); alpha, gamma act on the next frame only
+    d3[0] = 0.0f;
+    d3[1] = 0.0f;
+    d3[2] = q0.z * p0.z * (1.0f - p0.z);
+    d3[3] = q0.w * p0.w * (1.0f - p0.w);
+    const float ps[4] = {p1.x, p1.y, p1.z, p1.w}, pc[4] = {p2.x, p2.y, p2.z, p2.w};
+    const float gs[4] = {q1.x, q1.y, q1.z, q1.w}, gc[4] = {q2.x, q2.y, q2.z, q2.w};
+    for (int k = 0; k < 4; k++) {
+      d3[4 + k] = fabsf(out[4 + k]) < 5.0f ? gs[k] * ps[k] : 0.0f;
+      d3[8 + k] = fabsf(out[8 + k]) < 4.0f ? gc[k] * pc[k] : 0.0f;
+    }
+    for (int i = 0; i < 16; i++) {
+      float a = 0.f;
+      for (int j = 0; j < 12; j++) a += d3[j] * th[W3o + j * 16 + i];
+      d2[i] = h2[i] > 0.0f ? a : 0.0f;
+    }
+    for (int i = 0; i < 16; i++) {
+      float a = 0.f;
+      for (int j = 0; j < 16; j++) a += d2[j] * th[W2o + j * 16 + i];
+      d1[i] = h1[i] > 0.0f ? a : 0.0f;
+    }
+  }
+  for (int i = 0; i < 12; i++) sd3[i * MB_ROWS + r] = d3[i];
+  for (int i = 0; i < 16; i++) {
+    sd2[i * MB_ROWS + r] = d2[i];
+    sd1[i * MB_ROWS + r] = d1[i];
+    sh1[i * MB_ROWS + r] = h1[i];
+    sh2[i * MB_ROWS + r] = h2[i];
+  }
+  for (int i = 0; i < 20; i++) sf[i * MB_ROWS + r] = fe[i];
+  __syncthreads();
+  // weight gradient of the CTA: parameter p = outer product (delta_j, x_i) summed over rows
+  float *part = T.partials + (size_t)blockIdx.x * NW;
+  for (int p = threadIdx.x; p < NW; p += MB_ROWS) {
+    const float *dv, *xv = nullptr;
+    if (p < B1o) { dv = sd1 + (p / 20) * MB_ROWS; xv = sf + (p % 20) * MB_ROWS; }
+    else if (p < W2o) { dv = sd1 + (p - B1o) * MB_ROWS; }
+    else if (p < B2o) { const int q = p - W2o; dv = sd2 + (q / 16) * MB_ROWS; xv = sh1 + (q % 16) * MB_ROWS; }
+    else if (p < W3o) { dv = sd2 + (p - B2o) * MB_ROWS; }
+    else if (p < B3o) { const int q = p - W3o; dv = sd3 + (q / 16) * MB_ROWS; xv = sh2 + (q % 16) * MB_ROWS; }
+    else { dv = sd3 + (p - B3o) * MB_ROWS; }
+    float a = 0.f;
+    if (xv) for (int k = 0; k < MB_ROWS; k++) a += dv[k] * xv[k];
+    else for (int k = 0; k < MB_ROWS; k++) a += dv[k];
+    part[p] = a;
+  }
+}
+constexpr size_t MB_SMEM = (size_t)(NW + (12 + 16 + 16 + 20 + 16 + 16) * MB_ROWS) * sizeof(float);
+
+// dtheta += sum over CTAs of the partials, in FP64
+__global__ void k_reduce_partials(const float *partials, int nparts, double *grad) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= NW) return;
+  double a = 0.0;
+  for (int c = 0; c < nparts; c++) a += (double)partials[(size_t)c * NW + p];
+  grad[p] += a;
+}
+
+// Adam on the FP32 master weights (gradient in FP64, optionally clipped by global norm scale `scale`).
+__global__ void k_adam(float *theta, float *m, float *v, const double *grad, float lr, float b1, float b2, float eps,
+                       float bc1, float bc2, float scale) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= NW) return;
+  const float g = (float)grad[p] * scale;
+  m[p] = b1 * m[p] + (1.0f - b1) * g;
+  v[p] = b2 * v[p] + (1.0f - b2) * g * g;
+  const float mh = m[p] / bc1, vh = v[p] / bc2;
+  theta[p] -= lr * mh / (sqrtf(vh) + eps);
+}
+
+}  // namespace twin
+}  // namespace hush
+
+using namespace hush;
+using namespace hush::twin;
+
+struct hush_trainer_s {
+  hush_t *h = nullptr;
+  int W = 0, H = 0, W2 = 0, H2 = 0;
+  float *theta = nullptr, *m = nullptr, *v = nullptr;
+  double *grad = nullptr, *loss = nullptr, *loss_partials = nullptr;
+  float4 *par = nullptr, *B[3] = {}, *A1 = nullptr, *X = nullptr, *out[2] = {}, *gT = nullptr, *gT2 = nullptr,
+         *dB[3] = {}, *dpar = nullptr;
+  float *partials = nullptr;
+  int n_mlp_ctas = 0, n_loss_ctas = 0;
+  int cur = 0, has_prev = 0;
+  int adam_t = 0;
+  char *pool = nullptr;
+};
+
+static int tr_fail(hush_trainer_t *t, const std::string &m) { return hush_fail(t ? t->h : nullptr, HUSH_ERR_ARG, m); }
+
+extern "C" int hush_trainer_create(hush_t *h, const float *theta, hush_trainer_t **out) {
+  if (!h || !out) return hush_fail(h, HUSH_ERR_ARG, "hush_trainer_create: NULL argument");
+  *out = nullptr;
+  if (h->hidden != 16) return hush_fail(h, HUSH_ERR_ARG, "hush_trainer_create: the trainer needs the h = 16 network");
+  cudaSetDevice(h->dev);
+  hush_trainer_t *t = new hush_trainer_t();
+  t->h = h;
+  t->W = h->W; t->H = h->H; t->W2 = h->W2; t->H2 = h->H2;
+  const size_t full = (size_t)t->W * t->H, half = (size_t)t->W2 * t->H2;
+  t->n_mlp_ctas = (int)((half + MB_ROWS - 1) / MB_ROWS);
+  t->n_loss_ctas = (int)((full + 255) / 256);
+  auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t bytes = al(NW * 4) * 3 + al(NW * 8) + al(8) + al(t->n_loss_ctas * 8) + al(half * 48) * 2 +
+                       al(half * 16) * 6 + al(full * 16) * 6 + al((size_t)t->n_mlp_ctas * NW * 4);
+  cudaError_t e = cudaMalloc(&t->pool, bytes);
+  if (e != cudaSuccess) { delete t; return hush_cuda_fail(h, e, "cudaMalloc of the trainer"); }
+  cudaMemset(t->pool, 0, bytes);
+  size_t off = 0;
+  auto take = [&](size_t b) { char *p = t->pool + off; off += al(b); return p; };
+  t->theta = (float *)take(NW * 4); t->m = (float *)take(NW * 4); t->v = (float *)take(NW * 4);
+  t->grad = (double *)take(NW * 8); t->loss = (double *)take(8);
+  t->loss_partials = (double *)take(t->n_loss_ctas * 8);
+  t->par = (float4 *)take(half * 48); t->dpar = (float4 *)take(half * 48);
+  for (int i = 0; i < 3; i++) { t->B[i] = (float4 *)take(half * 16); t->dB[i] = (float4 *)take(half * 16); }
+  t->A1 = (float4 *)take(full * 16); t->X = (float4 *)take(full * 16);
+  t->out[0] = (float4 *)take(full * 16); t->out[1] = (float4 *)take(full * 16);
+  t->gT = (float4 *)take(full * 16); t->gT2 = (float4 *)take(full * 16);
+  t->partials = (float *)take((size_t)t->n_mlp_ctas * NW * 4);
+  e = cudaMemcpy(t->theta, theta ? theta : h->wf.data(), NW * 4, theta ? cudaMemcpyHostToDevice : cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { cudaFree(t->pool); delete t; return hush_cuda_fail(h, e, "cudaMemcpy of the weights"); }
+  cudaFuncSetAttribute(k_mlp_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MB_SMEM);
+  *out = t;
+  return HUSH_OK;
+}
+
+extern "C" void hush_trainer_destroy(hush_trainer_t *t) {
+  if (!t) return;
+  cudaSetDevice(t->h->dev);
+  cudaFree(t->pool);
+  delete t;
+}
+
+static TwinFrame make_twin(hush_trainer_t *t, const hush_inputs *in, const float *clean, const float *clean_prev,
+                           float lambda_t) {
+  TwinFrame T;
+  std::memset(&T, 0, sizeof(T));
+  T.f = hush_make_frame(t->h, in);
+  T.theta = t->theta;
+  T.par = t->par;
+  T.B1 = t->B[0]; T.B2 = t->B[1]; T.B3 = t->B[2];
+  T.A1 = t->A1; T.X = t->X;
+  T.out = t->out[t->cur];
+  T.out_prev = t->out[t->cur ^ 1];
+  T.clean = clean;
+  T.clean_prev = clean_prev;
+  T.gT = t->gT;
+  T.dB1 = t->dB[0]; T.dB2 = t->dB[1]; T.dB3 = t->dB[2];
+  T.dpar = t->dpar;
+  T.partials = t->partials;
+  T.loss_partials = t->loss_partials;
+  T.lambda_t = lambda_t;
+  T.has_prev = (t->has_prev && clean_prev && !t->h->reset) ? 1 : 0;
+  T.inv_n = 1.0f / (3.0f * (float)t->W * (float)t->H);
+  return T;
+}
+
+// Forward (and, if `backward`, the adjoint accumulated into the weight gradient) of one frame of the twin. Does not
+// advance the frame: repeated calls see the same history (finite differences); hush_trainer_end_frame advances.
+extern "C" int hush_trainer_frame(hush_trainer_t *t, const hush_inputs *in, const float *clean, const float *clean_prev,
+                                  float lambda_t, int backward, void *stream, double *loss_out) {
+  if (!t) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_trainer_frame: NULL trainer");
+  if (!clean) return tr_fail(t, "hush_trainer_frame: missing clean image");
+  int rc = hush_check_inputs(t->h, in);
+  if (rc != HUSH_OK) return rc;
+  cudaSetDevice(t->h->dev);
+  cudaStream_t st = (cudaStream_t)stream;
+  const TwinFrame T = make_twin(t, in, clean, clean_prev, lambda_t);
+  const HushFrame &f = T.f;
+  // TEMPORAL and the coarse levels as the reference passes (their outputs do not depend on the weights)
+  cudaError_t e = launch_pass(PASS_TEMPORAL, f, t->h->w16, st);
+  if (e == cudaSuccess) e = launch_pass(PASS_COARSE1, f, t->h->w16, st);
+  if (e == cudaSuccess) e = launch_pass(PASS_COARSE2, f, t->h->w16, st);
+  if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "trainer pass launch");
+  const int half = f.W2 * f.H2, full = f.W * f.H;
+  const dim3 blk(TW, TH), gh((f.W2 + TW - 1) / TW, (f.H2 + TH - 1) / TH), gf((f.W + TW - 1) / TW, (f.H + TH - 1) / TH);
+  k_mlp_fwd<<<(half + 127) / 128, 128, 0, st>>>(T);
+  k_mid_fwd<1><<<gh, blk, 0, st>>>(T);
+  k_mid_fwd<2><<<gh, blk, 0, st>>>(T);
+  k_mid_fwd<3><<<gh, blk, 0, st>>>(T);
+  k_fine_fwd<<<gf, blk, 0, st>>>(T);
+  k_taa_fwd<<<gf, blk, 0, st>>>(T);
+  k_loss<<<t->n_loss_ctas, 256, 0, st>>>(T, backward);
+  k_reduce_f64<<<1, 256, 0, st>>>(t->loss_partials, t->n_loss_ctas, t->loss);
+  if (backward) {
+    cudaMemsetAsync(t->gT2, 0, (size_t)full * 16, st);
+    cudaMemsetAsync(t->dpar, 0, (size_t)half * 48, st);
+    for (int i = 0; i < 3; i++) cudaMemsetAsync(t->dB[i], 0, (size_t)half * 16, st);
+    k_taa_bwd<<<gf, blk, 0, st>>>(T, t->gT, t->gT2);
+    k_fine_bwd<<<gf, blk, 0, st>>>(T, t->gT2);
+    k_mid_bwd<3><<<gh, blk, 0, st>>>(T);
+    k_mid_bwd<2><<<gh, blk, 0, st>>>(T);
+    k_mid_bwd<1><<<gh, blk, 0, st>>>(T);
+    k_mlp_bwd<<<t->n_mlp_ctas, MB_ROWS, MB_SMEM, st>>>(T);
+    k_reduce_partials<<<(NW + 127) / 128, 128, 0, st>>>(t->partials, t->n_mlp_ctas, t->grad);
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "trainer kernel launch");
+  if (loss_out) {
+    e = cudaMemcpyAsync(loss_out, t->loss, 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "reading the loss");
+  }
+  return HUSH_OK;
+}
+
+extern "C" int hush_trainer_end_frame(hush_trainer_t *t) {
+  if (!t) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_trainer_end_frame: NULL trainer");
+  t->has_prev = 1;
+  t->cur ^= 1;
+  return hush_end_frame(t->h);
+}
+
+extern "C" int hush_trainer_reset(hush_trainer_t *t) {
+  if (!t) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_trainer_reset: NULL trainer");
+  t->has_prev = 0;
+  return hush_reset(t->h);
+}
+
+extern "C" int hush_trainer_zero_grad(hush_trainer_t *t, void *stream) {
+  if (!t) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_trainer_zero_grad: NULL trainer");
+  cudaError_t e = cudaMemsetAsync(t->grad, 0, NW * 8, (cudaStream_t)stream);
+  return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, "cudaMemsetAsync");
+}
+
+extern "C" int hush_trainer_grad(hush_trainer_t *t, double *out) {
+  if (!t || !out) return hush_fail(t ? t->h : nullptr, HUSH_ERR_ARG, "hush_trainer_grad: NULL argument");
+  cudaError_t e = cudaMemcpy(out, t->grad, NW * 8, cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, "cudaMemcpy");
+}
+
+extern "C" int hush_trainer_theta(hush_trainer_t *t, float *get, const float *set) {
+  if (!t) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_trainer_theta: NULL trainer");
+  cudaError_t e = cudaSuccess;
+  if (set) e = cudaMemcpy(t->theta, set, NW * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && get) e = cudaMemcpy(get, t->theta, NW * 4, cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, "cudaMemcpy");
+}
+
+// dL/dpar of the last backward: 12 floats per half-res pixel (alpha gamma beta kappa s0..s3 c0..c3), and the FP32
+// parameters themselves.
+extern "C" int hush_trainer_par(hush_trainer_t *t, float *par, float *dpar) {
+  if (!t) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_trainer_par: NULL trainer");
+  const size_t n = (size_t)t->W2 * t->H2 * 48;
+  cudaError_t e = cudaSuccess;
+  if (par) e = cudaMemcpy(par, t->par, n, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && dpar) e = cudaMemcpy(dpar, t->dpar, n, cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, "cudaMemcpy");
+}
+
+// The FP32 TAA output of the last forward (rgba, W x H).
+extern "C" int hush_trainer_output(hush_trainer_t *t, float *out) {
+  if (!t || !out) return hush_fail(t ? t->h : nullptr, HUSH_ERR_ARG, "hush_trainer_output: NULL argument");
+  cudaError_t e = cudaMemcpy(out, t->out[t->cur], (size_t)t->W * t->H * 16, cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, "cudaMemcpy");
+}
+
+// Adam step on the accumulated gradient (global-norm clipped to `clip` if clip > 0); zeroes the gradient.
+extern "C" int hush_trainer_step(hush_trainer_t *t, float lr, float beta1, float beta2, float eps, float clip,
+                                 void *stream, double *grad_norm) {
+  if (!t) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_trainer_step: NULL trainer");
+  cudaSetDevice(t->h->dev);
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<double> g(NW);
+  cudaError_t e = cudaMemcpyAsync(g.data(), t->grad, NW * 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "reading the gradient");
+  double n2 = 0.0;
+  for (double x : g) n2 += x * x;
+  const double norm = std::sqrt(n2);
+  if (grad_norm) *grad_norm = norm;
+  const float scale = (clip > 0.0f && norm > clip) ? (float)(clip / norm) : 1.0f;
+  t->adam_t++;
+  const float bc1 = 1.0f - std::pow(beta1, (float)t->adam_t), bc2 = 1.0f - std::pow(beta2, (float)t->adam_t);
+  k_adam<<<(NW + 127) / 128, 128, 0, st>>>(t->theta, t->m, t->v, t->grad, lr, beta1, beta2, eps, bc1, bc2, scale);
+  e = cudaMemsetAsync(t->grad, 0, NW * 8, st);
+  return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, "cudaMemsetAsync");
+}
+
+// Rounds the FP32 master weights to the f16 blob (W1 b1 W2 b2 W3 b3, hush.js:20-21), hands it to the denoiser and,
+// if blob != NULL, to the caller (812 values).
+extern "C" int hush_trainer_export(hush_trainer_t *t, uint16_t *blob) {
+  if (!t) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_trainer_export: NULL trainer");
+  std::vector<float> th(NW);
+  cudaError_t e = cudaMemcpy(th.data(), t->theta, NW * 4, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "reading the weights");
+  std::vector<uint16_t> b(NW);
+  for (int i = 0; i < NW; i++) b[i] = __half_as_ushort(__float2half_rn(th[i]));
+  if (blob) std::memcpy(blob, b.data(), NW * 2);
+  return hush_set_weights(t->h, b.data(), NW);
+}

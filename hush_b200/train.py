@@ -1,0 +1,183 @@
+"""On-device training of the parameter MLP through the hand-written adjoint kernels (hush_trainer_* in include/hush.h).
+
+The reference's weights were trained offline by a PyTorch copy of its passes that is not shipped (README.md:137,
+src/denoise/hush.js:6-7). Here the frames come from the synthetic scene generator on the device, the target is the
+noise-free image, the loss is relative L1 of the TAA output plus a temporal-gradient term, and Adam updates FP32
+master weights; the result exports to the reference's f16 blob format (W1 b1 W2 b2 W3 b3, hush.js:20-21).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+from .hush import Hush, HushError, _fill_inputs, _stream_handle
+from .scene import NAMES, SceneConfig, frame_device
+
+NW = 812
+
+
+def xavier_init(seed: int = 0) -> np.ndarray:
+    """Xavier-uniform weights and zero biases of the 20-16-16-12 network in the blob layout."""
+    rng = np.random.default_rng(seed)
+    w = np.zeros(NW, np.float32)
+
+    def xav(n_out, n_in):
+        b = np.sqrt(6.0 / (n_in + n_out))
+        return rng.uniform(-b, b, n_out * n_in).astype(np.float32)
+
+    w[0:320] = xav(16, 20)
+    w[336:592] = xav(16, 16)
+    w[608:800] = xav(12, 16)
+    return w
+
+
+class Trainer:
+    """Training twin bound to one Hush instance (FP32 master weights, Adam state, gradient accumulator)."""
+
+    def __init__(self, hush: Hush, theta: np.ndarray | None = None):
+        self.hush = hush
+        self._theta = None if theta is None else np.ascontiguousarray(theta, np.float32)
+        h = C.c_void_p()
+        rc = L.lib().hush_trainer_create(hush._h, self._theta.ctypes.data if self._theta is not None else None,
+                                         C.byref(h))
+        if rc != L.HUSH_OK:
+            raise HushError(L.lib().hush_last_error(hush._h).decode())
+        self._t = h
+        self._inp = L.HushInputs()
+
+    def _check(self, rc):
+        if rc != L.HUSH_OK:
+            raise HushError(L.lib().hush_last_error(self.hush._h).decode())
+
+    def frame(self, inputs: dict, clean, clean_prev=None, lambda_t: float = 0.0, backward: bool = True,
+              stream=None) -> float:
+        """One frame: forward, loss and (if backward) the gradient added to the accumulator. Does not advance."""
+        _fill_inputs(self._inp, inputs)
+        loss = C.c_double()
+        self._check(L.lib().hush_trainer_frame(self._t, C.byref(self._inp), clean.data_ptr(),
+                                               clean_prev.data_ptr() if clean_prev is not None else None,
+                                               float(lambda_t), 1 if backward else 0,
+                                               C.c_void_p(_stream_handle(stream)), C.byref(loss)))
+        return loss.value
+
+    def end_frame(self):
+        self._check(L.lib().hush_trainer_end_frame(self._t))
+
+    def reset(self):
+        self._check(L.lib().hush_trainer_reset(self._t))
+
+    def zero_grad(self, stream=None):
+        self._check(L.lib().hush_trainer_zero_grad(self._t, C.c_void_p(_stream_handle(stream))))
+
+    def grad(self) -> np.ndarray:
+        g = np.zeros(NW, np.float64)
+        self._check(L.lib().hush_trainer_grad(self._t, g.ctypes.data))
+        return g
+
+    @property
+    def theta(self) -> np.ndarray:
+        t = np.zeros(NW, np.float32)
+        self._check(L.lib().hush_trainer_theta(self._t, t.ctypes.data, None))
+        return t
+
+    @theta.setter
+    def theta(self, v):
+        v = np.ascontiguousarray(v, np.float32)
+        self._check(L.lib().hush_trainer_theta(self._t, None, v.ctypes.data))
+
+    def par(self):
+        """(par, dpar): (h, w, 12) FP32 parameters of the last frame and their gradient."""
+        H2, W2 = (self.hush.height + 1) // 2, (self.hush.width + 1) // 2
+        p = np.zeros((H2, W2, 12), np.float32)
+        d = np.zeros((H2, W2, 12), np.float32)
+        self._check(L.lib().hush_trainer_par(self._t, p.ctypes.data, d.ctypes.data))
+        return p, d
+
+    def output(self) -> np.ndarray:
+        o = np.zeros((self.hush.height, self.hush.width, 4), np.float32)
+        self._check(L.lib().hush_trainer_output(self._t, o.ctypes.data))
+        return o
+
+    def step(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, clip=1.0, stream=None) -> float:
+        n = C.c_double()
+        self._check(L.lib().hush_trainer_step(self._t, lr, beta1, beta2, eps, clip,
+                                              C.c_void_p(_stream_handle(stream)), C.byref(n)))
+        return n.value
+
+    def export(self) -> np.ndarray:
+        b = np.zeros(NW, np.uint16)
+        self._check(L.lib().hush_trainer_export(self._t, b.ctypes.data))
+        return b
+
+    def destroy(self):
+        if getattr(self, "_t", None) and self._t.value:
+            L.lib().hush_trainer_destroy(self._t)
+            self._t = C.c_void_p()
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+@dataclass
+class TrainConfig:
+    """The training workload: windows of `frames` frames at `size`^2 from `seeds` generator seeds."""
+    size: int = 384
+    frames: int = 8
+    seeds: int = 2048
+    batch: int = 16
+    steps: int = 5000
+    lr: float = 1e-3
+    lambda_t: float = 0.5
+    clip: float = 1.0
+    init_seed: int = 0
+
+
+def window(cfg: TrainConfig, seed: int, buf=None):
+    """One training window generated on the device: list of (inputs, clean) for `frames` frames."""
+    sc = SceneConfig(cfg.size, cfg.size, cfg.frames, seed=seed, pan_min=0.0, pan_max=4.0, n_moving=3)
+    out = []
+    for t in range(cfg.frames):
+        out.append(frame_device(sc, t, out=None if buf is None else buf[t], clean=True))
+    return out
+
+
+def train(cfg: TrainConfig, log_every: int = 100, on_log=None, time_budget_s: float | None = None):
+    """Runs the training loop; returns (trainer, hush, history). A step = `batch` windows of `frames` frames."""
+    import torch
+
+    hush = Hush(0, {"width": cfg.size, "height": cfg.size, "schedule": "passes"})
+    tr = Trainer(hush, xavier_init(cfg.init_seed))
+    rng = np.random.default_rng(cfg.init_seed + 1)
+    bufs = [{n: torch.empty((cfg.size, cfg.size, 4), dtype=torch.float16, device="cuda") for n in NAMES}
+            for _ in range(cfg.frames)]
+    for b in bufs:
+        b["clean"] = torch.empty((cfg.size, cfg.size, 3), dtype=torch.float32, device="cuda")
+    hist = []
+    t0 = time.time()
+    for step in range(cfg.steps):
+        ts = time.perf_counter()
+        loss_sum = 0.0
+        for _ in range(cfg.batch):
+            seed = int(rng.integers(0, cfg.seeds))
+            win = window(cfg, seed, bufs)
+            tr.reset()
+            for t, fr in enumerate(win):
+                loss_sum += tr.frame(fr, fr["clean"], win[t - 1]["clean"] if t else None, cfg.lambda_t, True)
+                tr.end_frame()
+        gn = tr.step(cfg.lr, clip=cfg.clip)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - ts) * 1e3
+        rec = {"step": step, "loss": loss_sum / (cfg.batch * cfg.frames), "grad_norm": gn, "step_ms": ms}
+        hist.append(rec)
+        if on_log and (step % log_every == 0 or step == cfg.steps - 1):
+            on_log(rec)
+        if time_budget_s and time.time() - t0 > time_budget_s:
+            break
+    return tr, hush, hist

@@ -128,6 +128,39 @@ int hush_end_frame(hush_t *h);
 /* Device pointer and geometry of a state image. */
 int hush_buffer(hush_t *h, int id, void **dptr, int *width, int *height, int *texel_bytes);
 
+/* ---- training twin: forward / adjoint of the frame for on-device training of the parameter MLP --------------------
+ * No reference counterpart as an API: the reference's weights were trained offline by a PyTorch copy of the passes
+ * that it does not ship (README.md:137, hush.js:6-7). The twin runs the frame after TEMPORAL in FP32 without f16
+ * storage rounding; the loss is relative L1 of the TAA output against the noise-free image plus lambda times the
+ * same on frame differences. Gradients are exact for one frame with the temporal history held fixed; frames of a
+ * window accumulate (truncated backpropagation through time). Trainers are tied to one Hush instance (h = 16). */
+typedef struct hush_trainer_s hush_trainer_t;
+/* theta: 812 FP32 initial weights (W1 b1 W2 b2 W3 b3), NULL = the instance's current weights. */
+int hush_trainer_create(hush_t *h, const float *theta, hush_trainer_t **out);
+void hush_trainer_destroy(hush_trainer_t *t);
+/* One frame: TEMPORAL + coarse passes, twin forward, loss (in *loss_out, synchronising), and if backward != 0 the
+ * adjoint added to the weight gradient. clean / clean_prev: dense f32 rgb device images (clean_prev may be NULL).
+ * Does not advance the frame, so repeated calls see the same history. */
+int hush_trainer_frame(hush_trainer_t *t, const hush_inputs *in, const float *clean, const float *clean_prev,
+                       float lambda_t, int backward, void *stream, double *loss_out);
+int hush_trainer_end_frame(hush_trainer_t *t);
+int hush_trainer_reset(hush_trainer_t *t);
+int hush_trainer_zero_grad(hush_trainer_t *t, void *stream);
+/* The accumulated weight gradient (812 doubles). */
+int hush_trainer_grad(hush_trainer_t *t, double *out);
+/* Read (get != NULL) and / or replace (set != NULL) the FP32 master weights. */
+int hush_trainer_theta(hush_trainer_t *t, float *get, const float *set);
+/* The FP32 parameters and dL/dpar of the last frame: 12 floats per half-res pixel (alpha gamma beta kappa, s0..s3,
+ * c0..c3). Either pointer may be NULL. */
+int hush_trainer_par(hush_trainer_t *t, float *par, float *dpar);
+/* The FP32 TAA output of the last frame (rgba, W x H). */
+int hush_trainer_output(hush_trainer_t *t, float *out);
+/* Adam on the accumulated gradient (clipped to global norm `clip` if > 0), then zero it; *grad_norm = its norm. */
+int hush_trainer_step(hush_trainer_t *t, float lr, float beta1, float beta2, float eps, float clip, void *stream,
+                      double *grad_norm);
+/* Round the master weights to the f16 blob, install it in the denoiser and copy it to blob (if not NULL). */
+int hush_trainer_export(hush_trainer_t *t, uint16_t *blob);
+
 /* ---- SVGF baseline (src/denoise/svgf.js) ---------------------------------------------------------------------- */
 /* SVGFOptions (src/index.d.ts:63-72, svgf.js:278-281). iterations must be 1..5 (the reference's uniform array
  * holds 5 a-trous iterations, svgf.js:294). */

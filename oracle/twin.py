@@ -1,0 +1,235 @@
+"""FP64 restatement of the training twin (torch autograd): TEST INFRASTRUCTURE ONLY.
+
+The twin is the frame after TEMPORAL without f16 storage rounding: the MLP on FP32 master weights and its heads
+(src/denoise/hush.js:683-704, 357-362), the mid levels mid1-mid3 (hush.js:366, 753-754 via atrousFn 431-476), the
+fine level and recombination (hush.js:578-620) and TAA (hush.js:649-676), followed by the training loss. Its inputs
+are the frame's state as the CUDA trainer leaves it (features F0..F3, A0, key, coarse level, history, G-buffer). The
+autograd gradient of this float64 graph is the reference the hand-written CUDA adjoint is checked against.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+LUM = (0.2126, 0.7152, 0.0722)
+W1o, B1o = 0, 320
+W2o, B2o = 336, 592
+W3o, B3o = 608, 800
+
+
+def _t(a):
+    return torch.as_tensor(np.asarray(a, dtype=np.float64))
+
+
+def lum(c):
+    return c[..., 0] * LUM[0] + c[..., 1] * LUM[1] + c[..., 2] * LUM[2]
+
+
+def oct_dec(ex, ey):
+    vz = 1.0 - ex.abs() - ey.abs()
+    t = torch.clamp(-vz, min=0.0)
+    vx = ex + torch.where(ex >= 0, -t, t)
+    vy = ey + torch.where(ey >= 0, -t, t)
+    n = torch.stack([vx, vy, vz], -1)
+    return n / torch.clamp(n.norm(dim=-1, keepdim=True), min=1e-20)
+
+
+def pow128(x):
+    for _ in range(7):
+        x = x * x
+    return x
+
+
+def gather(img, yy, xx):
+    return img[yy.clamp(0, img.shape[0] - 1), xx.clamp(0, img.shape[1] - 1)]
+
+
+def filt(A, G, s, c, step, pref):
+    """atrousFn with R = 1 at every pixel of a (H, W) level; A (H, W, 4) colour + variance, G (H, W, 4) normal +
+    depth, s / c (H, W). Clamp-to-edge tiles, taps outside the image or on sky skipped."""
+    H, W = A.shape[:2]
+    ys, xs = torch.meshgrid(torch.arange(H), torch.arange(W), indexing="ij")
+    gp, cen = G, A
+    if pref:
+        def a(dx, dy):
+            return gather(A, ys + dy, xs + dx)[..., 3]
+        gv = 0.0625 * (a(-1, -1) + a(1, -1) + a(-1, 1) + a(1, 1)) + 0.125 * (a(0, -1) + a(-1, 0) + a(1, 0) + a(0, 1)) \
+            + 0.25 * cen[..., 3]
+    else:
+        gv = cen[..., 3]
+    lc = lum(cen)
+    sl = s / (torch.sqrt(torch.clamp(gv, min=1e-12)) + 1e-6)
+    zl, zr = gather(G, ys, xs - 1)[..., 3], gather(G, ys, xs + 1)[..., 3]
+    zu, zd = gather(G, ys - 1, xs)[..., 3], gather(G, ys + 1, xs)[..., 3]
+    big = torch.full_like(zl, 1e9)
+    gx = torch.minimum(torch.where(zr > 0, (zr - gp[..., 3]).abs(), big), torch.where(zl > 0, (zl - gp[..., 3]).abs(), big))
+    gy = torch.minimum(torch.where(zd > 0, (zd - gp[..., 3]).abs(), big), torch.where(zu > 0, (zu - gp[..., 3]).abs(), big))
+    zg = torch.minimum(torch.maximum(gx, gy), gp[..., 3])
+    cw = 0.25 * c
+    Wt = cw
+    S = cen[..., :3] * cw[..., None]
+    V = cen[..., 3] * cw * cw
+    for dy in (-1, 0, 1):
+        for dx in (-1, 0, 1):
+            if dx == 0 and dy == 0:
+                continue
+            hh = (0.5 if dx == 0 else 0.25) * (0.5 if dy == 0 else 0.25)
+            tx, ty = xs + dx * step, ys + dy * step
+            gq, cq = gather(G, ty, tx), gather(A, ty, tx)
+            ok = (tx >= 0) & (ty >= 0) & (tx < W) & (ty < H) & (gq[..., 3] >= 0)
+            iz = 1.0 / (zg * (math.sqrt(dx * dx + dy * dy) * step) + 1e-3)
+            wq = hh * pow128(torch.clamp((gq[..., :3] * gp[..., :3]).sum(-1), min=0.0)) * torch.exp(
+                -(gq[..., 3] - gp[..., 3]).abs() * iz - sl * (lum(cq) - lc).abs())
+            wq = torch.where(ok, wq, torch.zeros_like(wq))
+            Wt = Wt + wq
+            S = S + wq[..., None] * cq[..., :3]
+            V = V + wq * wq * cq[..., 3]
+    return torch.cat([S / Wt[..., None], (V / (Wt * Wt))[..., None]], -1)
+
+
+def jbw(frx, fry, j, nq, zq, n, z):
+    wb = (frx if (j & 1) else 1.0 - frx) * (fry if (j >> 1) else 1.0 - fry)
+    dn = torch.clamp((nq * n).sum(-1), min=0.0)
+    dn4 = (dn * dn) * (dn * dn)
+    return wb * torch.exp(-(zq - z).abs() / (0.05 * z + 1e-3)) * dn4 * dn4
+
+
+def tm(c):
+    return c / (1.0 + lum(c))[..., None]
+
+
+def to_ycocg(c):
+    r, g, b = c[..., 0], c[..., 1], c[..., 2]
+    return torch.stack([r * 0.25 + g * 0.5 + b * 0.25, r * 0.5 - b * 0.5, -r * 0.25 + g * 0.5 - b * 0.25], -1)
+
+
+def from_ycocg(c):
+    x, y, z = c[..., 0], c[..., 1], c[..., 2]
+    return torch.stack([x + y - z, x + z, x - y - z], -1)
+
+
+def unpack_half(a):
+    """(h, w, 8) float16 array -> float64 tensor."""
+    return _t(np.asarray(a, np.float16).astype(np.float64))
+
+
+def twin_loss(st: dict, theta, lambda_t=0.0, return_all=False):
+    """Loss of one frame. st: numpy arrays F0..F3 (h, w, 8) f16, A0 / key / material / emission / motion / taa_prev
+    (H, W, 4), C0 / CG (qh, qw, 4), clean / clean_prev (H, W, 3) f32, out_prev (H, W, 4) f32 or None, reset (bool).
+    theta: float64 tensor (812,) (may require grad)."""
+    F0, F1, F2, F3 = (unpack_half(st[k]) for k in ("F0", "F1", "F2", "F3"))
+    H2, W2 = F0.shape[:2]
+    feats = torch.cat([F0, F1, F2[..., :4]], -1)[..., :20]
+    guide_n = oct_dec(F3[..., 0], F3[..., 1])
+    Gh = torch.cat([guide_n, F3[..., 2:3]], -1)
+    sky_h = F3[..., 2] < 0
+    Ah = F2[..., 4:8]
+    w = theta
+    M1, b1 = w[W1o:B1o].view(16, 20), w[B1o:W2o]
+    M2, b2 = w[W2o:B2o].view(16, 16), w[B2o:W3o]
+    M3, b3 = w[W3o:B3o].view(12, 16), w[B3o:B3o + 12]
+    h1 = torch.relu(feats @ M1.T + b1)
+    h2 = torch.relu(h1 @ M2.T + b2)
+    o = h2 @ M3.T + b3
+    sig = torch.sigmoid
+    par = torch.stack([1 / 32 + (31 / 32) * sig(o[..., 0]), 0.5 + 7.5 * sig(o[..., 1]), sig(o[..., 2]), sig(o[..., 3])]
+                      + [0.25 * torch.exp(torch.clamp(o[..., 4 + k], -5, 5)) for k in range(4)]
+                      + [torch.exp(torch.clamp(o[..., 8 + k], -4, 4)) for k in range(4)], -1)
+    par = torch.where(sky_h[..., None], torch.zeros_like(par), par)
+    z4 = torch.zeros(H2, W2, 4, dtype=torch.float64)
+    B1 = torch.where(sky_h[..., None], z4, filt(Ah, Gh, par[..., 5], par[..., 9], 1, True))
+    B2 = torch.where(sky_h[..., None], z4, filt(B1, Gh, par[..., 6], par[..., 10], 2, False))
+    B3 = torch.where(sky_h[..., None], z4, filt(B2, Gh, par[..., 7], par[..., 11], 4, False))
+    # fine level at full resolution
+    A0 = _t(st["A0"])
+    key = _t(st["key"])
+    H, W = A0.shape[:2]
+    G = torch.cat([oct_dec(key[..., 0], key[..., 1]), key[..., 2:3]], -1)
+    ys, xs = torch.meshgrid(torch.arange(H), torch.arange(W), indexing="ij")
+    hp_y, hp_x = ys >> 1, xs >> 1
+    p_full = par[hp_y, hp_x]
+    A1 = filt(A0, G, p_full[..., 4], p_full[..., 8], 1, True)
+    sky = G[..., 3] < 0
+    f = A1[..., :3]
+    n, z = G[..., :3], G[..., 3]
+    hposx, hposy = (xs.double() + 0.5) / 2.0 - 0.5, (ys.double() + 0.5) / 2.0 - 0.5
+    hbx, hby = torch.floor(hposx), torch.floor(hposy)
+    uB = torch.zeros(H, W, 3, dtype=torch.float64)
+    uA = torch.zeros(H, W, 3, dtype=torch.float64)
+    swh = torch.zeros(H, W, dtype=torch.float64)
+    hsx, hsy = (W + 1) // 2, (H + 1) // 2
+    for j in range(4):
+        qx, qy = hbx.long() + (j & 1), hby.long() + (j >> 1)
+        ok = (qx >= 0) & (qy >= 0) & (qx < hsx) & (qy < hsy)
+        g = gather(Gh, qy, qx)
+        ok = ok & (g[..., 3] >= 0)
+        wj = jbw(hposx - hbx, hposy - hby, j, g[..., :3], g[..., 3], n, z)
+        wj = torch.where(ok, wj, torch.zeros_like(wj))
+        swh = swh + wj
+        uB = uB + wj[..., None] * gather(B3, qy, qx)[..., :3]
+        uA = uA + wj[..., None] * gather(Ah, qy, qx)[..., :3]
+    mid = swh > 1e-4
+    kappa, beta = p_full[..., 3], p_full[..., 2]
+    swh_s = torch.where(mid, swh, torch.ones_like(swh))
+    ill = torch.where(mid[..., None], uB / swh_s[..., None] + kappa[..., None] * (f - uA / swh_s[..., None]), f)
+    C0, CG = _t(st["C0"]), _t(st["CG"])
+    CGd = torch.cat([oct_dec(CG[..., 0], CG[..., 1]), CG[..., 2:3]], -1)
+    cposx, cposy = (xs.double() + 0.5) / 4.0 - 0.5, (ys.double() + 0.5) / 4.0 - 0.5
+    cbx, cby = torch.floor(cposx), torch.floor(cposy)
+    uC = torch.zeros(H, W, 3, dtype=torch.float64)
+    swq = torch.zeros(H, W, dtype=torch.float64)
+    qsx, qsy = (W + 3) // 4, (H + 3) // 4
+    for j in range(4):
+        qx, qy = cbx.long() + (j & 1), cby.long() + (j >> 1)
+        ok = (qx >= 0) & (qy >= 0) & (qx < qsx) & (qy < qsy)
+        g = gather(CGd, qy, qx)
+        ok = ok & (g[..., 3] >= 0)
+        wj = jbw(cposx - cbx, cposy - cby, j, g[..., :3], g[..., 3], n, z)
+        wj = torch.where(ok, wj, torch.zeros_like(wj))
+        swq = swq + wj
+        uC = uC + wj[..., None] * gather(C0, qy, qx)[..., :3]
+    coarse = swq > 1e-4
+    up = torch.where(coarse[..., None], uC / torch.where(coarse, swq, torch.ones_like(swq))[..., None], ill)
+    ill2 = ill + (up - ill) * beta[..., None]
+    alb, emi = _t(st["material"])[..., :3], _t(st["emission"])[..., :3]
+    X = torch.where(sky[..., None], emi, ill2 * alb + emi)
+    # TAA
+    cur = tm(X)
+    if st.get("reset", False):
+        res = cur
+    else:
+        Y = to_ycocg(tm(X))
+        win = [gather(Y, ys + dy, xs + dx) for dy in (-1, 0, 1) for dx in (-1, 0, 1)]
+        m1 = sum(win) / 9.0
+        v3 = sum((q - m1) ** 2 for q in win) / 9.0
+        sd = torch.sqrt(torch.clamp(v3, min=1e-12))
+        mv = _t(st["motion"])
+        uvx, uvy = (xs.double() + 0.5 + mv[..., 0]) / W, (ys.double() + 0.5 + mv[..., 1]) / H
+        inside = (uvx >= 0) & (uvy >= 0) & (uvx <= 1) & (uvy <= 1)
+        ppx, ppy = uvx * W - 0.5, uvy * H - 0.5
+        bx, by = torch.floor(ppx), torch.floor(ppy)
+        fx, fy = ppx - bx, ppy - by
+        prev = _t(st["taa_prev"])[..., :3]
+        hist = 0
+        for j in range(4):
+            ox, oy = j & 1, j >> 1
+            wb = (fx if ox else 1 - fx) * (fy if oy else 1 - fy)
+            hist = hist + wb[..., None] * gather(prev, by.long() + oy, bx.long() + ox)
+        hh = to_ycocg(tm(hist))
+        hh = torch.minimum(torch.maximum(hh, m1 - 1.25 * sd), m1 + 1.25 * sd)
+        hr = from_ycocg(hh)
+        res = torch.where(inside[..., None], hr + (cur - hr) * 0.1, cur)
+    out = res / torch.clamp(1.0 - lum(res), min=1e-4)[..., None]
+    clean = _t(st["clean"])
+    den = clean.abs() + 1e-2
+    N = 3.0 * H * W
+    loss = ((out - clean).abs() / den).sum() / N
+    if st.get("out_prev") is not None and lambda_t > 0 and not st.get("reset", False):
+        op = _t(st["out_prev"])[..., :3]
+        cp = _t(st["clean_prev"])
+        loss = loss + lambda_t * (((out - op) - (clean - cp)).abs() / den).sum() / N
+    if return_all:
+        return loss, {"par": par, "out": out, "X": X, "A1": A1, "B3": B3}
+    return loss
