@@ -84,6 +84,7 @@ _SIGS = {
     "hush_trainer_frame": (C.c_int, [_P, C.POINTER(HushInputs), C.c_void_p, C.c_void_p, C.c_float, C.c_int, _P,
                                      C.POINTER(C.c_double)]),
     "hush_trainer_end_frame": (C.c_int, [_P]),
+    "hush_trainer_loss_sum": (C.c_int, [_P, _P, C.POINTER(C.c_double)]),
     "hush_trainer_reset": (C.c_int, [_P]),
     "hush_trainer_zero_grad": (C.c_int, [_P, _P]),
     "hush_trainer_grad": (C.c_int, [_P, C.c_void_p]),

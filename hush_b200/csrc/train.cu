@@ -4,7 +4,7 @@
 // smooth function): the MLP on FP32 master weights (hush.js:683-704 / 357-362), the mid levels mid1-mid3 (hush.js:366,
 // 753-754), the fine level + recombination (hush.js:578-620) and TAA (hush.js:649-676). TEMPORAL and the coarse levels
 // run as the reference passes (their outputs do not depend on the weights within a frame). The loss is the relative L1
-// of the TAA output against the noise-free image plus a temporal-gradient term.
+// of the TAA output against the noise-free image (clipped at 1 per value) plus a temporal-gradient term.
 //
 // Gradients are exact for one frame with the temporal history held fixed (the history buffers are inputs of the
 // frame); over a window the per-frame gradients are summed (truncated backpropagation through time: the alpha / gamma
@@ -469,8 +469,9 @@ __global__ void k_taa_fwd(const TwinFrame T) {
 }
 
 // ------------------------------------------------------------------------------------------------ loss
-// L = (1 / 3N) sum |out - clean| / (|clean| + 1e-2) + lambda (1 / 3N) sum |d out - d clean| / (|clean| + 1e-2),
-// d = difference to the previous frame. Writes dL/dout (into gT, as the seed of the TAA adjoint) and per-CTA FP64
+// L = (1 / 3N) sum min(|out - clean| / (|clean| + 1e-2), 1) + lambda (1 / 3N) sum min(|d out - d clean| /
+// (|clean| + 1e-2), 1), d = difference to the previous frame. The clip at 1 keeps the TAA's itm singularity (outputs
+// up to 1e4 where the clipped history reaches luminance 1, hush.js:636) from dominating the gradient. Writes dL/dout (into gT, as the seed of the TAA adjoint) and per-CTA FP64
 // partial sums.
 __global__ void k_loss(const TwinFrame T, int backward) {
   const HushFrame &f = T.f;
@@ -483,14 +484,16 @@ __global__ void k_loss(const TwinFrame T, int backward) {
     for (int c = 0; c < 3; c++) {
       const float cl = T.clean[3 * i + c], den = fabsf(cl) + 1e-2f;
       const float d = ov[c] - cl;
-      l += fabs((double)d) / den;
-      g[c] = sgn(d) / den;
+      const double e = fabs((double)d) / den;
+      l += e < 1.0 ? e : 1.0;
+      g[c] = e < 1.0 ? sgn(d) / den : 0.0f;
       if (T.has_prev) {
         const float4 op = T.out_prev[i];
         const float opv[3] = {op.x, op.y, op.z};
         const float dd = (ov[c] - opv[c]) - (cl - T.clean_prev[3 * i + c]);
-        l += (double)T.lambda_t * fabs((double)dd) / den;
-        g[c] += T.lambda_t * sgn(dd) / den;
+        const double et = fabs((double)dd) / den;
+        l += (double)T.lambda_t * (et < 1.0 ? et : 1.0);
+        g[c] += et < 1.0 ? T.lambda_t * sgn(dd) / den : 0.0f;
       }
     }
     l *= T.inv_n;
@@ -508,7 +511,7 @@ __global__ void k_loss(const TwinFrame T, int backward) {
   }
 }
 
-__global__ void k_reduce_f64(const double *partials, int n, double *out) {
+__global__ void k_reduce_f64(const double *partials, int n, double *out, double *acc) {
   double v = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) v += partials[i];
   for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
@@ -518,7 +521,10 @@ __global__ void k_reduce_f64(const double *partials, int n, double *out) {
   if (threadIdx.x < 32) {
     double u = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
     for (int off = 16; off > 0; off >>= 1) u += __shfl_down_sync(0xffffffffu, u, off);
-    if (threadIdx.x == 0) *out = u;
+    if (threadIdx.x == 0) {
+      *out = u;
+      *acc += u;
+    }
   }
 }
 
@@ -752,7 +758,7 @@ struct hush_trainer_s {
   hush_t *h = nullptr;
   int W = 0, H = 0, W2 = 0, H2 = 0;
   float *theta = nullptr, *m = nullptr, *v = nullptr;
-  double *grad = nullptr, *loss = nullptr, *loss_partials = nullptr;
+  double *grad = nullptr, *loss = nullptr, *loss_acc = nullptr, *loss_partials = nullptr;
   float4 *par = nullptr, *B[3] = {}, *A1 = nullptr, *X = nullptr, *out[2] = {}, *gT = nullptr, *gT2 = nullptr,
          *dB[3] = {}, *dpar = nullptr;
   float *partials = nullptr;
@@ -776,7 +782,7 @@ extern "C" int hush_trainer_create(hush_t *h, const float *theta, hush_trainer_t
   t->n_mlp_ctas = (int)((half + MB_ROWS - 1) / MB_ROWS);
   t->n_loss_ctas = (int)((full + 255) / 256);
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-  const size_t bytes = al(NW * 4) * 3 + al(NW * 8) + al(8) + al(t->n_loss_ctas * 8) + al(half * 48) * 2 +
+  const size_t bytes = al(NW * 4) * 3 + al(NW * 8) + al(8) * 2 + al(t->n_loss_ctas * 8) + al(half * 48) * 2 +
                        al(half * 16) * 6 + al(full * 16) * 6 + al((size_t)t->n_mlp_ctas * NW * 4);
   cudaError_t e = cudaMalloc(&t->pool, bytes);
   if (e != cudaSuccess) { delete t; return hush_cuda_fail(h, e, "cudaMalloc of the trainer"); }
@@ -784,7 +790,7 @@ extern "C" int hush_trainer_create(hush_t *h, const float *theta, hush_trainer_t
   size_t off = 0;
   auto take = [&](size_t b) { char *p = t->pool + off; off += al(b); return p; };
   t->theta = (float *)take(NW * 4); t->m = (float *)take(NW * 4); t->v = (float *)take(NW * 4);
-  t->grad = (double *)take(NW * 8); t->loss = (double *)take(8);
+  t->grad = (double *)take(NW * 8); t->loss = (double *)take(8); t->loss_acc = (double *)take(8);
   t->loss_partials = (double *)take(t->n_loss_ctas * 8);
   t->par = (float4 *)take(half * 48); t->dpar = (float4 *)take(half * 48);
   for (int i = 0; i < 3; i++) { t->B[i] = (float4 *)take(half * 16); t->dB[i] = (float4 *)take(half * 16); }
@@ -856,7 +862,7 @@ extern "C" int hush_trainer_frame(hush_trainer_t *t, const hush_inputs *in, cons
   k_fine_fwd<<<gf, blk, 0, st>>>(T);
   k_taa_fwd<<<gf, blk, 0, st>>>(T);
   k_loss<<<t->n_loss_ctas, 256, 0, st>>>(T, backward);
-  k_reduce_f64<<<1, 256, 0, st>>>(t->loss_partials, t->n_loss_ctas, t->loss);
+  k_reduce_f64<<<1, 256, 0, st>>>(t->loss_partials, t->n_loss_ctas, t->loss, t->loss_acc);
   if (backward) {
     cudaMemsetAsync(t->gT2, 0, (size_t)full * 16, st);
     cudaMemsetAsync(t->dpar, 0, (size_t)half * 48, st);
@@ -877,6 +883,16 @@ extern "C" int hush_trainer_frame(hush_trainer_t *t, const hush_inputs *in, cons
     if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "reading the loss");
   }
   return HUSH_OK;
+}
+
+// Sum of the losses of the frames since the last call (read and zeroed; synchronises the stream).
+extern "C" int hush_trainer_loss_sum(hush_trainer_t *t, void *stream, double *out) {
+  if (!t || !out) return hush_fail(t ? t->h : nullptr, HUSH_ERR_ARG, "hush_trainer_loss_sum: NULL argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(out, t->loss_acc, 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(t->loss_acc, 0, 8, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, "reading the loss sum");
 }
 
 extern "C" int hush_trainer_end_frame(hush_trainer_t *t) {

@@ -54,15 +54,22 @@ class Trainer:
             raise HushError(L.lib().hush_last_error(self.hush._h).decode())
 
     def frame(self, inputs: dict, clean, clean_prev=None, lambda_t: float = 0.0, backward: bool = True,
-              stream=None) -> float:
-        """One frame: forward, loss and (if backward) the gradient added to the accumulator. Does not advance."""
+              stream=None, sync: bool = True):
+        """One frame: forward, loss and (if backward) the gradient added to the accumulator. Does not advance.
+        Returns the loss (synchronising) or None with sync=False (the loss is summed on the device)."""
         _fill_inputs(self._inp, inputs)
         loss = C.c_double()
         self._check(L.lib().hush_trainer_frame(self._t, C.byref(self._inp), clean.data_ptr(),
                                                clean_prev.data_ptr() if clean_prev is not None else None,
                                                float(lambda_t), 1 if backward else 0,
-                                               C.c_void_p(_stream_handle(stream)), C.byref(loss)))
-        return loss.value
+                                               C.c_void_p(_stream_handle(stream)), C.byref(loss) if sync else None))
+        return loss.value if sync else None
+
+    def loss_sum(self, stream=None) -> float:
+        """Sum of the frame losses since the previous call."""
+        v = C.c_double()
+        self._check(L.lib().hush_trainer_loss_sum(self._t, C.c_void_p(_stream_handle(stream)), C.byref(v)))
+        return v.value
 
     def end_frame(self):
         self._check(L.lib().hush_trainer_end_frame(self._t))
@@ -163,14 +170,14 @@ def train(cfg: TrainConfig, log_every: int = 100, on_log=None, time_budget_s: fl
     t0 = time.time()
     for step in range(cfg.steps):
         ts = time.perf_counter()
-        loss_sum = 0.0
         for _ in range(cfg.batch):
             seed = int(rng.integers(0, cfg.seeds))
             win = window(cfg, seed, bufs)
             tr.reset()
             for t, fr in enumerate(win):
-                loss_sum += tr.frame(fr, fr["clean"], win[t - 1]["clean"] if t else None, cfg.lambda_t, True)
+                tr.frame(fr, fr["clean"], win[t - 1]["clean"] if t else None, cfg.lambda_t, True, sync=False)
                 tr.end_frame()
+        loss_sum = tr.loss_sum()
         gn = tr.step(cfg.lr, clip=cfg.clip)
         torch.cuda.synchronize()
         ms = (time.perf_counter() - ts) * 1e3
@@ -181,3 +188,92 @@ def train(cfg: TrainConfig, log_every: int = 100, on_log=None, time_budget_s: fl
         if time_budget_s and time.time() - t0 > time_budget_s:
             break
     return tr, hush, hist
+
+
+def evaluate(weights_blob: np.ndarray | None, seeds, size: int = 384, frames: int = 8, svgf: bool = False):
+    """Error of the inference path on held-out windows: clipped relative L1 against the noise-free image and temporal
+    flicker (clipped relative L1 of frame differences), averaged over frames 1.. of each window. weights_blob = None
+    uses the built-in weights; svgf = True runs the SVGF baseline instead."""
+    import torch
+
+    from .svgf import SVGF
+
+    cfg = TrainConfig(size=size, frames=frames)
+    rel, flick = [], []
+    for seed in seeds:
+        win = window(cfg, int(seed))
+        if svgf:
+            den = SVGF(0, size, size)
+        else:
+            opts = {"width": size, "height": size}
+            if weights_blob is not None:
+                opts["weights"] = weights_blob.tobytes()
+            den = Hush(0, opts)
+        prev_out, prev_clean = None, None
+        for t, fr in enumerate(win):
+            if svgf:
+                g = dict(fr)
+                g["prevNormalDepth"] = win[t - 1]["normalDepth"] if t else fr["normalDepth"]
+                g["prevMotion"] = win[t - 1]["motion"] if t else fr["motion"]
+                out = den.encode(g).float()[..., :3]
+            else:
+                out = den.denoise(fr).float()[..., :3]
+            clean = fr["clean"]
+            d = clean.abs() + 1e-2
+            if t > 0:
+                rel.append(torch.clamp((out - clean).abs() / d, max=1.0).mean().item())
+                flick.append(torch.clamp(((out - prev_out) - (clean - prev_clean)).abs() / d, max=1.0).mean().item())
+            prev_out, prev_clean = out.clone(), clean
+        den.destroy()
+    return {"rel_l1": float(np.mean(rel)), "flicker": float(np.mean(flick)), "windows": len(seeds)}
+
+
+def main(argv=None):
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description="train the parameter MLP on device and evaluate against SVGF")
+    ap.add_argument("--steps", type=int, default=5000)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--size", type=int, default=384)
+    ap.add_argument("--frames", type=int, default=8)
+    ap.add_argument("--seeds", type=int, default=2048)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--time-budget", type=float, default=None, help="stop after this many seconds of training")
+    ap.add_argument("--eval-seeds", type=int, default=64)
+    ap.add_argument("--out", default=None, help="write the summary JSON here")
+    ap.add_argument("--weights-out", default=None, help="write the trained f16 blob here")
+    a = ap.parse_args(argv)
+    cfg = TrainConfig(size=a.size, frames=a.frames, seeds=a.seeds, batch=a.batch, steps=a.steps, lr=a.lr)
+    log = []
+
+    def on_log(rec):
+        log.append(rec)
+        print(json.dumps(rec), flush=True)
+
+    tr, hush, hist = train(cfg, log_every=50, on_log=on_log, time_budget_s=a.time_budget)
+    blob = tr.export()
+    if a.weights_out:
+        blob.tofile(a.weights_out)
+    held_out = [1_000_000 + i for i in range(a.eval_seeds)]
+    res = {
+        "config": vars(a),
+        "steps_run": len(hist),
+        "train_step_ms_median": float(np.median([h["step_ms"] for h in hist[1:]] or [hist[0]["step_ms"]])),
+        "loss_first": hist[0]["loss"], "loss_last": float(np.mean([h["loss"] for h in hist[-20:]])),
+        "eval_trained": evaluate(blob, held_out, a.size, a.frames),
+        "eval_builtin": evaluate(None, held_out, a.size, a.frames),
+        "eval_svgf": evaluate(None, held_out, a.size, a.frames, svgf=True),
+        "log": log,
+    }
+    print(json.dumps({k: v for k, v in res.items() if k != "log"}), flush=True)
+    if a.out:
+        with open(a.out, "w") as f:
+            json.dump(res, f, indent=1)
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+
+    sys.exit(main())

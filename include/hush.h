@@ -131,8 +131,8 @@ int hush_buffer(hush_t *h, int id, void **dptr, int *width, int *height, int *te
 /* ---- training twin: forward / adjoint of the frame for on-device training of the parameter MLP --------------------
  * No reference counterpart as an API: the reference's weights were trained offline by a PyTorch copy of the passes
  * that it does not ship (README.md:137, hush.js:6-7). The twin runs the frame after TEMPORAL in FP32 without f16
- * storage rounding; the loss is relative L1 of the TAA output against the noise-free image plus lambda times the
- * same on frame differences. Gradients are exact for one frame with the temporal history held fixed; frames of a
+ * storage rounding; the loss is relative L1 of the TAA output against the noise-free image (clipped at 1 per value)
+ * plus lambda times the same on frame differences. Gradients are exact for one frame with the temporal history held fixed; frames of a
  * window accumulate (truncated backpropagation through time). Trainers are tied to one Hush instance (h = 16). */
 typedef struct hush_trainer_s hush_trainer_t;
 /* theta: 812 FP32 initial weights (W1 b1 W2 b2 W3 b3), NULL = the instance's current weights. */
@@ -144,6 +144,8 @@ void hush_trainer_destroy(hush_trainer_t *t);
 int hush_trainer_frame(hush_trainer_t *t, const hush_inputs *in, const float *clean, const float *clean_prev,
                        float lambda_t, int backward, void *stream, double *loss_out);
 int hush_trainer_end_frame(hush_trainer_t *t);
+/* Sum of the frame losses since the previous call (synchronises `stream`, then restarts the sum). */
+int hush_trainer_loss_sum(hush_trainer_t *t, void *stream, double *out);
 int hush_trainer_reset(hush_trainer_t *t);
 int hush_trainer_zero_grad(hush_trainer_t *t, void *stream);
 /* The accumulated weight gradient (812 doubles). */

@@ -129,9 +129,12 @@ class OracleHush:
         return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint16)), (h.value, w.value, c.value)).view(np.float16)
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            lib().ho_hush_destroy(self._h)
-            self._h = None
+        try:
+            if getattr(self, "_h", None):
+                lib().ho_hush_destroy(self._h)
+                self._h = None
+        except Exception:  # interpreter shutdown
+            pass
 
 
 class OracleSVGF:
@@ -155,9 +158,12 @@ class OracleSVGF:
         lib().ho_svgf_reset(self._h)
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            lib().ho_svgf_destroy(self._h)
-            self._h = None
+        try:
+            if getattr(self, "_h", None):
+                lib().ho_svgf_destroy(self._h)
+                self._h = None
+        except Exception:  # interpreter shutdown
+            pass
 
 
 def f2h_rz(x: float) -> int:

@@ -2,7 +2,7 @@
 
 The twin is the frame after TEMPORAL without f16 storage rounding: the MLP on FP32 master weights and its heads
 (src/denoise/hush.js:683-704, 357-362), the mid levels mid1-mid3 (hush.js:366, 753-754 via atrousFn 431-476), the
-fine level and recombination (hush.js:578-620) and TAA (hush.js:649-676), followed by the training loss. Its inputs
+fine level and recombination (hush.js:578-620) and TAA (hush.js:649-676), followed by the training loss (relative L1 per value, clipped at 1). Its inputs
 are the frame's state as the CUDA trainer leaves it (features F0..F3, A0, key, coarse level, history, G-buffer). The
 autograd gradient of this float64 graph is the reference the hand-written CUDA adjoint is checked against.
 """
@@ -67,6 +67,9 @@ def filt(A, G, s, c, step, pref):
     gx = torch.minimum(torch.where(zr > 0, (zr - gp[..., 3]).abs(), big), torch.where(zl > 0, (zl - gp[..., 3]).abs(), big))
     gy = torch.minimum(torch.where(zd > 0, (zd - gp[..., 3]).abs(), big), torch.where(zu > 0, (zu - gp[..., 3]).abs(), big))
     zg = torch.minimum(torch.maximum(gx, gy), gp[..., 3])
+    # sky centres are discarded by the caller; a positive depth keeps their weights finite (an infinite weight in a
+    # discarded torch.where branch still turns the zero gradient into NaN)
+    zg = torch.where(gp[..., 3] >= 0, zg, torch.ones_like(zg))
     cw = 0.25 * c
     Wt = cw
     S = cen[..., :3] * cw[..., None]
@@ -137,11 +140,14 @@ def twin_loss(st: dict, theta, lambda_t=0.0, return_all=False):
     par = torch.stack([1 / 32 + (31 / 32) * sig(o[..., 0]), 0.5 + 7.5 * sig(o[..., 1]), sig(o[..., 2]), sig(o[..., 3])]
                       + [0.25 * torch.exp(torch.clamp(o[..., 4 + k], -5, 5)) for k in range(4)]
                       + [torch.exp(torch.clamp(o[..., 8 + k], -4, 4)) for k in range(4)], -1)
+    # rows of sky blocks carry zeros; the levels see c = 1 there so that the masked-out branches stay finite (a 0/0
+    # in an unselected torch.where branch would turn its zero gradient into NaN)
+    par_f = torch.where(sky_h[..., None], torch.ones_like(par), par)
     par = torch.where(sky_h[..., None], torch.zeros_like(par), par)
     z4 = torch.zeros(H2, W2, 4, dtype=torch.float64)
-    B1 = torch.where(sky_h[..., None], z4, filt(Ah, Gh, par[..., 5], par[..., 9], 1, True))
-    B2 = torch.where(sky_h[..., None], z4, filt(B1, Gh, par[..., 6], par[..., 10], 2, False))
-    B3 = torch.where(sky_h[..., None], z4, filt(B2, Gh, par[..., 7], par[..., 11], 4, False))
+    B1 = torch.where(sky_h[..., None], z4, filt(Ah, Gh, par_f[..., 5], par_f[..., 9], 1, True))
+    B2 = torch.where(sky_h[..., None], z4, filt(B1, Gh, par_f[..., 6], par_f[..., 10], 2, False))
+    B3 = torch.where(sky_h[..., None], z4, filt(B2, Gh, par_f[..., 7], par_f[..., 11], 4, False))
     # fine level at full resolution
     A0 = _t(st["A0"])
     key = _t(st["key"])
@@ -150,10 +156,11 @@ def twin_loss(st: dict, theta, lambda_t=0.0, return_all=False):
     ys, xs = torch.meshgrid(torch.arange(H), torch.arange(W), indexing="ij")
     hp_y, hp_x = ys >> 1, xs >> 1
     p_full = par[hp_y, hp_x]
-    A1 = filt(A0, G, p_full[..., 4], p_full[..., 8], 1, True)
+    pf_full = par_f[hp_y, hp_x]
+    A1 = filt(A0, G, pf_full[..., 4], pf_full[..., 8], 1, True)
     sky = G[..., 3] < 0
     f = A1[..., :3]
-    n, z = G[..., :3], G[..., 3]
+    n, z = G[..., :3], torch.where(G[..., 3] >= 0, G[..., 3], torch.ones_like(G[..., 3]))  # sky: see filt()
     hposx, hposy = (xs.double() + 0.5) / 2.0 - 0.5, (ys.double() + 0.5) / 2.0 - 0.5
     hbx, hby = torch.floor(hposx), torch.floor(hposy)
     uB = torch.zeros(H, W, 3, dtype=torch.float64)
@@ -225,11 +232,11 @@ def twin_loss(st: dict, theta, lambda_t=0.0, return_all=False):
     clean = _t(st["clean"])
     den = clean.abs() + 1e-2
     N = 3.0 * H * W
-    loss = ((out - clean).abs() / den).sum() / N
+    loss = torch.clamp((out - clean).abs() / den, max=1.0).sum() / N
     if st.get("out_prev") is not None and lambda_t > 0 and not st.get("reset", False):
         op = _t(st["out_prev"])[..., :3]
         cp = _t(st["clean_prev"])
-        loss = loss + lambda_t * (((out - op) - (clean - cp)).abs() / den).sum() / N
+        loss = loss + lambda_t * torch.clamp(((out - op) - (clean - cp)).abs() / den, max=1.0).sum() / N
     if return_all:
         return loss, {"par": par, "out": out, "X": X, "A1": A1, "B3": B3}
     return loss

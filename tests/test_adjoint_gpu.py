@@ -45,16 +45,13 @@ def _capture(g, tr, host, t, lambda_t):
 def test_adjoint_matches_fp64_autograd():
     lam = 0.5
     g, tr, host, cleans, t = _setup(lambda_t=lam)
-    # previous frame's FP32 output for the temporal term
-    out_prev = tr.output() if False else None
     tr.zero_grad()
     loss = tr.frame(_dev(host[t]), cleans[t], cleans[t - 1], lam, backward=True)
     torch.cuda.synchronize()
     d_cuda = tr.grad()
     par_c, dpar_c = tr.par()
     st = _capture(g, tr, host, t, lam)
-    # the trainer's temporal term uses its own previous FP32 output; read it by re-running frame t-1 is not needed:
-    # compare without the temporal term through lambda = 0 on both sides below, and with it through FD
+    # the temporal term (lambda > 0) is covered by the finite-difference test; here lambda = 0 on both sides
     theta = torch.tensor(tr.theta.astype(np.float64), requires_grad=True)
     tr.zero_grad()
     loss0 = tr.frame(_dev(host[t]), cleans[t], None, 0.0, backward=True)
@@ -63,6 +60,7 @@ def test_adjoint_matches_fp64_autograd():
     parts["par"].retain_grad()
     lt.backward()
     d_ref = theta.grad.numpy()
+    assert np.isfinite(d_ref).all() and np.isfinite(d_cuda0).all()
     assert abs(loss0 - lt.item()) <= 1e-4 * abs(lt.item()), (loss0, lt.item())
     scale = np.abs(d_ref).max()
     err = np.abs(d_cuda0 - d_ref)
@@ -124,10 +122,10 @@ def test_fp64_reference_matches_its_own_finite_differences():
 def test_training_steps_reduce_the_loss():
     from hush_b200.train import TrainConfig, train
 
-    cfg = TrainConfig(size=64, frames=4, seeds=8, batch=2, steps=30, lr=3e-3, lambda_t=0.25)
+    cfg = TrainConfig(size=64, frames=4, seeds=8, batch=2, steps=60, lr=1e-3, lambda_t=0.25)
     tr, hush, hist = train(cfg)
-    first = np.mean([h["loss"] for h in hist[:5]])
-    last = np.mean([h["loss"] for h in hist[-5:]])
+    first = np.mean([h["loss"] for h in hist[:10]])
+    last = np.mean([h["loss"] for h in hist[-10:]])
     assert np.isfinite(last) and last < first, (first, last)
     blob = tr.export()
     assert blob.dtype == np.uint16 and blob.size == 812 and hush.hidden == 16
