@@ -142,6 +142,7 @@ def twin_loss(st: dict, theta, lambda_t=0.0, return_all=False):
                       + [torch.exp(torch.clamp(o[..., 8 + k], -4, 4)) for k in range(4)], -1)
     # rows of sky blocks carry zeros; the levels see c = 1 there so that the masked-out branches stay finite (a 0/0
     # in an unselected torch.where branch would turn its zero gradient into NaN)
+    par_raw = par
     par_f = torch.where(sky_h[..., None], torch.ones_like(par), par)
     par = torch.where(sky_h[..., None], torch.zeros_like(par), par)
     z4 = torch.zeros(H2, W2, 4, dtype=torch.float64)
@@ -238,5 +239,5 @@ def twin_loss(st: dict, theta, lambda_t=0.0, return_all=False):
         cp = _t(st["clean_prev"])
         loss = loss + lambda_t * torch.clamp(((out - op) - (clean - cp)).abs() / den, max=1.0).sum() / N
     if return_all:
-        return loss, {"par": par, "out": out, "X": X, "A1": A1, "B3": B3}
+        return loss, {"par": par, "par_raw": par_raw, "out": out, "X": X, "A1": A1, "B3": B3}
     return loss
