@@ -94,6 +94,7 @@ _SIGS = {
     "hush_trainer_step": (C.c_int, [_P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, _P,
                                     C.POINTER(C.c_double)]),
     "hush_trainer_export": (C.c_int, [_P, C.c_void_p]),
+    "hush_mlp_grad_noalloc": (C.c_int, [C.c_void_p] * 6 + [C.c_int, C.c_int, C.c_void_p, _P]),
     "svgf_options_default": (SvgfOptions, []),
     "svgf_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(SvgfOptions), C.c_int, C.POINTER(_P)]),
     "svgf_destroy": (None, [_P]),

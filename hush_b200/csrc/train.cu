@@ -980,3 +980,168 @@ extern "C" int hush_trainer_export(hush_trainer_t *t, uint16_t *blob) {
   if (blob) std::memcpy(blob, b.data(), NW * 2);
   return hush_set_weights(t->h, b.data(), NW);
 }
+
+// ------------------------------------------------------------------------------------------------ no-allocation
+// MLP weight gradient for callers that cannot allocate device memory: the same per-row adjoint as k_mlp_bwd, with
+// its per-CTA partial sums in a fixed file-scope device array instead of trainer-owned scratch. Some hosts forbid
+// device allocation after start-up (a render or training loop with a fixed memory budget, where cudaMalloc would
+// synchronise the device or fail under memory pressure mid-frame) or only lend the library buffers they own (an
+// engine or a browser GPU process that manages all device memory itself). The array is allocated when the library
+// is loaded, on every GPU that loads it, and stays until the process exits.
+namespace hush {
+namespace twin {
+
+constexpr int NA_ROWS = 64;                 // rows per chunk (one thread per row)
+constexpr int NA_MAX_CTAS = 512;            // CTAs, hence partial sums, at most
+constexpr long NA_MAX_ROWS = 16L << 20;     // 16,777,216 rows: a 4096 x 4096 half-resolution image
+
+// 512 partial sums x 812 floats = 1.66 MB, shared by every call on the device.
+static __device__ __align__(256) float g_noalloc_partials[NA_MAX_CTAS * NW];
+
+// Grid-stride over chunks of NA_ROWS rows; each CTA keeps its parameter sums in registers (thread t owns parameters
+// t, t + 64, ...) and writes them once to partials[blockIdx.x]: every slot the reduction reads is overwritten first,
+// so nothing has to start at zero.
+__global__ void __launch_bounds__(NA_ROWS) k_mlp_grad_noalloc(const uint4 *F0, const uint4 *F1, const uint4 *F2,
+                                                              const uint4 *F3, const float4 *dpar, const float *theta,
+                                                              int rows, float *partials) {
+  __shared__ float th[NW];
+  __shared__ float sd3[12][NA_ROWS], sd2[16][NA_ROWS], sd1[16][NA_ROWS], sf[20][NA_ROWS], sh1[16][NA_ROWS],
+      sh2[16][NA_ROWS];
+  for (int i = threadIdx.x; i < NW; i += NA_ROWS) th[i] = theta[i];
+  constexpr int PER = (NW + NA_ROWS - 1) / NA_ROWS;  // 13 parameters per thread
+  float acc[PER];
+#pragma unroll
+  for (int k = 0; k < PER; k++) acc[k] = 0.0f;
+  HushFrame f;
+  f.F0 = const_cast<uint4 *>(F0); f.F1 = const_cast<uint4 *>(F1); f.F2 = const_cast<uint4 *>(F2);
+  __syncthreads();
+  const int nchunks = (rows + NA_ROWS - 1) / NA_ROWS;
+  for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+    const int r = threadIdx.x, o = chunk * NA_ROWS + r;
+    float fe[20], h1[16], h2[16], out[12], d3[12], d2[16], d1[16];
+#pragma unroll
+    for (int i = 0; i < 20; i++) fe[i] = 0.f;
+#pragma unroll
+    for (int i = 0; i < 16; i++) h1[i] = h2[i] = d2[i] = d1[i] = 0.f;
+#pragma unroll
+    for (int i = 0; i < 12; i++) d3[i] = 0.f;
+    if (o < rows && f3_guide_tw(F3, o).w >= 0.0f) {
+      load_features(f, o, fe);
+      mlp_full(th, fe, h1, h2, out);
+      const float4 q0 = dpar[3 * o], q1 = dpar[3 * o + 1], q2 = dpar[3 * o + 2];
+      float4 p0, p1, p2;
+      mlp_heads(out, p0, p1, p2);
+      d3[2] = q0.z * p0.z * (1.0f - p0.z);
+      d3[3] = q0.w * p0.w * (1.0f - p0.w);
+      const float ps[4] = {p1.x, p1.y, p1.z, p1.w}, pc[4] = {p2.x, p2.y, p2.z, p2.w};
+      const float gs[4] = {q1.x, q1.y, q1.z, q1.w}, gc[4] = {q2.x, q2.y, q2.z, q2.w};
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        d3[4 + k] = fabsf(out[4 + k]) < 5.0f ? gs[k] * ps[k] : 0.0f;
+        d3[8 + k] = fabsf(out[8 + k]) < 4.0f ? gc[k] * pc[k] : 0.0f;
+      }
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        float a = 0.f;
+#pragma unroll
+        for (int j = 0; j < 12; j++) a += d3[j] * th[W3o + j * 16 + i];
+        d2[i] = h2[i] > 0.0f ? a : 0.0f;
+      }
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        float a = 0.f;
+#pragma unroll
+        for (int j = 0; j < 16; j++) a += d2[j] * th[W2o + j * 16 + i];
+        d1[i] = h1[i] > 0.0f ? a : 0.0f;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 12; i++) sd3[i][r] = d3[i];
+#pragma unroll
+    for (int i = 0; i < 16; i++) { sd2[i][r] = d2[i]; sd1[i][r] = d1[i]; sh1[i][r] = h1[i]; sh2[i][r] = h2[i]; }
+#pragma unroll
+    for (int i = 0; i < 20; i++) sf[i][r] = fe[i];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+      const int p = threadIdx.x + k * NA_ROWS;
+      if (p >= NW) continue;
+      const float *dv, *xv = nullptr;
+      if (p < B1o) { dv = sd1[p / 20]; xv = sf[p % 20]; }
+      else if (p < W2o) { dv = sd1[p - B1o]; }
+      else if (p < B2o) { const int q = p - W2o; dv = sd2[q / 16]; xv = sh1[q % 16]; }
+      else if (p < W3o) { dv = sd2[p - B2o]; }
+      else if (p < B3o) { const int q = p - W3o; dv = sd3[q / 16]; xv = sh2[q % 16]; }
+      else { dv = sd3[p - B3o]; }
+      float a = 0.f;
+      if (xv) for (int j = 0; j < NA_ROWS; j++) a += dv[j] * xv[j];
+      else for (int j = 0; j < NA_ROWS; j++) a += dv[j];
+      acc[k] += a;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int k = 0; k < PER; k++) {
+    const int p = threadIdx.x + k * NA_ROWS;
+    if (p < NW) partials[(size_t)blockIdx.x * NW + p] = acc[k];
+  }
+}
+
+// dtheta = sum over the grid's partials, in FP64 (overwrites dtheta)
+__global__ void k_mlp_grad_noalloc_reduce(const float *partials, int nparts, double *dtheta) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= NW) return;
+  double a = 0.0;
+  for (int c = 0; c < nparts; c++) a += (double)partials[(size_t)c * NW + p];
+  dtheta[p] = a;
+}
+
+}  // namespace twin
+}  // namespace hush
+
+#include <mutex>
+
+// Host-side address of g_noalloc_partials per device: the symbol's name in host code is only a stand-in, so the
+// device address is looked up once per device (with that device current) and cached.
+static std::mutex g_noalloc_mu;
+static float *g_noalloc_ptr[64] = {};
+
+extern "C" int hush_mlp_grad_noalloc(const void *F0, const void *F1, const void *F2, const void *F3,
+                                     const float *dpar, const float *theta, int width2, int height2, double *dtheta,
+                                     void *stream) {
+  using namespace hush::twin;
+  if (!F0 || !F1 || !F2 || !F3 || !dpar || !theta || !dtheta)
+    return hush_fail(nullptr, HUSH_ERR_ARG, "hush_mlp_grad_noalloc: NULL argument");
+  if (width2 <= 0 || height2 <= 0)
+    return hush_fail(nullptr, HUSH_ERR_ARG, "hush_mlp_grad_noalloc: bad size " + std::to_string(width2) + "x" +
+                                                std::to_string(height2));
+  const long rows = (long)width2 * (long)height2;
+  if (rows > NA_MAX_ROWS)
+    return hush_fail(nullptr, HUSH_ERR_ARG,
+                     "hush_mlp_grad_noalloc: " + std::to_string(rows) + " rows exceed the maximum of " +
+                         std::to_string(NA_MAX_ROWS) + " (the fixed scratch holds " + std::to_string(NA_MAX_CTAS) +
+                         " partial sums)");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return hush_cuda_fail(nullptr, e, "cudaGetDevice");
+  if (dev < 0 || dev >= 64) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_mlp_grad_noalloc: device ordinal >= 64");
+  float *partials = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void *p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+      if (e != cudaSuccess) return hush_cuda_fail(nullptr, e, "cudaGetSymbolAddress of the fixed scratch");
+      g_noalloc_ptr[dev] = (float *)p;
+    }
+    partials = g_noalloc_ptr[dev];
+  }
+  const int nchunks = (int)((rows + NA_ROWS - 1) / NA_ROWS);
+  const int grid = nchunks < NA_MAX_CTAS ? nchunks : NA_MAX_CTAS;
+  cudaStream_t st = (cudaStream_t)stream;
+  k_mlp_grad_noalloc<<<grid, NA_ROWS, 0, st>>>((const uint4 *)F0, (const uint4 *)F1, (const uint4 *)F2,
+                                               (const uint4 *)F3, (const float4 *)dpar, theta, (int)rows, partials);
+  k_mlp_grad_noalloc_reduce<<<(NW + 127) / 128, 128, 0, st>>>(partials, grid, dtheta);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(nullptr, e, "hush_mlp_grad_noalloc launch");
+}

@@ -163,6 +163,19 @@ int hush_trainer_step(hush_trainer_t *t, float lr, float beta1, float beta2, flo
 /* Round the master weights to the f16 blob, install it in the denoiser and copy it to blob (if not NULL). */
 int hush_trainer_export(hush_trainer_t *t, uint16_t *blob);
 
+/* Weight gradient of the parameter MLP (812 doubles in dtheta, overwritten) from a half-resolution image of rows:
+ * packed features F0..F3 (16-byte texels, width2 x height2, as hush_buffer returns them), dL/dpar (12 floats per
+ * row, as hush_trainer_par lays them out) and FP32 weights theta (812). The same computation as the weight-gradient
+ * part of hush_trainer_frame, but it allocates nothing: no counterpart in the reference. It exists for callers that
+ * cannot allocate device memory after start-up (a render or training loop with a fixed memory budget, where an
+ * allocation would synchronise the device or fail mid-frame) or that only lend the library buffers they own. Its
+ * scratch is a fixed 1.66 MB device array (512 partial sums) that every GPU loading the library holds until exit;
+ * at most 16,777,216 rows (4096 x 4096) are accepted, larger sizes fail with HUSH_ERR_ARG. The first call on a device
+ * looks up that array's device address, so make it before any stream capture. Calls share the array: calls that
+ * overlap on the GPU (different streams, or different threads) race. Errors: hush_global_error(). */
+int hush_mlp_grad_noalloc(const void *F0, const void *F1, const void *F2, const void *F3, const float *dpar,
+                          const float *theta, int width2, int height2, double *dtheta, void *stream);
+
 /* ---- SVGF baseline (src/denoise/svgf.js) ---------------------------------------------------------------------- */
 /* SVGFOptions (src/index.d.ts:63-72, svgf.js:278-281). iterations must be 1..5 (the reference's uniform array
  * holds 5 a-trous iterations, svgf.js:294). */
