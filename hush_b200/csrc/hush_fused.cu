@@ -107,13 +107,39 @@ struct K1Smem {
   float4 Ns[K1_NT];          // octDec(P2.xy) and 1 for pixels with a surface, zeros otherwise
 };
 
-// pixel() of hush.js:111-223 over the (r, g, b, L) tile; same arithmetic as temporal_pixel(). Writes A0, mom, key
-// and the pixel's entries of the shared feature-input arrays.
-HD_INL void temporal_pixel_fast(const HushFrame &f, int px, int py, K1Smem &S, int ti, int li) {
+// The loads of one pixel's pixel(): its G-buffer texels and the reprojection gathers of the previous frame's key,
+// colour and moments (bilinear footprint) and par0. Issued before the tile arithmetic and the barrier so that the
+// dependent-load chain (motion -> footprint) overlaps them.
+struct PixLoads {
+  uint2 nd, mv, mat, k4[4], c4[4], m4[4], pq;
+};
+
+HD_INL void pixel_issue(const HushFrame &f, int px, int py, PixLoads &L) {
+  const int W = f.W, H = f.H;
+  L.nd = __ldg(f.nd + py * f.p_nd + px);
+  L.mv = __ldg(f.mv + py * f.p_mv + px);
+  L.mat = __ldg(f.mat + py * f.p_mat + px);
+  if (f.reset) return;
+  const float4 mv = h4_to_f4(L.mv);
+  const float ppx = (float)px + mv.x, ppy = (float)py + mv.y;
+  const int bix = __float2int_rz(floorf(ppx)), biy = __float2int_rz(floorf(ppy));
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int q = clampi(biy + (i >> 1), 0, H - 1) * W + clampi(bix + (i & 1), 0, W - 1);
+    L.k4[i] = __ldg(f.key_prev + q);
+    L.c4[i] = __ldg(f.hist_prev + q);
+    L.m4[i] = __ldg(f.mom_prev + q);
+  }
+  const int cx = __float2int_rz(floorf(ppx + 0.5f)), cy = __float2int_rz(floorf(ppy + 0.5f));
+  L.pq = __ldg(f.par0_prev + (clampi(cy, 0, H - 1) >> 1) * f.W2 + (clampi(cx, 0, W - 1) >> 1));
+}
+
+// pixel() of hush.js:111-223 over the (r, g, b, L) tile from the preloaded texels; same arithmetic as
+// temporal_pixel(). Writes A0, mom, key and the pixel's entries of the shared feature-input arrays.
+HD_INL void temporal_pixel_fast(const HushFrame &f, int px, int py, K1Smem &S, int ti, int li, const PixLoads &PL) {
   constexpr int SW = K1_SW;
   const int W = f.W, H = f.H;
-  const uint2 ndr = __ldg(f.nd + py * f.p_nd + px), mvr = __ldg(f.mv + py * f.p_mv + px);
-  const float4 nd = h4_to_f4(ndr), mv = h4_to_f4(mvr);
+  const float4 nd = h4_to_f4(PL.nd), mv = h4_to_f4(PL.mv);
   const int oi = py * W + px;
   const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
   if (nd.w < 0.0f) {
@@ -124,8 +150,6 @@ HD_INL void temporal_pixel_fast(const HushFrame &f, int px, int py, K1Smem &S, i
     S.Ns[li] = z4;
     return;
   }
-  // reprojection gathers first (the dependent-load chain), kept packed until used
-  uint2 k4[4], c4[4], m4[4], pqr = make_uint2(0, 0);
   float fx = 0.f, fy = 0.f;
   int bix = 0, biy = 0, cx = 0, cy = 0;
   if (!f.reset) {
@@ -135,18 +159,11 @@ HD_INL void temporal_pixel_fast(const HushFrame &f, int px, int py, K1Smem &S, i
     fy = ppy - by;
     bix = __float2int_rz(bx);
     biy = __float2int_rz(by);
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-      const int q = clampi(biy + (i >> 1), 0, H - 1) * W + clampi(bix + (i & 1), 0, W - 1);
-      k4[i] = __ldg(f.key_prev + q);
-      c4[i] = __ldg(f.hist_prev + q);
-      m4[i] = __ldg(f.mom_prev + q);
-    }
     cx = __float2int_rz(floorf(ppx + 0.5f));
     cy = __float2int_rz(floorf(ppy + 0.5f));
-    pqr = __ldg(f.par0_prev + (clampi(cy, 0, H - 1) >> 1) * f.W2 + (clampi(cx, 0, W - 1) >> 1));
   }
-  const uint2 mrr = __ldg(f.mat + py * f.p_mat + px);
+  const uint2 *k4 = PL.k4, *c4 = PL.c4, *m4 = PL.m4;
+  const uint2 pqr = PL.pq, mrr = PL.mat;
   // 3x3 statistics of the illumination (valid neighbours), two passes
   const float4 illum = S.I[ti];
   const float l = illum.w;
@@ -384,14 +401,35 @@ __global__ void __launch_bounds__(K1_NT, 3)
   } else {
     for (int i = li; i < MLP_FP32_BLOB_BYTES / 16; i += NT) reinterpret_cast<uint4 *>(X_.w)[i] = __ldg(blob + i);
   }
-  // phase 1: illumination tile
+  // phase 1: all tile loads, the pixel's own loads and its reprojection gathers in flight together, then the
+  // illumination tile
   const int ox = blockIdx.x * K1_TW - 1, oy = blockIdx.y * K1_TH - 1;
-  for (int i = li; i < SW * SH; i += NT) {
+  constexpr int NIT = (SW * SH + NT - 1) / NT;
+  uint2 tn[NIT], tr[NIT], tmt[NIT];
+  bool tin[NIT];
+#pragma unroll
+  for (int it = 0; it < NIT; it++) {
+    const int i = li + it * NT;
     const int qx = ox + i % SW, qy = oy + i / SW;
+    tin[it] = i < SW * SH && qx >= 0 && qy >= 0 && qx < f.W && qy < f.H;
+    const int cxq = clampi(qx, 0, f.W - 1), cyq = clampi(qy, 0, f.H - 1);
+    tn[it] = __ldg(f.nd + cyq * f.p_nd + cxq);
+    tr[it] = __ldg(f.rad + cyq * f.p_rad + cxq);
+    tmt[it] = __ldg(f.mat + cyq * f.p_mat + cxq);
+  }
+  const int tx = li % K1_TW, ty = li / K1_TW;
+  const int px = blockIdx.x * K1_TW + tx, py = blockIdx.y * K1_TH + ty;
+  const bool pin = px < f.W && py < f.H;
+  PixLoads PL;
+  if (pin) pixel_issue(f, px, py, PL);
+#pragma unroll
+  for (int it = 0; it < NIT; it++) {
+    const int i = li + it * NT;
+    if (i >= SW * SH) continue;
     float4 e = make_float4(0.f, 0.f, 0.f, L_INVALID);
     float2 lq = make_float2(0.f, 0.f);
-    if (qx >= 0 && qy >= 0 && qx < f.W && qy < f.H && ldh(f.nd, qy * f.p_nd + qx).w >= 0.0f) {
-      const float4 r = ldh(f.rad, qy * f.p_rad + qx), m = ldh(f.mat, qy * f.p_mat + qx);
+    if (tin[it] && h4_to_f4(tn[it]).w >= 0.0f) {
+      const float4 r = h4_to_f4(tr[it]), m = h4_to_f4(tmt[it]);
       e.x = r.x / fmaxf(m.x, 1e-3f);
       e.y = r.y / fmaxf(m.y, 1e-3f);
       e.z = r.z / fmaxf(m.z, 1e-3f);
@@ -404,16 +442,12 @@ __global__ void __launch_bounds__(K1_NT, 3)
   __syncthreads();
   if constexpr (TC) umma::fence_after_sync();
   // phase 2: one pixel per thread
-  {
-    const int tx = li % K1_TW, ty = li / K1_TW;
-    const int px = blockIdx.x * K1_TW + tx, py = blockIdx.y * K1_TH + ty;
-    if (px < f.W && py < f.H) {
-      temporal_pixel_fast(f, px, py, S, (ty + 1) * SW + tx + 1, li);
-    } else {
-      const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-      S.P0[li] = z4; S.P1[li] = z4; S.P2[li] = make_float4(0.f, 0.f, -1.0f, 0.f); S.P3[li] = z4; S.P4[li] = z4;
-      S.Ns[li] = z4;
-    }
+  if (pin) {
+    temporal_pixel_fast(f, px, py, S, (ty + 1) * SW + tx + 1, li, PL);
+  } else {
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    S.P0[li] = z4; S.P1[li] = z4; S.P2[li] = make_float4(0.f, 0.f, -1.0f, 0.f); S.P3[li] = z4; S.P4[li] = z4;
+    S.Ns[li] = z4;
   }
   __syncthreads();
   // phase 3a: block features, one thread per block (warps 0-1)
