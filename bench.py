@@ -284,6 +284,32 @@ def run_ours(args):
     h2d = sum(host[0][n].numel() * 2 for n in scene.NAMES)
     d2h = out_host.numel() * 2
 
+    # ---- the other MLP form on the same frames, device-resident inputs (BF16 tensor-core MLP vs FP32 plain MLP)
+    alt = "bf16" if args.mlp != "bf16" else "fp32"
+    hush_alt = Hush(local, {"width": W, "height": H, "mlp": alt, "schedule": args.schedule, "graph": args.graph})
+    n_alt = min(args.steps, 512)
+
+    def step_alt(i):
+        k = i % nseq
+        if k == 32 or (k == 0 and i > 0):
+            hush_alt.reset()
+        return hush_alt.denoise(frames[k], stream=stream)
+
+    for i in range(args.warmup):
+        step_alt(i)
+    barrier()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    for i in range(args.warmup, args.warmup + n_alt):
+        step_alt(i)
+    g1.record(stream)
+    barrier()
+    alt_ms = max_over_ranks(g0.elapsed_time(g1)) / n_alt
+    hush_alt.destroy()
+
+    # ---- one training step of the parameter MLP (data-parallel over the ranks when N > 1)
+    train_ms = None if args.no_train else _train_step_ms(local, stream, barrier, max_over_ranks)
+
     if rank != 0:
         hush.destroy()
         if world > 1:
@@ -329,7 +355,11 @@ def run_ours(args):
         "e2e": {"value": round(e2e_ms / world, 4), "unit": "ms/frame", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": n_kernels * args.steps,
+        "mlp_forms": {args.mlp: {"ms_per_frame": round(ms_frame, 4)},
+                      alt: {"ms_per_frame": round(alt_ms, 4), "frames": n_alt}},
     }
+    if train_ms is not None:
+        line["train"] = train_ms
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = _cpu_baseline_sample()
     print(json.dumps(line), flush=True)
@@ -337,6 +367,52 @@ def run_ours(args):
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def _train_step_ms(local, stream, barrier, max_over_ranks, warmup=2, steps=5):
+    """Device time of one training step: 16 windows x 8 frames of 384x384 generated on the device, the twin's
+    forward + adjoint per frame, the gradient / loss all-reduce across ranks (N > 1) and the Adam step."""
+    import torch
+
+    from hush_b200 import Hush
+    from hush_b200.dp import DataParallel, finish_step
+    from hush_b200.scene import NAMES
+    from hush_b200.train import TrainConfig, Trainer, window, xavier_init
+
+    cfg = TrainConfig()
+    dp = DataParallel()
+    th = Hush(local, {"width": cfg.size, "height": cfg.size, "schedule": "passes"})
+    tr = Trainer(th, xavier_init(cfg.init_seed))
+    rng = dp.seed_rng(cfg.init_seed + 1)
+    bufs = [{n: torch.empty((cfg.size, cfg.size, 4), dtype=torch.float16, device=f"cuda:{local}") for n in NAMES}
+            for _ in range(cfg.frames)]
+    for b in bufs:
+        b["clean"] = torch.empty((cfg.size, cfg.size, 3), dtype=torch.float32, device=f"cuda:{local}")
+
+    def one():
+        for _ in range(cfg.batch):
+            win = window(cfg, dp.window_seed(rng, cfg.seeds), bufs)
+            tr.reset()
+            for t, fr in enumerate(win):
+                tr.frame(fr, fr["clean"], win[t - 1]["clean"] if t else None, cfg.lambda_t, True, sync=False)
+                tr.end_frame()
+        return finish_step(tr, dp, cfg.batch * cfg.frames, cfg.lr, cfg.clip)
+
+    for _ in range(warmup):
+        one()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    losses = [one()[0] for _ in range(steps)]
+    e1.record(stream)
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1)) / steps
+    tr.destroy()
+    th.destroy()
+    return {"step_ms": round(ms, 3), "steps": steps, "warmup": warmup, "world": dp.world,
+            "windows_per_step": cfg.batch * dp.world, "frames_per_step": cfg.batch * cfg.frames * dp.world,
+            "size": f"{cfg.size}x{cfg.size}", "loss_last": round(losses[-1], 5),
+            "note": "window generation, twin forward + adjoint of every frame, gradient all-reduce (N > 1), Adam"}
 
 
 def main(argv=None):
@@ -349,6 +425,7 @@ def main(argv=None):
     ap.add_argument("--schedule", default="fused", choices=["fused", "passes"])
     ap.add_argument("--graph", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-train", action="store_true", help="skip the training-step timing")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

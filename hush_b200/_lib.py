@@ -88,6 +88,7 @@ _SIGS = {
     "hush_trainer_reset": (C.c_int, [_P]),
     "hush_trainer_zero_grad": (C.c_int, [_P, _P]),
     "hush_trainer_grad": (C.c_int, [_P, C.c_void_p]),
+    "hush_trainer_accumulators": (C.c_int, [_P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "hush_trainer_theta": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
     "hush_trainer_par": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
     "hush_trainer_output": (C.c_int, [_P, C.c_void_p]),

@@ -920,6 +920,15 @@ extern "C" int hush_trainer_grad(hush_trainer_t *t, double *out) {
   return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, "cudaMemcpy");
 }
 
+// Device addresses of the gradient accumulator (812 doubles) and the loss sum (1 double), valid for the trainer's
+// life, so that data-parallel callers can all-reduce them in place on the trainer's stream before hush_trainer_step.
+extern "C" int hush_trainer_accumulators(hush_trainer_t *t, double **grad, double **loss_sum) {
+  if (!t) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_trainer_accumulators: NULL trainer");
+  if (grad) *grad = t->grad;
+  if (loss_sum) *loss_sum = t->loss_acc;
+  return HUSH_OK;
+}
+
 extern "C" int hush_trainer_theta(hush_trainer_t *t, float *get, const float *set) {
   if (!t) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_trainer_theta: NULL trainer");
   cudaError_t e = cudaSuccess;

@@ -14,7 +14,8 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib as L
-from .hush import Hush, HushError, _fill_inputs, _stream_handle
+from .dp import DataParallel, finish_step
+from .hush import Hush, HushError, _DevView, _fill_inputs, _stream_handle
 from .scene import NAMES, SceneConfig, frame_device
 
 NW = 812
@@ -84,6 +85,16 @@ class Trainer:
         g = np.zeros(NW, np.float64)
         self._check(L.lib().hush_trainer_grad(self._t, g.ctypes.data))
         return g
+
+    def accumulators(self):
+        """(grad, loss_sum): torch views of the device gradient accumulator (812 float64) and loss sum (1 float64)."""
+        import torch
+
+        g, l = C.c_void_p(), C.c_void_p()
+        self._check(L.lib().hush_trainer_accumulators(self._t, C.byref(g), C.byref(l)))
+        dev = torch.device("cuda", self.hush.device)
+        return (torch.as_tensor(_DevView(g.value, 1, 1, NW, "<f8"), device=dev).view(NW),
+                torch.as_tensor(_DevView(l.value, 1, 1, 1, "<f8"), device=dev).view(1))
 
     @property
     def theta(self) -> np.ndarray:
@@ -155,37 +166,48 @@ def window(cfg: TrainConfig, seed: int, buf=None):
     return out
 
 
-def train(cfg: TrainConfig, log_every: int = 100, on_log=None, time_budget_s: float | None = None):
-    """Runs the training loop; returns (trainer, hush, history). A step = `batch` windows of `frames` frames."""
+def train(cfg: TrainConfig, log_every: int = 100, on_log=None, time_budget_s: float | None = None,
+          dp: DataParallel | None = None, device: int = 0):
+    """Runs the training loop; returns (trainer, hush, history). A step = `batch` windows of `frames` frames on each
+    rank; with dp (one process per GPU) the ranks draw disjoint window seeds and average gradient and loss before
+    the shared Adam step, so the global batch is batch x world windows."""
     import torch
 
-    hush = Hush(0, {"width": cfg.size, "height": cfg.size, "schedule": "passes"})
+    dp = dp or DataParallel()
+    hush = Hush(device, {"width": cfg.size, "height": cfg.size, "schedule": "passes"})
     tr = Trainer(hush, xavier_init(cfg.init_seed))
-    rng = np.random.default_rng(cfg.init_seed + 1)
-    bufs = [{n: torch.empty((cfg.size, cfg.size, 4), dtype=torch.float16, device="cuda") for n in NAMES}
+    if dp.world > 1:  # every rank starts from rank 0's weights
+        th = torch.from_numpy(tr.theta).cuda(device)
+        dp.broadcast_(th)
+        tr.theta = th.cpu().numpy()
+    rng = dp.seed_rng(cfg.init_seed + 1)
+    bufs = [{n: torch.empty((cfg.size, cfg.size, 4), dtype=torch.float16, device=f"cuda:{device}") for n in NAMES}
             for _ in range(cfg.frames)]
     for b in bufs:
-        b["clean"] = torch.empty((cfg.size, cfg.size, 3), dtype=torch.float32, device="cuda")
+        b["clean"] = torch.empty((cfg.size, cfg.size, 3), dtype=torch.float32, device=f"cuda:{device}")
     hist = []
     t0 = time.time()
     for step in range(cfg.steps):
         ts = time.perf_counter()
         for _ in range(cfg.batch):
-            seed = int(rng.integers(0, cfg.seeds))
-            win = window(cfg, seed, bufs)
+            win = window(cfg, dp.window_seed(rng, cfg.seeds), bufs)
             tr.reset()
             for t, fr in enumerate(win):
                 tr.frame(fr, fr["clean"], win[t - 1]["clean"] if t else None, cfg.lambda_t, True, sync=False)
                 tr.end_frame()
-        loss_sum = tr.loss_sum()
-        gn = tr.step(cfg.lr, clip=cfg.clip)
+        loss, gn = finish_step(tr, dp, cfg.batch * cfg.frames, cfg.lr, cfg.clip)
         torch.cuda.synchronize()
         ms = (time.perf_counter() - ts) * 1e3
-        rec = {"step": step, "loss": loss_sum / (cfg.batch * cfg.frames), "grad_norm": gn, "step_ms": ms}
+        rec = {"step": step, "loss": loss, "grad_norm": gn, "step_ms": ms}
         hist.append(rec)
         if on_log and (step % log_every == 0 or step == cfg.steps - 1):
             on_log(rec)
-        if time_budget_s and time.time() - t0 > time_budget_s:
+        stop = bool(time_budget_s and time.time() - t0 > time_budget_s)
+        if dp.world > 1:  # every rank stops at the same step
+            flag = torch.tensor([1.0 if stop else 0.0], device=f"cuda:{device}")
+            dp.average_(flag)
+            stop = flag.item() > 0
+        if stop:
             break
     return tr, hush, hist
 
@@ -229,12 +251,19 @@ def evaluate(weights_blob: np.ndarray | None, seeds, size: int = 384, frames: in
 
 
 def main(argv=None):
+    """Command line. Under torchrun (WORLD_SIZE > 1) it trains data-parallel over NCCL, one GPU per rank; rank 0
+    evaluates and writes the outputs."""
     import argparse
+    import datetime
     import json
+    import os
+
+    import torch
+    import torch.distributed as dist
 
     ap = argparse.ArgumentParser(description="train the parameter MLP on device and evaluate against SVGF")
     ap.add_argument("--steps", type=int, default=5000)
-    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--batch", type=int, default=16, help="windows per step on each rank")
     ap.add_argument("--size", type=int, default=384)
     ap.add_argument("--frames", type=int, default=8)
     ap.add_argument("--seeds", type=int, default=2048)
@@ -244,21 +273,36 @@ def main(argv=None):
     ap.add_argument("--out", default=None, help="write the summary JSON here")
     ap.add_argument("--weights-out", default=None, help="write the trained f16 blob here")
     a = ap.parse_args(argv)
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dp = DataParallel()
     cfg = TrainConfig(size=a.size, frames=a.frames, seeds=a.seeds, batch=a.batch, steps=a.steps, lr=a.lr)
     log = []
 
     def on_log(rec):
         log.append(rec)
-        print(json.dumps(rec), flush=True)
+        if dp.rank == 0:
+            print(json.dumps(rec), flush=True)
 
-    tr, hush, hist = train(cfg, log_every=50, on_log=on_log, time_budget_s=a.time_budget)
+    tr, hush, hist = train(cfg, log_every=50, on_log=on_log, time_budget_s=a.time_budget, dp=dp, device=local)
     blob = tr.export()
+    div = dp.max_divergence(torch.from_numpy(tr.theta).cuda(local))
+    if dp.rank != 0:
+        tr.destroy()
+        hush.destroy()
+        dist.destroy_process_group()
+        return 0
     if a.weights_out:
         blob.tofile(a.weights_out)
     held_out = [1_000_000 + i for i in range(a.eval_seeds)]
     res = {
         "config": vars(a),
+        "world": dp.world,
         "steps_run": len(hist),
+        "theta_max_divergence_over_ranks": div,
         "train_step_ms_median": float(np.median([h["step_ms"] for h in hist[1:]] or [hist[0]["step_ms"]])),
         "loss_first": hist[0]["loss"], "loss_last": float(np.mean([h["loss"] for h in hist[-20:]])),
         "eval_trained": evaluate(blob, held_out, a.size, a.frames),
@@ -270,6 +314,8 @@ def main(argv=None):
     if a.out:
         with open(a.out, "w") as f:
             json.dump(res, f, indent=1)
+    if dp.world > 1:
+        dist.destroy_process_group()
     return 0
 
 

@@ -150,6 +150,10 @@ int hush_trainer_reset(hush_trainer_t *t);
 int hush_trainer_zero_grad(hush_trainer_t *t, void *stream);
 /* The accumulated weight gradient (812 doubles). */
 int hush_trainer_grad(hush_trainer_t *t, double *out);
+/* Device addresses of the gradient accumulator (812 doubles) and of the loss sum (1 double), valid until
+ * hush_trainer_destroy. Data-parallel training all-reduces both in place (e.g. NCCL, on the trainer's stream) between
+ * the last hush_trainer_frame of a step and hush_trainer_step. Either pointer may be NULL. */
+int hush_trainer_accumulators(hush_trainer_t *t, double **grad, double **loss_sum);
 /* Read (get != NULL) and / or replace (set != NULL) the FP32 master weights. */
 int hush_trainer_theta(hush_trainer_t *t, float *get, const float *set);
 /* The FP32 parameters and dL/dpar of the last frame: 12 floats per half-res pixel (alpha gamma beta kappa, s0..s3,

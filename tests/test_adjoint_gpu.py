@@ -130,3 +130,20 @@ def test_training_steps_reduce_the_loss():
     assert np.isfinite(last) and last < first, (first, last)
     blob = tr.export()
     assert blob.dtype == np.uint16 and blob.size == 812 and hush.hidden == 16
+
+
+def test_accumulator_views_alias_the_device_gradient():
+    """The device views used by data-parallel training read and write the trainer's own accumulators."""
+    g, tr, host, cleans, t = _setup()
+    tr.zero_grad()
+    tr.loss_sum()  # restart the loss sum (the set-up frames added theirs)
+    loss = tr.frame(_dev(host[t]), cleans[t], cleans[t - 1], 0.5, backward=True)
+    grad, loss_acc = tr.accumulators()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(grad.cpu().numpy(), tr.grad())
+    assert loss_acc.item() == pytest.approx(loss, rel=1e-12)
+    grad.mul_(0.5)  # what the all-reduce mean does in place with one rank contributing half
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(tr.grad(), grad.cpu().numpy())
+    assert tr.loss_sum() == pytest.approx(loss, rel=1e-12)
+    assert loss_acc.item() == 0.0
