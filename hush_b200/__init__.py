@@ -5,6 +5,7 @@ parameter MLP, a 5-level edge-aware a-trous pyramid and TAA) as sm_100a CUDA ker
 The compute path is libhush_b200.so (C ABI in include/hush.h); this package is its host-side mirror.
 """
 from .hush import Hush, HushError, HushTimer, builtin_weights, decode_weights, hiddenOf  # noqa: F401
+from .post import Post  # noqa: F401
 from .svgf import SVGF  # noqa: F401
 
-__all__ = ["Hush", "HushError", "HushTimer", "SVGF", "hiddenOf", "builtin_weights", "decode_weights"]
+__all__ = ["Hush", "HushError", "HushTimer", "Post", "SVGF", "hiddenOf", "builtin_weights", "decode_weights"]

@@ -51,6 +51,19 @@ class HushScene(C.Structure):
                 ("seed", C.c_uint32)]
 
 
+class HushPostDesc(C.Structure):
+    _fields_ = [("device", C.c_int), ("format", C.c_int), ("bloom", C.c_float), ("vignette", C.c_float)]
+
+
+class HushPostInputs(C.Structure):
+    _fields_ = [("left", C.c_void_p), ("right", C.c_void_p), ("mid", C.c_void_p), ("width", C.c_int),
+                ("height", C.c_int), ("split", C.c_float), ("split2", C.c_float), ("exposure", C.c_float),
+                ("line", C.c_float), ("same", C.c_int)]
+
+
+POST_LEVELS = 6
+POST_RGBA8, POST_BGRA8, POST_RGBA32F = 0, 1, 2
+
 _P = C.c_void_p
 _SIGS = {
     "hush_hidden_of": (C.c_int, [C.c_long]),
@@ -104,6 +117,14 @@ _SIGS = {
     "svgf_encode": (C.c_int, [_P, C.POINTER(SvgfInputs), _P, C.POINTER(_P)]),
     "svgf_output": (_P, [_P]),
     "svgf_last_error": (C.c_char_p, [_P]),
+    "hush_post_desc_default": (HushPostDesc, []),
+    "hush_post_inputs_default": (HushPostInputs, []),
+    "hush_post_create": (C.c_int, [C.POINTER(HushPostDesc), C.POINTER(_P)]),
+    "hush_post_destroy": (None, [_P]),
+    "hush_post_set": (C.c_int, [_P, C.c_float, C.c_float]),
+    "hush_post_encode": (C.c_int, [_P, C.POINTER(HushPostInputs), _P, C.c_int, C.c_int, C.c_size_t, _P]),
+    "hush_post_buffer": (_P, [_P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "hush_post_last_error": (C.c_char_p, [_P]),
     "hush_scene_frame_host": (C.c_int, [C.POINTER(HushScene), C.c_int] + [C.c_void_p] * 6),
     "hush_scene_frame_device": (C.c_int, [C.POINTER(HushScene), C.c_int] + [C.c_void_p] * 7),
 }

@@ -205,6 +205,38 @@ int svgf_encode(svgf_t *s, const svgf_inputs *in, void *stream, const void **out
 const void *svgf_output(const svgf_t *s);
 const char *svgf_last_error(const svgf_t *s);
 
+/* ---- display post of the demo (src/demo/post.js) on a headless target ------------------------------------------
+ * new Post(device, format, {bloom, vignette}) (post.js:137-156) and Post.encode (post.js:191-210): split-screen
+ * composite of left | mid | right (linear HDR rgba16float, dense, width x height), six-level bloom, vignette, AgX,
+ * sRGB and divider line. The canvas is replaced by a caller-owned device buffer of target_width x target_height
+ * texels in `format` (the bloom / vignette strengths are instance state as in the reference). */
+#define HUSH_POST_LEVELS 6
+#define HUSH_POST_RGBA8 0   /* 4 x u8 unorm, r g b a */
+#define HUSH_POST_BGRA8 1   /* 4 x u8 unorm, b g r a (the usual canvas format) */
+#define HUSH_POST_RGBA32F 2 /* 4 x f32: the colour before 8-bit quantisation */
+typedef struct hush_post_s hush_post_t;
+typedef struct {
+  int device, format;
+  float bloom, vignette; /* defaults 0.03 and 0.35 (post.js:138) */
+} hush_post_desc;
+typedef struct {
+  const void *left, *right, *mid; /* mid NULL = right (post.js:191) */
+  int width, height;
+  float split, split2, exposure, line; /* defaults 0.5, 0.5 (= split), 1, 1.5 */
+  int same;                            /* 1: every third shows the middle third of its own image */
+} hush_post_inputs;
+hush_post_desc hush_post_desc_default(void);
+hush_post_inputs hush_post_inputs_default(void);
+int hush_post_create(const hush_post_desc *desc, hush_post_t **out);
+void hush_post_destroy(hush_post_t *p);
+int hush_post_set(hush_post_t *p, float bloom, float vignette);
+/* Enqueues the 13 passes on `stream`; target_pitch in bytes (0 = dense). */
+int hush_post_encode(hush_post_t *p, const hush_post_inputs *in, void *target, int target_width, int target_height,
+                     size_t target_pitch, void *stream);
+/* level 0: the composited HDR image; 1..6: the bloom levels as the last encode left them (rgba16float). */
+const void *hush_post_buffer(const hush_post_t *p, int level, int *width, int *height);
+const char *hush_post_last_error(const hush_post_t *p);
+
 /* ---- synthetic G-buffer scenes (benchmark / test / training inputs) ------------------------------------------ */
 typedef struct {
   int width, height, n_objects, n_moving;

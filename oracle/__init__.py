@@ -35,6 +35,14 @@ class _SvgfInputs(C.Structure):
                                            "prev_normal_depth", "prev_motion")]
 
 
+class _PostArgs(C.Structure):
+    _fields_ = [("left", C.c_void_p), ("right", C.c_void_p), ("mid", C.c_void_p), ("width", C.c_int),
+                ("height", C.c_int), ("out_width", C.c_int), ("out_height", C.c_int), ("split", C.c_float),
+                ("split2", C.c_float), ("exposure", C.c_float), ("line", C.c_float), ("bloom", C.c_float),
+                ("vignette", C.c_float), ("same", C.c_int)]
+
+
+POST_LEVELS = 6
 _lib = None
 
 
@@ -65,6 +73,8 @@ def lib():
             "ho_svgf_destroy": (None, [P]),
             "ho_svgf_reset": (None, [P]),
             "ho_svgf_encode": (P, [P, C.POINTER(_SvgfInputs)]),
+            "ho_post_level_size": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+            "ho_post": (C.c_int, [C.POINTER(_PostArgs), P, P, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -184,3 +194,34 @@ def mlp(weights: np.ndarray, features: np.ndarray, fp64=False) -> np.ndarray:
     o = np.zeros(12, dtype=np.float32)
     lib().ho_mlp(w.ctypes.data, w.size, f.ctypes.data, o.ctypes.data, 1 if fp64 else 0)
     return o
+
+
+def post_level_size(width: int, height: int, level: int):
+    w, h = C.c_int(), C.c_int()
+    if lib().ho_post_level_size(int(width), int(height), int(level), C.byref(w), C.byref(h)) != 0:
+        raise ValueError(f"no post level {level}")
+    return w.value, h.value
+
+
+def post(left, right, mid=None, split=0.5, split2=None, same=False, exposure=1.0, out_size=None, line=1.5,
+         bloom=0.03, vignette=0.35):
+    """Post.encode of src/demo/post.js on (H, W, 4) float16 arrays. Returns dict with 'hdr' (H, W, 4) float16,
+    'levels' (list of six float16 arrays), 'f32' (OH, OW, 4) float32 and 'rgba8' (OH, OW, 4) uint8."""
+    Hh, Ww = left.shape[:2]
+    OW, OH = out_size or (Ww, Hh)
+    arrs = [_as_u16(a) for a in (left, right, mid if mid is not None else right)]
+    a = _PostArgs(arrs[0].ctypes.data, arrs[1].ctypes.data, arrs[2].ctypes.data if mid is not None else None,
+                  Ww, Hh, OW, OH, split, split if split2 is None else split2, exposure, line, bloom, vignette,
+                  1 if same else 0)
+    sizes = [post_level_size(Ww, Hh, i) for i in range(1, POST_LEVELS + 1)]
+    hdr = np.zeros((Hh, Ww, 4), np.uint16)
+    lev = np.zeros(sum(w * h * 4 for w, h in sizes), np.uint16)
+    f32 = np.zeros((OH, OW, 4), np.float32)
+    u8 = np.zeros((OH, OW, 4), np.uint8)
+    if lib().ho_post(C.byref(a), hdr.ctypes.data, lev.ctypes.data, f32.ctypes.data, u8.ctypes.data) != 0:
+        raise ValueError("oracle post: bad arguments")
+    levels, o = [], 0
+    for w, h in sizes:
+        levels.append(lev[o:o + w * h * 4].reshape(h, w, 4).view(np.float16))
+        o += w * h * 4
+    return {"hdr": hdr.view(np.float16), "levels": levels, "f32": f32, "rgba8": u8}

@@ -84,6 +84,21 @@ void ho_svgf_destroy(ho_svgf *s);
 void ho_svgf_reset(ho_svgf *s);
 const uint16_t *ho_svgf_encode(ho_svgf *s, const ho_svgf_inputs *in);
 
+/* ---- display post (src/demo/post.js), post_oracle.cpp ---------------------------------------------------------
+ * Post.encode (post.js:191-210) over dense rgba16float images left / right / mid (mid NULL = right) of
+ * width x height, into an out_width x out_height target. hdr_out (width x height x 4 u16), levels_out (the six bloom
+ * levels, level 1 first, max(1, size >> i) each, 4 u16 per texel), out_f32 (the FINAL colour before 8-bit
+ * quantisation) and out_rgba8 may each be NULL. */
+#define HO_POST_LEVELS 6
+typedef struct {
+  const uint16_t *left, *right, *mid;
+  int width, height, out_width, out_height;
+  float split, split2, exposure, line, bloom, vignette;
+  int same;
+} ho_post_args;
+int ho_post_level_size(int width, int height, int level, int *w, int *h);
+int ho_post(const ho_post_args *a, uint16_t *hdr_out, uint16_t *levels_out, float *out_f32, uint8_t *out_rgba8);
+
 #ifdef __cplusplus
 }
 #endif
