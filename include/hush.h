@@ -205,6 +205,94 @@ int svgf_encode(svgf_t *s, const svgf_inputs *in, void *stream, const void **out
 const void *svgf_output(const svgf_t *s);
 const char *svgf_last_error(const svgf_t *s);
 
+/* ---- path tracer (src/pt): scene buffers, BVH, 1 spp + G-buffer frames -----------------------------------------
+ * SceneGPU (src/pt/scene.js:22-344) without three.js: meshes arrive as world-space arrays grouped into at most 8
+ * BLAS (group flags: dynamic = re-posed by hush_pt_scene_update with exact previous positions, no shadow = skipped by
+ * shadow rays). PathTracer (src/pt/pathtracer.js:14-162): two G-buffer slots of five dense rgba16float images
+ * (radiance, normalDepth, motion, material, emission: exactly the Hush inputs) or a float4 accumulation buffer. */
+#define HUSH_PT_MAX_BLAS 8
+#define HUSH_PT_MAX_LIGHTS 8
+#define HUSH_PT_TEX_SIZE 1024
+#define HUSH_PT_TEX_MIPS 11
+#define HUSH_PT_ENV_GW 256
+#define HUSH_PT_ENV_GH 128
+#define HUSH_PT_GROUP_DYNAMIC 1
+#define HUSH_PT_GROUP_NO_SHADOW 2
+typedef struct hush_pt_scene_s hush_pt_scene_t;
+typedef struct hush_pt_s hush_pt_t;
+/* Material record in the reference's GPU layout (scene.js:50-56, 305-310): base rgb + alpha cutoff, emissive rgb,
+ * (roughness, metalness, transmission, ior), texture layers (base, normal, arm; -1 = none), (uv scale xy, normal
+ * scale, 0). */
+typedef struct {
+  float base[4], emissive[4], pbr[4];
+  int32_t tex[4];
+  float uv[4];
+} hush_pt_material;
+typedef struct { uint32_t node_offset, tri_offset, node_count, flags; } hush_pt_blas;
+typedef struct { float pos[4], prev_pos[4], radiance[4], params[4]; } hush_pt_light; /* params.x: 0 sun, 1 sphere */
+/* Frame uniforms, the 960-byte layout of the reference's uniform buffer (pathtracer.wgsl.js:22-46, written by
+ * writeUniforms, pathtracer.js:105-149); matrices column-major. */
+typedef struct {
+  float cam_pos[4], cam_right[4], cam_up[4], cam_fwd[4];
+  float view_proj[16], prev_view_proj[16];
+  uint32_t size[2], frame, mode;
+  float jitter[2];
+  uint32_t spp, max_bounces;
+  float sky_zenith[4], sky_horizon[4], ground[4];
+  uint32_t counts[4];
+  float clamp_lum, pixel_angle, shadow_tau, clamp_direct;
+  float env[4];
+  hush_pt_blas blas[HUSH_PT_MAX_BLAS];
+  hush_pt_light lights[HUSH_PT_MAX_LIGHTS];
+} hush_pt_frame;
+
+hush_pt_material hush_pt_material_default(void);
+int hush_pt_scene_create(int device, hush_pt_scene_t **out);
+void hush_pt_scene_destroy(hush_pt_scene_t *s);
+/* Returns the material id (>= 0; it is also the object id the G-buffer reports) or -1. */
+int hush_pt_scene_add_material(hush_pt_scene_t *s, const hush_pt_material *m);
+/* rgba8 image (any size; resampled to 1024^2, 11 box-filtered mips); returns the texture layer or -1. */
+int hush_pt_scene_add_texture(hush_pt_scene_t *s, const uint8_t *rgba, int width, int height);
+/* One BLAS from world-space vertices (pos: 3 floats, nrm: 3 floats or NULL = +y, uv: 2 floats or NULL = 0) and
+ * triangles (idx: 3 vertex indices, mat: material id per triangle). Returns the group id or -1. */
+int hush_pt_scene_add_group(hush_pt_scene_t *s, int flags, const float *pos, const float *nrm, const float *uv,
+                            int n_verts, const uint32_t *idx, const uint32_t *mat, int n_tris);
+/* Builds every group's BVH (binned SAH, bvh.js:12-143), packs it (bvh.js:186-210) and uploads the scene. */
+int hush_pt_scene_build(hush_pt_scene_t *s);
+/* SceneGPU.update for one dynamic group (scene.js:225-270): the current positions become the previous ones, pos
+ * (and nrm, or area-weighted smooth normals when NULL) become current, the BVH is refitted and re-uploaded. */
+int hush_pt_scene_update(hush_pt_scene_t *s, int group, const float *pos, const float *nrm, void *stream);
+/* The BLAS table for the frame uniforms (scene.js:338-343); returns the group count. */
+int hush_pt_scene_blas(const hush_pt_scene_t *s, hush_pt_blas *out, int max);
+/* Sizes and device buffers (packed nodes, triangles, triangle indices, vertices, materials) for inspection. */
+int hush_pt_scene_info(const hush_pt_scene_t *s, int *tri_total, int *node_total, int *vert_total, int *max_depth);
+int hush_pt_scene_device(const hush_pt_scene_t *s, const void **nodes, const void **tris, const void **tri_idx,
+                         const void **verts, const void **mats, const void **tex);
+/* The BVH builder alone (host; bvh.js:12-143): nodes (8 floats per node, room for 2 * max(1, n) nodes), order;
+ * returns the node count. */
+int hush_pt_bvh_build(const float *pos, int tri_count, float *nodes, uint32_t *order, int *max_depth);
+/* prepareEnvMap (src/pt/envmap.js:85-105), host: cuts the sun out of rgba (w x h x 4 floats, row 0 = up; in place),
+ * writes the rgba16float map (w x h x 4) and the alias table (256 x 128 cells x 4 floats); returns 1 when a sun was
+ * cut (its direction and irradiance in sun_dir / sun_irr). */
+int hush_pt_env_prepare(float *rgba, int width, int height, int sun, double sun_cone_deg, uint16_t *half_out,
+                        float *table_out, double sun_dir[3], double sun_irr[3]);
+/* JITTER (pathtracer.js:6-12): 16 Halton(2, 3) subpixel offsets in pixels, x y pairs. */
+void hush_pt_jitter(float out[32]);
+
+int hush_pt_create(hush_pt_scene_t *scene, int width, int height, hush_pt_t **out);
+void hush_pt_destroy(hush_pt_t *p);
+int hush_pt_resize(hush_pt_t *p, int width, int height);
+/* The environment map (host rgba16float w x h and its alias table) or NULL to unbind (analytic sky). */
+int hush_pt_set_envmap(hush_pt_t *p, const uint16_t *half_rgba, int width, int height, const float *table);
+/* One dispatch (pathtracer.js:152-159): mode 0 writes G-buffer slot `slot`, mode 1 adds spp paths per pixel to the
+ * accumulation buffer. f->size must equal the tracer's size. */
+int hush_pt_encode(hush_pt_t *p, const hush_pt_frame *f, int slot, void *stream);
+/* which: 0 radiance, 1 normalDepth, 2 motion, 3 material, 4 emission. */
+const void *hush_pt_gbuffer(const hush_pt_t *p, int slot, int which);
+float *hush_pt_accum(const hush_pt_t *p);
+int hush_pt_clear_accum(hush_pt_t *p, void *stream);
+const char *hush_pt_last_error(void);
+
 /* ---- display post of the demo (src/demo/post.js) on a headless target ------------------------------------------
  * new Post(device, format, {bloom, vignette}) (post.js:137-156) and Post.encode (post.js:191-210): split-screen
  * composite of left | mid | right (linear HDR rgba16float, dense, width x height), six-level bloom, vignette, AgX,

@@ -99,6 +99,67 @@ typedef struct {
 int ho_post_level_size(int width, int height, int level, int *w, int *h);
 int ho_post(const ho_post_args *a, uint16_t *hdr_out, uint16_t *levels_out, float *out_f32, uint8_t *out_rgba8);
 
+/* ---- path tracer (src/pt/pathtracer.wgsl.js, bvh.js, scene.js, envmap.js), pt_oracle.cpp -----------------------
+ * Frame uniforms in the byte layout of the reference's uniform buffer (pathtracer.wgsl.js:22-46, written by
+ * pathtracer.js:105-149): 960 bytes. Matrices are column-major (three.js elements order). */
+#define HO_PT_MAX_BLAS 8
+#define HO_PT_MAX_LIGHTS 8
+#define HO_PT_ENV_GW 256
+#define HO_PT_ENV_GH 128
+#define HO_PT_TEX_SIZE 1024
+#define HO_PT_TEX_MIPS 11
+typedef struct { uint32_t node_offset, tri_offset, node_count, flags; } ho_pt_blas; /* flags: 1 dynamic, 2 no shadow */
+typedef struct { float pos[4], prev_pos[4], radiance[4], params[4]; } ho_pt_light;
+typedef struct {
+  float cam_pos[4], cam_right[4], cam_up[4], cam_fwd[4];
+  float view_proj[16], prev_view_proj[16];
+  uint32_t size[2], frame, mode;
+  float jitter[2];
+  uint32_t spp, max_bounces;
+  float sky_zenith[4], sky_horizon[4], ground[4];
+  uint32_t counts[4]; /* blas count, light count, sample offset, 0 */
+  float clamp_lum, pixel_angle, shadow_tau, clamp_direct;
+  float env[4]; /* intensity, cos / sin of the rotation about +y, 1 if a map is bound */
+  ho_pt_blas blas[HO_PT_MAX_BLAS];
+  ho_pt_light lights[HO_PT_MAX_LIGHTS];
+} ho_pt_frame;
+/* Scene buffers in the reference's GPU layouts (scene.js:167-171, 210-222, 294-311): packed BVH nodes (16 floats),
+ * triangles (12 floats), triangle indices (4 u32: a, b, c, material | f16 texture LOD << 16), vertices (12 floats:
+ * pos.xyz, u, prev.xyz, 0, normal.xyz, v), materials (20 x 4 bytes, tex as int32), the rgba8 texture array
+ * (layers x 11 mips from 1024^2, level-major inside a layer) and the equirect environment map (rgba16float) with its
+ * alias table (4 floats per cell of the 256 x 128 grid). */
+typedef struct {
+  const float *nodes, *tris, *verts, *mats;
+  const uint32_t *tri_idx;
+  const uint8_t *tex;
+  int tex_layers;
+  const uint16_t *env;
+  int env_w, env_h;
+  const float *env_table;
+} ho_pt_scene;
+/* main() of pathtracer.wgsl.js:648-672 over the whole image: mode 0 writes the five rgba16float G-buffer images
+ * (radiance, normalDepth, motion, material, emission; dense), mode 1 adds to accum (4 floats per pixel). */
+int ho_pt_render(const ho_pt_scene *s, const ho_pt_frame *f, uint16_t *const gbuf[5], float *accum);
+/* One path of tracePath (pathtracer.wgsl.js:511-646) for pixel (x, y) with the RNG seeded as main() does; out:
+ * radiance rgb, primary emission rgb, normal xyz, depth, motion xy, object id, previous depth, albedo rgb, rough. */
+void ho_pt_pixel(const ho_pt_scene *s, const ho_pt_frame *f, int x, int y, float out[18]);
+/* Closest hit of a ray through the BVHs and sphere lights (traceScene, 212-221): t, triangle (or -1), light, u, v. */
+void ho_pt_trace(const ho_pt_scene *s, const ho_pt_frame *f, const float o[3], const float d[3], float out[5]);
+/* bvh.js: buildBVH (12-143; nodes: 8 floats per node, room for 2 * max(1, n) nodes; returns the node count),
+ * refitBVH (147-171), packedCount (178-183), packBVH (186-210). */
+int ho_bvh_build(const float *pos, int tri_count, float *nodes, uint32_t *order, int *max_depth);
+void ho_bvh_refit(float *nodes, int node_count, const float *tri_pos);
+int ho_bvh_packed_count(const float *nodes, int node_count);
+void ho_bvh_pack(const float *nodes, int node_count, float *out);
+/* scene.js computeTriLod (178-208): the f16 bits of log2(texels per world unit) for one triangle. */
+uint16_t ho_tri_lod(const float *va, const float *vb, const float *vc, int tex_size);
+/* envmap.js prepareEnvMap (85-105): cuts the sun out of rgba (in place), writes the rgba16float map and the alias
+ * table; returns 1 and the sun's direction / irradiance if one was cut. */
+int ho_env_prepare(float *rgba, int w, int h, int sun, double sun_cone_deg, uint16_t *half_out, float *table_out,
+                   double sun_dir[3], double sun_irr[3]);
+/* pathtracer.js JITTER (6-12): 16 Halton(2, 3) phases in pixels. */
+void ho_pt_jitter(float out[32]);
+
 #ifdef __cplusplus
 }
 #endif
