@@ -97,15 +97,23 @@ HD_INL bool tc_layer(TcSmem &S, int li, bool first, uint32_t b_off, uint32_t kco
   return ok;
 }
 
-// Shared memory of the fused temporal kernel. Per-pixel arrays are structure-of-arrays (16-byte stride, no bank
-// conflicts for the 128-bit accesses).
-constexpr int K1_SW = K1_TW + 2, K1_SH = K1_TH + 2, K1_NT = K1_TW * K1_TH;
+// Shared memory of the fused temporal kernel: the illumination tile (apron 1). Rows are stored with a stride of 36
+// entries (34 used): with the quad mapping of pixels to threads (a warp covers 16 x 2 pixels), the two rows a
+// quarter-warp reads then fall into disjoint bank halves.
+constexpr int K1_SWL = K1_TW + 2, K1_SW = K1_TW + 4, K1_SH = K1_TH + 2, K1_NT = K1_TW * K1_TH;
 struct K1Smem {
-  float4 I[K1_SW * K1_SH];   // illumination (r, g, b) and L (luminance or L_INVALID), apron 1
+  float4 I[K1_SW * K1_SH];   // illumination (r, g, b) and L (luminance or L_INVALID)
   float2 Lq[K1_SW * K1_SH];  // (E * qf16(L), 1) for valid entries, (0, 0) otherwise: the 4x4 block statistics
-  float4 P0[K1_NT], P1[K1_NT], P2[K1_NT], P3[K1_NT], P4[K1_NT];  // pixel() feature inputs
-  float4 Ns[K1_NT];          // octDec(P2.xy) and 1 for pixels with a surface, zeros otherwise
 };
+
+// pixel()'s inputs to block(): P0..P4 as block() reads them and the decoded normal (Ns.w = 1 with a surface).
+struct PixOut {
+  float4 P0, P1, P2, P3, P4, Ns;
+};
+HD_INL PixOut pix_none() {
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  return PixOut{z4, z4, make_float4(0.f, 0.f, -1.0f, 0.f), z4, z4, z4};
+}
 
 // The loads of one pixel's pixel(): its G-buffer texels and the reprojection gathers of the previous frame's key,
 // colour and moments (bilinear footprint) and par0. Issued before the tile arithmetic and the barrier so that the
@@ -135,8 +143,8 @@ HD_INL void pixel_issue(const HushFrame &f, int px, int py, PixLoads &L) {
 }
 
 // pixel() of hush.js:111-223 over the (r, g, b, L) tile from the preloaded texels; same arithmetic as
-// temporal_pixel(). Writes A0, mom, key and the pixel's entries of the shared feature-input arrays.
-HD_INL void temporal_pixel_fast(const HushFrame &f, int px, int py, K1Smem &S, int ti, int li, const PixLoads &PL) {
+// temporal_pixel(). Writes A0, mom, key and returns the pixel's inputs to block().
+HD_INL PixOut temporal_pixel_fast(const HushFrame &f, int px, int py, const K1Smem &S, int ti, const PixLoads &PL) {
   constexpr int SW = K1_SW;
   const int W = f.W, H = f.H;
   const float4 nd = h4_to_f4(PL.nd), mv = h4_to_f4(PL.mv);
@@ -146,9 +154,7 @@ HD_INL void temporal_pixel_fast(const HushFrame &f, int px, int py, K1Smem &S, i
     f.A0[oi] = make_uint2(0, 0);
     f.mom[oi] = make_uint2(0, 0);
     sth(f.key, oi, make_float4(0.f, 0.f, -1.0f, mv.z));
-    S.P0[li] = z4; S.P1[li] = z4; S.P2[li] = make_float4(0.f, 0.f, -1.0f, 0.f); S.P3[li] = z4; S.P4[li] = z4;
-    S.Ns[li] = z4;
-    return;
+    return pix_none();
   }
   float fx = 0.f, fy = 0.f;
   int bix = 0, biy = 0, cx = 0, cy = 0;
@@ -267,94 +273,68 @@ HD_INL void temporal_pixel_fast(const HushFrame &f, int px, int py, K1Smem &S, i
   const float m1 = E * qf16(nmx);
   const float m2 = E * E * qf16(nmy);
   const float ox = qf16(oc.x), oy = qf16(oc.y);
-  S.P0[li] = make_float4(E * lum(Aq), E * qf16(l), fmaxf(m2 - m1 * m1, 0.0f), len1);
-  S.P1[li] = make_float4(qf16(v), qf16(lag), E * qf16(nfast), m1);
-  S.P2[li] = make_float4(ox, oy, qf16(nd.w), qf16(sqrtf(mv.x * mv.x + mv.y * mv.y)));
-  S.P3[li] = h4_to_f4(mrr);
-  S.P4[li] = Aq;
-  float4 ns = oct_dec(ox, oy);  // block() decodes the stored oct normal (hush.js:238)
-  ns.w = 1.0f;
-  S.Ns[li] = ns;
+  PixOut o;
+  o.P0 = make_float4(E * lum(Aq), E * qf16(l), fmaxf(m2 - m1 * m1, 0.0f), len1);
+  o.P1 = make_float4(qf16(v), qf16(lag), E * qf16(nfast), m1);
+  o.P2 = make_float4(ox, oy, qf16(nd.w), qf16(sqrtf(mv.x * mv.x + mv.y * mv.y)));
+  o.P3 = h4_to_f4(mrr);
+  o.P4 = Aq;
+  o.Ns = oct_dec(ox, oy);  // block() decodes the stored oct normal (hush.js:238)
+  o.Ns.w = 1.0f;
+  return o;
 }
 
-// block() (hush.js:226-282) for block (lbx, lby) of the tile, one thread per block: the 20 features, the block mean
-// colour AC and the guide G = (oct normal, Z, count). Returns nv > 0.
-HD_INL bool block_features_tile(const K1Smem &S, int lbx, int lby, float E, float *f, float4 &AC, float4 &G) {
+// Sums over the 4 lanes of a quad (lanes 4b..4b+3 hold the pixels of one 2x2 block).
+constexpr unsigned FULL = 0xffffffffu;
+HD_INL float qsum(float v) {
+  v += __shfl_xor_sync(FULL, v, 1);
+  return v + __shfl_xor_sync(FULL, v, 2);
+}
+HD_INL float4 qsum4(float4 v) { return make_float4(qsum(v.x), qsum(v.y), qsum(v.z), qsum(v.w)); }
+HD_INL float qmin(float v) {
+  v = fminf(v, __shfl_xor_sync(FULL, v, 1));
+  return fminf(v, __shfl_xor_sync(FULL, v, 2));
+}
+HD_INL float qmax(float v) {
+  v = fmaxf(v, __shfl_xor_sync(FULL, v, 1));
+  return fmaxf(v, __shfl_xor_sync(FULL, v, 2));
+}
+HD_INL float4 scale4(float4 v, float k) { return make_float4(v.x * k, v.y * k, v.z * k, v.w * k); }
+
+// block() (hush.js:226-282) for the 2x2 block of this lane's quad (lane j holds pixel (j & 1, j >> 1) of block
+// (lbx, lby)); every lane of the quad returns the 20 features, the block mean colour AC and the guide
+// G = (oct normal, Z, count). Returns nv > 0. All 32 lanes of the warp must call it.
+HD_INL bool block_features_quad(const K1Smem &S, const PixOut &p, int lbx, int lby, int j, float *f, float4 &AC,
+                                float4 &G) {
   constexpr int SW = K1_SW;
-  const int p0 = (2 * lby) * K1_TW + 2 * lbx;
-  const int pj[4] = {p0, p0 + 1, p0 + K1_TW, p0 + K1_TW + 1};
-  float nv = 0.f;
-  float4 S0 = make_float4(0.f, 0.f, 0.f, 0.f), S1 = S0, S3 = S0;
-  AC = S0;
-  float Nx = 0.f, Ny = 0.f, Nz = 0.f, MV = 0.f, Z = 0.f;
-  float la[4], zs[4];
-  float4 ns[4];
-  bool ok[4];
-#pragma unroll
-  for (int j = 0; j < 4; j++) {
-    ns[j] = S.Ns[pj[j]];
-    ok[j] = ns[j].w != 0.0f;
-    la[j] = 0.f; zs[j] = 0.f;
-    if (!ok[j]) continue;
-    const float4 q0 = S.P0[pj[j]], q1 = S.P1[pj[j]], q2 = S.P2[pj[j]], q3 = S.P3[pj[j]], q4 = S.P4[pj[j]];
-    nv += 1.0f;
-    la[j] = q0.x;
-    zs[j] = q2.z;
-    S0.x += q0.x; S0.y += q0.y; S0.z += q0.z; S0.w += q0.w;
-    S1.x += q1.x; S1.y += q1.y; S1.z += q1.z; S1.w += q1.w;
-    Nx += ns[j].x; Ny += ns[j].y; Nz += ns[j].z;
-    S3.x += q3.x; S3.y += q3.y; S3.z += q3.z; S3.w += q3.w;
-    AC.x += q4.x; AC.y += q4.y; AC.z += q4.z; AC.w += q4.w;
-    MV += q2.w;
-    Z += q2.z;
-  }
-  if (nv == 0.0f) {
-    G = make_float4(0.f, 0.f, -1.0f, 0.f);
-    return false;
-  }
-  const float k = 1.0f / nv;
-  S0.x *= k; S0.y *= k; S0.z *= k; S0.w *= k;
-  S1.x *= k; S1.y *= k; S1.z *= k; S1.w *= k;
-  Nx *= k; Ny *= k; Nz *= k;
-  S3.x *= k; S3.y *= k; S3.z *= k; S3.w *= k;
-  AC.x *= k; AC.y *= k; AC.z *= k; AC.w *= k;
-  MV *= k;
-  Z *= k;
-  const float Lacc = S0.x;
-  float VA = 0.f;
-#pragma unroll
-  for (int j = 0; j < 4; j++)
-    if (ok[j]) VA += (la[j] - Lacc) * (la[j] - Lacc);
-  VA *= k;
-  // 4x4 neighbourhood (block +-1), top-left at tile position (2 lbx, 2 lby) including the apron
-  const int t0 = (2 * lby) * SW + 2 * lbx;
-  float s1 = 0.f, n4 = 0.f;
-#pragma unroll
-  for (int j = 0; j < 16; j++) {
-    const float2 q = S.Lq[t0 + (j >> 2) * SW + (j & 3)];
-    s1 += q.y * q.x;
-    n4 += q.y;
-  }
+  const bool ok = p.Ns.w != 0.0f;
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  const float nv = qsum(ok ? 1.0f : 0.0f);
+  float4 S0 = qsum4(ok ? p.P0 : z4), S1 = qsum4(ok ? p.P1 : z4), S3 = qsum4(ok ? p.P3 : z4);
+  AC = qsum4(ok ? p.P4 : z4);
+  const float Nx = qsum(ok ? p.Ns.x : 0.f), Ny = qsum(ok ? p.Ns.y : 0.f), Nz = qsum(ok ? p.Ns.z : 0.f);
+  const float MV = qsum(ok ? p.P2.w : 0.f), Zs = qsum(ok ? p.P2.z : 0.f);
+  // the 4x4 luminance neighbourhood (block +-1): lane j takes row j of the window
+  const float4 *lq = reinterpret_cast<const float4 *>(&S.Lq[(2 * lby + j) * SW + 2 * lbx]);
+  const float4 qa = lq[0], qb = lq[1];  // (x, y) pairs of 4 consecutive entries
+  const float s1 = qsum(qa.y * qa.x + qa.w * qa.z + qb.y * qb.x + qb.w * qb.z);
+  const float n4 = qsum(qa.y + qa.w + qb.y + qb.w);
   const float mu4 = s1 / fmaxf(n4, 1.0f);
-  float var4 = 0.f;
-#pragma unroll
-  for (int j = 0; j < 16; j++) {
-    const float2 q = S.Lq[t0 + (j >> 2) * SW + (j & 3)];
-    const float d = q.x - mu4;
-    var4 += q.y * d * d;
-  }
-  var4 /= fmaxf(n4, 1.0f);
-  const float nl = fmaxf(sqrtf(Nx * Nx + Ny * Ny + Nz * Nz), 1e-6f);
-  const float4 Nn = make_float4(Nx / nl, Ny / nl, Nz / nl, 0.f);
-  float zmax = -1e30f, zmin = 1e30f, mind = 1e30f;
-#pragma unroll
-  for (int j = 0; j < 4; j++) {
-    if (ok[j]) {
-      zmax = fmaxf(zmax, zs[j]);
-      zmin = fminf(zmin, zs[j]);
-      mind = fminf(mind, dot3(ns[j], Nn));
-    }
-  }
+  const float da = qa.x - mu4, db = qa.z - mu4, dc = qb.x - mu4, dd = qb.z - mu4;
+  const float var4 = qsum(qa.y * da * da + qa.w * db * db + qb.y * dc * dc + qb.w * dd * dd) / fmaxf(n4, 1.0f);
+  const float k = nv > 0.0f ? 1.0f / nv : 0.0f;  // no early exit: every lane takes part in every shuffle
+  S0 = scale4(S0, k);
+  S1 = scale4(S1, k);
+  S3 = scale4(S3, k);
+  AC = scale4(AC, k);
+  const float Lacc = S0.x;
+  const float dl = p.P0.x - Lacc;
+  const float VA = qsum(ok ? dl * dl : 0.f) * k;
+  const float nx = Nx * k, ny = Ny * k, nz = Nz * k;
+  const float nl = fmaxf(sqrtf(nx * nx + ny * ny + nz * nz), 1e-6f);
+  const float4 Nn = make_float4(nx / nl, ny / nl, nz / nl, 0.f);
+  const float zmax = qmax(ok ? p.P2.z : -1e30f), zmin = qmin(ok ? p.P2.z : 1e30f);
+  const float mind = qmin(ok ? dot3(p.Ns, Nn) : 1e30f);
   const float dz = fminf(fmaxf((zmax - zmin) / fmaxf(zmin, 1e-6f), 0.0f), 1.0f);
   const float dn = fminf(fmaxf(1.0f - mind, 0.0f), 2.0f);
   const float2 oc = oct_enc(Nn.x, Nn.y, Nn.z);
@@ -363,16 +343,18 @@ HD_INL bool block_features_tile(const K1Smem &S, int lbx, int lby, float E, floa
   f[7] = log1p_w(fabsf(S1.z - S1.w) / (S1.w + 1e-3f));
   f[8] = oc.x; f[9] = oc.y; f[10] = dz; f[11] = dn;
   f[12] = S3.x; f[13] = S3.y; f[14] = S3.z; f[15] = S3.w;
-  f[16] = 1.0f - nv / 4.0f; f[17] = log1p_w(MV); f[18] = log1p_w(mu4); f[19] = log1p_w(VA);
-  G = make_float4(oc.x, oc.y, Z, nv);
+  f[16] = 1.0f - nv / 4.0f; f[17] = log1p_w(MV * k); f[18] = log1p_w(mu4); f[19] = log1p_w(VA);
+  if (nv == 0.0f) {  // hush.js:241-244: no valid pixel
+    G = make_float4(0.f, 0.f, -1.0f, 0.f);
+    return false;
+  }
+  G = make_float4(oc.x, oc.y, Zs * k, nv);
   return true;
 }
 
 struct FpSmem {
   float4 w[MLP_FP32_BLOB_BYTES / 16];  // transposed weights + biases (mlp_fp32_build_blob)
-  float4 fe[K1_NB][5];                 // features of each block, as stored
-  float4 h[K1_NB][4];                  // hidden activations of each block, exchanged within its 4-lane group
-  uint32_t flags[K1_NB];               // bit 0: block inside the half-res image, bit 1: block has valid pixels
+  float4 h[K1_NB][4];                  // hidden activations of each block, exchanged within its quad
 };
 
 HD_INL float4 ffma4(float s, float4 w, float4 a) {  // a + s * w as two packed FP32x2 FMAs
@@ -402,22 +384,25 @@ __global__ void __launch_bounds__(K1_NT, 3)
     for (int i = li; i < MLP_FP32_BLOB_BYTES / 16; i += NT) reinterpret_cast<uint4 *>(X_.w)[i] = __ldg(blob + i);
   }
   // phase 1: all tile loads, the pixel's own loads and its reprojection gathers in flight together, then the
-  // illumination tile
+  // illumination tile. Pixels map to threads by quads: lane j of quad b = li / 4 holds pixel (j & 1, j >> 1) of the
+  // tile's 2x2 block b, so block() and the MLP of a block run inside its quad without a block-wide barrier.
   const int ox = blockIdx.x * K1_TW - 1, oy = blockIdx.y * K1_TH - 1;
-  constexpr int NIT = (SW * SH + NT - 1) / NT;
+  constexpr int SWL = K1_SWL, NIT = (SWL * SH + NT - 1) / NT;
   uint2 tn[NIT], tr[NIT], tmt[NIT];
   bool tin[NIT];
 #pragma unroll
   for (int it = 0; it < NIT; it++) {
     const int i = li + it * NT;
-    const int qx = ox + i % SW, qy = oy + i / SW;
-    tin[it] = i < SW * SH && qx >= 0 && qy >= 0 && qx < f.W && qy < f.H;
+    const int qx = ox + i % SWL, qy = oy + i / SWL;
+    tin[it] = i < SWL * SH && qx >= 0 && qy >= 0 && qx < f.W && qy < f.H;
     const int cxq = clampi(qx, 0, f.W - 1), cyq = clampi(qy, 0, f.H - 1);
     tn[it] = __ldg(f.nd + cyq * f.p_nd + cxq);
     tr[it] = __ldg(f.rad + cyq * f.p_rad + cxq);
     tmt[it] = __ldg(f.mat + cyq * f.p_mat + cxq);
   }
-  const int tx = li % K1_TW, ty = li / K1_TW;
+  const int b = li >> 2, j = li & 3;
+  const int lbx = b % (K1_TW / 2), lby = b / (K1_TW / 2);
+  const int tx = 2 * lbx + (j & 1), ty = 2 * lby + (j >> 1);
   const int px = blockIdx.x * K1_TW + tx, py = blockIdx.y * K1_TH + ty;
   const bool pin = px < f.W && py < f.H;
   PixLoads PL;
@@ -425,7 +410,7 @@ __global__ void __launch_bounds__(K1_NT, 3)
 #pragma unroll
   for (int it = 0; it < NIT; it++) {
     const int i = li + it * NT;
-    if (i >= SW * SH) continue;
+    if (i >= SWL * SH) continue;
     float4 e = make_float4(0.f, 0.f, 0.f, L_INVALID);
     float2 lq = make_float2(0.f, 0.f);
     if (tin[it] && h4_to_f4(tn[it]).w >= 0.0f) {
@@ -436,67 +421,53 @@ __global__ void __launch_bounds__(K1_NT, 3)
       e.w = lum3(e.x, e.y, e.z);
       lq = make_float2(E * qf16(e.w), 1.0f);
     }
-    S.I[i] = e;
-    S.Lq[i] = lq;
+    const int si = (i / SWL) * SW + i % SWL;
+    S.I[si] = e;
+    S.Lq[si] = lq;
   }
   __syncthreads();
   if constexpr (TC) umma::fence_after_sync();
-  // phase 2: one pixel per thread
-  if (pin) {
-    temporal_pixel_fast(f, px, py, S, (ty + 1) * SW + tx + 1, li, PL);
-  } else {
-    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    S.P0[li] = z4; S.P1[li] = z4; S.P2[li] = make_float4(0.f, 0.f, -1.0f, 0.f); S.P3[li] = z4; S.P4[li] = z4;
-    S.Ns[li] = z4;
-  }
-  __syncthreads();
-  // phase 3a: block features, one thread per block (warps 0-1)
-  if (li < K1_NB) {
-    const int lbx = li % (K1_TW / 2), lby = li / (K1_TW / 2);
-    const int X = blockIdx.x * (K1_TW / 2) + lbx, Y = blockIdx.y * (K1_TH / 2) + lby;
-    const bool valid = X < f.W2 && Y < f.H2;
-    const int o = Y * f.W2 + X;
-    float fe[N_FEAT];
-    float4 AC, G;
-    const bool ok = block_features_tile(S, lbx, lby, E, fe, AC, G);
-    if (valid) {
+  // phase 2: pixel() per thread, then block() per quad
+  const PixOut po = pin ? temporal_pixel_fast(f, px, py, S, (ty + 1) * SW + tx + 1, PL) : pix_none();
+  const int X = blockIdx.x * (K1_TW / 2) + lbx, Y = blockIdx.y * (K1_TH / 2) + lby;
+  const bool valid = X < f.W2 && Y < f.H2;
+  const int o = Y * f.W2 + X;
+  float fe[N_FEAT];
+  float4 AC, G;
+  const bool ok = block_features_quad(S, po, lbx, lby, j, fe, AC, G);
+  if (valid) {  // one store per lane of the quad
+    if (j == 0) {
       // block means and guide: F2.zw and F3.xy of hush.js:280-281 (hush.js:241-244 without valid pixels)
       f.Ah[o] = ok ? make_uint2(pk(AC.x, AC.y), pk(AC.z, AC.w)) : make_uint2(0, 0);
+    } else if (j == 1) {
       f.Gh[o] = ok ? make_uint2(pk(G.x, G.y), pk(G.z, G.w)) : make_uint2(pk(0.f, 0.f), pk(-1.0f, 0.f));
+    } else if (j == 2) {
       // the decoded guide every half-res consumer forms from F3 (octDec of the stored oct normal, stored depth)
       float4 gd = oct_dec(ok ? quant1(qf16(G.x)) : 0.f, ok ? quant1(qf16(G.y)) : 0.f);
       gd.w = ok ? quant1(qf16(G.z)) : -1.0f;
       f.Gd[o] = gd;
     }
-    // the MLP sees the features as stored (packed f16, hush.js:278-280, 348-353)
+  }
+  // the MLP sees the features as stored (packed f16, hush.js:278-280, 348-353)
 #pragma unroll
-    for (int i = 0; i < N_FEAT; i++) fe[i] = ok ? __half2float(__ushort_as_half(f2h(qf16(fe[i])))) : 0.0f;
-    X_.flags[li] = (valid ? 1u : 0u) | (ok ? 2u : 0u);
-    if constexpr (TC) {
+  for (int i = 0; i < N_FEAT; i++) fe[i] = ok ? __half2float(__ushort_as_half(f2h(qf16(fe[i])))) : 0.0f;
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  if constexpr (TC) {
+    // lane j writes K columns 8j..8j+7 of the block's operand row (features 0..19, zero padded to 32)
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      if (j != c) continue;
       float v8[8];
 #pragma unroll
-      for (int c = 0; c < 4; c++) {
-#pragma unroll
-        for (int e = 0; e < 8; e++) v8[e] = 8 * c + e < N_FEAT ? fe[8 * c + e] : 0.0f;
-        *reinterpret_cast<uint4 *>(X_.a1 + umma::kmajor_off(li, 8 * c, 4)) = pack8<BF16>(v8);
-      }
-    } else {
-#pragma unroll
-      for (int c = 0; c < 5; c++) X_.fe[li][c] = make_float4(fe[4 * c], fe[4 * c + 1], fe[4 * c + 2], fe[4 * c + 3]);
+      for (int e = 0; e < 8; e++) v8[e] = 8 * c + e < N_FEAT ? fe[8 * c + e] : 0.0f;
+      *reinterpret_cast<uint4 *>(X_.a1 + umma::kmajor_off(b, 8 * c, 4)) = pack8<BF16>(v8);
     }
-  }
-  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-  if constexpr (!TC) {
+    if (j == 0) X_.flags[b] = (valid ? 1u : 0u) | (ok ? 2u : 0u);
     __syncthreads();
-    // phase 3b: FP32 MLP, a 4-lane group per block, lane k owns hidden units 4k..4k+3 and outputs k, 4+k, 8+k
-    const int b = li >> 2, k = li & 3;
+  } else {
+    // FP32 MLP inside the quad: lane k owns hidden units 4k..4k+3 and outputs k, 4+k, 8+k
+    const int k = j;
     const float4 *Wt = X_.w;
-    float fe[N_FEAT];
-#pragma unroll
-    for (int c = 0; c < 5; c++) {
-      const float4 t = X_.fe[b][c];
-      fe[4 * c] = t.x; fe[4 * c + 1] = t.y; fe[4 * c + 2] = t.z; fe[4 * c + 3] = t.w;
-    }
     float4 a = Wt[MLP_FP32_B1 + k];
 #pragma unroll
     for (int i = 0; i < N_FEAT; i++) a = ffma4(fe[i], Wt[MLP_FP32_W1 + i * 4 + k], a);
@@ -533,22 +504,20 @@ __global__ void __launch_bounds__(K1_NT, 3)
     float c0[4], c1[4], c2[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-      c0[q] = __shfl_sync(0xffffffffu, p0, base + q);
-      c1[q] = __shfl_sync(0xffffffffu, p1, base + q);
-      c2[q] = __shfl_sync(0xffffffffu, p2, base + q);
+      c0[q] = __shfl_sync(FULL, p0, base + q);
+      c1[q] = __shfl_sync(FULL, p1, base + q);
+      c2[q] = __shfl_sync(FULL, p2, base + q);
     }
-    const uint32_t fl = X_.flags[b];
-    if ((fl & 1u) && k < 3) {
-      const int lbx = b % (K1_TW / 2), lby = b / (K1_TW / 2);
-      const int o = (blockIdx.y * (K1_TH / 2) + lby) * f.W2 + blockIdx.x * (K1_TW / 2) + lbx;
+    if (valid && k < 3) {
       // INFER on a block without valid pixels writes zeros (hush.js:343-346)
-      const float4 v = !(fl & 2u) ? z4
+      const float4 v = !ok ? z4
                        : k == 0 ? make_float4(c0[0], c0[1], c0[2], c0[3])
                        : k == 1 ? make_float4(c1[0], c1[1], c1[2], c1[3])
                                 : make_float4(c2[0], c2[1], c2[2], c2[3]);
       sth(k == 0 ? f.par0 : k == 1 ? f.par1 : f.par2, o, v);
     }
-  } else {
+  }
+  if constexpr (TC) {
     if (li >= K1_NB) return;
     // warps 0-1: one row (block) per thread through the three tensor-core layers
     constexpr int B1 = 16 * N_FEAT, B2 = B1 + 16 + 16 * 16, B3 = B2 + 16 + N_OUT * 16;
