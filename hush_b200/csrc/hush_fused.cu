@@ -106,6 +106,13 @@ struct K1Smem {
   float2 Lq[K1_SW * K1_SH];  // (E * qf16(L), 1) for valid entries, (0, 0) otherwise: the 4x4 block statistics
 };
 
+// The illumination tile around one pixel: T(dx, dy) is the entry dx columns right and dy rows below it.
+struct RowTile {
+  const float4 *I;
+  int ti;
+  HD_INL float4 operator()(int dx, int dy) const { return I[ti + dy * K1_SW + dx]; }
+};
+
 // pixel()'s inputs to block(): P0..P4 as block() reads them and the decoded normal (Ns.w = 1 with a surface).
 struct PixOut {
   float4 P0, P1, P2, P3, P4, Ns;
@@ -144,8 +151,8 @@ HD_INL void pixel_issue(const HushFrame &f, int px, int py, PixLoads &L) {
 
 // pixel() of hush.js:111-223 over the (r, g, b, L) tile from the preloaded texels; same arithmetic as
 // temporal_pixel(). Writes A0, mom, key and returns the pixel's inputs to block().
-HD_INL PixOut temporal_pixel_fast(const HushFrame &f, int px, int py, const K1Smem &S, int ti, const PixLoads &PL) {
-  constexpr int SW = K1_SW;
+template <class Tile>
+HD_INL PixOut temporal_pixel_fast(const HushFrame &f, int px, int py, const Tile &T, const PixLoads &PL) {
   const int W = f.W, H = f.H;
   const float4 nd = h4_to_f4(PL.nd), mv = h4_to_f4(PL.mv);
   const int oi = py * W + px;
@@ -171,12 +178,12 @@ HD_INL PixOut temporal_pixel_fast(const HushFrame &f, int px, int py, const K1Sm
   const uint2 *k4 = PL.k4, *c4 = PL.c4, *m4 = PL.m4;
   const uint2 pqr = PL.pq, mrr = PL.mat;
   // 3x3 statistics of the illumination (valid neighbours), two passes
-  const float4 illum = S.I[ti];
+  const float4 illum = T(0, 0);
   const float l = illum.w;
   float s1x = 0.f, s1y = 0.f, s1z = 0.f, cnt = 0.f;
 #pragma unroll
   for (int j = 0; j < 9; j++) {
-    const float4 c = S.I[ti + (j / 3 - 1) * SW + (j % 3 - 1)];
+    const float4 c = T(j % 3 - 1, j / 3 - 1);
     s1x += c.x; s1y += c.y; s1z += c.z;  // invalid entries hold rgb = 0
     cnt += l_valid(c.w) ? 1.0f : 0.0f;
   }
@@ -186,7 +193,7 @@ HD_INL PixOut temporal_pixel_fast(const HushFrame &f, int px, int py, const K1Sm
   float svx = 0.f, svy = 0.f, svz = 0.f, svar = 0.f;
 #pragma unroll
   for (int j = 0; j < 9; j++) {
-    const float4 c = S.I[ti + (j / 3 - 1) * SW + (j % 3 - 1)];
+    const float4 c = T(j % 3 - 1, j / 3 - 1);
     if (l_valid(c.w)) {
       const float dx = c.x - mux, dy = c.y - muy, dz = c.z - muz, dl = c.w - slm;
       svx += dx * dx; svy += dy * dy; svz += dz * dz;
@@ -428,7 +435,7 @@ __global__ void __launch_bounds__(K1_NT, 3)
   __syncthreads();
   if constexpr (TC) umma::fence_after_sync();
   // phase 2: pixel() per thread, then block() per quad
-  const PixOut po = pin ? temporal_pixel_fast(f, px, py, S, (ty + 1) * SW + tx + 1, PL) : pix_none();
+  const PixOut po = pin ? temporal_pixel_fast(f, px, py, RowTile{S.I, (ty + 1) * SW + tx + 1}, PL) : pix_none();
   const int X = blockIdx.x * (K1_TW / 2) + lbx, Y = blockIdx.y * (K1_TH / 2) + lby;
   const bool valid = X < f.W2 && Y < f.H2;
   const int o = Y * f.W2 + X;
@@ -560,6 +567,223 @@ __global__ void __launch_bounds__(K1_NT, 3)
     sth(f.par1, orow, p1);
     sth(f.par2, orow, p2);
   }
+}
+
+// ------------------------------------------------------------------------------------------------ stage 0, FP32 form
+// One thread per 2x2 block: tile 64 x 16 pixels = 32 x 8 blocks, 256 threads. Each thread runs pixel() for its four
+// pixels in block order, accumulates block()'s sums in registers in the WGSL's order (hush.js:226-282), forms the 20
+// features once and runs the whole FP32 MLP (weights read as shared-memory broadcasts), so after the tile barrier no
+// thread waits for another. The tile is stored column-parity-split (even and odd columns in separate rows of 33
+// entries): neighbouring threads, two pixel columns apart, then read consecutive 16-byte entries.
+constexpr int KB_TW = 64, KB_TH = 16, KB_NT = (KB_TW / 2) * (KB_TH / 2);
+constexpr int KB_SWL = KB_TW + 2, KB_SH = KB_TH + 2, KB_HW = KB_SWL / 2;
+HD_INL int kb_tix(int r, int c) { return (2 * r + (c & 1)) * KB_HW + (c >> 1); }
+
+struct KbSmem {
+  float4 I[2 * KB_HW * KB_SH];   // illumination (r, g, b) and L (luminance or L_INVALID), apron 1
+  float2 Lq[2 * KB_HW * KB_SH];  // (E * qf16(L), 1) for valid entries, (0, 0) otherwise
+  float4 w[MLP_FP32_BLOB_BYTES / 16];
+};
+
+struct ParityTile {
+  const float4 *I;
+  int r, c;  // tile row / column of the pixel
+  HD_INL float4 operator()(int dx, int dy) const { return I[kb_tix(r + dy, c + dx)]; }
+};
+
+__global__ void __launch_bounds__(KB_NT, 2)
+    k_temporal_block(const __grid_constant__ HushFrame f, const uint4 *__restrict__ blob) {
+  __shared__ KbSmem S;
+  const int li = threadIdx.x;
+  const float E = f.exposure;
+  for (int i = li; i < MLP_FP32_BLOB_BYTES / 16; i += KB_NT) reinterpret_cast<uint4 *>(S.w)[i] = __ldg(blob + i);
+  const int lbx = li % (KB_TW / 2), lby = li / (KB_TW / 2);
+  const int px0 = blockIdx.x * KB_TW + 2 * lbx, py0 = blockIdx.y * KB_TH + 2 * lby;
+  // phase 1: the first pixel's loads and gathers in flight with the tile loads
+  PixLoads PL;
+  if (px0 < f.W && py0 < f.H) pixel_issue(f, px0, py0, PL);
+  const int ox = blockIdx.x * KB_TW - 1, oy = blockIdx.y * KB_TH - 1;
+  constexpr int N = KB_SWL * KB_SH;
+#pragma unroll 1
+  for (int i0 = 0; i0 < N; i0 += 2 * KB_NT) {
+    uint2 tn[2], tr[2], tm[2];
+    bool tin[2];
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int i = i0 + u * KB_NT + li;
+      const int qx = ox + i % KB_SWL, qy = oy + i / KB_SWL;
+      tin[u] = i < N && qx >= 0 && qy >= 0 && qx < f.W && qy < f.H;
+      const int cx = clampi(qx, 0, f.W - 1), cy = clampi(qy, 0, f.H - 1);
+      tn[u] = __ldg(f.nd + cy * f.p_nd + cx);
+      tr[u] = __ldg(f.rad + cy * f.p_rad + cx);
+      tm[u] = __ldg(f.mat + cy * f.p_mat + cx);
+    }
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int i = i0 + u * KB_NT + li;
+      if (i >= N) continue;
+      float4 e = make_float4(0.f, 0.f, 0.f, L_INVALID);
+      float2 lq = make_float2(0.f, 0.f);
+      if (tin[u] && h4_to_f4(tn[u]).w >= 0.0f) {
+        const float4 r = h4_to_f4(tr[u]), m = h4_to_f4(tm[u]);
+        e.x = r.x / fmaxf(m.x, 1e-3f);
+        e.y = r.y / fmaxf(m.y, 1e-3f);
+        e.z = r.z / fmaxf(m.z, 1e-3f);
+        e.w = lum3(e.x, e.y, e.z);
+        lq = make_float2(E * qf16(e.w), 1.0f);
+      }
+      const int t = kb_tix(i / KB_SWL, i % KB_SWL);
+      S.I[t] = e;
+      S.Lq[t] = lq;
+    }
+  }
+  __syncthreads();
+  // phase 2: pixel() of the four pixels (block order: top-left, top-right, bottom-left, bottom-right), block() sums
+  float nv = 0.f, Nx = 0.f, Ny = 0.f, Nz = 0.f, MV = 0.f, Z = 0.f;
+  float4 S0 = make_float4(0.f, 0.f, 0.f, 0.f), S1 = S0, S3 = S0, AC = S0;
+  float la[4], zs[4], nx4[4], ny4[4], nz4[4];
+  bool okp[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int px = px0 + (q & 1), py = py0 + (q >> 1);
+    const bool pin = px < f.W && py < f.H;
+    if (q > 0 && pin) pixel_issue(f, px, py, PL);
+    const PixOut p = pin ? temporal_pixel_fast(f, px, py, ParityTile{S.I, 2 * lby + (q >> 1) + 1, 2 * lbx + (q & 1) + 1}, PL)
+                         : pix_none();
+    okp[q] = p.Ns.w != 0.0f;
+    la[q] = p.P0.x;
+    zs[q] = p.P2.z;
+    nx4[q] = p.Ns.x; ny4[q] = p.Ns.y; nz4[q] = p.Ns.z;
+    if (okp[q]) {
+      nv += 1.0f;
+      S0.x += p.P0.x; S0.y += p.P0.y; S0.z += p.P0.z; S0.w += p.P0.w;
+      S1.x += p.P1.x; S1.y += p.P1.y; S1.z += p.P1.z; S1.w += p.P1.w;
+      Nx += p.Ns.x; Ny += p.Ns.y; Nz += p.Ns.z;
+      S3.x += p.P3.x; S3.y += p.P3.y; S3.z += p.P3.z; S3.w += p.P3.w;
+      AC.x += p.P4.x; AC.y += p.P4.y; AC.z += p.P4.z; AC.w += p.P4.w;
+      MV += p.P2.w;
+      Z += p.P2.z;
+    }
+  }
+  // phase 3: block() (hush.js:226-282)
+  const int X = blockIdx.x * (KB_TW / 2) + lbx, Y = blockIdx.y * (KB_TH / 2) + lby;
+  const bool valid = X < f.W2 && Y < f.H2;
+  const bool ok = nv != 0.0f;
+  float fe[N_FEAT];
+  float4 G = make_float4(0.f, 0.f, -1.0f, 0.f);
+  {
+    const float k = ok ? 1.0f / nv : 0.0f;
+    S0 = scale4(S0, k); S1 = scale4(S1, k); S3 = scale4(S3, k); AC = scale4(AC, k);
+    Nx *= k; Ny *= k; Nz *= k;
+    MV *= k;
+    Z *= k;
+    const float Lacc = S0.x;
+    float VA = 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (okp[q]) VA += (la[q] - Lacc) * (la[q] - Lacc);
+    VA *= k;
+    // 4x4 neighbourhood (block +-1) of the quantised luminance, row-major
+    float s1 = 0.f, n4 = 0.f;
+    float2 w16[16];
+#pragma unroll
+    for (int e = 0; e < 16; e++) {
+      w16[e] = S.Lq[kb_tix(2 * lby + (e >> 2), 2 * lbx + (e & 3))];
+      s1 += w16[e].y * w16[e].x;
+      n4 += w16[e].y;
+    }
+    const float mu4 = s1 / fmaxf(n4, 1.0f);
+    float var4 = 0.f;
+#pragma unroll
+    for (int e = 0; e < 16; e++) {
+      const float d = w16[e].x - mu4;
+      var4 += w16[e].y * d * d;
+    }
+    var4 /= fmaxf(n4, 1.0f);
+    const float nl = fmaxf(sqrtf(Nx * Nx + Ny * Ny + Nz * Nz), 1e-6f);
+    const float nnx = Nx / nl, nny = Ny / nl, nnz = Nz / nl;
+    float zmax = -1e30f, zmin = 1e30f, mind = 1e30f;
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (okp[q]) {
+        zmax = fmaxf(zmax, zs[q]);
+        zmin = fminf(zmin, zs[q]);
+        mind = fminf(mind, nx4[q] * nnx + ny4[q] * nny + nz4[q] * nnz);
+      }
+    const float dz = fminf(fmaxf((zmax - zmin) / fmaxf(zmin, 1e-6f), 0.0f), 1.0f);
+    const float dn = fminf(fmaxf(1.0f - mind, 0.0f), 2.0f);
+    const float2 oc = oct_enc(nnx, nny, nnz);
+    fe[0] = log1p_w(Lacc); fe[1] = log1p_w(S0.y); fe[2] = log1p_w(S0.z); fe[3] = log1p_w(var4);
+    fe[4] = S0.w / HMAX; fe[5] = S1.x; fe[6] = log1p_w(S1.y);
+    fe[7] = log1p_w(fabsf(S1.z - S1.w) / (S1.w + 1e-3f));
+    fe[8] = oc.x; fe[9] = oc.y; fe[10] = dz; fe[11] = dn;
+    fe[12] = S3.x; fe[13] = S3.y; fe[14] = S3.z; fe[15] = S3.w;
+    fe[16] = 1.0f - nv / 4.0f; fe[17] = log1p_w(MV); fe[18] = log1p_w(mu4); fe[19] = log1p_w(VA);
+    if (ok) G = make_float4(oc.x, oc.y, Z, nv);
+  }
+  const int o = Y * f.W2 + X;
+  if (valid) {
+    // block means and guide: F2.zw and F3.xy of hush.js:280-281 (hush.js:241-244 without valid pixels)
+    f.Ah[o] = ok ? make_uint2(pk(AC.x, AC.y), pk(AC.z, AC.w)) : make_uint2(0, 0);
+    f.Gh[o] = ok ? make_uint2(pk(G.x, G.y), pk(G.z, G.w)) : make_uint2(pk(0.f, 0.f), pk(-1.0f, 0.f));
+    // the decoded guide every half-res consumer forms from F3 (octDec of the stored oct normal, stored depth)
+    float4 gd = oct_dec(ok ? quant1(qf16(G.x)) : 0.f, ok ? quant1(qf16(G.y)) : 0.f);
+    gd.w = ok ? quant1(qf16(G.z)) : -1.0f;
+    f.Gd[o] = gd;
+  }
+  if (!valid) return;
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (!ok) {  // INFER on a block without valid pixels writes zeros (hush.js:343-346)
+    sth(f.par0, o, z4); sth(f.par1, o, z4); sth(f.par2, o, z4);
+    return;
+  }
+  // phase 4: the MLP (hush.js:681-704) on the features as stored (packed f16, hush.js:278-280, 348-353); each unit
+  // is its bias plus the inputs in increasing index, FP32 with packed FP32x2 FMAs
+#pragma unroll
+  for (int i = 0; i < N_FEAT; i++) fe[i] = __half2float(__ushort_as_half(f2h(qf16(fe[i]))));
+  const float4 *Wt = S.w;
+  float4 a[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) a[q] = Wt[MLP_FP32_B1 + q];
+#pragma unroll
+  for (int i = 0; i < N_FEAT; i++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) a[q] = ffma4(fe[i], Wt[MLP_FP32_W1 + i * 4 + q], a[q]);
+  float h[16];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    h[4 * q] = fmaxf(a[q].x, 0.f); h[4 * q + 1] = fmaxf(a[q].y, 0.f);
+    h[4 * q + 2] = fmaxf(a[q].z, 0.f); h[4 * q + 3] = fmaxf(a[q].w, 0.f);
+  }
+#pragma unroll
+  for (int q = 0; q < 4; q++) a[q] = Wt[MLP_FP32_B2 + q];
+#pragma unroll
+  for (int i = 0; i < 16; i++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) a[q] = ffma4(h[i], Wt[MLP_FP32_W2 + i * 4 + q], a[q]);
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    h[4 * q] = fmaxf(a[q].x, 0.f); h[4 * q + 1] = fmaxf(a[q].y, 0.f);
+    h[4 * q + 2] = fmaxf(a[q].z, 0.f); h[4 * q + 3] = fmaxf(a[q].w, 0.f);
+  }
+#pragma unroll
+  for (int q = 0; q < 4; q++) a[q] = Wt[MLP_FP32_B3 + q];  // (output q, 4 + q, 8 + q, 0)
+#pragma unroll
+  for (int i = 0; i < 16; i++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) a[q] = ffma4(h[i], Wt[MLP_FP32_W3 + i * 4 + q], a[q]);
+  float out[N_OUT];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    out[q] = a[q].x;
+    out[4 + q] = a[q].y;
+    out[8 + q] = a[q].z;
+  }
+  float4 p0, p1, p2;
+  mlp_heads(out, p0, p1, p2);
+  sth(f.par0, o, p0);
+  sth(f.par1, o, p1);
+  sth(f.par2, o, p2);
 }
 
 // ------------------------------------------------------------------------------------------------ half / quarter
@@ -873,7 +1097,9 @@ cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpW16 &w16,
       if (mlp_mode == 1) k_temporal_fused<true, true><<<grid, K1_TW * K1_TH, 0, st>>>(f, w16, blob);
       else if (mlp_mode == 2)
         k_temporal_fused<true, false><<<grid, K1_TW * K1_TH, 0, st>>>(f, w16, blob + MLP_TC_BLOB_BYTES / 16);
-      else k_temporal_fused<false, false><<<grid, K1_TW * K1_TH, 0, st>>>(f, w16, blob + 2 * MLP_TC_BLOB_BYTES / 16);
+      else
+        k_temporal_block<<<dim3((f.W + KB_TW - 1) / KB_TW, (f.H + KB_TH - 1) / KB_TH), KB_NT, 0, st>>>(
+            f, blob + 2 * MLP_TC_BLOB_BYTES / 16);
       break;
     }
     case 1: k_half_stage<1><<<hx * hy + qx * qy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx); break;
