@@ -31,31 +31,12 @@ HD_INL float4 gh_decode(float4 g) {  // (oct normal, depth, count) -> (normal, d
 }
 
 // ------------------------------------------------------------------------------------------------ stage 0
-// Tile 32 x 8 pixels = 16 x 4 blocks, 256 threads, three phases:
-//   1. illumination tile (apron 1) in shared memory as (r, g, b, L): L = luminance, or L_INVALID outside the image
-//      or on sky
-//   2. pixel(): one pixel per thread (hush.js:111-223), feature inputs P0..P4 to shared memory
-//   3. block() (hush.js:226-282), one thread per 2x2 block, from the per-pixel terms phases 1-2 left in shared
-//      memory (decoded normals, quantised luminances). The FP32 MLP then splits each layer over a 4-lane group per
-//      block (4 hidden units per lane, packed FP32x2 FMAs, transposed weights in shared memory); the tensor-core form
-//      (TC) writes the features as MMA operand rows and warps 0-1 run the three layers as tcgen05 MMAs (M = 128 with
-//      64 rows used, N = 16, K = 32 / 16 / 16) on bf16 or f16 operands with FP32 accumulation in TMEM; bias, ReLU and
-//      the heads stay FP32.
-constexpr int K1_TW = 32, K1_TH = 8;
-constexpr int K1_NB = (K1_TW / 2) * (K1_TH / 2);  // 64 blocks
+// TEMPORAL pixel() (hush.js:111-223), block() (hush.js:226-282) and INFER's MLP with its heads (hush.js:312-365) in
+// one kernel, one thread per 2x2 block (k_temporal_block below).
 constexpr uint32_t MBAR_POLLS = 1u << 22;
 // L of a tile entry outside the image or on sky (a valid luminance is finite and far above it)
 constexpr float L_INVALID = -1e30f;
 HD_INL bool l_valid(float L) { return L > -1e29f; }
-
-struct TcSmem {
-  alignas(128) uint8_t a1[128 * 32 * 2];  // layer-1 A: 128 rows x K 32 (features 0..19, zero padded)
-  alignas(128) uint8_t a2[128 * 16 * 2];  // layer-2 / layer-3 A: 128 rows x K 16
-  alignas(128) uint8_t b[MLP_TC_BLOB_BYTES];  // B1 (16 x 32), B2 (16 x 16), B3 (16 x 16)
-  alignas(8) uint64_t mbar;
-  uint32_t tmem;
-  uint32_t flags[K1_NB];  // bit 0: block inside the half-res image, bit 1: block has valid pixels
-};
 
 template <bool BF16>
 HD_INL uint16_t to_op(float v) {
@@ -71,47 +52,6 @@ HD_INL uint4 pack8(const float *v) {
   q.w = (uint32_t)to_op<BF16>(v[6]) | ((uint32_t)to_op<BF16>(v[7]) << 16);
   return q;
 }
-
-// One MMA layer of the tensor-core MLP, run by warps 0-1: thread 0 issues after the 64-thread barrier and commits;
-// every thread waits for the phase and loads its row (16 columns). Returns false if the wait gave up.
-HD_INL bool tc_layer(TcSmem &S, int li, bool first, uint32_t b_off, uint32_t kcore_b, uint32_t idesc, uint32_t phase,
-                     float *d) {
-  umma::fence_before_sync();
-  umma::fence_proxy_async();
-  asm volatile("bar.sync 1, 64;" ::: "memory");
-  const uint32_t mbar = umma::smem_u32(&S.mbar);
-  if (li == 0) {
-    umma::fence_after_sync();
-    const uint32_t a = umma::smem_u32(first ? S.a1 : S.a2);
-    const uint32_t kcore_a = first ? 4u : 2u;
-    const uint32_t b = umma::smem_u32(S.b) + b_off;
-    const int kblocks = first ? 2 : 1;
-    for (int kb = 0; kb < kblocks; kb++)
-      umma::mma_f16(S.tmem, umma::sdesc(a + 256u * kb, 128, 128 * kcore_a),
-                    umma::sdesc(b + 256u * kb, 128, 128 * kcore_b), idesc, kb > 0 ? 1u : 0u);
-    umma::commit(mbar);
-  }
-  const bool ok = umma::mbar_wait_bounded(mbar, phase, MBAR_POLLS);
-  umma::fence_after_sync();
-  umma::ld16(S.tmem + ((uint32_t)(32 * (li >> 5)) << 16), d);
-  return ok;
-}
-
-// Shared memory of the fused temporal kernel: the illumination tile (apron 1). Rows are stored with a stride of 36
-// entries (34 used): with the quad mapping of pixels to threads (a warp covers 16 x 2 pixels), the two rows a
-// quarter-warp reads then fall into disjoint bank halves.
-constexpr int K1_SWL = K1_TW + 2, K1_SW = K1_TW + 4, K1_SH = K1_TH + 2, K1_NT = K1_TW * K1_TH;
-struct K1Smem {
-  float4 I[K1_SW * K1_SH];   // illumination (r, g, b) and L (luminance or L_INVALID)
-  float2 Lq[K1_SW * K1_SH];  // (E * qf16(L), 1) for valid entries, (0, 0) otherwise: the 4x4 block statistics
-};
-
-// The illumination tile around one pixel: T(dx, dy) is the entry dx columns right and dy rows below it.
-struct RowTile {
-  const float4 *I;
-  int ti;
-  HD_INL float4 operator()(int dx, int dy) const { return I[ti + dy * K1_SW + dx]; }
-};
 
 // pixel()'s inputs to block(): P0..P4 as block() reads them and the decoded normal (Ns.w = 1 with a surface).
 struct PixOut {
@@ -291,78 +231,7 @@ HD_INL PixOut temporal_pixel_fast(const HushFrame &f, int px, int py, const Tile
   return o;
 }
 
-// Sums over the 4 lanes of a quad (lanes 4b..4b+3 hold the pixels of one 2x2 block).
-constexpr unsigned FULL = 0xffffffffu;
-HD_INL float qsum(float v) {
-  v += __shfl_xor_sync(FULL, v, 1);
-  return v + __shfl_xor_sync(FULL, v, 2);
-}
-HD_INL float4 qsum4(float4 v) { return make_float4(qsum(v.x), qsum(v.y), qsum(v.z), qsum(v.w)); }
-HD_INL float qmin(float v) {
-  v = fminf(v, __shfl_xor_sync(FULL, v, 1));
-  return fminf(v, __shfl_xor_sync(FULL, v, 2));
-}
-HD_INL float qmax(float v) {
-  v = fmaxf(v, __shfl_xor_sync(FULL, v, 1));
-  return fmaxf(v, __shfl_xor_sync(FULL, v, 2));
-}
 HD_INL float4 scale4(float4 v, float k) { return make_float4(v.x * k, v.y * k, v.z * k, v.w * k); }
-
-// block() (hush.js:226-282) for the 2x2 block of this lane's quad (lane j holds pixel (j & 1, j >> 1) of block
-// (lbx, lby)); every lane of the quad returns the 20 features, the block mean colour AC and the guide
-// G = (oct normal, Z, count). Returns nv > 0. All 32 lanes of the warp must call it.
-HD_INL bool block_features_quad(const K1Smem &S, const PixOut &p, int lbx, int lby, int j, float *f, float4 &AC,
-                                float4 &G) {
-  constexpr int SW = K1_SW;
-  const bool ok = p.Ns.w != 0.0f;
-  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-  const float nv = qsum(ok ? 1.0f : 0.0f);
-  float4 S0 = qsum4(ok ? p.P0 : z4), S1 = qsum4(ok ? p.P1 : z4), S3 = qsum4(ok ? p.P3 : z4);
-  AC = qsum4(ok ? p.P4 : z4);
-  const float Nx = qsum(ok ? p.Ns.x : 0.f), Ny = qsum(ok ? p.Ns.y : 0.f), Nz = qsum(ok ? p.Ns.z : 0.f);
-  const float MV = qsum(ok ? p.P2.w : 0.f), Zs = qsum(ok ? p.P2.z : 0.f);
-  // the 4x4 luminance neighbourhood (block +-1): lane j takes row j of the window
-  const float4 *lq = reinterpret_cast<const float4 *>(&S.Lq[(2 * lby + j) * SW + 2 * lbx]);
-  const float4 qa = lq[0], qb = lq[1];  // (x, y) pairs of 4 consecutive entries
-  const float s1 = qsum(qa.y * qa.x + qa.w * qa.z + qb.y * qb.x + qb.w * qb.z);
-  const float n4 = qsum(qa.y + qa.w + qb.y + qb.w);
-  const float mu4 = s1 / fmaxf(n4, 1.0f);
-  const float da = qa.x - mu4, db = qa.z - mu4, dc = qb.x - mu4, dd = qb.z - mu4;
-  const float var4 = qsum(qa.y * da * da + qa.w * db * db + qb.y * dc * dc + qb.w * dd * dd) / fmaxf(n4, 1.0f);
-  const float k = nv > 0.0f ? 1.0f / nv : 0.0f;  // no early exit: every lane takes part in every shuffle
-  S0 = scale4(S0, k);
-  S1 = scale4(S1, k);
-  S3 = scale4(S3, k);
-  AC = scale4(AC, k);
-  const float Lacc = S0.x;
-  const float dl = p.P0.x - Lacc;
-  const float VA = qsum(ok ? dl * dl : 0.f) * k;
-  const float nx = Nx * k, ny = Ny * k, nz = Nz * k;
-  const float nl = fmaxf(sqrtf(nx * nx + ny * ny + nz * nz), 1e-6f);
-  const float4 Nn = make_float4(nx / nl, ny / nl, nz / nl, 0.f);
-  const float zmax = qmax(ok ? p.P2.z : -1e30f), zmin = qmin(ok ? p.P2.z : 1e30f);
-  const float mind = qmin(ok ? dot3(p.Ns, Nn) : 1e30f);
-  const float dz = fminf(fmaxf((zmax - zmin) / fmaxf(zmin, 1e-6f), 0.0f), 1.0f);
-  const float dn = fminf(fmaxf(1.0f - mind, 0.0f), 2.0f);
-  const float2 oc = oct_enc(Nn.x, Nn.y, Nn.z);
-  f[0] = log1p_w(Lacc); f[1] = log1p_w(S0.y); f[2] = log1p_w(S0.z); f[3] = log1p_w(var4);
-  f[4] = S0.w / HMAX; f[5] = S1.x; f[6] = log1p_w(S1.y);
-  f[7] = log1p_w(fabsf(S1.z - S1.w) / (S1.w + 1e-3f));
-  f[8] = oc.x; f[9] = oc.y; f[10] = dz; f[11] = dn;
-  f[12] = S3.x; f[13] = S3.y; f[14] = S3.z; f[15] = S3.w;
-  f[16] = 1.0f - nv / 4.0f; f[17] = log1p_w(MV * k); f[18] = log1p_w(mu4); f[19] = log1p_w(VA);
-  if (nv == 0.0f) {  // hush.js:241-244: no valid pixel
-    G = make_float4(0.f, 0.f, -1.0f, 0.f);
-    return false;
-  }
-  G = make_float4(oc.x, oc.y, Zs * k, nv);
-  return true;
-}
-
-struct FpSmem {
-  float4 w[MLP_FP32_BLOB_BYTES / 16];  // transposed weights + biases (mlp_fp32_build_blob)
-  float4 h[K1_NB][4];                  // hidden activations of each block, exchanged within its quad
-};
 
 HD_INL float4 ffma4(float s, float4 w, float4 a) {  // a + s * w as two packed FP32x2 FMAs
   const float2 lo = __ffma2_rn(make_float2(s, s), make_float2(w.x, w.y), make_float2(a.x, a.y));
@@ -370,211 +239,14 @@ HD_INL float4 ffma4(float s, float4 w, float4 a) {  // a + s * w as two packed F
   return make_float4(lo.x, lo.y, hi.x, hi.y);
 }
 
-template <bool TC, bool BF16>
-__global__ void __launch_bounds__(K1_NT, 3)
-    k_temporal_fused(const __grid_constant__ HushFrame f, const __grid_constant__ MlpW16 w, const uint4 *blob) {
-  constexpr int SW = K1_SW, SH = K1_SH, NT = K1_NT;
-  __shared__ K1Smem S;
-  __shared__ std::conditional_t<TC, TcSmem, FpSmem> X_;
-  const int li = threadIdx.x;
-  const float E = f.exposure;
-  if constexpr (TC) {
-    if (li < 32) {
-      umma::tmem_alloc(umma::smem_u32(&X_.tmem), 32);
-      umma::tmem_relinquish();
-    }
-    if (li == 0) umma::mbar_init(umma::smem_u32(&X_.mbar), 1);
-    if (li < MLP_TC_BLOB_BYTES / 16) reinterpret_cast<uint4 *>(X_.b)[li] = __ldg(blob + li);
-    umma::fence_proxy_async();
-    umma::fence_before_sync();
-  } else {
-    for (int i = li; i < MLP_FP32_BLOB_BYTES / 16; i += NT) reinterpret_cast<uint4 *>(X_.w)[i] = __ldg(blob + i);
-  }
-  // phase 1: all tile loads, the pixel's own loads and its reprojection gathers in flight together, then the
-  // illumination tile. Pixels map to threads by quads: lane j of quad b = li / 4 holds pixel (j & 1, j >> 1) of the
-  // tile's 2x2 block b, so block() and the MLP of a block run inside its quad without a block-wide barrier.
-  const int ox = blockIdx.x * K1_TW - 1, oy = blockIdx.y * K1_TH - 1;
-  constexpr int SWL = K1_SWL, NIT = (SWL * SH + NT - 1) / NT;
-  uint2 tn[NIT], tr[NIT], tmt[NIT];
-  bool tin[NIT];
-#pragma unroll
-  for (int it = 0; it < NIT; it++) {
-    const int i = li + it * NT;
-    const int qx = ox + i % SWL, qy = oy + i / SWL;
-    tin[it] = i < SWL * SH && qx >= 0 && qy >= 0 && qx < f.W && qy < f.H;
-    const int cxq = clampi(qx, 0, f.W - 1), cyq = clampi(qy, 0, f.H - 1);
-    tn[it] = __ldg(f.nd + cyq * f.p_nd + cxq);
-    tr[it] = __ldg(f.rad + cyq * f.p_rad + cxq);
-    tmt[it] = __ldg(f.mat + cyq * f.p_mat + cxq);
-  }
-  const int b = li >> 2, j = li & 3;
-  const int lbx = b % (K1_TW / 2), lby = b / (K1_TW / 2);
-  const int tx = 2 * lbx + (j & 1), ty = 2 * lby + (j >> 1);
-  const int px = blockIdx.x * K1_TW + tx, py = blockIdx.y * K1_TH + ty;
-  const bool pin = px < f.W && py < f.H;
-  PixLoads PL;
-  if (pin) pixel_issue(f, px, py, PL);
-#pragma unroll
-  for (int it = 0; it < NIT; it++) {
-    const int i = li + it * NT;
-    if (i >= SWL * SH) continue;
-    float4 e = make_float4(0.f, 0.f, 0.f, L_INVALID);
-    float2 lq = make_float2(0.f, 0.f);
-    if (tin[it] && h4_to_f4(tn[it]).w >= 0.0f) {
-      const float4 r = h4_to_f4(tr[it]), m = h4_to_f4(tmt[it]);
-      e.x = r.x / fmaxf(m.x, 1e-3f);
-      e.y = r.y / fmaxf(m.y, 1e-3f);
-      e.z = r.z / fmaxf(m.z, 1e-3f);
-      e.w = lum3(e.x, e.y, e.z);
-      lq = make_float2(E * qf16(e.w), 1.0f);
-    }
-    const int si = (i / SWL) * SW + i % SWL;
-    S.I[si] = e;
-    S.Lq[si] = lq;
-  }
-  __syncthreads();
-  if constexpr (TC) umma::fence_after_sync();
-  // phase 2: pixel() per thread, then block() per quad
-  const PixOut po = pin ? temporal_pixel_fast(f, px, py, RowTile{S.I, (ty + 1) * SW + tx + 1}, PL) : pix_none();
-  const int X = blockIdx.x * (K1_TW / 2) + lbx, Y = blockIdx.y * (K1_TH / 2) + lby;
-  const bool valid = X < f.W2 && Y < f.H2;
-  const int o = Y * f.W2 + X;
-  float fe[N_FEAT];
-  float4 AC, G;
-  const bool ok = block_features_quad(S, po, lbx, lby, j, fe, AC, G);
-  if (valid) {  // one store per lane of the quad
-    if (j == 0) {
-      // block means and guide: F2.zw and F3.xy of hush.js:280-281 (hush.js:241-244 without valid pixels)
-      f.Ah[o] = ok ? make_uint2(pk(AC.x, AC.y), pk(AC.z, AC.w)) : make_uint2(0, 0);
-    } else if (j == 1) {
-      f.Gh[o] = ok ? make_uint2(pk(G.x, G.y), pk(G.z, G.w)) : make_uint2(pk(0.f, 0.f), pk(-1.0f, 0.f));
-    } else if (j == 2) {
-      // the decoded guide every half-res consumer forms from F3 (octDec of the stored oct normal, stored depth)
-      float4 gd = oct_dec(ok ? quant1(qf16(G.x)) : 0.f, ok ? quant1(qf16(G.y)) : 0.f);
-      gd.w = ok ? quant1(qf16(G.z)) : -1.0f;
-      f.Gd[o] = gd;
-    }
-  }
-  // the MLP sees the features as stored (packed f16, hush.js:278-280, 348-353)
-#pragma unroll
-  for (int i = 0; i < N_FEAT; i++) fe[i] = ok ? __half2float(__ushort_as_half(f2h(qf16(fe[i])))) : 0.0f;
-  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-  if constexpr (TC) {
-    // lane j writes K columns 8j..8j+7 of the block's operand row (features 0..19, zero padded to 32)
-#pragma unroll
-    for (int c = 0; c < 4; c++) {
-      if (j != c) continue;
-      float v8[8];
-#pragma unroll
-      for (int e = 0; e < 8; e++) v8[e] = 8 * c + e < N_FEAT ? fe[8 * c + e] : 0.0f;
-      *reinterpret_cast<uint4 *>(X_.a1 + umma::kmajor_off(b, 8 * c, 4)) = pack8<BF16>(v8);
-    }
-    if (j == 0) X_.flags[b] = (valid ? 1u : 0u) | (ok ? 2u : 0u);
-    __syncthreads();
-  } else {
-    // FP32 MLP inside the quad: lane k owns hidden units 4k..4k+3 and outputs k, 4+k, 8+k
-    const int k = j;
-    const float4 *Wt = X_.w;
-    float4 a = Wt[MLP_FP32_B1 + k];
-#pragma unroll
-    for (int i = 0; i < N_FEAT; i++) a = ffma4(fe[i], Wt[MLP_FP32_W1 + i * 4 + k], a);
-    X_.h[b][k] = make_float4(fmaxf(a.x, 0.f), fmaxf(a.y, 0.f), fmaxf(a.z, 0.f), fmaxf(a.w, 0.f));
-    __syncwarp();
-    float h[16];
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const float4 t = X_.h[b][q];
-      h[4 * q] = t.x; h[4 * q + 1] = t.y; h[4 * q + 2] = t.z; h[4 * q + 3] = t.w;
-    }
-    __syncwarp();
-    a = Wt[MLP_FP32_B2 + k];
-#pragma unroll
-    for (int i = 0; i < 16; i++) a = ffma4(h[i], Wt[MLP_FP32_W2 + i * 4 + k], a);
-    X_.h[b][k] = make_float4(fmaxf(a.x, 0.f), fmaxf(a.y, 0.f), fmaxf(a.z, 0.f), fmaxf(a.w, 0.f));
-    __syncwarp();
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const float4 t = X_.h[b][q];
-      h[4 * q] = t.x; h[4 * q + 1] = t.y; h[4 * q + 2] = t.z; h[4 * q + 3] = t.w;
-    }
-    a = Wt[MLP_FP32_B3 + k];
-#pragma unroll
-    for (int i = 0; i < 16; i++) a = ffma4(h[i], Wt[MLP_FP32_W3 + i * 4 + k], a);
-    // heads (hush.js:357-362) for component k of par0, par1, par2
-    const float p0 = k == 0 ? 1.0f / 32.0f + (31.0f / 32.0f) * sigmoidf_(a.x)
-                     : k == 1 ? 0.5f + 7.5f * sigmoidf_(a.x)
-                              : sigmoidf_(a.x);
-    const float p1 = 0.25f * expf(fminf(fmaxf(a.y, -5.0f), 5.0f));
-    const float p2 = expf(fminf(fmaxf(a.z, -4.0f), 4.0f));
-    // lane k stores texel par_k (k < 3)
-    const uint32_t base = (threadIdx.x & 31) & ~3u;
-    float c0[4], c1[4], c2[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      c0[q] = __shfl_sync(FULL, p0, base + q);
-      c1[q] = __shfl_sync(FULL, p1, base + q);
-      c2[q] = __shfl_sync(FULL, p2, base + q);
-    }
-    if (valid && k < 3) {
-      // INFER on a block without valid pixels writes zeros (hush.js:343-346)
-      const float4 v = !ok ? z4
-                       : k == 0 ? make_float4(c0[0], c0[1], c0[2], c0[3])
-                       : k == 1 ? make_float4(c1[0], c1[1], c1[2], c1[3])
-                                : make_float4(c2[0], c2[1], c2[2], c2[3]);
-      sth(k == 0 ? f.par0 : k == 1 ? f.par1 : f.par2, o, v);
-    }
-  }
-  if constexpr (TC) {
-    if (li >= K1_NB) return;
-    // warps 0-1: one row (block) per thread through the three tensor-core layers
-    constexpr int B1 = 16 * N_FEAT, B2 = B1 + 16 + 16 * 16, B3 = B2 + 16 + N_OUT * 16;
-    constexpr uint32_t ID = umma::idesc_f16(BF16 ? 1 : 0, 128, 16);
-    float row[16], d[16], out[N_OUT];
-    bool good = tc_layer(X_, li, true, 0, 4, ID, 0, d);
-#pragma unroll
-    for (int j = 0; j < 16; j++) row[j] = fmaxf(d[j] + w.w[B1 + j], 0.0f);
-    *reinterpret_cast<uint4 *>(X_.a2 + umma::kmajor_off(li, 0, 2)) = pack8<BF16>(row);
-    *reinterpret_cast<uint4 *>(X_.a2 + umma::kmajor_off(li, 8, 2)) = pack8<BF16>(row + 8);
-    good &= tc_layer(X_, li, false, 1024, 2, ID, 1, d);
-#pragma unroll
-    for (int j = 0; j < 16; j++) row[j] = fmaxf(d[j] + w.w[B2 + j], 0.0f);
-    *reinterpret_cast<uint4 *>(X_.a2 + umma::kmajor_off(li, 0, 2)) = pack8<BF16>(row);
-    *reinterpret_cast<uint4 *>(X_.a2 + umma::kmajor_off(li, 8, 2)) = pack8<BF16>(row + 8);
-    good &= tc_layer(X_, li, false, 1536, 2, ID, 0, d);
-#pragma unroll
-    for (int j = 0; j < N_OUT; j++) out[j] = d[j] + w.w[B3 + j];
-    umma::fence_before_sync();
-    asm volatile("bar.sync 1, 64;" ::: "memory");
-    if (li < 32) {
-      umma::fence_after_sync();
-      umma::tmem_dealloc(X_.tmem, 32);
-    }
-    if (!good) {
-      atomicOr(f.err, 1u);
-      return;
-    }
-    const uint32_t fl = X_.flags[li];
-    if (!(fl & 1u)) return;
-    const int Xr = blockIdx.x * (K1_TW / 2) + li % (K1_TW / 2), Yr = blockIdx.y * (K1_TH / 2) + li / (K1_TW / 2);
-    const int orow = Yr * f.W2 + Xr;
-    if (!(fl & 2u)) {
-      sth(f.par0, orow, z4); sth(f.par1, orow, z4); sth(f.par2, orow, z4);
-      return;
-    }
-    float4 p0, p1, p2;
-    mlp_heads(out, p0, p1, p2);
-    sth(f.par0, orow, p0);
-    sth(f.par1, orow, p1);
-    sth(f.par2, orow, p2);
-  }
-}
-
-// ------------------------------------------------------------------------------------------------ stage 0, FP32 form
+// ------------------------------------------------------------------------------------------------ k_temporal_block
 // One thread per 2x2 block: tile 64 x 16 pixels = 32 x 8 blocks, 256 threads. Each thread runs pixel() for its four
 // pixels in block order, accumulates block()'s sums in registers in the WGSL's order (hush.js:226-282), forms the 20
 // features once and runs the whole FP32 MLP (weights read as shared-memory broadcasts), so after the tile barrier no
 // thread waits for another. The tile is stored column-parity-split (even and odd columns in separate rows of 33
-// entries): neighbouring threads, two pixel columns apart, then read consecutive 16-byte entries.
+// entries): neighbouring threads, two pixel columns apart, then read consecutive 16-byte entries. The tensor-core
+// forms instead write each block's features as one operand row and run each layer as two tcgen05 MMAs (M = 128,
+// N = 16) over the CTA's 256 rows, FP32 accumulators in TMEM; bias, ReLU and the heads stay FP32.
 constexpr int KB_TW = 64, KB_TH = 16, KB_NT = (KB_TW / 2) * (KB_TH / 2);
 constexpr int KB_SWL = KB_TW + 2, KB_SH = KB_TH + 2, KB_HW = KB_SWL / 2;
 HD_INL int kb_tix(int r, int c) { return (2 * r + (c & 1)) * KB_HW + (c >> 1); }
@@ -584,6 +256,46 @@ struct KbSmem {
   float2 Lq[2 * KB_HW * KB_SH];  // (E * qf16(L), 1) for valid entries, (0, 0) otherwise
   float4 w[MLP_FP32_BLOB_BYTES / 16];
 };
+// Tensor-core forms: the same tile plus the MMA operands of the CTA's 256 rows (one per block) in the K-major
+// no-swizzle layout: A1 256 x 32 (features, zero padded), A2 256 x 16 (hidden layers), B1 / B2 / B3.
+struct KbTcSmem {
+  float4 I[2 * KB_HW * KB_SH];
+  float2 Lq[2 * KB_HW * KB_SH];
+  alignas(128) uint8_t a1[KB_NT * 32 * 2];
+  alignas(128) uint8_t a2[KB_NT * 16 * 2];
+  alignas(128) uint8_t b[MLP_TC_BLOB_BYTES];
+  alignas(8) uint64_t mbar;
+  uint32_t tmem;
+};
+
+// One MMA layer over the CTA's 256 rows: rows 0-127 and 128-255 go to TMEM columns [0, 16) and [16, 32) of the
+// 128 lanes. Every thread of the CTA takes part (the operand rows were written by all of them); thread 0 issues and
+// commits, all wait on the mbarrier (bounded) and load their own row: warp w reads lanes 32 (w % 4) of column block
+// w / 4. Returns false if the wait gave up.
+HD_INL bool tc_layer_256(KbTcSmem &S, int li, const uint8_t *a, uint32_t kcore_a, int kblocks, uint32_t b_off,
+                         uint32_t kcore_b, uint32_t idesc, uint32_t phase, float *d) {
+  umma::fence_proxy_async();
+  umma::fence_before_sync();
+  __syncthreads();
+  const uint32_t mbar = umma::smem_u32(&S.mbar);
+  if (li == 0) {
+    umma::fence_after_sync();
+    const uint32_t b = umma::smem_u32(S.b) + b_off;
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+      const uint32_t a0 = umma::smem_u32(a) + (uint32_t)half * 16u * 128u * kcore_a;
+      for (int kb = 0; kb < kblocks; kb++)
+        umma::mma_f16(S.tmem + 16u * half, umma::sdesc(a0 + 256u * kb, 128, 128 * kcore_a),
+                      umma::sdesc(b + 256u * kb, 128, 128 * kcore_b), idesc, kb > 0 ? 1u : 0u);
+    }
+    umma::commit(mbar);
+  }
+  const bool ok = umma::mbar_wait_bounded(mbar, phase, MBAR_POLLS);
+  umma::fence_after_sync();
+  const int w = li >> 5;
+  umma::ld16(S.tmem + ((uint32_t)(32 * (w & 3)) << 16) + 16u * (uint32_t)(w >> 2), d);
+  return ok;
+}
 
 struct ParityTile {
   const float4 *I;
@@ -591,12 +303,29 @@ struct ParityTile {
   HD_INL float4 operator()(int dx, int dy) const { return I[kb_tix(r + dy, c + dx)]; }
 };
 
+// MODE 0: FP32 MLP per thread; 1 / 2: tensor-core MLP on bf16 / f16 operands (dynamic shared memory).
+template <int MODE>
 __global__ void __launch_bounds__(KB_NT, 2)
-    k_temporal_block(const __grid_constant__ HushFrame f, const uint4 *__restrict__ blob) {
-  __shared__ KbSmem S;
+    k_temporal_block(const __grid_constant__ HushFrame f, const __grid_constant__ MlpW16 wts,
+                     const uint4 *__restrict__ blob) {
+  constexpr bool TC = MODE != 0;
+  using Smem = std::conditional_t<TC, KbTcSmem, KbSmem>;
+  extern __shared__ __align__(128) unsigned char kb_smem[];
+  Smem &S = *reinterpret_cast<Smem *>(kb_smem);
   const int li = threadIdx.x;
   const float E = f.exposure;
-  for (int i = li; i < MLP_FP32_BLOB_BYTES / 16; i += KB_NT) reinterpret_cast<uint4 *>(S.w)[i] = __ldg(blob + i);
+  if constexpr (TC) {
+    if (li < 32) {
+      umma::tmem_alloc(umma::smem_u32(&S.tmem), 32);
+      umma::tmem_relinquish();
+    }
+    if (li == 0) umma::mbar_init(umma::smem_u32(&S.mbar), 1);
+    if (li < MLP_TC_BLOB_BYTES / 16) reinterpret_cast<uint4 *>(S.b)[li] = __ldg(blob + li);
+    umma::fence_proxy_async();
+    umma::fence_before_sync();
+  } else {
+    for (int i = li; i < MLP_FP32_BLOB_BYTES / 16; i += KB_NT) reinterpret_cast<uint4 *>(S.w)[i] = __ldg(blob + i);
+  }
   const int lbx = li % (KB_TW / 2), lby = li / (KB_TW / 2);
   const int px0 = blockIdx.x * KB_TW + 2 * lbx, py0 = blockIdx.y * KB_TH + 2 * lby;
   // phase 1: the first pixel's loads and gathers in flight with the tile loads
@@ -638,6 +367,7 @@ __global__ void __launch_bounds__(KB_NT, 2)
     }
   }
   __syncthreads();
+  if constexpr (TC) umma::fence_after_sync();
   // phase 2: pixel() of the four pixels (block order: top-left, top-right, bottom-left, bottom-right), block() sums
   float nv = 0.f, Nx = 0.f, Ny = 0.f, Nz = 0.f, MV = 0.f, Z = 0.f;
   float4 S0 = make_float4(0.f, 0.f, 0.f, 0.f), S1 = S0, S3 = S0, AC = S0;
@@ -731,8 +461,59 @@ __global__ void __launch_bounds__(KB_NT, 2)
     gd.w = ok ? quant1(qf16(G.z)) : -1.0f;
     f.Gd[o] = gd;
   }
-  if (!valid) return;
   const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  if constexpr (TC) {
+    // phase 4 (tensor cores): every thread writes its block's operand row (zeros for blocks outside the image or
+    // without valid pixels) and takes part in all three layers
+    constexpr bool BF16 = MODE == 1;
+    constexpr int B1 = 16 * N_FEAT, B2 = B1 + 16 + 16 * 16, B3 = B2 + 16 + N_OUT * 16;
+    constexpr uint32_t ID = umma::idesc_f16(BF16 ? 1 : 0, 128, 16);
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      float v8[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++)
+        v8[e] = (8 * c + e < N_FEAT && valid && ok) ? __half2float(__ushort_as_half(f2h(qf16(fe[8 * c + e])))) : 0.f;
+      *reinterpret_cast<uint4 *>(S.a1 + umma::kmajor_off(li, 8 * c, 4)) = pack8<BF16>(v8);
+    }
+    float row[16], d[16];
+    bool good = tc_layer_256(S, li, S.a1, 4, 2, 0, 4, ID, 0, d);
+#pragma unroll
+    for (int j = 0; j < 16; j++) row[j] = fmaxf(d[j] + wts.w[B1 + j], 0.0f);
+    *reinterpret_cast<uint4 *>(S.a2 + umma::kmajor_off(li, 0, 2)) = pack8<BF16>(row);
+    *reinterpret_cast<uint4 *>(S.a2 + umma::kmajor_off(li, 8, 2)) = pack8<BF16>(row + 8);
+    good &= tc_layer_256(S, li, S.a2, 2, 1, 1024, 2, ID, 1, d);
+#pragma unroll
+    for (int j = 0; j < 16; j++) row[j] = fmaxf(d[j] + wts.w[B2 + j], 0.0f);
+    *reinterpret_cast<uint4 *>(S.a2 + umma::kmajor_off(li, 0, 2)) = pack8<BF16>(row);
+    *reinterpret_cast<uint4 *>(S.a2 + umma::kmajor_off(li, 8, 2)) = pack8<BF16>(row + 8);
+    good &= tc_layer_256(S, li, S.a2, 2, 1, 1536, 2, ID, 0, d);
+    float out[N_OUT];
+#pragma unroll
+    for (int j = 0; j < N_OUT; j++) out[j] = d[j] + wts.w[B3 + j];
+    umma::fence_before_sync();
+    __syncthreads();
+    if (li < 32) {
+      umma::fence_after_sync();
+      umma::tmem_dealloc(S.tmem, 32);
+    }
+    if (!good) {
+      atomicOr(f.err, 1u);
+      return;
+    }
+    if (!valid) return;
+    if (!ok) {
+      sth(f.par0, o, z4); sth(f.par1, o, z4); sth(f.par2, o, z4);
+      return;
+    }
+    float4 p0, p1, p2;
+    mlp_heads(out, p0, p1, p2);
+    sth(f.par0, o, p0);
+    sth(f.par1, o, p1);
+    sth(f.par2, o, p2);
+    return;
+  }
+  if (!valid) return;
   if (!ok) {  // INFER on a block without valid pixels writes zeros (hush.js:343-346)
     sth(f.par0, o, z4); sth(f.par1, o, z4); sth(f.par2, o, z4);
     return;
@@ -741,7 +522,8 @@ __global__ void __launch_bounds__(KB_NT, 2)
   // is its bias plus the inputs in increasing index, FP32 with packed FP32x2 FMAs
 #pragma unroll
   for (int i = 0; i < N_FEAT; i++) fe[i] = __half2float(__ushort_as_half(f2h(qf16(fe[i]))));
-  const float4 *Wt = S.w;
+  const float4 *Wt;
+  if constexpr (!TC) Wt = S.w;
   float4 a[4];
 #pragma unroll
   for (int q = 0; q < 4; q++) a[q] = Wt[MLP_FP32_B1 + q];
@@ -1091,15 +873,28 @@ cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpW16 &w16,
   const int qx = (f.W4 + HT_W - 1) / HT_W, qy = (f.H4 + HT_H - 1) / HT_H;
   switch (stage) {
     case 0: {
-      const dim3 grid((f.W + K1_TW - 1) / K1_TW, (f.H + K1_TH - 1) / K1_TH);
       // blob: bf16 operands, f16 operands, then the transposed FP32 weights
       const uint4 *blob = (const uint4 *)mlp_tc;
-      if (mlp_mode == 1) k_temporal_fused<true, true><<<grid, K1_TW * K1_TH, 0, st>>>(f, w16, blob);
-      else if (mlp_mode == 2)
-        k_temporal_fused<true, false><<<grid, K1_TW * K1_TH, 0, st>>>(f, w16, blob + MLP_TC_BLOB_BYTES / 16);
-      else
-        k_temporal_block<<<dim3((f.W + KB_TW - 1) / KB_TW, (f.H + KB_TH - 1) / KB_TH), KB_NT, 0, st>>>(
-            f, blob + 2 * MLP_TC_BLOB_BYTES / 16);
+      int dev = 0;
+      cudaGetDevice(&dev);
+      if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+      const dim3 g((f.W + KB_TW - 1) / KB_TW, (f.H + KB_TH - 1) / KB_TH);
+      if (mlp_mode == 0) {
+        k_temporal_block<0><<<g, KB_NT, sizeof(KbSmem), st>>>(f, w16, blob + 2 * MLP_TC_BLOB_BYTES / 16);
+      } else {
+        // the tensor-core forms need more than 48 KB of dynamic shared memory: opt in once per device
+        static bool opted[2][64] = {};
+        const int m = mlp_mode == 1 ? 0 : 1;
+        if (!opted[m][dev]) {
+          const cudaError_t e = cudaFuncSetAttribute(m == 0 ? k_temporal_block<1> : k_temporal_block<2>,
+                                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)sizeof(KbTcSmem));
+          if (e != cudaSuccess) return e;
+          opted[m][dev] = true;
+        }
+        if (m == 0) k_temporal_block<1><<<g, KB_NT, sizeof(KbTcSmem), st>>>(f, w16, blob);
+        else k_temporal_block<2><<<g, KB_NT, sizeof(KbTcSmem), st>>>(f, w16, blob + MLP_TC_BLOB_BYTES / 16);
+      }
       break;
     }
     case 1: k_half_stage<1><<<hx * hy + qx * qy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx); break;
