@@ -795,22 +795,46 @@ __global__ void __launch_bounds__(FT_W *FT_H, 3) k_fine_final_fused(const __grid
   sth(f.X, o, make_float4(ix * alb.x + emi.x, iy * alb.y + emi.y, iz * alb.z + emi.z, 0.0f));
 }
 
-// TAA (hush.js:639-677) with a 32 x 8 tile.
+// TAA (hush.js:639-677) with a 32 x 8 tile. The pixel's motion, colour and the four history texels of its bilinear
+// footprint are loaded before the tile barrier, so the motion -> history dependency overlaps the tile loads.
 __global__ void __launch_bounds__(FT_W *FT_H) k_taa_fused(const __grid_constant__ HushFrame f) {
-  constexpr int SW = FT_W + 2, SH = FT_H + 2;
+  constexpr int SW = FT_W + 2, SH = FT_H + 2, NT = FT_W * FT_H, NIT = (SW * SH + NT - 1) / NT;
   __shared__ float3 sX[SW * SH];
   const int li = threadIdx.x;
+  const int tx = li % FT_W, ty = li / FT_W;
+  const int px = blockIdx.x * FT_W + tx, py = blockIdx.y * FT_H + ty;
+  const int cpx = min(px, f.W - 1), cpy = min(py, f.H - 1);
+  const uint2 mvr = __ldg(f.mv + cpy * f.p_mv + cpx);
   const int ox = blockIdx.x * FT_W - 1, oy = blockIdx.y * FT_H - 1;
-  for (int i = li; i < SW * SH; i += FT_W * FT_H) {
-    const float4 x = ldh(f.X, clampi(oy + i / SW, 0, f.H - 1) * f.W + clampi(ox + i % SW, 0, f.W - 1));
+  uint2 tl[NIT];
+#pragma unroll
+  for (int it = 0; it < NIT; it++) {
+    const int i = min(li + it * NT, SW * SH - 1);
+    tl[it] = __ldg(f.X + clampi(oy + i / SW, 0, f.H - 1) * f.W + clampi(ox + i % SW, 0, f.W - 1));
+  }
+  const uint2 xr = __ldg(f.X + cpy * f.W + cpx);
+  // the history footprint (clamped loads; used only when the reprojected position lies inside the image)
+  const float4 mv = h4_to_f4(mvr);
+  const float szx = (float)f.W, szy = (float)f.H;
+  const float uvx = ((float)px + 0.5f + mv.x) / szx, uvy = ((float)py + 0.5f + mv.y) / szy;
+  const float ppx = uvx * szx - 0.5f, ppy = uvy * szy - 0.5f;
+  const float bxf = floorf(ppx), byf = floorf(ppy);
+  const int ibx = (int)bxf, iby = (int)byf;
+  uint2 hq[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+    hq[j] = __ldg(f.taa_prev + clampi(iby + (j >> 1), 0, f.H - 1) * f.W + clampi(ibx + (j & 1), 0, f.W - 1));
+#pragma unroll
+  for (int it = 0; it < NIT; it++) {
+    const int i = li + it * NT;
+    if (i >= SW * SH) continue;
+    const float4 x = h4_to_f4(tl[it]);
     sX[i] = to_ycocg(tmap(make_float3(x.x, x.y, x.z)));
   }
   __syncthreads();
-  const int tx = li % FT_W, ty = li / FT_W;
-  const int px = blockIdx.x * FT_W + tx, py = blockIdx.y * FT_H + ty;
   if (px >= f.W || py >= f.H) return;
   const int o = py * f.W + px;
-  const float4 x = ldh(f.X, o);
+  const float4 x = h4_to_f4(xr);
   const float3 cur = tmap(make_float3(x.x, x.y, x.z));
   float3 r;
   if (f.reset) {
@@ -833,21 +857,15 @@ __global__ void __launch_bounds__(FT_W *FT_H) k_taa_fused(const __grid_constant_
     }
     const float sdx = sqrtf(fmaxf(v3.x / 9.0f, 1e-12f)), sdy = sqrtf(fmaxf(v3.y / 9.0f, 1e-12f)),
                 sdz = sqrtf(fmaxf(v3.z / 9.0f, 1e-12f));
-    const float4 mv = ldh(f.mv, py * f.p_mv + px);
-    const float szx = (float)f.W, szy = (float)f.H;
-    const float uvx = ((float)px + 0.5f + mv.x) / szx, uvy = ((float)py + 0.5f + mv.y) / szy;
     float3 res = cur;
     if (uvx >= 0.0f && uvy >= 0.0f && uvx <= 1.0f && uvy <= 1.0f) {
-      const float ppx = uvx * szx - 0.5f, ppy = uvy * szy - 0.5f;
-      const float bxf = floorf(ppx), byf = floorf(ppy);
       const float fx = ppx - bxf, fy = ppy - byf;
-      const int ibx = (int)bxf, iby = (int)byf;
       float3 hist = make_float3(0.f, 0.f, 0.f);
 #pragma unroll
       for (int j = 0; j < 4; j++) {
         const int oxj = j & 1, oyj = j >> 1;
         const float wb = (oxj == 1 ? fx : 1.0f - fx) * (oyj == 1 ? fy : 1.0f - fy);
-        const float4 t = ldh(f.taa_prev, clampi(iby + oyj, 0, f.H - 1) * f.W + clampi(ibx + oxj, 0, f.W - 1));
+        const float4 t = h4_to_f4(hq[j]);
         hist.x += wb * t.x; hist.y += wb * t.y; hist.z += wb * t.z;
       }
       float3 hh = to_ycocg(tmap(hist));
