@@ -1,12 +1,15 @@
 """Benchmark of the Hush denoise path on synthetic 1080p G-buffer sequences.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--mlp fp32|bf16|f16]
+                    [--no-graph] [--workload 1080p|4k]
 
 A step is one denoised 1920x1080 frame of the seeded 64-frame sequence (3 independently moving objects, camera pan
 U[0,4] px/frame with 0.2 deg/frame yaw, a camera cut and reset() at frame 32); longer runs loop over the sequence
-with a reset() at every restart. Inputs are generated on the device
+with a reset() at every restart. Each frame is replayed as one CUDA graph (re-captured and updated in place when
+the input buffers change; --no-graph launches the six kernels directly). Inputs are generated on the device
 before timing, so the timed region starts with them resident in HBM; every frame reads its own 83 MB of inputs plus
-~230 MB of state, more than the 126 MB L2, so no L2 flush is needed between frames.
+~230 MB of state, more than the 126 MB L2, so no L2 flush is needed between frames. --workload 4k runs the 3840x2160
+workload instead (BF16 MLP, one graph per frame).
 
 Prints one JSON line (rank 0). For N > 1 (torchrun), every rank denoises its own independent sequence on its own GPU
 (replicas: the path has no cross-GPU exchange); value = total frames / max-over-ranks time.
@@ -27,6 +30,14 @@ sys.path.insert(0, ROOT)
 
 METRIC = "1080p ms/frame + %HBM roofline, BF16-MLP vs FP32 plain; train-step ms at equal error"
 W, H, SEQ = 1920, 1080, 64
+WORKLOAD = ("1920x1080 64-frame sequence, 3 moving objects, pan U[0,4] px/frame, cut at 32 (reset); inputs generated "
+            "on the device")
+
+
+def _scene_cfg():
+    from hush_b200 import scene
+
+    return scene.CONFIG_1080P if W == 1920 else scene.CONFIG_4K
 
 # Algorithmic bytes per launch of each fused stage at this build's formats (8 B per rgba16float texel), per
 # full-res pixel (P), half-res pixel (h) and quarter-res pixel (q): unique global reads + writes.
@@ -124,8 +135,8 @@ class ClockSampler:
 
 
 def _cpu_baseline_sample(frames: int = 3):
-    """The oracle (f32 restatement of the reference's passes, OpenMP over rows) on 1080p frames: ms/frame over the
-    frames after the first, all host threads."""
+    """The oracle (f32 restatement of the reference's passes, OpenMP over rows) on frames of the bench's sequence:
+    ms/frame over the frames after the first, all host threads."""
     import numpy as np  # noqa: F401
 
     import oracle
@@ -133,7 +144,7 @@ def _cpu_baseline_sample(frames: int = 3):
 
     oracle.set_threads(0)
     cores = os.cpu_count() or 1
-    cfg = scene.CONFIG_1080P
+    cfg = _scene_cfg()
     o = oracle.OracleHush(W, H, builtin_weights())
     times = []
     for i in range(frames):
@@ -143,7 +154,7 @@ def _cpu_baseline_sample(frames: int = 3):
         times.append(time.perf_counter() - t)
     ms = 1000.0 * statistics.mean(times[1:] if len(times) > 1 else times)
     return {"value": round(ms, 3), "unit": "ms/frame", "cores": cores, "kind": "port",
-            "sample": f"{frames} frames of the 1920x1080 sequence (frame 0 untimed), oracle f32, {cores} threads"}
+            "sample": f"{frames} frames of the {W}x{H} sequence (frame 0 untimed), oracle f32, {cores} threads"}
 
 
 def run_reference(args):
@@ -155,7 +166,7 @@ def run_reference(args):
 
     oracle.set_threads(0)
     cores = os.cpu_count() or 1
-    cfg = scene.CONFIG_1080P
+    cfg = _scene_cfg()
     o = oracle.OracleHush(W, H, builtin_weights())
     # bounded sample: the CPU takes ~0.3 s per 1080p frame, so at most 2 warm-up and 24 timed frames
     warm, steps = min(args.warmup, 2), min(args.steps, 24)
@@ -202,7 +213,7 @@ def run_ours(args):
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     dev = torch.device("cuda", local)
-    cfg = scene.CONFIG_1080P.with_(seed=1 + rank)
+    cfg = _scene_cfg().with_(seed=1 + rank)
     nseq = min(SEQ, args.warmup + args.steps)
     # the sequence, generated on the device (untimed)
     frames = [scene.frame_device(cfg, i) for i in range(nseq)]
@@ -340,8 +351,7 @@ def run_ours(args):
         "metric": METRIC, "value": round(ms_frame / world, 4), "unit": "ms/frame", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_frame, 4), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "1920x1080 64-frame sequence, 3 moving objects, pan U[0,4] px/frame, cut at 32 "
-                               "(reset); inputs generated on the device",
+        "config": {"workload": WORKLOAD,
                    "width": W, "height": H, "mlp": args.mlp, "schedule": args.schedule, "graph": bool(args.graph),
                    "l2": "no flush: each frame reads 83 MB of fresh inputs + ~230 MB of state (> 126 MB L2)",
                    "parallelism": f"replicas x{world}"},
@@ -423,11 +433,24 @@ def main(argv=None):
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mlp", default="fp32", choices=["fp32", "bf16", "f16"])
     ap.add_argument("--schedule", default="fused", choices=["fused", "passes"])
-    ap.add_argument("--graph", action="store_true")
+    ap.add_argument("--no-graph", dest="graph", action="store_false",
+                    help="launch the six kernels of each frame directly instead of replaying the frame as a CUDA graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-train", action="store_true", help="skip the training-step timing")
+    ap.add_argument("--workload", default="1080p", choices=["1080p", "4k"],
+                    help="4k: the 3840x2160 workload (32 objects, 8 moving, 20%% sky, pan U[0,6], 2%% fireflies x100) "
+                         "with the BF16 MLP and each frame replayed as one CUDA graph")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
+    if args.workload == "4k":
+        global W, H, SEQ, WORKLOAD
+        W, H, SEQ = 3840, 2160, 16
+        WORKLOAD = ("3840x2160 sequence (16 frames resident, looped with reset), 32 objects, 8 moving, 20% sky, "
+                    "pan U[0,6] px/frame, 2% fireflies x100; BF16 MLP, one CUDA graph per frame")
+        if "--mlp" not in (argv or sys.argv):
+            args.mlp = "bf16"
+        args.graph = True
+        args.no_train = True
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -367,8 +367,8 @@ extern "C" int hush_denoise(hush_t *h, const hush_inputs *in, void *stream, cons
     bool hit = h->gexec[cur] && h->gkey_reset[cur] == f.reset && h->gkey_exposure[cur] == f.exposure &&
                std::memcmp(h->gkey[cur], key, sizeof(key)) == 0;
     if (!hit) {
-      if (h->gexec[cur]) cudaGraphExecDestroy(h->gexec[cur]);
-      h->gexec[cur] = nullptr;
+      // capture the frame again; an existing executable graph of the same parity is updated in place (same
+      // kernels, new parameters), which is much cheaper than instantiating a new one
       cudaStream_t cs;
       cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
       if (e != cudaSuccess) return hush_cuda_fail(h, e, "cudaStreamCreate");
@@ -380,9 +380,22 @@ extern "C" int hush_denoise(hush_t *h, const hush_inputs *in, void *stream, cons
       cudaStreamDestroy(cs);
       if (rc != HUSH_OK) { if (g) cudaGraphDestroy(g); return rc; }
       if (e != cudaSuccess) return hush_cuda_fail(h, e, "cudaStreamEndCapture");
-      e = cudaGraphInstantiate(&h->gexec[cur], g, 0);
+      bool updated = false;
+      if (h->gexec[cur]) {
+        cudaGraphExecUpdateResultInfo info;
+        updated = cudaGraphExecUpdate(h->gexec[cur], g, &info) == cudaSuccess;
+        if (!updated) {
+          cudaGetLastError();  // clear the update failure; instantiate instead
+          cudaGraphExecDestroy(h->gexec[cur]);
+          h->gexec[cur] = nullptr;
+        }
+      }
+      if (!updated) e = cudaGraphInstantiate(&h->gexec[cur], g, 0);
       cudaGraphDestroy(g);
-      if (e != cudaSuccess) return hush_cuda_fail(h, e, "cudaGraphInstantiate");
+      if (e != cudaSuccess) {
+        h->gexec[cur] = nullptr;
+        return hush_cuda_fail(h, e, "cudaGraphInstantiate");
+      }
       std::memcpy(h->gkey[cur], key, sizeof(key));
       h->gkey_reset[cur] = f.reset;
       h->gkey_exposure[cur] = f.exposure;
