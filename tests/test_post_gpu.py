@@ -82,3 +82,16 @@ def test_errors():
         Post(0, "rgb565")
     with pytest.raises(HushError, match="target must be"):
         post.encode(a, a, target=torch.zeros((8, 8, 4), dtype=torch.float32, device="cuda"))
+
+
+@pytest.mark.parametrize("fmt", ["rgba8unorm", "rgba32float"])
+def test_even_size_takes_the_separable_bloom_path(fmt):
+    # target = HDR size = twice the first bloom level: FINAL reads the HDR texel directly and the bloom through the
+    # 4 x 4 separable form of its nine bilinear taps
+    H, W = 96, 160
+    left, right = _hdr(H, W, 7), _hdr(H, W, 8)
+    post = Post(0, fmt, bloom=0.4)
+    got = post.encode(torch.from_numpy(left).cuda(), torch.from_numpy(right).cuda(), split=0.3)
+    torch.cuda.synchronize()
+    want = oracle.post(left, right, split=0.3, bloom=0.4)
+    _check(post, want, got.cpu().numpy(), fmt)
