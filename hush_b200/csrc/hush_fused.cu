@@ -706,11 +706,36 @@ __global__ void __launch_bounds__(HT_W *HT_H) k_half_stage(const __grid_constant
 // ------------------------------------------------------------------------------------------------ stage 4 / 5
 constexpr int FT_W = 32, FT_H = 8;
 
+// FINE_FINAL with a 32 x 8 tile. Before the barrier the CTA stages, besides the A0 / guide tile of the fine filter,
+// everything its pixels' recombination reads: the half-res footprint (guide Gd, block means Ah, mid level Bh0; 18 x 6
+// texels, decoded once), the quarter-res footprint (guide CGd, coarse level C0; 10 x 4) and the per-block filter
+// parameters (s0, c0, beta, kappa; 16 x 4). Each texel is then read from shared memory by the 16 or so taps that use
+// it instead of being fetched and decoded per tap.
+constexpr int FH_W = FT_W / 2 + 2, FH_H = FT_H / 2 + 2, FQ_W = FT_W / 4 + 2, FQ_H = FT_H / 4 + 2;
 __global__ void __launch_bounds__(FT_W *FT_H, 3) k_fine_final_fused(const __grid_constant__ HushFrame f) {
   constexpr int AP = 1, SW = FT_W + 2, SH = FT_H + 2;
+  constexpr int NH = FH_W * FH_H, NQ = FQ_W * FQ_H, NP = (FT_W / 2) * (FT_H / 2);
   __shared__ float4 sA[SW * SH], sG[SW * SH];
+  __shared__ float4 sHG[NH], sHA[NH], sHB[NH], sQG[NQ], sQC[NQ], sPar[NP];
   const int li = threadIdx.x;
   const int bx = blockIdx.x * FT_W, by = blockIdx.y * FT_H;
+  const int hx0 = bx / 2 - 1, hy0 = by / 2 - 1, qx0 = bx / 4 - 1, qy0 = by / 4 - 1;
+  if (li < NH) {
+    const int q = clampi(hy0 + li / FH_W, 0, f.H2 - 1) * f.W2 + clampi(hx0 + li % FH_W, 0, f.W2 - 1);
+    sHG[li] = __ldg(f.Gd + q);
+    sHA[li] = ldh(f.Ah, q);
+    sHB[li] = ldh(f.Bh0, q);
+  } else if (li < NH + NQ) {
+    const int i = li - NH;
+    const int r = clampi(qy0 + i / FQ_W, 0, f.H4 - 1) * f.W4 + clampi(qx0 + i % FQ_W, 0, f.W4 - 1);
+    sQG[i] = __ldg(f.CGd + r);
+    sQC[i] = ldh(f.C0, r);
+  } else if (li < NH + NQ + NP) {
+    const int i = li - NH - NQ;
+    const int hq = clampi(by / 2 + i / (FT_W / 2), 0, f.H2 - 1) * f.W2 + clampi(bx / 2 + i % (FT_W / 2), 0, f.W2 - 1);
+    const float4 p0 = ldh(f.par0, hq);
+    sPar[i] = make_float4(ldh(f.par1, hq).x, ldh(f.par2, hq).x, p0.z, p0.w);  // s0, c0, beta, kappa
+  }
   for (int i = li; i < SW * SH; i += FT_W * FT_H) {
     const int q = clampi(by - AP + i / SW, 0, f.H - 1) * f.W + clampi(bx - AP + i % SW, 0, f.W - 1);
     sA[i] = ldh(f.A0, q);
@@ -731,11 +756,10 @@ __global__ void __launch_bounds__(FT_W *FT_H, 3) k_fine_final_fused(const __grid
     sth(f.X, o, make_float4(emi.x, emi.y, emi.z, 0.f));
     return;
   }
-  const int hp = (py >> 1) * f.W2 + (px >> 1);
-  const float4 A1 = filt<1, 1, true, SW>(sA, sG, lx, ly, px, py, f.W, f.H, ldh(f.par1, hp).x, ldh(f.par2, hp).x);
+  const float4 pr = sPar[((py - by) >> 1) * (FT_W / 2) + ((px - bx) >> 1)];
+  const float4 A1 = filt<1, 1, true, SW>(sA, sG, lx, ly, px, py, f.W, f.H, pr.x, pr.y);
   sth(f.hist, o, A1);
-  // recombination (hush.js:580-620) with the half-res block means (Ah) and decoded guides (Gd, CGd); the loads of all
-  // eight footprint texels are issued before any weight is formed
+  // recombination (hush.js:580-620) with the half-res block means (Ah) and decoded guides (Gd, CGd)
   const float fx = qf16(A1.x), fy = qf16(A1.y), fz = qf16(A1.z);
   const float z = gp.w;
   const int hsx = (f.W + 1) / 2, hsy = (f.H + 1) / 2;
@@ -744,30 +768,15 @@ __global__ void __launch_bounds__(FT_W *FT_H, 3) k_fine_final_fused(const __grid
   const int qsx = (f.W + 3) / 4, qsy = (f.H + 3) / 4;
   const float cposx = ((float)px + 0.5f) / 4.0f - 0.5f, cposy = ((float)py + 0.5f) / 4.0f - 0.5f;
   const float cbx = floorf(cposx), cby = floorf(cposy);
-  float4 gh[4], cg[4];
-  uint2 ah[4], bm[4], cc[4];
-  bool inh[4], inq[4];
-#pragma unroll
-  for (int j = 0; j < 4; j++) {
-    const int qx = (int)hbx + (j & 1), qy = (int)hby + (j >> 1);
-    inh[j] = qx >= 0 && qy >= 0 && qx < hsx && qy < hsy;
-    const int q = clampi(qy, 0, f.H2 - 1) * f.W2 + clampi(qx, 0, f.W2 - 1);
-    gh[j] = __ldg(f.Gd + q);
-    ah[j] = __ldg(f.Ah + q);
-    bm[j] = __ldg(f.Bh0 + q);
-    const int rx = (int)cbx + (j & 1), ry = (int)cby + (j >> 1);
-    inq[j] = rx >= 0 && ry >= 0 && rx < qsx && ry < qsy;
-    const int r = clampi(ry, 0, f.H4 - 1) * f.W4 + clampi(rx, 0, f.W4 - 1);
-    cg[j] = __ldg(f.CGd + r);
-    cc[j] = __ldg(f.C0 + r);
-  }
-  const float4 pr = ldh(f.par0, hp);
   float uBx = 0.f, uBy = 0.f, uBz = 0.f, uAx = 0.f, uAy = 0.f, uAz = 0.f, swh = 0.f;
 #pragma unroll
   for (int j = 0; j < 4; j++) {
-    if (!inh[j] || gh[j].w < 0.0f) continue;
-    const float w = jbw(hposx - hbx, hposy - hby, j, gh[j], gh[j].w, gp, z);
-    const float4 a = h4_to_f4(ah[j]), m = h4_to_f4(bm[j]);
+    const int qx = (int)hbx + (j & 1), qy = (int)hby + (j >> 1);
+    const int t = (qy - hy0) * FH_W + (qx - hx0);
+    const float4 gh = sHG[t];
+    if (!(qx >= 0 && qy >= 0 && qx < hsx && qy < hsy) || gh.w < 0.0f) continue;
+    const float w = jbw(hposx - hbx, hposy - hby, j, gh, gh.w, gp, z);
+    const float4 a = sHA[t], m = sHB[t];
     swh += w;
     uBx += w * m.x; uBy += w * m.y; uBz += w * m.z;
     uAx += w * a.x; uAy += w * a.y; uAz += w * a.z;
@@ -781,9 +790,12 @@ __global__ void __launch_bounds__(FT_W *FT_H, 3) k_fine_final_fused(const __grid
   float uCx = 0.f, uCy = 0.f, uCz = 0.f, swq = 0.f;
 #pragma unroll
   for (int j = 0; j < 4; j++) {
-    if (!inq[j] || cg[j].w < 0.0f) continue;
-    const float w = jbw(cposx - cbx, cposy - cby, j, cg[j], cg[j].w, gp, z);
-    const float4 c = h4_to_f4(cc[j]);
+    const int rx = (int)cbx + (j & 1), ry = (int)cby + (j >> 1);
+    const int t = (ry - qy0) * FQ_W + (rx - qx0);
+    const float4 cg = sQG[t];
+    if (!(rx >= 0 && ry >= 0 && rx < qsx && ry < qsy) || cg.w < 0.0f) continue;
+    const float w = jbw(cposx - cbx, cposy - cby, j, cg, cg.w, gp, z);
+    const float4 c = sQC[t];
     swq += w;
     uCx += w * c.x; uCy += w * c.y; uCz += w * c.z;
   }
