@@ -83,6 +83,8 @@ _SIGS = {
     "hush_get_frame": (C.c_int, [_P]),
     "hush_denoise": (C.c_int, [_P, C.POINTER(HushInputs), _P, C.POINTER(_P)]),
     "hush_output": (_P, [_P]),
+    "hush_denoise_host": (C.c_int, [_P, C.POINTER(HushInputs), _P, C.c_size_t, _P]),
+    "hush_host_join": (C.c_int, [_P, _P]),
     "hush_timer_enable": (C.c_int, [_P, C.c_int]),
     "hush_timer_read": (C.c_int, [_P, C.POINTER(HushTiming), C.c_int]),
     "hush_set_graph": (C.c_int, [_P, C.c_int]),

@@ -68,11 +68,22 @@ static void drop_graphs(hush_t *h) {
   }
 }
 
+static void free_host_staging(hush_t *h) {
+  if (h->hin_pool) {
+    cudaDeviceSynchronize();  // copies into the staging sets may still be in flight
+    cudaFree(h->hin_pool);
+  }
+  h->hin_pool = nullptr;
+  for (auto &set : h->hin)
+    for (auto &p : set) p = nullptr;
+}
+
 static void free_state(hush_t *h) {
   if (h->pool) cudaFree(h->pool);
   h->pool = nullptr;
   h->pool_bytes = 0;
   drop_graphs(h);
+  free_host_staging(h);
 }
 
 // resize (hush.js:764-794): one pool for every state image, 256-byte aligned sub-allocations, zero-initialised like
@@ -210,6 +221,11 @@ extern "C" void hush_destroy(hush_t *h) {
   if (h->tc_blob_dev) cudaFree(h->tc_blob_dev);
   for (int i = 0; i < 17; i++)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+  for (int i = 0; i < 2; i++)
+    for (cudaEvent_t e : {h->ev_in[i], h->ev_used[i], h->ev_out[i]})
+      if (e) cudaEventDestroy(e);
+  if (h->h2d) cudaStreamDestroy(h->h2d);
+  if (h->d2h) cudaStreamDestroy(h->d2h);
   delete h;
 }
 
@@ -411,6 +427,77 @@ extern "C" int hush_denoise(hush_t *h, const hush_inputs *in, void *stream, cons
   h->last_out = h->taa[cur];
   if (out) *out = h->last_out;
   return HUSH_OK;
+}
+
+// Host-buffer frames. Frame t uses staging set t & 1: its five input copies run on the copy-in stream after frame
+// t - 2 has finished reading that set, the frame runs on `stream` after its copies, and the output copy runs on the
+// copy-out stream after the frame; frame t + 2, which rewrites the same output image, waits for that copy. So the
+// input copy of frame t + 1 and the output copy of frame t - 1 overlap frame t's kernels.
+extern "C" int hush_denoise_host(hush_t *h, const hush_inputs *in, void *out_host, size_t out_pitch, void *stream) {
+  if (!h) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_denoise_host: NULL instance");
+  int rc = hush_check_inputs(h, in);
+  if (rc != HUSH_OK) return rc;
+  if (!out_host) return hush_fail(h, HUSH_ERR_ARG, "hush_denoise_host: missing output buffer");
+  const size_t row = (size_t)h->W * 8, opitch = out_pitch ? out_pitch : row;
+  if (opitch < row) return hush_fail(h, HUSH_ERR_ARG, "hush_denoise_host: output pitch is smaller than a row");
+  cudaSetDevice(h->dev);
+  cudaError_t e = cudaSuccess;
+  if (!h->h2d) {
+    e = cudaStreamCreateWithFlags(&h->h2d, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->d2h, cudaStreamNonBlocking);
+    for (int i = 0; i < 2 && e == cudaSuccess; i++)
+      for (cudaEvent_t *ev : {&h->ev_in[i], &h->ev_used[i], &h->ev_out[i]})
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return hush_cuda_fail(h, e, "hush_denoise_host: stream / event creation");
+    for (int i = 0; i < 2 && e == cudaSuccess; i++) {  // nothing to wait for before the first frames
+      e = cudaEventRecord(h->ev_used[i], h->h2d);
+      if (e == cudaSuccess) e = cudaEventRecord(h->ev_out[i], h->d2h);
+    }
+    if (e != cudaSuccess) return hush_cuda_fail(h, e, "hush_denoise_host: cudaEventRecord");
+  }
+  if (!h->hin_pool) {
+    const size_t img = ((size_t)h->W * h->H * 8 + 255) & ~(size_t)255;
+    e = cudaMalloc(&h->hin_pool, img * 10);
+    if (e != cudaSuccess) {
+      h->hin_pool = nullptr;
+      return hush_cuda_fail(h, e, "hush_denoise_host: staging allocation");
+    }
+    for (int s = 0; s < 2; s++)
+      for (int k = 0; k < 5; k++) h->hin[s][k] = reinterpret_cast<uint2 *>(static_cast<char *>(h->hin_pool) + img * (5 * s + k));
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const int s = h->frame & 1;
+  const void *src[5] = {in->radiance, in->normal_depth, in->motion, in->material, in->emission};
+  e = cudaStreamWaitEvent(h->h2d, h->ev_used[s], 0);
+  for (int k = 0; k < 5 && e == cudaSuccess; k++) {
+    const size_t sp = in->pitch[k] ? in->pitch[k] : row;
+    e = cudaMemcpy2DAsync(h->hin[s][k], row, src[k], sp, row, (size_t)h->H, cudaMemcpyHostToDevice, h->h2d);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(h->ev_in[s], h->h2d);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(st, h->ev_in[s], 0);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(st, h->ev_out[s], 0);  // frame t - 2's output copy is done
+  if (e != cudaSuccess) return hush_cuda_fail(h, e, "hush_denoise_host: input copies");
+  hush_inputs dev{};
+  const void **dst[5] = {&dev.radiance, &dev.normal_depth, &dev.motion, &dev.material, &dev.emission};
+  for (int k = 0; k < 5; k++) *dst[k] = h->hin[s][k];
+  const void *out = nullptr;
+  rc = hush_denoise(h, &dev, stream, &out);
+  if (rc != HUSH_OK) return rc;
+  e = cudaEventRecord(h->ev_used[s], st);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(h->d2h, h->ev_used[s], 0);
+  if (e == cudaSuccess) e = cudaMemcpy2DAsync(out_host, opitch, out, row, row, (size_t)h->H, cudaMemcpyDeviceToHost, h->d2h);
+  if (e == cudaSuccess) e = cudaEventRecord(h->ev_out[s], h->d2h);
+  return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(h, e, "hush_denoise_host: output copy");
+}
+
+// `stream` waits until every output copy enqueued by hush_denoise_host so far has landed in host memory.
+extern "C" int hush_host_join(hush_t *h, void *stream) {
+  if (!h) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_host_join: NULL instance");
+  if (!h->d2h) return HUSH_OK;
+  cudaSetDevice(h->dev);
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < 2 && e == cudaSuccess; i++) e = cudaStreamWaitEvent((cudaStream_t)stream, h->ev_out[i], 0);
+  return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(h, e, "hush_host_join");
 }
 
 extern "C" const void *hush_output(const hush_t *h) {

@@ -43,6 +43,12 @@ struct hush_s {
   int gkey_reset[2] = {-1, -1};
   float gkey_exposure[2] = {0, 0};
   cudaStream_t gstream[2] = {nullptr, nullptr};
+  // host-buffer frames (hush_denoise_host): two device staging sets for the five inputs, a copy-in and a copy-out
+  // stream, and the events that order them against the frames
+  void *hin_pool = nullptr;
+  uint2 *hin[2][5] = {};
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaEvent_t ev_in[2] = {}, ev_used[2] = {}, ev_out[2] = {};
 };
 
 // helpers of hush_api.cu

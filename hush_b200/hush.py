@@ -203,6 +203,37 @@ class Hush:
             L.lib().hush_timer_enable(self._h, 0)
         return device_view(out.value, self.height, self.width)
 
+    def denoise_host(self, inputs: dict, out=None, stream=None):
+        """One frame with the G-buffer in host memory: (H, W, 4) float16 CPU tensors (pinned for asynchronous
+        copies) in, the output copied into `out` (a CPU float16 tensor, allocated pinned if None). Calls overlap
+        their copies with the previous frame's kernels; `out` is complete after host_join(stream) and a synchronize
+        (hush_denoise_host / hush_host_join)."""
+        import torch
+
+        inp = L.HushInputs()
+        for k, name in enumerate(INPUTS):
+            t = inputs.get(name) if inputs is not None else None
+            if t is None:
+                raise HushError(f"Hush.denoise: missing input '{name}'")
+            if t.is_cuda or t.dtype.itemsize != 2 or t.dim() != 3 or t.shape[2] != 4 or t.stride(2) != 1 \
+                    or t.stride(1) != 4:
+                raise HushError(f"Hush.denoise_host: '{name}' must be a host (H, W, 4) float16 tensor with dense rows")
+            setattr(inp, _FIELD[name], t.data_ptr())
+            inp.width[k], inp.height[k] = t.shape[1], t.shape[0]
+            inp.pitch[k] = t.stride(0) * 2
+        if out is None:
+            out = torch.empty((self.height, self.width, 4), dtype=torch.float16).pin_memory()
+        if out.is_cuda or out.dtype != torch.float16 or tuple(out.shape) != (self.height, self.width, 4) \
+                or out.stride(1) != 4 or out.stride(2) != 1:
+            raise HushError("Hush.denoise_host: out must be a host (H, W, 4) float16 tensor with dense rows")
+        _check(L.lib().hush_denoise_host(self._h, C.byref(inp), out.data_ptr(), out.stride(0) * 2,
+                                         C.c_void_p(_stream_handle(stream))), self._h)
+        return out
+
+    def host_join(self, stream=None):
+        """`stream` waits for every output copy denoise_host enqueued."""
+        _check(L.lib().hush_host_join(self._h, C.c_void_p(_stream_handle(stream))), self._h)
+
     def timings(self) -> list:
         """[(label, ms)] of the last timed frame (synchronises on its events)."""
         arr = (L.HushTiming * 16)()

@@ -93,6 +93,16 @@ int hush_get_frame(const hush_t *h);
  * (in *out) the instance-owned output image (rgba16float, dense, linear HDR, alpha 1). Two images alternate from
  * frame to frame: the pointer stays valid until the next-but-one call (hush.js:796-798). */
 int hush_denoise(hush_t *h, const hush_inputs *in, void *stream, const void **out);
+/* denoise with the G-buffer in host memory (a CPU renderer, a replayed capture): the five inputs (rgba16float,
+ * `pitch` in bytes, pinned host memory for truly asynchronous copies) are copied into one of two instance-owned
+ * device staging sets on a copy-in stream, the frame runs on `stream`, and the output is copied to out_host
+ * (W x H rgba16float, out_pitch bytes, 0 = dense) on a copy-out stream. Consecutive calls overlap: frame t + 1's
+ * input copies and frame t - 1's output copy run during frame t's kernels. The call only enqueues; out_host is
+ * valid once hush_host_join's stream (or the device) has synchronised. No counterpart in the reference (its inputs
+ * are GPU textures); it is the host-buffer form of Hush.denoise. */
+int hush_denoise_host(hush_t *h, const hush_inputs *in, void *out_host, size_t out_pitch, void *stream);
+/* `stream` waits for every output copy hush_denoise_host has enqueued. */
+int hush_host_join(hush_t *h, void *stream);
 /* output getter (hush.js:798): the last frame's output image. */
 const void *hush_output(const hush_t *h);
 

@@ -334,3 +334,34 @@ def test_config5_4k_graph_bf16_and_fp32():
     assert np.mean(err["bf16"]) <= np.mean(err["fp32"]) * 1.01 + 1e-4, err
     for h in (g16, d16, g32):
         h.destroy()
+
+
+def test_host_buffer_frames_match_device_frames():
+    """hush_denoise_host (pinned host inputs copied in on a copy stream, output copied back on another, adjacent frames
+    overlapping) gives the device path's output bit for bit, also into a pitched host buffer."""
+    cfg = scene.SceneConfig(160, 96, 5, n_moving=2, seed=33)
+    host = [{k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in scene.frame_host(cfg, i).items()
+             if k in oracle.INPUTS} for i in range(cfg.frames)]
+    a = Hush(0, {"width": cfg.width, "height": cfg.height})
+    b = Hush(0, {"width": cfg.width, "height": cfg.height})
+    backing = [torch.zeros((cfg.height, cfg.width + 8, 4), dtype=torch.float16).pin_memory() for _ in range(2)]
+    got = []
+    for i, f in enumerate(host):
+        ref = a.denoise({k: v.cuda() for k, v in f.items()}).clone()
+        out = backing[i & 1][:, :cfg.width]  # rows of W + 8 texels: a pitched host target
+        b.denoise_host(f, out)
+        b.host_join()
+        torch.cuda.synchronize()
+        got.append(out.clone())
+        assert torch.equal(got[-1], ref.cpu()), i
+    # back to back without synchronising: copies of adjacent frames overlap the kernels
+    c = Hush(0, {"width": cfg.width, "height": cfg.height})
+    outs = [torch.zeros((cfg.height, cfg.width, 4), dtype=torch.float16).pin_memory() for _ in host]
+    for f, o in zip(host, outs):
+        c.denoise_host(f, o)
+    c.host_join()
+    torch.cuda.synchronize()
+    for i in range(len(host)):
+        assert torch.equal(outs[i], got[i]), i
+    with pytest.raises(HushError, match="host"):
+        b.denoise_host({k: v.cuda() for k, v in host[0].items()})
