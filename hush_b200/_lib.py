@@ -61,6 +61,11 @@ class HushPostInputs(C.Structure):
                 ("line", C.c_float), ("same", C.c_int)]
 
 
+# the training twin's passes (hush_twin_pass) and buffers (hush_trainer_buf)
+TWIN_PASSES = ["mlp", "mid1", "mid2", "mid3", "fine", "taa", "loss"]
+TWIN_BUF_NAMES = ["THETA", "GRAD", "LOSS", "PAR", "DPAR", "B1", "B2", "B3", "DB1", "DB2", "DB3", "A1", "X", "DX", "OUT",
+                  "OUT_PREV", "DOUT"]
+
 POST_LEVELS = 6
 POST_RGBA8, POST_BGRA8, POST_RGBA32F = 0, 1, 2
 
@@ -110,6 +115,15 @@ _SIGS = {
     "hush_trainer_step": (C.c_int, [_P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, _P,
                                     C.POINTER(C.c_double)]),
     "hush_trainer_export": (C.c_int, [_P, C.c_void_p]),
+    "hush_train_step": (C.c_int, [_P, C.POINTER(HushInputs), C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_float,
+                                  C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, _P, C.POINTER(C.c_double),
+                                  C.POINTER(C.c_double)]),
+    "hush_trainer_begin": (C.c_int, [_P, C.POINTER(HushInputs), C.c_void_p, C.c_void_p, C.c_float, _P]),
+    "hush_trainer_zero_adjoints": (C.c_int, [_P, _P]),
+    "hush_trainer_buffer": (C.c_int, [_P, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_int)]),
+    "hush_trainer_pass": (C.c_int, [_P, C.c_int, C.c_int, _P]),
+    **{f"hush_{p}_{d}": (C.c_int, [_P, _P]) for p in TWIN_PASSES for d in ("fwd", "bwd")},
     "hush_mlp_grad_noalloc": (C.c_int, [C.c_void_p] * 6 + [C.c_int, C.c_int, C.c_void_p, _P]),
     "svgf_options_default": (SvgfOptions, []),
     "svgf_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(SvgfOptions), C.c_int, C.POINTER(_P)]),

@@ -523,7 +523,7 @@ __global__ void k_reduce_f64(const double *partials, int n, double *out, double 
     for (int off = 16; off > 0; off >>= 1) u += __shfl_down_sync(0xffffffffu, u, off);
     if (threadIdx.x == 0) {
       *out = u;
-      *acc += u;
+      if (acc) *acc += u;
     }
   }
 }
@@ -539,6 +539,12 @@ HD_INL float3 itm_adjoint(const TaaF &A, float3 g) {
     r.x += k * 0.2126f; r.y += k * 0.7152f; r.z += k * 0.0722f;
   }
   return r;
+}
+// adjoint of tm(X) = X / (1 + lum(X)) at X
+HD_INL float3 tm_adjoint(float4 Xv, float4 gt) {
+  const float L1 = 1.0f + lum(Xv);
+  const float k = (gt.x * Xv.x + gt.y * Xv.y + gt.z * Xv.z) / (L1 * L1);
+  return make_float3(gt.x / L1 - k * 0.2126f, gt.y / L1 - k * 0.7152f, gt.z / L1 - k * 0.0722f);
 }
 HD_INL float3 ycocg_adjoint(float3 g) {  // transpose of to_ycocg
   return make_float3(0.25f * g.x + 0.5f * g.y - 0.25f * g.z, 0.5f * g.x + 0.5f * g.z, 0.25f * g.x - 0.5f * g.y - 0.25f * g.z);
@@ -580,8 +586,21 @@ __global__ void k_taa_bwd(const TwinFrame T, const float4 *gout, float4 *gT) {
   atomic_add4(gT + o, make_float4(gcur.x, gcur.y, gcur.z, 0.f));
 }
 
+// dX += tm adjoint of the tone-mapped-colour gradient at every pixel (the per-pass TAA adjoint's second step; the fused
+// frame folds it into k_fine_bwd, where sky pixels need no dX).
+__global__ void k_tm_bwd(const TwinFrame T, const float4 *gtm, float4 *dX) {
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= T.f.W * T.f.H) return;
+  const float3 g = tm_adjoint(T.X[o], gtm[o]);
+  const float4 d = dX[o];
+  dX[o] = make_float4(d.x + g.x, d.y + g.y, d.z + g.z, d.w);
+}
+
 // Pass 2 (per full pixel): dL/dX from the tm gradient; then recombination, fine-level parameter and mid-level input
 // gradients.
+// SEED_TM: the seed is the gradient w.r.t. the tone-mapped colour tm(X) (the fused frame); else w.r.t. X itself (the
+// per-pass pair, whose TAA adjoint has already applied the tm adjoint).
+template <bool SEED_TM>
 __global__ void __launch_bounds__(TW *TH) k_fine_bwd(const TwinFrame T, const float4 *gT) {
   constexpr int AP = 1, SW = TW + 2, SH = TH + 2;
   __shared__ float4 sA[SW * SH], sG[SW * SH];
@@ -602,11 +621,8 @@ __global__ void __launch_bounds__(TW *TH) k_fine_bwd(const TwinFrame T, const fl
   const int o = py * f.W + px, ti = (threadIdx.y + AP) * SW + threadIdx.x + AP;
   const float4 gp = sG[ti];
   if (gp.w < 0.0f) return;  // X = emission: no dependence on the parameters
-  // tm adjoint: tm(X) = X / (1 + lum(X))
-  const float4 Xv = T.X[o], gt = gT[o];
-  const float L1 = 1.0f + lum(Xv);
-  const float k = (gt.x * Xv.x + gt.y * Xv.y + gt.z * Xv.z) / (L1 * L1);
-  const float3 gX = make_float3(gt.x / L1 - k * 0.2126f, gt.y / L1 - k * 0.7152f, gt.z / L1 - k * 0.0722f);
+  const float4 gt = gT[o];
+  const float3 gX = SEED_TM ? tm_adjoint(T.X[o], gt) : make_float3(gt.x, gt.y, gt.z);
   const float4 alb = ldh(f.mat, py * f.p_mat + px);
   const int hp = (py >> 1) * f.W2 + (px >> 1);
   const float4 p0 = T.par[3 * hp], p1 = T.par[3 * hp + 1], p2 = T.par[3 * hp + 2];
@@ -678,9 +694,11 @@ __global__ void __launch_bounds__(MB_ROWS) k_mlp_bwd(const TwinFrame T) {
     mlp_full(th, fe, h1, h2, out);
     const float4 q0 = T.dpar[3 * o], q1 = T.dpar[3 * o + 1], q2 = T.dpar[3 * o + 2];
     const float4 p0 = T.par[3 * o], p1 = T.par[3 * o + 1], p2 = T.par[3 * o + 2];
-    // heads (hush.js:357-362); alpha, gamma act on the next frame only
-    d3[0] = 0.0f;
-    d3[1] = 0.0f;
+    // heads (hush.js:357-362); alpha and gamma act on the next frame's temporal blend only, so within a frame their
+    // dL/dpar is zero; the per-pass MLP adjoint still carries a seed given for them
+    const float sa = sigmoidf_(out[0]), sg = sigmoidf_(out[1]);
+    d3[0] = q0.x * (31.0f / 32.0f) * sa * (1.0f - sa);
+    d3[1] = q0.y * 7.5f * sg * (1.0f - sg);
     d3[2] = q0.z * p0.z * (1.0f - p0.z);
     d3[3] = q0.w * p0.w * (1.0f - p0.w);
     const float ps[4] = {p1.x, p1.y, p1.z, p1.w}, pc[4] = {p2.x, p2.y, p2.z, p2.w};
@@ -760,12 +778,14 @@ struct hush_trainer_s {
   float *theta = nullptr, *m = nullptr, *v = nullptr;
   double *grad = nullptr, *loss = nullptr, *loss_acc = nullptr, *loss_partials = nullptr;
   float4 *par = nullptr, *B[3] = {}, *A1 = nullptr, *X = nullptr, *out[2] = {}, *gT = nullptr, *gT2 = nullptr,
-         *dB[3] = {}, *dpar = nullptr;
+         *dB[3] = {}, *dpar = nullptr, *dX = nullptr;
   float *partials = nullptr;
   int n_mlp_ctas = 0, n_loss_ctas = 0;
   int cur = 0, has_prev = 0;
   int adam_t = 0;
   char *pool = nullptr;
+  TwinFrame T{};  // the frame fixed by hush_trainer_begin for the per-pass calls
+  int begun = 0;
 };
 
 static int tr_fail(hush_trainer_t *t, const std::string &m) { return hush_fail(t ? t->h : nullptr, HUSH_ERR_ARG, m); }
@@ -783,7 +803,7 @@ extern "C" int hush_trainer_create(hush_t *h, const float *theta, hush_trainer_t
   t->n_loss_ctas = (int)((full + 255) / 256);
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
   const size_t bytes = al(NW * 4) * 3 + al(NW * 8) + al(8) * 2 + al(t->n_loss_ctas * 8) + al(half * 48) * 2 +
-                       al(half * 16) * 6 + al(full * 16) * 6 + al((size_t)t->n_mlp_ctas * NW * 4);
+                       al(half * 16) * 6 + al(full * 16) * 7 + al((size_t)t->n_mlp_ctas * NW * 4);
   cudaError_t e = cudaMalloc(&t->pool, bytes);
   if (e != cudaSuccess) { delete t; return hush_cuda_fail(h, e, "cudaMalloc of the trainer"); }
   cudaMemset(t->pool, 0, bytes);
@@ -796,7 +816,7 @@ extern "C" int hush_trainer_create(hush_t *h, const float *theta, hush_trainer_t
   for (int i = 0; i < 3; i++) { t->B[i] = (float4 *)take(half * 16); t->dB[i] = (float4 *)take(half * 16); }
   t->A1 = (float4 *)take(full * 16); t->X = (float4 *)take(full * 16);
   t->out[0] = (float4 *)take(full * 16); t->out[1] = (float4 *)take(full * 16);
-  t->gT = (float4 *)take(full * 16); t->gT2 = (float4 *)take(full * 16);
+  t->gT = (float4 *)take(full * 16); t->gT2 = (float4 *)take(full * 16); t->dX = (float4 *)take(full * 16);
   t->partials = (float *)take((size_t)t->n_mlp_ctas * NW * 4);
   e = cudaMemcpy(t->theta, theta ? theta : h->wf.data(), NW * 4, theta ? cudaMemcpyHostToDevice : cudaMemcpyHostToDevice);
   if (e != cudaSuccess) { cudaFree(t->pool); delete t; return hush_cuda_fail(h, e, "cudaMemcpy of the weights"); }
@@ -842,6 +862,8 @@ extern "C" int hush_trainer_frame(hush_trainer_t *t, const hush_inputs *in, cons
                                   float lambda_t, int backward, void *stream, double *loss_out) {
   if (!t) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_trainer_frame: NULL trainer");
   if (!clean) return tr_fail(t, "hush_trainer_frame: missing clean image");
+  if (t->W != t->h->W || t->H != t->h->H)
+    return tr_fail(t, "hush_trainer_frame: the denoiser was resized after the trainer was created");
   int rc = hush_check_inputs(t->h, in);
   if (rc != HUSH_OK) return rc;
   cudaSetDevice(t->h->dev);
@@ -868,7 +890,7 @@ extern "C" int hush_trainer_frame(hush_trainer_t *t, const hush_inputs *in, cons
     cudaMemsetAsync(t->dpar, 0, (size_t)half * 48, st);
     for (int i = 0; i < 3; i++) cudaMemsetAsync(t->dB[i], 0, (size_t)half * 16, st);
     k_taa_bwd<<<gf, blk, 0, st>>>(T, t->gT, t->gT2);
-    k_fine_bwd<<<gf, blk, 0, st>>>(T, t->gT2);
+    k_fine_bwd<true><<<gf, blk, 0, st>>>(T, t->gT2);
     k_mid_bwd<3><<<gh, blk, 0, st>>>(T);
     k_mid_bwd<2><<<gh, blk, 0, st>>>(T);
     k_mid_bwd<1><<<gh, blk, 0, st>>>(T);
@@ -897,6 +919,7 @@ extern "C" int hush_trainer_loss_sum(hush_trainer_t *t, void *stream, double *ou
 
 extern "C" int hush_trainer_end_frame(hush_trainer_t *t) {
   if (!t) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_trainer_end_frame: NULL trainer");
+  t->begun = 0;
   t->has_prev = 1;
   t->cur ^= 1;
   return hush_end_frame(t->h);
@@ -904,6 +927,7 @@ extern "C" int hush_trainer_end_frame(hush_trainer_t *t) {
 
 extern "C" int hush_trainer_reset(hush_trainer_t *t) {
   if (!t) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_trainer_reset: NULL trainer");
+  t->begun = 0;
   t->has_prev = 0;
   return hush_reset(t->h);
 }
@@ -988,6 +1012,163 @@ extern "C" int hush_trainer_export(hush_trainer_t *t, uint16_t *blob) {
   for (int i = 0; i < NW; i++) b[i] = __half_as_ushort(__float2half_rn(th[i]));
   if (blob) std::memcpy(blob, b.data(), NW * 2);
   return hush_set_weights(t->h, b.data(), NW);
+}
+
+// ------------------------------------------------------------------------------------------------ per-pass pairs
+// The twin's passes one at a time, each as a forward / adjoint pair over the trainer's buffers: the same kernels as
+// hush_trainer_frame, except that the TAA adjoint finishes with the tm adjoint (dX rather than d tm(X)) and the fine
+// adjoint starts from dX.
+extern "C" int hush_trainer_begin(hush_trainer_t *t, const hush_inputs *in, const float *clean, const float *clean_prev,
+                                  float lambda_t, void *stream) {
+  if (!t) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_trainer_begin: NULL trainer");
+  t->begun = 0;
+  if (!clean) return tr_fail(t, "hush_trainer_begin: missing clean image");
+  if (t->W != t->h->W || t->H != t->h->H)
+    return tr_fail(t, "hush_trainer_begin: the denoiser was resized after the trainer was created");
+  int rc = hush_check_inputs(t->h, in);
+  if (rc != HUSH_OK) return rc;
+  cudaSetDevice(t->h->dev);
+  cudaStream_t st = (cudaStream_t)stream;
+  t->T = make_twin(t, in, clean, clean_prev, lambda_t);
+  cudaError_t e = launch_pass(PASS_TEMPORAL, t->T.f, t->h->w16, st);
+  if (e == cudaSuccess) e = launch_pass(PASS_COARSE1, t->T.f, t->h->w16, st);
+  if (e == cudaSuccess) e = launch_pass(PASS_COARSE2, t->T.f, t->h->w16, st);
+  if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "trainer pass launch");
+  t->begun = 1;
+  return HUSH_OK;
+}
+
+extern "C" int hush_trainer_zero_adjoints(hush_trainer_t *t, void *stream) {
+  if (!t) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_trainer_zero_adjoints: NULL trainer");
+  cudaSetDevice(t->h->dev);
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t full = (size_t)t->W * t->H, half = (size_t)t->W2 * t->H2;
+  cudaError_t e = cudaMemsetAsync(t->dX, 0, full * 16, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(t->gT, 0, full * 16, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(t->dpar, 0, half * 48, st);
+  for (int i = 0; i < 3 && e == cudaSuccess; i++) e = cudaMemsetAsync(t->dB[i], 0, half * 16, st);
+  return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, "cudaMemsetAsync");
+}
+
+static int run_twin_pass(hush_trainer_t *t, int pass, int backward, void *stream, const char *who) {
+  if (!t) return hush_fail(nullptr, HUSH_ERR_ARG, std::string(who) + ": NULL trainer");
+  if (pass < 0 || pass >= HUSH_TWIN_PASSES) return tr_fail(t, std::string(who) + ": unknown pass");
+  if (!t->begun) return tr_fail(t, std::string(who) + ": no frame; call hush_trainer_begin first");
+  cudaSetDevice(t->h->dev);
+  cudaStream_t st = (cudaStream_t)stream;
+  const TwinFrame &T = t->T;
+  const HushFrame &f = T.f;
+  const int half = f.W2 * f.H2, full = f.W * f.H;
+  const dim3 blk(TW, TH), gh((f.W2 + TW - 1) / TW, (f.H2 + TH - 1) / TH), gf((f.W + TW - 1) / TW, (f.H + TH - 1) / TH);
+  cudaError_t e = cudaSuccess;
+  switch (pass) {
+    case HUSH_TWIN_MLP:
+      if (!backward) {
+        k_mlp_fwd<<<(half + 127) / 128, 128, 0, st>>>(T);
+      } else {
+        k_mlp_bwd<<<t->n_mlp_ctas, MB_ROWS, MB_SMEM, st>>>(T);
+        k_reduce_partials<<<(NW + 127) / 128, 128, 0, st>>>(t->partials, t->n_mlp_ctas, t->grad);
+      }
+      break;
+    case HUSH_TWIN_MID1:
+      if (backward) k_mid_bwd<1><<<gh, blk, 0, st>>>(T); else k_mid_fwd<1><<<gh, blk, 0, st>>>(T);
+      break;
+    case HUSH_TWIN_MID2:
+      if (backward) k_mid_bwd<2><<<gh, blk, 0, st>>>(T); else k_mid_fwd<2><<<gh, blk, 0, st>>>(T);
+      break;
+    case HUSH_TWIN_MID3:
+      if (backward) k_mid_bwd<3><<<gh, blk, 0, st>>>(T); else k_mid_fwd<3><<<gh, blk, 0, st>>>(T);
+      break;
+    case HUSH_TWIN_FINE:
+      if (backward) k_fine_bwd<false><<<gf, blk, 0, st>>>(T, t->dX); else k_fine_fwd<<<gf, blk, 0, st>>>(T);
+      break;
+    case HUSH_TWIN_TAA:
+      if (!backward) {
+        k_taa_fwd<<<gf, blk, 0, st>>>(T);
+      } else {
+        e = cudaMemsetAsync(t->gT2, 0, (size_t)full * 16, st);
+        k_taa_bwd<<<gf, blk, 0, st>>>(T, t->gT, t->gT2);
+        k_tm_bwd<<<(full + 255) / 256, 256, 0, st>>>(T, t->gT2, t->dX);
+      }
+      break;
+    default:  // HUSH_TWIN_LOSS
+      k_loss<<<t->n_loss_ctas, 256, 0, st>>>(T, backward);
+      k_reduce_f64<<<1, 256, 0, st>>>(t->loss_partials, t->n_loss_ctas, t->loss, nullptr);
+      break;
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, (std::string(who) + ": kernel launch").c_str());
+}
+
+extern "C" int hush_trainer_pass(hush_trainer_t *t, int pass, int backward, void *stream) {
+  return run_twin_pass(t, pass, backward, stream, "hush_trainer_pass");
+}
+extern "C" int hush_mlp_fwd(hush_trainer_t *t, void *stream) { return run_twin_pass(t, HUSH_TWIN_MLP, 0, stream, "hush_mlp_fwd"); }
+extern "C" int hush_mlp_bwd(hush_trainer_t *t, void *stream) { return run_twin_pass(t, HUSH_TWIN_MLP, 1, stream, "hush_mlp_bwd"); }
+extern "C" int hush_mid1_fwd(hush_trainer_t *t, void *stream) { return run_twin_pass(t, HUSH_TWIN_MID1, 0, stream, "hush_mid1_fwd"); }
+extern "C" int hush_mid1_bwd(hush_trainer_t *t, void *stream) { return run_twin_pass(t, HUSH_TWIN_MID1, 1, stream, "hush_mid1_bwd"); }
+extern "C" int hush_mid2_fwd(hush_trainer_t *t, void *stream) { return run_twin_pass(t, HUSH_TWIN_MID2, 0, stream, "hush_mid2_fwd"); }
+extern "C" int hush_mid2_bwd(hush_trainer_t *t, void *stream) { return run_twin_pass(t, HUSH_TWIN_MID2, 1, stream, "hush_mid2_bwd"); }
+extern "C" int hush_mid3_fwd(hush_trainer_t *t, void *stream) { return run_twin_pass(t, HUSH_TWIN_MID3, 0, stream, "hush_mid3_fwd"); }
+extern "C" int hush_mid3_bwd(hush_trainer_t *t, void *stream) { return run_twin_pass(t, HUSH_TWIN_MID3, 1, stream, "hush_mid3_bwd"); }
+extern "C" int hush_fine_fwd(hush_trainer_t *t, void *stream) { return run_twin_pass(t, HUSH_TWIN_FINE, 0, stream, "hush_fine_fwd"); }
+extern "C" int hush_fine_bwd(hush_trainer_t *t, void *stream) { return run_twin_pass(t, HUSH_TWIN_FINE, 1, stream, "hush_fine_bwd"); }
+extern "C" int hush_taa_fwd(hush_trainer_t *t, void *stream) { return run_twin_pass(t, HUSH_TWIN_TAA, 0, stream, "hush_taa_fwd"); }
+extern "C" int hush_taa_bwd(hush_trainer_t *t, void *stream) { return run_twin_pass(t, HUSH_TWIN_TAA, 1, stream, "hush_taa_bwd"); }
+extern "C" int hush_loss_fwd(hush_trainer_t *t, void *stream) { return run_twin_pass(t, HUSH_TWIN_LOSS, 0, stream, "hush_loss_fwd"); }
+extern "C" int hush_loss_bwd(hush_trainer_t *t, void *stream) { return run_twin_pass(t, HUSH_TWIN_LOSS, 1, stream, "hush_loss_bwd"); }
+
+extern "C" int hush_trainer_buffer(hush_trainer_t *t, int which, void **ptr, int *width, int *height, int *channels) {
+  if (!t || !ptr) return hush_fail(t ? t->h : nullptr, HUSH_ERR_ARG, "hush_trainer_buffer: NULL argument");
+  void *p = nullptr;
+  int w = t->W, h = t->H, c = 4;
+  switch (which) {
+    case HUSH_TB_THETA: p = t->theta; w = NW; h = 1; c = 1; break;
+    case HUSH_TB_GRAD: p = t->grad; w = NW; h = 1; c = 1; break;
+    case HUSH_TB_LOSS: p = t->loss; w = 1; h = 1; c = 1; break;
+    case HUSH_TB_PAR: p = t->par; w = t->W2; h = t->H2; c = 12; break;
+    case HUSH_TB_DPAR: p = t->dpar; w = t->W2; h = t->H2; c = 12; break;
+    case HUSH_TB_B1: case HUSH_TB_B2: case HUSH_TB_B3:
+      p = t->B[which - HUSH_TB_B1]; w = t->W2; h = t->H2; break;
+    case HUSH_TB_DB1: case HUSH_TB_DB2: case HUSH_TB_DB3:
+      p = t->dB[which - HUSH_TB_DB1]; w = t->W2; h = t->H2; break;
+    case HUSH_TB_A1: p = t->A1; break;
+    case HUSH_TB_X: p = t->X; break;
+    case HUSH_TB_DX: p = t->dX; break;
+    case HUSH_TB_OUT: p = t->out[t->cur]; break;
+    case HUSH_TB_OUT_PREV: p = t->out[t->cur ^ 1]; break;
+    case HUSH_TB_DOUT: p = t->gT; break;
+    default: return tr_fail(t, "hush_trainer_buffer: unknown buffer");
+  }
+  *ptr = p;
+  if (width) *width = w;
+  if (height) *height = h;
+  if (channels) *channels = c;
+  return HUSH_OK;
+}
+
+// One optimiser step over a batch of windows, as the training loop runs it on one GPU: per window a history reset,
+// then every frame forward and backward (the temporal term from the window's second frame on) and end-of-frame; then
+// Adam on the summed gradient.
+extern "C" int hush_train_step(hush_trainer_t *t, const hush_inputs *frames, const float *const *cleans, int n_windows,
+                               int n_frames, float lambda_t, float lr, float beta1, float beta2, float eps, float clip,
+                               void *stream, double *loss_mean, double *grad_norm) {
+  if (!t || !frames || !cleans) return hush_fail(t ? t->h : nullptr, HUSH_ERR_ARG, "hush_train_step: NULL argument");
+  if (n_windows < 1 || n_frames < 1) return tr_fail(t, "hush_train_step: empty batch");
+  double s = 0.0;
+  int rc = hush_trainer_loss_sum(t, stream, &s);  // restart the loss sum
+  for (int w = 0; w < n_windows && rc == HUSH_OK; w++) {
+    rc = hush_trainer_reset(t);
+    for (int i = 0; i < n_frames && rc == HUSH_OK; i++) {
+      const size_t k = (size_t)w * n_frames + i;
+      rc = hush_trainer_frame(t, frames + k, cleans[k], i ? cleans[k - 1] : nullptr, lambda_t, 1, stream, nullptr);
+      if (rc == HUSH_OK) rc = hush_trainer_end_frame(t);
+    }
+  }
+  if (rc == HUSH_OK) rc = hush_trainer_loss_sum(t, stream, &s);
+  if (rc != HUSH_OK) return rc;
+  if (loss_mean) *loss_mean = s / ((double)n_windows * n_frames);
+  return hush_trainer_step(t, lr, beta1, beta2, eps, clip, stream, grad_norm);
 }
 
 // ------------------------------------------------------------------------------------------------ no-allocation

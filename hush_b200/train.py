@@ -131,6 +131,56 @@ class Trainer:
         self._check(L.lib().hush_trainer_export(self._t, b.ctypes.data))
         return b
 
+    # ---- the passes as forward / adjoint pairs (hush_trainer_begin, hush_<pass>_fwd / _bwd) ----
+    def begin(self, inputs: dict, clean, clean_prev=None, lambda_t: float = 0.0, stream=None):
+        """TEMPORAL and the coarse levels for the frame; fixes the frame for fwd() / bwd(). The tensors must stay
+        alive until the frame's last pass call."""
+        _fill_inputs(self._inp, inputs)
+        self._begun = (inputs, clean, clean_prev)
+        self._check(L.lib().hush_trainer_begin(self._t, C.byref(self._inp), clean.data_ptr(),
+                                               clean_prev.data_ptr() if clean_prev is not None else None,
+                                               float(lambda_t), C.c_void_p(_stream_handle(stream))))
+
+    def fwd(self, name: str, stream=None):
+        """Forward of one pass ("mlp", "mid1", "mid2", "mid3", "fine", "taa", "loss")."""
+        self._check(getattr(L.lib(), f"hush_{name}_fwd")(self._t, C.c_void_p(_stream_handle(stream))))
+
+    def bwd(self, name: str, stream=None):
+        """Adjoint of one pass: adds into the gradients of its inputs (the loss adjoint sets dOUT)."""
+        self._check(getattr(L.lib(), f"hush_{name}_bwd")(self._t, C.c_void_p(_stream_handle(stream))))
+
+    def zero_adjoints(self, stream=None):
+        self._check(L.lib().hush_trainer_zero_adjoints(self._t, C.c_void_p(_stream_handle(stream))))
+
+    def buffer(self, name: str):
+        """Torch view of a trainer buffer (hush_trainer_buf): THETA / GRAD (812,), LOSS (1,), PAR / DPAR (h, w, 12),
+        B1..B3 / DB1..DB3 (h, w, 4), A1 / X / DX / OUT / OUT_PREV / DOUT (H, W, 4)."""
+        import torch
+
+        ptr, w, h, c = C.c_void_p(), C.c_int(), C.c_int(), C.c_int()
+        self._check(L.lib().hush_trainer_buffer(self._t, L.TWIN_BUF_NAMES.index(name), C.byref(ptr), C.byref(w),
+                                                C.byref(h), C.byref(c)))
+        ts = "<f8" if name in ("GRAD", "LOSS") else "<f4"
+        v = torch.as_tensor(_DevView(ptr.value, h.value, w.value, c.value, ts),
+                            device=torch.device("cuda", self.hush.device))
+        return v.view(-1) if h.value == 1 and c.value == 1 else v
+
+    def train_step(self, windows, lambda_t=0.5, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, clip=1.0, stream=None):
+        """hush_train_step over a batch: windows = list of windows, each a list of input dicts with a "clean" (H, W, 3)
+        float32 CUDA tensor. Returns (mean frame loss, gradient norm)."""
+        nw, nf = len(windows), len(windows[0])
+        if any(len(w) != nf for w in windows):
+            raise HushError("train_step: windows must have the same number of frames")
+        ins = (L.HushInputs * (nw * nf))()
+        cl = (C.c_void_p * (nw * nf))()
+        for i, fr in enumerate(f for w in windows for f in w):
+            _fill_inputs(ins[i], fr)
+            cl[i] = fr["clean"].data_ptr()
+        loss, gn = C.c_double(), C.c_double()
+        self._check(L.lib().hush_train_step(self._t, ins, cl, nw, nf, float(lambda_t), lr, beta1, beta2, eps, clip,
+                                            C.c_void_p(_stream_handle(stream)), C.byref(loss), C.byref(gn)))
+        return loss.value, gn.value
+
     def destroy(self):
         if getattr(self, "_t", None) and self._t.value:
             L.lib().hush_trainer_destroy(self._t)

@@ -177,6 +177,80 @@ int hush_trainer_step(hush_trainer_t *t, float lr, float beta1, float beta2, flo
 /* Round the master weights to the f16 blob, install it in the denoiser and copy it to blob (if not NULL). */
 int hush_trainer_export(hush_trainer_t *t, uint16_t *blob);
 
+/* One optimiser step over a batch, as a one-GPU training loop runs it: for each of n_windows windows of n_frames
+ * frames (frames[] and cleans[] window-major; cleans[] holds device pointers to dense f32 rgb images) a history
+ * reset, then per frame hush_trainer_frame with backward (clean_prev = the window's previous frame from its second
+ * frame on) and hush_trainer_end_frame; then hush_trainer_step. *loss_mean = the mean frame loss of the batch (the
+ * loss sum is restarted first). Synchronises `stream`. Data-parallel callers all-reduce between the frames and the
+ * step instead (hush_trainer_accumulators). */
+int hush_train_step(hush_trainer_t *t, const hush_inputs *frames, const float *const *cleans, int n_windows,
+                    int n_frames, float lambda_t, float lr, float beta1, float beta2, float eps, float clip,
+                    void *stream, double *loss_mean, double *grad_norm);
+
+/* ---- the twin's passes as forward / adjoint pairs -----------------------------------------------------------------
+ * Each pass of the twin on its own, for gradient checks and for hosts that schedule the passes themselves. The
+ * reference's passes (hush.js:835-874) map as: INFER = MLP + MID1, mid2 / mid3 = MID2 / MID3, FINE_FINAL = FINE,
+ * TAA = TAA; TEMPORAL and the coarse levels run in hush_trainer_begin (their outputs do not depend on the weights).
+ * hush_trainer_begin fixes the frame: the inputs must stay valid until its last pass call, and hush_trainer_end_frame
+ * or hush_trainer_reset ends it. A forward pass overwrites its outputs. An adjoint pass ADDS into the gradients of its
+ * inputs (hush_trainer_zero_adjoints clears dX, dOUT, dPAR and dB1..dB3), except the loss adjoint, which sets dOUT;
+ * the MLP adjoint adds dL/dtheta into the weight-gradient accumulator (GRAD). Adjoints recompute what they need from
+ * the pass's inputs (the a-trous weights included) and need the pass's forward inputs in place, not its outputs.
+ * Running LOSS, TAA, FINE, MID3, MID2, MID1, MLP backward after the forward chain gives hush_trainer_frame's
+ * gradient. */
+typedef enum {
+  HUSH_TWIN_MLP = 0, /* theta, features F0..F2, guide F3        -> PAR      | dPAR -> GRAD                     */
+  HUSH_TWIN_MID1 = 1, /* block means (F2), guide, PAR            -> B1       | dB1  -> dPAR (s1, c1)            */
+  HUSH_TWIN_MID2 = 2, /* B1, guide, PAR                          -> B2       | dB2  -> dB1, dPAR (s2, c2)       */
+  HUSH_TWIN_MID3 = 3, /* B2, guide, PAR                          -> B3       | dB3  -> dB2, dPAR (s3, c3)       */
+  HUSH_TWIN_FINE = 4, /* A0, key, PAR, B3, C0, CG, G-buffer      -> A1, X    | dX   -> dB3, dPAR (s0 c0 beta kappa) */
+  HUSH_TWIN_TAA = 5,  /* X, motion, previous TAA output          -> OUT      | dOUT -> dX                       */
+  HUSH_TWIN_LOSS = 6, /* OUT, clean, clean_prev, OUT_PREV        -> LOSS     | 1    -> dOUT                     */
+  HUSH_TWIN_PASSES = 7
+} hush_twin_pass;
+
+/* The trainer's buffers (device memory owned by the trainer, valid until hush_trainer_destroy; OUT / OUT_PREV swap at
+ * hush_trainer_end_frame). Element types: THETA f32, GRAD and LOSS f64, the rest f32. */
+typedef enum {
+  HUSH_TB_THETA = 0,    /* 812 x 1 x 1: FP32 master weights (W1 b1 W2 b2 W3 b3)                      */
+  HUSH_TB_GRAD = 1,     /* 812 x 1 x 1: weight-gradient accumulator                                  */
+  HUSH_TB_LOSS = 2,     /* 1 x 1 x 1: the last loss                                                  */
+  HUSH_TB_PAR = 3,      /* W2 x H2 x 12: alpha gamma beta kappa, s0..s3, c0..c3 per half-res pixel   */
+  HUSH_TB_DPAR = 4,     /* W2 x H2 x 12                                                              */
+  HUSH_TB_B1 = 5, HUSH_TB_B2 = 6, HUSH_TB_B3 = 7,     /* W2 x H2 x 4: mid levels (rgb, variance)      */
+  HUSH_TB_DB1 = 8, HUSH_TB_DB2 = 9, HUSH_TB_DB3 = 10, /* W2 x H2 x 4                                 */
+  HUSH_TB_A1 = 11,      /* W x H x 4: fine level                                                     */
+  HUSH_TB_X = 12,       /* W x H x 4: recombined colour (the TAA input)                              */
+  HUSH_TB_DX = 13,      /* W x H x 4                                                                 */
+  HUSH_TB_OUT = 14,     /* W x H x 4: TAA output of this frame                                       */
+  HUSH_TB_OUT_PREV = 15, /* W x H x 4: TAA output of the previous frame (the temporal loss term)     */
+  HUSH_TB_DOUT = 16,    /* W x H x 4                                                                 */
+  HUSH_TB_COUNT = 17
+} hush_trainer_buf;
+
+/* TEMPORAL and the coarse levels for the frame's inputs, and the frame context for the pass calls (clean: dense f32
+ * rgb, required; clean_prev may be NULL). */
+int hush_trainer_begin(hush_trainer_t *t, const hush_inputs *in, const float *clean, const float *clean_prev,
+                       float lambda_t, void *stream);
+int hush_trainer_zero_adjoints(hush_trainer_t *t, void *stream);
+int hush_trainer_buffer(hush_trainer_t *t, int which, void **ptr, int *width, int *height, int *channels);
+/* pass: a hush_twin_pass; backward != 0 runs its adjoint. The named pairs below are the same calls. */
+int hush_trainer_pass(hush_trainer_t *t, int pass, int backward, void *stream);
+int hush_mlp_fwd(hush_trainer_t *t, void *stream);
+int hush_mlp_bwd(hush_trainer_t *t, void *stream);
+int hush_mid1_fwd(hush_trainer_t *t, void *stream);
+int hush_mid1_bwd(hush_trainer_t *t, void *stream);
+int hush_mid2_fwd(hush_trainer_t *t, void *stream);
+int hush_mid2_bwd(hush_trainer_t *t, void *stream);
+int hush_mid3_fwd(hush_trainer_t *t, void *stream);
+int hush_mid3_bwd(hush_trainer_t *t, void *stream);
+int hush_fine_fwd(hush_trainer_t *t, void *stream);
+int hush_fine_bwd(hush_trainer_t *t, void *stream);
+int hush_taa_fwd(hush_trainer_t *t, void *stream);
+int hush_taa_bwd(hush_trainer_t *t, void *stream);
+int hush_loss_fwd(hush_trainer_t *t, void *stream);
+int hush_loss_bwd(hush_trainer_t *t, void *stream);
+
 /* Weight gradient of the parameter MLP (812 doubles in dtheta, overwritten) from a half-resolution image of rows:
  * packed features F0..F3 (16-byte texels, width2 x height2, as hush_buffer returns them), dL/dpar (12 floats per
  * row, as hush_trainer_par lays them out) and FP32 weights theta (812). The same computation as the weight-gradient

@@ -118,17 +118,20 @@ def unpack_half(a):
     return _t(np.asarray(a, np.float16).astype(np.float64))
 
 
-def twin_loss(st: dict, theta, lambda_t=0.0, return_all=False):
-    """Loss of one frame. st: numpy arrays F0..F3 (h, w, 8) f16, A0 / key / material / emission / motion / taa_prev
-    (H, W, 4), C0 / CG (qh, qw, 4), clean / clean_prev (H, W, 3) f32, out_prev (H, W, 4) f32 or None, reset (bool).
-    theta: float64 tensor (812,) (may require grad)."""
+def half_inputs(st: dict):
+    """Half-resolution inputs of the twin from the packed features: (features (h, w, 20), guide (h, w, 4) = oct-decoded
+    normal + depth, sky mask (h, w), block means (h, w, 4))."""
     F0, F1, F2, F3 = (unpack_half(st[k]) for k in ("F0", "F1", "F2", "F3"))
-    H2, W2 = F0.shape[:2]
     feats = torch.cat([F0, F1, F2[..., :4]], -1)[..., :20]
     guide_n = oct_dec(F3[..., 0], F3[..., 1])
     Gh = torch.cat([guide_n, F3[..., 2:3]], -1)
     sky_h = F3[..., 2] < 0
     Ah = F2[..., 4:8]
+    return feats, Gh, sky_h, Ah
+
+
+def mlp(feats, theta, sky_h):
+    """The MLP and its heads (hush.js:683-704, 357-362): (par_raw, par) with par zero on sky rows, (h, w, 12)."""
     w = theta
     M1, b1 = w[W1o:B1o].view(16, 20), w[B1o:W2o]
     M2, b2 = w[W2o:B2o].view(16, 16), w[B2o:W3o]
@@ -140,16 +143,27 @@ def twin_loss(st: dict, theta, lambda_t=0.0, return_all=False):
     par = torch.stack([1 / 32 + (31 / 32) * sig(o[..., 0]), 0.5 + 7.5 * sig(o[..., 1]), sig(o[..., 2]), sig(o[..., 3])]
                       + [0.25 * torch.exp(torch.clamp(o[..., 4 + k], -5, 5)) for k in range(4)]
                       + [torch.exp(torch.clamp(o[..., 8 + k], -4, 4)) for k in range(4)], -1)
+    return par, torch.where(sky_h[..., None], torch.zeros_like(par), par)
+
+
+def _par_f(par, sky_h):
     # rows of sky blocks carry zeros; the levels see c = 1 there so that the masked-out branches stay finite (a 0/0
     # in an unselected torch.where branch would turn its zero gradient into NaN)
-    par_raw = par
-    par_f = torch.where(sky_h[..., None], torch.ones_like(par), par)
-    par = torch.where(sky_h[..., None], torch.zeros_like(par), par)
-    z4 = torch.zeros(H2, W2, 4, dtype=torch.float64)
-    B1 = torch.where(sky_h[..., None], z4, filt(Ah, Gh, par_f[..., 5], par_f[..., 9], 1, True))
-    B2 = torch.where(sky_h[..., None], z4, filt(B1, Gh, par_f[..., 6], par_f[..., 10], 2, False))
-    B3 = torch.where(sky_h[..., None], z4, filt(B2, Gh, par_f[..., 7], par_f[..., 11], 4, False))
-    # fine level at full resolution
+    return torch.where(sky_h[..., None], torch.ones_like(par), par)
+
+
+def mid(k: int, src, Gh, sky_h, par):
+    """Mid level k = 1, 2, 3 (hush.js:366, 753-754): B_k = filt(src; s_k, c_k) with step 1, 2, 4; level 1 reads the
+    block means with the variance prefilter. Zero on sky rows."""
+    pf = _par_f(par, sky_h)
+    step = (1, 2, 4)[k - 1]
+    z4 = torch.zeros(*src.shape[:2], 4, dtype=torch.float64)
+    return torch.where(sky_h[..., None], z4, filt(src, Gh, pf[..., 4 + k], pf[..., 8 + k], step, k == 1))
+
+
+def fine(st: dict, par, B3, Gh, sky_h, Ah):
+    """Fine level and recombination (hush.js:578-620): (A1, X), (H, W, 4) and (H, W, 3)."""
+    par_f = _par_f(par, sky_h)
     A0 = _t(st["A0"])
     key = _t(st["key"])
     H, W = A0.shape[:2]
@@ -178,10 +192,10 @@ def twin_loss(st: dict, theta, lambda_t=0.0, return_all=False):
         swh = swh + wj
         uB = uB + wj[..., None] * gather(B3, qy, qx)[..., :3]
         uA = uA + wj[..., None] * gather(Ah, qy, qx)[..., :3]
-    mid = swh > 1e-4
+    mid_ok = swh > 1e-4
     kappa, beta = p_full[..., 3], p_full[..., 2]
-    swh_s = torch.where(mid, swh, torch.ones_like(swh))
-    ill = torch.where(mid[..., None], uB / swh_s[..., None] + kappa[..., None] * (f - uA / swh_s[..., None]), f)
+    swh_s = torch.where(mid_ok, swh, torch.ones_like(swh))
+    ill = torch.where(mid_ok[..., None], uB / swh_s[..., None] + kappa[..., None] * (f - uA / swh_s[..., None]), f)
     C0, CG = _t(st["C0"]), _t(st["CG"])
     CGd = torch.cat([oct_dec(CG[..., 0], CG[..., 1]), CG[..., 2:3]], -1)
     cposx, cposy = (xs.double() + 0.5) / 4.0 - 0.5, (ys.double() + 0.5) / 4.0 - 0.5
@@ -203,7 +217,13 @@ def twin_loss(st: dict, theta, lambda_t=0.0, return_all=False):
     ill2 = ill + (up - ill) * beta[..., None]
     alb, emi = _t(st["material"])[..., :3], _t(st["emission"])[..., :3]
     X = torch.where(sky[..., None], emi, ill2 * alb + emi)
-    # TAA
+    return A1, X
+
+
+def taa(st: dict, X):
+    """TAA (hush.js:649-676) on the recombined colour X (H, W, 3): the output (H, W, 3)."""
+    H, W = X.shape[:2]
+    ys, xs = torch.meshgrid(torch.arange(H), torch.arange(W), indexing="ij")
     cur = tm(X)
     if st.get("reset", False):
         res = cur
@@ -229,7 +249,13 @@ def twin_loss(st: dict, theta, lambda_t=0.0, return_all=False):
         hh = torch.minimum(torch.maximum(hh, m1 - 1.25 * sd), m1 + 1.25 * sd)
         hr = from_ycocg(hh)
         res = torch.where(inside[..., None], hr + (cur - hr) * 0.1, cur)
-    out = res / torch.clamp(1.0 - lum(res), min=1e-4)[..., None]
+    return res / torch.clamp(1.0 - lum(res), min=1e-4)[..., None]
+
+
+def loss_of(st: dict, out, lambda_t=0.0):
+    """The training loss of a TAA output (H, W, 3): clipped relative L1 against st["clean"] plus lambda_t times the
+    same on the difference to the previous frame (st["out_prev"], st["clean_prev"])."""
+    H, W = out.shape[:2]
     clean = _t(st["clean"])
     den = clean.abs() + 1e-2
     N = 3.0 * H * W
@@ -238,6 +264,21 @@ def twin_loss(st: dict, theta, lambda_t=0.0, return_all=False):
         op = _t(st["out_prev"])[..., :3]
         cp = _t(st["clean_prev"])
         loss = loss + lambda_t * torch.clamp(((out - op) - (clean - cp)).abs() / den, max=1.0).sum() / N
+    return loss
+
+
+def twin_loss(st: dict, theta, lambda_t=0.0, return_all=False):
+    """Loss of one frame. st: numpy arrays F0..F3 (h, w, 8) f16, A0 / key / material / emission / motion / taa_prev
+    (H, W, 4), C0 / CG (qh, qw, 4), clean / clean_prev (H, W, 3) f32, out_prev (H, W, 4) f32 or None, reset (bool).
+    theta: float64 tensor (812,) (may require grad)."""
+    feats, Gh, sky_h, Ah = half_inputs(st)
+    par_raw, par = mlp(feats, theta, sky_h)
+    B1 = mid(1, Ah, Gh, sky_h, par)
+    B2 = mid(2, B1, Gh, sky_h, par)
+    B3 = mid(3, B2, Gh, sky_h, par)
+    A1, X = fine(st, par, B3, Gh, sky_h, Ah)
+    out = taa(st, X)
+    loss = loss_of(st, out, lambda_t)
     if return_all:
         return loss, {"par": par, "par_raw": par_raw, "out": out, "X": X, "A1": A1, "B3": B3}
     return loss
