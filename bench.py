@@ -344,6 +344,9 @@ def run_ours(args):
                 "algorithmic_bytes_per_launch": per_stage[dominant]["bytes"]}
     filt_bytes = sum(v["bytes"] for v in per_stage.values() if v["bytes"])
     filt_ms = sum(v["ms"] for v in per_stage.values())
+    # the filter passes alone (every stage after TEMPORAL + MLP): their summed bytes over their summed time
+    fp = [v for k, v in per_stage.items() if k != "temporal+mlp" and v["bytes"]]
+    fp_bytes, fp_ms = sum(v["bytes"] for v in fp), sum(v["ms"] for v in fp)
     n_kernels = 6 if args.schedule == "fused" and args.mlp == "fp32" else 8
     line = {
         "metric": METRIC, "value": round(ms_frame / world, 4), "unit": "ms/frame", "n_gpus": world,
@@ -358,6 +361,10 @@ def run_ours(args):
                       "gbs": round(filt_bytes / (filt_ms * 1e-3) / 1e9, 1) if filt_ms else None,
                       "frac": round(filt_bytes / (filt_ms * 1e-3) / 1e9 / peak, 4) if filt_ms else None,
                       "compulsory_108B_per_px_ms": round(108 * P / (peak * 1e9) * 1e3, 4)},
+        "filter_passes": {"stages": [k for k in per_stage if k != "temporal+mlp"], "bytes": fp_bytes,
+                          "ms": round(fp_ms, 4),
+                          "gbs": round(fp_bytes / (fp_ms * 1e-3) / 1e9, 1) if fp_ms else None,
+                          "frac": round(fp_bytes / (fp_ms * 1e-3) / 1e9 / peak, 4) if fp_ms else None},
         "stages": per_stage,
         "clocks": clocks,
         "e2e": {"value": round(e2e_ms / world, 4), "unit": "ms/frame", "h2d_bytes_per_step": h2d,
