@@ -391,26 +391,18 @@ def _train_step_ms(local, stream, barrier, max_over_ranks, warmup=2, steps=5):
 
     from hush_b200 import Hush
     from hush_b200.dp import DataParallel, finish_step
-    from hush_b200.scene import NAMES
-    from hush_b200.train import TrainConfig, Trainer, window, xavier_init
+    from hush_b200.train import TrainConfig, Trainer, window_scene, xavier_init
 
     cfg = TrainConfig()
     dp = DataParallel()
     th = Hush(local, {"width": cfg.size, "height": cfg.size, "schedule": "passes"})
     tr = Trainer(th, xavier_init(cfg.init_seed))
     rng = dp.seed_rng(cfg.init_seed + 1)
-    bufs = [{n: torch.empty((cfg.size, cfg.size, 4), dtype=torch.float16, device=f"cuda:{local}") for n in NAMES}
-            for _ in range(cfg.frames)]
-    for b in bufs:
-        b["clean"] = torch.empty((cfg.size, cfg.size, 3), dtype=torch.float32, device=f"cuda:{local}")
+    sc = window_scene(cfg)
 
     def one():
-        for _ in range(cfg.batch):
-            win = window(cfg, dp.window_seed(rng, cfg.seeds), bufs)
-            tr.reset()
-            for t, fr in enumerate(win):
-                tr.frame(fr, fr["clean"], win[t - 1]["clean"] if t else None, cfg.lambda_t, True, sync=False)
-                tr.end_frame()
+        tr.windows(sc, [dp.window_seed(rng, cfg.seeds) for _ in range(cfg.batch)], cfg.frames, cfg.lambda_t,
+                   stream=stream)
         return finish_step(tr, dp, cfg.batch * cfg.frames, cfg.lr, cfg.clip)
 
     for _ in range(warmup):

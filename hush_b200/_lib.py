@@ -118,6 +118,8 @@ _SIGS = {
     "hush_train_step": (C.c_int, [_P, C.POINTER(HushInputs), C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_float,
                                   C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, _P, C.POINTER(C.c_double),
                                   C.POINTER(C.c_double)]),
+    "hush_trainer_windows": (C.c_int, [_P, C.POINTER(HushScene), C.POINTER(C.c_uint32), C.c_int, C.c_int,
+                                       C.c_float, _P]),
     "hush_trainer_begin": (C.c_int, [_P, C.POINTER(HushInputs), C.c_void_p, C.c_void_p, C.c_float, _P]),
     "hush_trainer_zero_adjoints": (C.c_int, [_P, _P]),
     "hush_trainer_buffer": (C.c_int, [_P, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int), C.POINTER(C.c_int),

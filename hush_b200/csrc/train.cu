@@ -48,6 +48,8 @@ struct TwinFrame {
   float lambda_t;         // weight of the temporal term
   int has_prev;
   float inv_n;            // 1 / (3 * pixels)
+  float4 *gtm;            // full: gradient scratch of the tone-mapped colour (TAA adjoint, scattered)
+  int zero_adj;           // forward kernels clear the adjoint accumulators (dpar, dB1..dB3, gtm) they precede
 };
 
 HD_INL float4 f3_guide_tw(const uint4 *F3, int i) {
@@ -108,6 +110,7 @@ __global__ void k_mlp_fwd(const TwinFrame T) {
   const int o = blockIdx.x * blockDim.x + threadIdx.x;
   if (o >= f.W2 * f.H2) return;
   const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (T.zero_adj) { T.dpar[3 * o] = z4; T.dpar[3 * o + 1] = z4; T.dpar[3 * o + 2] = z4; }
   if (f3_guide_tw(f.F3, o).w < 0.0f) {
     T.par[3 * o] = z4; T.par[3 * o + 1] = z4; T.par[3 * o + 2] = z4;
     sth(f.par0, o, z4); sth(f.par1, o, z4); sth(f.par2, o, z4);
@@ -245,6 +248,7 @@ __global__ void __launch_bounds__(TW *TH) k_mid_fwd(const TwinFrame T) {
   const int X = bx + threadIdx.x, Y = by + threadIdx.y;
   if (X >= f.W2 || Y >= f.H2) return;
   const int o = Y * f.W2 + X, ti = (threadIdx.y + AP) * SW + threadIdx.x + AP;
+  if (T.zero_adj) (K == 1 ? T.dB1 : (K == 2 ? T.dB2 : T.dB3))[o] = make_float4(0.f, 0.f, 0.f, 0.f);
   if (sG[ti].w < 0.0f) { dst[o] = make_float4(0.f, 0.f, 0.f, 0.f); return; }
   const float4 p1 = T.par[3 * o + 1], p2 = T.par[3 * o + 2];
   const float s = K == 1 ? p1.y : (K == 2 ? p1.z : p1.w), c = K == 1 ? p2.y : (K == 2 ? p2.z : p2.w);
@@ -464,6 +468,7 @@ __global__ void k_taa_fwd(const TwinFrame T) {
   TaaF A;
   taa_fwd(T, px, py, A);
   const int o = py * f.W + px;
+  if (T.zero_adj) T.gtm[o] = make_float4(0.f, 0.f, 0.f, 0.f);
   T.out[o] = make_float4(A.out.x, A.out.y, A.out.z, 1.0f);
   sth(f.taa, o, make_float4(A.out.x, A.out.y, A.out.z, 1.0f));
 }
@@ -668,34 +673,63 @@ __global__ void __launch_bounds__(TW *TH) k_fine_bwd(const TwinFrame T, const fl
 }
 
 // ------------------------------------------------------------------------------------------------ MLP adjoint
-// One row (half-res pixel) per thread: heads adjoint, then the three layers; the weight gradient of the CTA's rows is
-// reduced in shared memory (rows x activations stored transposed) and written as one partial per CTA.
-constexpr int MB_ROWS = 128;
+// One row (half-res pixel) per thread: the forward layers, the heads adjoint, then the deltas of the three layers.
+// Each row's activations and deltas go to shared memory as one record (stride MB_REC, odd, so the rows' writes fall
+// in distinct banks), written as they are formed so that few stay live in registers. The CTA then forms its weight
+// gradient as 120 items, one per thread: a (layer, output j, column chunk) of the weight matrix with its bias as the
+// last column, accumulated over the CTA's rows in row order with one delta load per row shared by the chunk's
+// columns, and writes it as one partial.
+constexpr int MB_ROWS = 128, MB_REC = 97;
+constexpr int RF = 0, RH1 = 20, RH2 = 36, RD1 = 52, RD2 = 68, RD3 = 84;  // fe | h1 | h2 | d1 | d2 | d3 in a record
+constexpr int MB_ITEMS = 120, MB_CHUNK = 9;
 __global__ void __launch_bounds__(MB_ROWS) k_mlp_bwd(const TwinFrame T) {
   extern __shared__ float sm[];
-  float *th = sm;                               // NW
-  float *sd3 = th + NW;                         // [12][ROWS]
-  float *sd2 = sd3 + 12 * MB_ROWS;              // [16][ROWS]
-  float *sd1 = sd2 + 16 * MB_ROWS;              // [16][ROWS]
-  float *sf = sd1 + 16 * MB_ROWS;               // [20][ROWS]
-  float *sh1 = sf + 20 * MB_ROWS;               // [16][ROWS]
-  float *sh2 = sh1 + 16 * MB_ROWS;              // [16][ROWS]
+  float *th = sm;         // NW
+  float *rec = th + NW;   // [ROWS][MB_REC]
   for (int i = threadIdx.x; i < NW; i += MB_ROWS) th[i] = T.theta[i];
   __syncthreads();
   const HushFrame &f = T.f;
   const int r = threadIdx.x;
   const int o = blockIdx.x * MB_ROWS + r;
-  float fe[20], h1[16], h2[16], out[12], d3[12], d2[16], d1[16];
-  for (int i = 0; i < 20; i++) fe[i] = 0.f;
-  for (int i = 0; i < 16; i++) h1[i] = h2[i] = d2[i] = d1[i] = 0.f;
-  for (int i = 0; i < 12; i++) d3[i] = 0.f;
+  float *my = rec + r * MB_REC;
   if (o < f.W2 * f.H2 && f3_guide_tw(f.F3, o).w >= 0.0f) {
+    float fe[20];
     load_features(f, o, fe);
-    mlp_full(th, fe, h1, h2, out);
-    const float4 q0 = T.dpar[3 * o], q1 = T.dpar[3 * o + 1], q2 = T.dpar[3 * o + 2];
-    const float4 p0 = T.par[3 * o], p1 = T.par[3 * o + 1], p2 = T.par[3 * o + 2];
+#pragma unroll
+    for (int i = 0; i < 20; i++) my[RF + i] = fe[i];
+    // forward (hush.js:683-704: bias, then the inputs in increasing index)
+#pragma unroll 2
+    for (int j = 0; j < 16; j++) {
+      float a = th[B1o + j];
+#pragma unroll
+      for (int i = 0; i < 20; i++) a = a + fe[i] * th[W1o + j * 20 + i];
+      my[RH1 + j] = fmaxf(a, 0.0f);
+    }
+    float h[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) h[i] = my[RH1 + i];
+#pragma unroll 2
+    for (int j = 0; j < 16; j++) {
+      float a = th[B2o + j];
+#pragma unroll
+      for (int i = 0; i < 16; i++) a = a + h[i] * th[W2o + j * 16 + i];
+      my[RH2 + j] = fmaxf(a, 0.0f);
+    }
+#pragma unroll
+    for (int i = 0; i < 16; i++) h[i] = my[RH2 + i];
+    float out[12];
+#pragma unroll
+    for (int j = 0; j < 12; j++) {
+      float a = th[B3o + j];
+#pragma unroll
+      for (int i = 0; i < 16; i++) a = a + h[i] * th[W3o + j * 16 + i];
+      out[j] = a;
+    }
     // heads (hush.js:357-362); alpha and gamma act on the next frame's temporal blend only, so within a frame their
     // dL/dpar is zero; the per-pass MLP adjoint still carries a seed given for them
+    const float4 q0 = T.dpar[3 * o], q1 = T.dpar[3 * o + 1], q2 = T.dpar[3 * o + 2];
+    const float4 p0 = T.par[3 * o], p1 = T.par[3 * o + 1], p2 = T.par[3 * o + 2];
+    float d3[12];
     const float sa = sigmoidf_(out[0]), sg = sigmoidf_(out[1]);
     d3[0] = q0.x * (31.0f / 32.0f) * sa * (1.0f - sa);
     d3[1] = q0.y * 7.5f * sg * (1.0f - sg);
@@ -703,56 +737,91 @@ __global__ void __launch_bounds__(MB_ROWS) k_mlp_bwd(const TwinFrame T) {
     d3[3] = q0.w * p0.w * (1.0f - p0.w);
     const float ps[4] = {p1.x, p1.y, p1.z, p1.w}, pc[4] = {p2.x, p2.y, p2.z, p2.w};
     const float gs[4] = {q1.x, q1.y, q1.z, q1.w}, gc[4] = {q2.x, q2.y, q2.z, q2.w};
+#pragma unroll
     for (int k = 0; k < 4; k++) {
       d3[4 + k] = fabsf(out[4 + k]) < 5.0f ? gs[k] * ps[k] : 0.0f;
       d3[8 + k] = fabsf(out[8 + k]) < 4.0f ? gc[k] * pc[k] : 0.0f;
     }
+#pragma unroll
+    for (int j = 0; j < 12; j++) my[RD3 + j] = d3[j];
+    // deltas: d2 = relu'(h2) * W3^T d3 (h holds h2), d1 = relu'(h1) * W2^T d2
+    float d2[16];
+#pragma unroll
     for (int i = 0; i < 16; i++) {
       float a = 0.f;
+#pragma unroll
       for (int j = 0; j < 12; j++) a += d3[j] * th[W3o + j * 16 + i];
-      d2[i] = h2[i] > 0.0f ? a : 0.0f;
+      d2[i] = h[i] > 0.0f ? a : 0.0f;
+      my[RD2 + i] = d2[i];
     }
+#pragma unroll
+    for (int i = 0; i < 16; i++) h[i] = my[RH1 + i];
+#pragma unroll
     for (int i = 0; i < 16; i++) {
       float a = 0.f;
+#pragma unroll
       for (int j = 0; j < 16; j++) a += d2[j] * th[W2o + j * 16 + i];
-      d1[i] = h1[i] > 0.0f ? a : 0.0f;
+      my[RD1 + i] = h[i] > 0.0f ? a : 0.0f;
     }
+  } else {  // rows outside the image or on sky carry zeros
+#pragma unroll 4
+    for (int i = 0; i < MB_REC - 1; i++) my[i] = 0.0f;
   }
-  for (int i = 0; i < 12; i++) sd3[i * MB_ROWS + r] = d3[i];
-  for (int i = 0; i < 16; i++) {
-    sd2[i * MB_ROWS + r] = d2[i];
-    sd1[i * MB_ROWS + r] = d1[i];
-    sh1[i * MB_ROWS + r] = h1[i];
-    sh2[i * MB_ROWS + r] = h2[i];
-  }
-  for (int i = 0; i < 20; i++) sf[i * MB_ROWS + r] = fe[i];
   __syncthreads();
-  // weight gradient of the CTA: parameter p = outer product (delta_j, x_i) summed over rows
+  // weight gradient of the CTA. Item it: layer 1 rows j in 3 chunks of 7 of its 21 columns, layer 2 rows in chunks
+  // 6 / 6 / 5 of 17, layer 3 rows in chunks 9 / 8 of 17; the last column of a row is its bias (x = 1).
+  const int it = threadIdx.x;
+  if (it >= MB_ITEMS) return;
+  int L, j, c0, c1;
+  if (it < 48) { L = 0; j = it / 3; c0 = 7 * (it % 3); c1 = c0 + 7; }
+  else if (it < 96) { L = 1; j = (it - 48) / 3; c0 = 6 * ((it - 48) % 3); c1 = min(c0 + 6, 17); }
+  else { L = 2; j = (it - 96) / 2; c0 = 9 * ((it - 96) % 2); c1 = min(c0 + 9, 17); }
+  const int n_in = L == 0 ? 20 : 16;
+  const int d_off = (L == 0 ? RD1 : (L == 1 ? RD2 : RD3)) + j;
+  const int x_off = (L == 0 ? RF : (L == 1 ? RH1 : RH2)) + c0;
+  const int w_off = (L == 0 ? W1o : (L == 1 ? W2o : W3o)) + j * n_in + c0;
+  const int b_off = (L == 0 ? B1o : (L == 1 ? B2o : B3o)) + j;
+  const int nx = min(c1, n_in) - c0;
+  const bool bias = c1 > n_in;
+  float acc[MB_CHUNK], accb = 0.f;
+#pragma unroll
+  for (int c = 0; c < MB_CHUNK; c++) acc[c] = 0.f;
+#pragma unroll 4
+  for (int k = 0; k < MB_ROWS; k++) {
+    const float *R = rec + k * MB_REC;
+    const float dv = R[d_off];
+#pragma unroll
+    for (int c = 0; c < MB_CHUNK; c++)
+      if (c < nx) acc[c] += dv * R[x_off + c];
+    accb += dv;
+  }
   float *part = T.partials + (size_t)blockIdx.x * NW;
-  for (int p = threadIdx.x; p < NW; p += MB_ROWS) {
-    const float *dv, *xv = nullptr;
-    if (p < B1o) { dv = sd1 + (p / 20) * MB_ROWS; xv = sf + (p % 20) * MB_ROWS; }
-    else if (p < W2o) { dv = sd1 + (p - B1o) * MB_ROWS; }
-    else if (p < B2o) { const int q = p - W2o; dv = sd2 + (q / 16) * MB_ROWS; xv = sh1 + (q % 16) * MB_ROWS; }
-    else if (p < W3o) { dv = sd2 + (p - B2o) * MB_ROWS; }
-    else if (p < B3o) { const int q = p - W3o; dv = sd3 + (q / 16) * MB_ROWS; xv = sh2 + (q % 16) * MB_ROWS; }
-    else { dv = sd3 + (p - B3o) * MB_ROWS; }
-    float a = 0.f;
-    if (xv) for (int k = 0; k < MB_ROWS; k++) a += dv[k] * xv[k];
-    else for (int k = 0; k < MB_ROWS; k++) a += dv[k];
-    part[p] = a;
+#pragma unroll
+  for (int c = 0; c < MB_CHUNK; c++)
+    if (c < nx) part[w_off + c] = acc[c];
+  if (bias) part[b_off] = accb;
+}
+constexpr size_t MB_SMEM = (size_t)(NW + MB_ROWS * MB_REC) * sizeof(float);
+
+// dtheta += sum over CTAs of the partials, in FP64 and in a fixed order: 32 parameters per block on the lanes, the
+// CTAs split over the 8 warps (c = w, w + 8, ...), then the 8 warp sums added in warp order.
+constexpr int RP_THREADS = 256, RP_PARAMS = 32;
+__global__ void __launch_bounds__(RP_THREADS) k_reduce_partials(const float *partials, int nparts, double *grad) {
+  __shared__ double ws[RP_THREADS / 32][RP_PARAMS];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int p = blockIdx.x * RP_PARAMS + lane;
+  double a = 0.0;
+  if (p < NW)
+    for (int c = w; c < nparts; c += RP_THREADS / 32) a += (double)partials[(size_t)c * NW + p];
+  ws[w][lane] = a;
+  __syncthreads();
+  if (w == 0 && p < NW) {
+    double s = 0.0;
+    for (int k = 0; k < RP_THREADS / 32; k++) s += ws[k][lane];
+    grad[p] += s;
   }
 }
-constexpr size_t MB_SMEM = (size_t)(NW + (12 + 16 + 16 + 20 + 16 + 16) * MB_ROWS) * sizeof(float);
-
-// dtheta += sum over CTAs of the partials, in FP64
-__global__ void k_reduce_partials(const float *partials, int nparts, double *grad) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= NW) return;
-  double a = 0.0;
-  for (int c = 0; c < nparts; c++) a += (double)partials[(size_t)c * NW + p];
-  grad[p] += a;
-}
+constexpr int RP_BLOCKS = (NW + RP_PARAMS - 1) / RP_PARAMS;
 
 // Adam on the FP32 master weights (gradient in FP64, optionally clipped by global norm scale `scale`).
 __global__ void k_adam(float *theta, float *m, float *v, const double *grad, float lr, float b1, float b2, float eps,
@@ -786,6 +855,14 @@ struct hush_trainer_s {
   char *pool = nullptr;
   TwinFrame T{};  // the frame fixed by hush_trainer_begin for the per-pass calls
   int begun = 0;
+  char *win_pool = nullptr;  // hush_trainer_windows: one window of generated frames (inputs + noise-free image)
+  int win_frames = 0;
+  // hush_trainer_windows replays a window's training frames as a CUDA graph, one per (frame parity, output slot) at
+  // the window's start; captured for one (frame count, lambda, exposure) and re-captured when those change
+  cudaGraphExec_t win_graph[4] = {};
+  int wg_frames = 0;
+  float wg_lambda = 0.f, wg_exposure = 0.f;
+  cudaStream_t cap = nullptr;
 };
 
 static int tr_fail(hush_trainer_t *t, const std::string &m) { return hush_fail(t ? t->h : nullptr, HUSH_ERR_ARG, m); }
@@ -828,7 +905,11 @@ extern "C" int hush_trainer_create(hush_t *h, const float *theta, hush_trainer_t
 extern "C" void hush_trainer_destroy(hush_trainer_t *t) {
   if (!t) return;
   cudaSetDevice(t->h->dev);
+  for (cudaGraphExec_t &g : t->win_graph)
+    if (g) cudaGraphExecDestroy(g);
+  if (t->cap) cudaStreamDestroy(t->cap);
   cudaFree(t->pool);
+  cudaFree(t->win_pool);
   delete t;
 }
 
@@ -846,6 +927,8 @@ static TwinFrame make_twin(hush_trainer_t *t, const hush_inputs *in, const float
   T.clean = clean;
   T.clean_prev = clean_prev;
   T.gT = t->gT;
+  T.gtm = t->gT2;
+  T.zero_adj = 0;
   T.dB1 = t->dB[0]; T.dB2 = t->dB[1]; T.dB3 = t->dB[2];
   T.dpar = t->dpar;
   T.partials = t->partials;
@@ -868,7 +951,8 @@ extern "C" int hush_trainer_frame(hush_trainer_t *t, const hush_inputs *in, cons
   if (rc != HUSH_OK) return rc;
   cudaSetDevice(t->h->dev);
   cudaStream_t st = (cudaStream_t)stream;
-  const TwinFrame T = make_twin(t, in, clean, clean_prev, lambda_t);
+  TwinFrame T = make_twin(t, in, clean, clean_prev, lambda_t);
+  T.zero_adj = backward ? 1 : 0;  // the forward kernels clear the adjoint accumulators the backward adds into
   const HushFrame &f = T.f;
   // TEMPORAL and the coarse levels as the reference passes (their outputs do not depend on the weights)
   cudaError_t e = launch_pass(PASS_TEMPORAL, f, t->h->w16, st);
@@ -886,16 +970,13 @@ extern "C" int hush_trainer_frame(hush_trainer_t *t, const hush_inputs *in, cons
   k_loss<<<t->n_loss_ctas, 256, 0, st>>>(T, backward);
   k_reduce_f64<<<1, 256, 0, st>>>(t->loss_partials, t->n_loss_ctas, t->loss, t->loss_acc);
   if (backward) {
-    cudaMemsetAsync(t->gT2, 0, (size_t)full * 16, st);
-    cudaMemsetAsync(t->dpar, 0, (size_t)half * 48, st);
-    for (int i = 0; i < 3; i++) cudaMemsetAsync(t->dB[i], 0, (size_t)half * 16, st);
     k_taa_bwd<<<gf, blk, 0, st>>>(T, t->gT, t->gT2);
     k_fine_bwd<true><<<gf, blk, 0, st>>>(T, t->gT2);
     k_mid_bwd<3><<<gh, blk, 0, st>>>(T);
     k_mid_bwd<2><<<gh, blk, 0, st>>>(T);
     k_mid_bwd<1><<<gh, blk, 0, st>>>(T);
     k_mlp_bwd<<<t->n_mlp_ctas, MB_ROWS, MB_SMEM, st>>>(T);
-    k_reduce_partials<<<(NW + 127) / 128, 128, 0, st>>>(t->partials, t->n_mlp_ctas, t->grad);
+    k_reduce_partials<<<RP_BLOCKS, RP_THREADS, 0, st>>>(t->partials, t->n_mlp_ctas, t->grad);
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "trainer kernel launch");
@@ -1014,6 +1095,113 @@ extern "C" int hush_trainer_export(hush_trainer_t *t, uint16_t *blob) {
   return hush_set_weights(t->h, b.data(), NW);
 }
 
+// Windows of the analytic scene generator, trained in place: for each seed, the window's frames are generated on the
+// device into trainer-owned buffers and run forward + backward as hush_train_step runs them (history reset at the
+// window's start, the temporal term from its second frame on), accumulating gradient and loss without a step.
+// One window's training frames on `st` from the generated frames in win_pool: history reset, then per frame forward
+// + backward and end-of-frame.
+static int window_frames(hush_trainer_t *t, int n_frames, size_t img, size_t per, float lambda_t, cudaStream_t st) {
+  int rc = hush_trainer_reset(t);
+  for (int i = 0; i < n_frames && rc == HUSH_OK; i++) {
+    char *b = t->win_pool + per * i;
+    hush_inputs in;
+    std::memset(&in, 0, sizeof(in));
+    in.radiance = b; in.normal_depth = b + img; in.motion = b + 2 * img; in.material = b + 3 * img;
+    in.emission = b + 4 * img;
+    const float *clean = (const float *)(b + 5 * img);
+    const float *clean_prev = i ? (const float *)(t->win_pool + per * (i - 1) + 5 * img) : nullptr;
+    rc = hush_trainer_frame(t, &in, clean, clean_prev, lambda_t, 1, st, nullptr);
+    if (rc == HUSH_OK) rc = hush_trainer_end_frame(t);
+  }
+  return rc;
+}
+
+static void drop_window_graphs(hush_trainer_t *t) {
+  for (cudaGraphExec_t &g : t->win_graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+// Windows of the analytic scene generator, trained in place: for each seed, the window's frames are generated on the
+// device into trainer-owned buffers and run forward + backward as hush_train_step runs them (history reset at the
+// window's start, the temporal term from its second frame on), accumulating gradient and loss without a step. The
+// training frames of a window replay as one CUDA graph: every kernel argument of a window is fixed by the buffers,
+// lambda, the exposure and the frame parity / output slot at its start, which the graph cache is keyed on; the host
+// state (frame counter, history flags) advances exactly as the direct calls advance it. The generation runs outside
+// the graph because its scene parameters change with the seed.
+extern "C" int hush_trainer_windows(hush_trainer_t *t, const hush_scene *sc, const uint32_t *seeds, int n_windows,
+                                    int n_frames, float lambda_t, void *stream) {
+  if (!t || !sc || !seeds) return hush_fail(t ? t->h : nullptr, HUSH_ERR_ARG, "hush_trainer_windows: NULL argument");
+  if (n_windows < 1 || n_frames < 1) return tr_fail(t, "hush_trainer_windows: empty batch");
+  if (sc->width != t->W || sc->height != t->H)
+    return tr_fail(t, "hush_trainer_windows: the scene size differs from the trainer's");
+  if (t->W != t->h->W || t->H != t->h->H)
+    return tr_fail(t, "hush_trainer_windows: the denoiser was resized after the trainer was created");
+  cudaSetDevice(t->h->dev);
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t full = (size_t)t->W * t->H, img = (full * 8 + 255) & ~(size_t)255,
+               cl = (full * 12 + 255) & ~(size_t)255, per = 5 * img + cl;
+  if (t->win_frames < n_frames) {
+    drop_window_graphs(t);
+    cudaFree(t->win_pool);
+    t->win_pool = nullptr;
+    t->win_frames = 0;
+    cudaError_t e = cudaMalloc(&t->win_pool, per * n_frames);
+    if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "cudaMalloc of the window buffers");
+    t->win_frames = n_frames;
+  }
+  if (t->wg_frames != n_frames || t->wg_lambda != lambda_t || t->wg_exposure != t->h->exposure) {
+    drop_window_graphs(t);
+    t->wg_frames = n_frames;
+    t->wg_lambda = lambda_t;
+    t->wg_exposure = t->h->exposure;
+  }
+  if (!t->cap) {
+    cudaError_t e = cudaStreamCreateWithFlags(&t->cap, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "cudaStreamCreate");
+  }
+  hush_scene w = *sc;
+  for (int k = 0; k < n_windows; k++) {
+    w.seed = seeds[k];
+    for (int i = 0; i < n_frames; i++) {
+      char *b = t->win_pool + per * i;
+      const int rc = hush_scene_frame_device(&w, i, b, b + img, b + 2 * img, b + 3 * img, b + 4 * img, b + 5 * img, st);
+      if (rc != HUSH_OK) return hush_fail(t->h, rc, "hush_trainer_windows: scene generation failed");
+    }
+    cudaGraphExec_t &g = t->win_graph[((t->h->frame & 1) << 1) | (t->cur & 1)];
+    if (g) {  // replay, then advance the host state as the frames would
+      cudaError_t e = cudaGraphLaunch(g, st);
+      if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "cudaGraphLaunch of a training window");
+      int rc = hush_trainer_reset(t);
+      for (int i = 0; i < n_frames && rc == HUSH_OK; i++) rc = hush_trainer_end_frame(t);
+      if (rc != HUSH_OK) return rc;
+      continue;
+    }
+    // capture on the trainer's own stream (the caller's may be the legacy default stream, which cannot capture);
+    // the host state advances during the capture exactly once, as it does for the launch that follows
+    const int f0 = t->h->frame;
+    const bool reset0 = t->h->reset;
+    const void *last0 = t->h->last_out;
+    const int cur0 = t->cur, prev0 = t->has_prev;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(t->cap, cudaStreamCaptureModeThreadLocal);
+    int rc = e == cudaSuccess ? window_frames(t, n_frames, img, per, lambda_t, t->cap) : HUSH_ERR_CUDA;
+    const cudaError_t e2 = e == cudaSuccess ? cudaStreamEndCapture(t->cap, &graph) : e;
+    if (rc == HUSH_OK && e2 == cudaSuccess) e = cudaGraphInstantiate(&g, graph, 0);
+    else e = e2 != cudaSuccess ? e2 : cudaErrorUnknown;
+    if (graph) cudaGraphDestroy(graph);
+    if (e == cudaSuccess) e = cudaGraphLaunch(g, st);
+    if (e != cudaSuccess) {  // capture not possible here: undo the host state and run the frames directly
+      cudaGetLastError();
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+      t->h->frame = f0; t->h->reset = reset0; t->h->last_out = last0;
+      t->cur = cur0; t->has_prev = prev0;
+      rc = window_frames(t, n_frames, img, per, lambda_t, st);
+    }
+    if (rc != HUSH_OK) return rc;
+  }
+  return HUSH_OK;
+}
+
 // ------------------------------------------------------------------------------------------------ per-pass pairs
 // The twin's passes one at a time, each as a forward / adjoint pair over the trainer's buffers: the same kernels as
 // hush_trainer_frame, except that the TAA adjoint finishes with the tm adjoint (dX rather than d tm(X)) and the fine
@@ -1067,7 +1255,7 @@ static int run_twin_pass(hush_trainer_t *t, int pass, int backward, void *stream
         k_mlp_fwd<<<(half + 127) / 128, 128, 0, st>>>(T);
       } else {
         k_mlp_bwd<<<t->n_mlp_ctas, MB_ROWS, MB_SMEM, st>>>(T);
-        k_reduce_partials<<<(NW + 127) / 128, 128, 0, st>>>(t->partials, t->n_mlp_ctas, t->grad);
+        k_reduce_partials<<<RP_BLOCKS, RP_THREADS, 0, st>>>(t->partials, t->n_mlp_ctas, t->grad);
       }
       break;
     case HUSH_TWIN_MID1:

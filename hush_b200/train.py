@@ -16,7 +16,7 @@ import numpy as np
 from . import _lib as L
 from .dp import DataParallel, finish_step
 from .hush import Hush, HushError, _DevView, _fill_inputs, _stream_handle
-from .scene import NAMES, SceneConfig, frame_device
+from .scene import SceneConfig, frame_device
 
 NW = 812
 
@@ -65,6 +65,14 @@ class Trainer:
                                                float(lambda_t), 1 if backward else 0,
                                                C.c_void_p(_stream_handle(stream)), C.byref(loss) if sync else None))
         return loss.value if sync else None
+
+    def windows(self, scene_cfg: SceneConfig, seeds, n_frames: int, lambda_t: float = 0.0, stream=None):
+        """hush_trainer_windows: for each seed, the n_frames frames of scene_cfg with that seed generated on the
+        device and run forward + backward (history reset per window); gradient and loss accumulate, no step."""
+        sc = scene_cfg.c()
+        arr = (C.c_uint32 * len(seeds))(*[int(x) & 0xFFFFFFFF for x in seeds])
+        self._check(L.lib().hush_trainer_windows(self._t, C.byref(sc), arr, len(seeds), int(n_frames),
+                                                 float(lambda_t), C.c_void_p(_stream_handle(stream))))
 
     def loss_sum(self, stream=None) -> float:
         """Sum of the frame losses since the previous call."""
@@ -207,9 +215,14 @@ class TrainConfig:
     init_seed: int = 0
 
 
+def window_scene(cfg: TrainConfig, seed: int = 0) -> SceneConfig:
+    """The generator configuration of a training window: 3 independently moving objects, pan U[0,4] px/frame."""
+    return SceneConfig(cfg.size, cfg.size, cfg.frames, seed=seed, pan_min=0.0, pan_max=4.0, n_moving=3)
+
+
 def window(cfg: TrainConfig, seed: int, buf=None):
     """One training window generated on the device: list of (inputs, clean) for `frames` frames."""
-    sc = SceneConfig(cfg.size, cfg.size, cfg.frames, seed=seed, pan_min=0.0, pan_max=4.0, n_moving=3)
+    sc = window_scene(cfg, seed)
     out = []
     for t in range(cfg.frames):
         out.append(frame_device(sc, t, out=None if buf is None else buf[t], clean=True))
@@ -231,20 +244,13 @@ def train(cfg: TrainConfig, log_every: int = 100, on_log=None, time_budget_s: fl
         dp.broadcast_(th)
         tr.theta = th.cpu().numpy()
     rng = dp.seed_rng(cfg.init_seed + 1)
-    bufs = [{n: torch.empty((cfg.size, cfg.size, 4), dtype=torch.float16, device=f"cuda:{device}") for n in NAMES}
-            for _ in range(cfg.frames)]
-    for b in bufs:
-        b["clean"] = torch.empty((cfg.size, cfg.size, 3), dtype=torch.float32, device=f"cuda:{device}")
+    sc = window_scene(cfg)
     hist = []
     t0 = time.time()
     for step in range(cfg.steps):
         ts = time.perf_counter()
-        for _ in range(cfg.batch):
-            win = window(cfg, dp.window_seed(rng, cfg.seeds), bufs)
-            tr.reset()
-            for t, fr in enumerate(win):
-                tr.frame(fr, fr["clean"], win[t - 1]["clean"] if t else None, cfg.lambda_t, True, sync=False)
-                tr.end_frame()
+        seeds = [dp.window_seed(rng, cfg.seeds) for _ in range(cfg.batch)]
+        tr.windows(sc, seeds, cfg.frames, cfg.lambda_t)  # generation + forward + adjoint of every frame, on device
         loss, gn = finish_step(tr, dp, cfg.batch * cfg.frames, cfg.lr, cfg.clip)
         torch.cuda.synchronize()
         ms = (time.perf_counter() - ts) * 1e3

@@ -187,6 +187,16 @@ int hush_train_step(hush_trainer_t *t, const hush_inputs *frames, const float *c
                     int n_frames, float lambda_t, float lr, float beta1, float beta2, float eps, float clip,
                     void *stream, double *loss_mean, double *grad_norm);
 
+/* The training windows of the analytic scene generator (hush_scene_frame_device, declared below), without a
+ * host round trip per frame: for each of n_windows seeds, the n_frames frames of scene *sc with that seed are
+ * generated on the device into trainer-owned buffers (allocated on first use) and run as hush_train_step runs a
+ * window (history reset, then per frame forward + backward with the temporal term from the second frame on, and
+ * end-of-frame). Adds into the gradient and loss accumulators; no optimiser step (the caller all-reduces across ranks
+ * if it trains data-parallel, then calls hush_trainer_step). sc's size must be the trainer's. */
+struct hush_scene_s;
+int hush_trainer_windows(hush_trainer_t *t, const struct hush_scene_s *sc, const uint32_t *seeds, int n_windows,
+                         int n_frames, float lambda_t, void *stream);
+
 /* ---- the twin's passes as forward / adjoint pairs -----------------------------------------------------------------
  * Each pass of the twin on its own, for gradient checks and for hosts that schedule the passes themselves. The
  * reference's passes (hush.js:835-874) map as: INFER = MLP + MID1, mid2 / mid3 = MID2 / MID3, FINE_FINAL = FINE,
@@ -410,7 +420,7 @@ const void *hush_post_buffer(const hush_post_t *p, int level, int *width, int *h
 const char *hush_post_last_error(const hush_post_t *p);
 
 /* ---- synthetic G-buffer scenes (benchmark / test / training inputs) ------------------------------------------ */
-typedef struct {
+typedef struct hush_scene_s {
   int width, height, n_objects, n_moving;
   float sky_frac, pan_min, pan_max, yaw_deg, firefly_rate, firefly_scale;
   int cut_frame;
