@@ -863,6 +863,15 @@ struct hush_trainer_s {
   int wg_frames = 0;
   float wg_lambda = 0.f, wg_exposure = 0.f;
   cudaStream_t cap = nullptr;
+  // hush_trainer_windows runs windows concurrently on lanes: lane 0 is this trainer, lanes 1.. are helper trainers on
+  // private Hush instances of the same size (their own history), reading this trainer's weights and accumulating
+  // into their own gradient / loss, which are added into this trainer's after the batch
+  hush_trainer_t *lane[4] = {};
+  hush_t *lane_h[4] = {};
+  cudaStream_t lane_st[4] = {};
+  cudaEvent_t lane_ev[4] = {};
+  cudaEvent_t fork_ev = nullptr;
+  bool is_lane = false;
 };
 
 static int tr_fail(hush_trainer_t *t, const std::string &m) { return hush_fail(t ? t->h : nullptr, HUSH_ERR_ARG, m); }
@@ -905,6 +914,15 @@ extern "C" int hush_trainer_create(hush_t *h, const float *theta, hush_trainer_t
 extern "C" void hush_trainer_destroy(hush_trainer_t *t) {
   if (!t) return;
   cudaSetDevice(t->h->dev);
+  for (int l = 1; l < 4; l++) {
+    if (t->lane[l]) hush_trainer_destroy(t->lane[l]);
+    if (t->lane_h[l]) hush_destroy(t->lane_h[l]);
+  }
+  for (int l = 0; l < 4; l++) {
+    if (t->lane_st[l]) cudaStreamDestroy(t->lane_st[l]);
+    if (t->lane_ev[l]) cudaEventDestroy(t->lane_ev[l]);
+  }
+  if (t->fork_ev) cudaEventDestroy(t->fork_ev);
   for (cudaGraphExec_t &g : t->win_graph)
     if (g) cudaGraphExecDestroy(g);
   if (t->cap) cudaStreamDestroy(t->cap);
@@ -1128,16 +1146,9 @@ static void drop_window_graphs(hush_trainer_t *t) {
 // lambda, the exposure and the frame parity / output slot at its start, which the graph cache is keyed on; the host
 // state (frame counter, history flags) advances exactly as the direct calls advance it. The generation runs outside
 // the graph because its scene parameters change with the seed.
-extern "C" int hush_trainer_windows(hush_trainer_t *t, const hush_scene *sc, const uint32_t *seeds, int n_windows,
-                                    int n_frames, float lambda_t, void *stream) {
-  if (!t || !sc || !seeds) return hush_fail(t ? t->h : nullptr, HUSH_ERR_ARG, "hush_trainer_windows: NULL argument");
-  if (n_windows < 1 || n_frames < 1) return tr_fail(t, "hush_trainer_windows: empty batch");
-  if (sc->width != t->W || sc->height != t->H)
-    return tr_fail(t, "hush_trainer_windows: the scene size differs from the trainer's");
-  if (t->W != t->h->W || t->H != t->h->H)
-    return tr_fail(t, "hush_trainer_windows: the denoiser was resized after the trainer was created");
-  cudaSetDevice(t->h->dev);
-  cudaStream_t st = (cudaStream_t)stream;
+// The windows seeds[0], seeds[stride], ... in order on one trainer and stream.
+static int windows_serial(hush_trainer_t *t, const hush_scene *sc, const uint32_t *seeds, int n_windows, int stride,
+                          int n_frames, float lambda_t, cudaStream_t st) {
   const size_t full = (size_t)t->W * t->H, img = (full * 8 + 255) & ~(size_t)255,
                cl = (full * 12 + 255) & ~(size_t)255, per = 5 * img + cl;
   if (t->win_frames < n_frames) {
@@ -1160,7 +1171,7 @@ extern "C" int hush_trainer_windows(hush_trainer_t *t, const hush_scene *sc, con
     if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "cudaStreamCreate");
   }
   hush_scene w = *sc;
-  for (int k = 0; k < n_windows; k++) {
+  for (int k = 0; k < n_windows; k += stride) {
     w.seed = seeds[k];
     for (int i = 0; i < n_frames; i++) {
       char *b = t->win_pool + per * i;
@@ -1200,6 +1211,99 @@ extern "C" int hush_trainer_windows(hush_trainer_t *t, const hush_scene *sc, con
     if (rc != HUSH_OK) return rc;
   }
   return HUSH_OK;
+}
+
+// this trainer's accumulators += the helper lanes' (in lane order), which are cleared
+struct LaneAcc {
+  double *grad[4], *loss[4];
+  int n;
+};
+__global__ void k_sum_lanes(double *grad, double *loss, LaneAcc la) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < NW) {
+    double g = grad[p];
+    for (int l = 0; l < la.n; l++) { g += la.grad[l][p]; la.grad[l][p] = 0.0; }
+    grad[p] = g;
+  }
+  if (p == 0) {
+    double s = *loss;
+    for (int l = 0; l < la.n; l++) { s += *la.loss[l]; *la.loss[l] = 0.0; }
+    *loss = s;
+  }
+}
+
+constexpr int TRAIN_LANES = 4;
+
+static int make_lanes(hush_trainer_t *t, int n) {
+  hush_t *h = t->h;
+  for (int l = 0; l < n; l++) {
+    if (!t->lane_st[l]) {
+      cudaError_t e = cudaStreamCreateWithFlags(&t->lane_st[l], cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->lane_ev[l], cudaEventDisableTiming);
+      if (e != cudaSuccess) return hush_cuda_fail(h, e, "creating a training lane");
+    }
+    if (l == 0 || t->lane[l]) continue;
+    hush_desc d = hush_desc_default(t->W, t->H);
+    d.exposure = h->exposure;
+    d.schedule = HUSH_SCHED_PASSES;
+    d.device = h->dev;
+    int rc = hush_create(&d, &t->lane_h[l]);
+    if (rc == HUSH_OK) rc = hush_trainer_create(t->lane_h[l], nullptr, &t->lane[l]);
+    if (rc != HUSH_OK) return hush_fail(h, rc, std::string("creating a training lane: ") + hush_global_error());
+    t->lane[l]->theta = t->theta;  // the helper reads this trainer's master weights
+    t->lane[l]->is_lane = true;
+  }
+  if (!t->fork_ev) {
+    cudaError_t e = cudaEventCreateWithFlags(&t->fork_ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return hush_cuda_fail(h, e, "creating a training lane");
+  }
+  t->lane[0] = t;
+  return HUSH_OK;
+}
+
+// Windows of the analytic scene generator, trained in place: for each seed, the window's frames are generated on the
+// device and run forward + backward as hush_train_step runs them. Up to TRAIN_LANES windows run concurrently, window
+// k on lane k % lanes (each lane its own stream, history and accumulators, the lanes forked from and joined back to
+// `stream`); the lanes' gradients and losses are then added into this trainer's in lane order.
+extern "C" int hush_trainer_windows(hush_trainer_t *t, const hush_scene *sc, const uint32_t *seeds, int n_windows,
+                                    int n_frames, float lambda_t, void *stream) {
+  if (!t || !sc || !seeds) return hush_fail(t ? t->h : nullptr, HUSH_ERR_ARG, "hush_trainer_windows: NULL argument");
+  if (n_windows < 1 || n_frames < 1) return tr_fail(t, "hush_trainer_windows: empty batch");
+  if (sc->width != t->W || sc->height != t->H)
+    return tr_fail(t, "hush_trainer_windows: the scene size differs from the trainer's");
+  if (t->W != t->h->W || t->H != t->h->H)
+    return tr_fail(t, "hush_trainer_windows: the denoiser was resized after the trainer was created");
+  if (t->is_lane) return tr_fail(t, "hush_trainer_windows: called on a helper lane");
+  cudaSetDevice(t->h->dev);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int n = n_windows < TRAIN_LANES ? n_windows : TRAIN_LANES;
+  if (n == 1) return windows_serial(t, sc, seeds, n_windows, 1, n_frames, lambda_t, st);
+  int rc = make_lanes(t, n);
+  if (rc != HUSH_OK) return rc;
+  cudaError_t e = cudaEventRecord(t->fork_ev, st);
+  for (int l = 0; l < n && e == cudaSuccess; l++) e = cudaStreamWaitEvent(t->lane_st[l], t->fork_ev, 0);
+  if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "forking the training lanes");
+  for (int l = 0; l < n && rc == HUSH_OK; l++) {
+    hush_trainer_t *lt = t->lane[l];
+    if (l > 0) {
+      hush_set_exposure(lt->h, t->h->exposure);
+      rc = windows_serial(lt, sc, seeds + l, n_windows - l, n, n_frames, lambda_t, t->lane_st[l]);
+      if (rc != HUSH_OK) rc = hush_fail(t->h, rc, std::string("training lane: ") + hush_last_error(lt->h));
+    } else {
+      rc = windows_serial(t, sc, seeds, n_windows, n, n_frames, lambda_t, t->lane_st[0]);
+    }
+  }
+  // join every lane that was forked, whatever happened above
+  for (int l = 0; l < n; l++) {
+    if (cudaEventRecord(t->lane_ev[l], t->lane_st[l]) == cudaSuccess) cudaStreamWaitEvent(st, t->lane_ev[l], 0);
+  }
+  if (rc != HUSH_OK) return rc;
+  LaneAcc la{};
+  la.n = n - 1;
+  for (int l = 1; l < n; l++) { la.grad[l - 1] = t->lane[l]->grad; la.loss[l - 1] = t->lane[l]->loss_acc; }
+  k_sum_lanes<<<(NW + 255) / 256, 256, 0, st>>>(t->grad, t->loss_acc, la);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, "summing the training lanes");
 }
 
 // ------------------------------------------------------------------------------------------------ per-pass pairs

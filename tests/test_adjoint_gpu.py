@@ -150,41 +150,34 @@ def test_accumulator_views_alias_the_device_gradient():
 
 
 def test_native_windows_match_the_per_frame_loop():
-    """hush_trainer_windows (generation and frames on the device, each window's frames replayed as a CUDA graph)
-    accumulates the same loss and gradient as the per-frame loop over the same generated windows. Three windows of
-    three frames: the first two capture a graph each (the frame parity alternates), the third replays the first."""
+    """hush_trainer_windows (generation and frames on the device, windows on concurrent lanes, each window's frames
+    replayed as a CUDA graph) accumulates the same loss and gradient as the per-frame loop over the same generated
+    windows. Batches of three windows of three frames: the first two batches capture each lane's graphs for both
+    frame parities, the third replays them; a one-window batch runs on the caller's stream."""
     from hush_b200.train import TrainConfig, window, window_scene
 
     cfg = TrainConfig(size=64, frames=3)
-    seeds = [11, 12, 13]
     theta = xavier_init(9)
     a = Trainer(Hush(0, {"width": 64, "height": 64, "schedule": "passes"}), theta)
-    a.zero_grad()
-    a.loss_sum()
-    a.windows(window_scene(cfg), seeds, cfg.frames, 0.5)
-    la, ga = a.loss_sum(), a.grad()
     b = Trainer(Hush(0, {"width": 64, "height": 64, "schedule": "passes"}), theta)
-    b.zero_grad()
-    b.loss_sum()
-    for s in seeds:
-        win = window(cfg, s)
-        b.reset()
-        for t, fr in enumerate(win):
-            b.frame(fr, fr["clean"], win[t - 1]["clean"] if t else None, 0.5, backward=True, sync=False)
-            b.end_frame()
-    lb, gb = b.loss_sum(), b.grad()
-    assert la == pytest.approx(lb, rel=1e-12)
-    assert np.abs(ga - gb).max() <= 1e-5 * np.abs(gb).max()
-    assert np.abs(gb).max() > 0
-    assert a.hush.frame == b.hush.frame == 9
-    # a second batch replays the cached graphs from the state the first left
-    a.windows(window_scene(cfg), [14], cfg.frames, 0.5)
-    b.zero_grad()
-    b.loss_sum()
-    win = window(cfg, 14)
-    b.reset()
-    for t, fr in enumerate(win):
-        b.frame(fr, fr["clean"], win[t - 1]["clean"] if t else None, 0.5, backward=True, sync=False)
-        b.end_frame()
-    a.zero_grad()  # compare losses only (a's gradient also holds the first batch)
-    assert a.loss_sum() == pytest.approx(b.loss_sum(), rel=1e-12)
+
+    def loop(seeds):
+        b.zero_grad()
+        b.loss_sum()
+        for s in seeds:
+            win = window(cfg, s)
+            b.reset()
+            for t, fr in enumerate(win):
+                b.frame(fr, fr["clean"], win[t - 1]["clean"] if t else None, 0.5, backward=True, sync=False)
+                b.end_frame()
+        return b.loss_sum(), b.grad()
+
+    for seeds in ([11, 12, 13], [14, 15, 16], [17, 18, 19], [20]):
+        a.zero_grad()
+        a.loss_sum()
+        a.windows(window_scene(cfg), seeds, cfg.frames, 0.5)
+        la, ga = a.loss_sum(), a.grad()
+        lb, gb = loop(seeds)
+        assert la == pytest.approx(lb, rel=1e-12), seeds
+        assert np.abs(ga - gb).max() <= 1e-5 * np.abs(gb).max(), seeds
+        assert np.abs(gb).max() > 0
