@@ -93,6 +93,8 @@ _SIGS = {
     "hush_timer_enable": (C.c_int, [_P, C.c_int]),
     "hush_timer_read": (C.c_int, [_P, C.POINTER(HushTiming), C.c_int]),
     "hush_set_graph": (C.c_int, [_P, C.c_int]),
+    "hush_kernel_status": (C.c_int, [_P, C.POINTER(C.c_uint)]),
+    "hush_selftest_wait": (C.c_int, [_P, C.c_uint32, _P]),
     "hush_last_error": (C.c_char_p, [_P]),
     "hush_global_error": (C.c_char_p, []),
     "hush_run_pass": (C.c_int, [_P, C.c_int, C.POINTER(HushInputs), _P]),
@@ -118,6 +120,7 @@ _SIGS = {
     "hush_train_step": (C.c_int, [_P, C.POINTER(HushInputs), C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_float,
                                   C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, _P, C.POINTER(C.c_double),
                                   C.POINTER(C.c_double)]),
+    "hush_trainer_set_mlp": (C.c_int, [_P, C.c_int]),
     "hush_trainer_windows": (C.c_int, [_P, C.POINTER(HushScene), C.POINTER(C.c_uint32), C.c_int, C.c_int,
                                        C.c_float, _P]),
     "hush_trainer_begin": (C.c_int, [_P, C.POINTER(HushInputs), C.c_void_p, C.c_void_p, C.c_float, _P]),

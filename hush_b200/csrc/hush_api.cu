@@ -10,6 +10,7 @@
 #include "hush.h"
 #include "hush_instance.h"
 #include "hush_internal.h"
+#include "umma.cuh"
 #include "weights_builtin.inc"  // generated at build time from hush_b200/data/hush-weights.bin
 
 using namespace hush;
@@ -554,6 +555,42 @@ extern "C" int hush_run_pass(hush_t *h, int pass, const hush_inputs *in, void *s
   cudaError_t e = launch_pass(pass, f, h->w16, (cudaStream_t)stream);
   if (e != cudaSuccess) return hush_cuda_fail(h, e, "kernel launch");
   return HUSH_OK;
+}
+
+// ------------------------------------------------------------------------------------------------ kernel status
+// The kernels' error word: bits are set where a bounded wait gave up (1: the tensor-core MLP of stage 0, 2: the
+// trainer's tensor-core MLP, 4: the wait self-test). Reading it synchronises the device.
+extern "C" int hush_kernel_status(hush_t *h, unsigned *word) {
+  if (!h) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_kernel_status: NULL instance");
+  cudaSetDevice(h->dev);
+  unsigned w = 0;
+  cudaError_t e = cudaMemcpy(&w, h->err, sizeof(w), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && w) e = cudaMemset(h->err, 0, sizeof(w));
+  if (e != cudaSuccess) return hush_cuda_fail(h, e, "reading the kernel error word");
+  if (word) *word = w;
+  if (w) {
+    char msg[96];
+    std::snprintf(msg, sizeof(msg), "Hush: a kernel's bounded wait gave up (error word 0x%x)", w);
+    return hush_fail(h, HUSH_ERR_KERNEL, msg);
+  }
+  return HUSH_OK;
+}
+
+// A wait that runs out: one thread waits on an mbarrier nothing arrives at, `polls` times, then sets bit 4 of the
+// error word and returns, as every bounded wait in the kernels does.
+__global__ void k_wait_selftest(unsigned *err, uint32_t polls) {
+  __shared__ alignas(8) uint64_t mbar;
+  const uint32_t a = umma::smem_u32(&mbar);
+  umma::mbar_init(a, 1);
+  if (!umma::mbar_wait_bounded(a, 0, polls)) atomicOr(err, 4u);
+}
+
+extern "C" int hush_selftest_wait(hush_t *h, uint32_t polls, void *stream) {
+  if (!h) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_selftest_wait: NULL instance");
+  cudaSetDevice(h->dev);
+  k_wait_selftest<<<1, 1, 0, (cudaStream_t)stream>>>(h->err, polls);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(h, e, "hush_selftest_wait");
 }
 
 extern "C" int hush_end_frame(hush_t *h) {

@@ -12,10 +12,12 @@
 // a-trous weight from the level's input instead of storing the weights, accumulates input gradients of the levels with
 // atomics, reduces the weight gradient per CTA in FP32 and across CTAs in FP64, and updates FP32 master weights with
 // Adam.
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -24,6 +26,7 @@
 #include "hush_device.cuh"
 #include "hush_instance.h"
 #include "hush_internal.h"
+#include "umma.cuh"
 
 namespace hush {
 namespace twin {
@@ -823,6 +826,263 @@ __global__ void __launch_bounds__(RP_THREADS) k_reduce_partials(const float *par
 }
 constexpr int RP_BLOCKS = (NW + RP_PARAMS - 1) / RP_PARAMS;
 
+// ------------------------------------------------------------------------------------------------ MLP on tensor cores
+// The twin's MLP as tcgen05 GEMM tiles on bf16 (or f16) operands with FP32 accumulation in TMEM: 128 rows per CTA
+// (one per thread), each layer one M = 128, N = 16 MMA (K = 32 / 16 / 16); the adjoint's delta products d2 = d3 W3
+// and d1 = d2 W2 the same way, and the CTA's whole weight gradient as one M = 128, N = 64, K = 128 product of the
+// deltas (rows m: d1 | d2 | d3) and the activations (rows n: features | h1 | h2 | 1, the last giving the biases) over
+// the CTA's rows. Operands are K-major without swizzle (8-row x 16-byte core matrices); one thread issues and commits,
+// everyone waits on the mbarrier with a bounded poll and reads its own TMEM lane (warp w: lanes 32 w ..). Bias, ReLU,
+// the heads and their adjoint stay FP32, as do the FP32 master weights the operands are rounded from.
+constexpr int TC_ROWS = 128;
+constexpr uint32_t TC_POLLS = 1u << 22;
+struct TcTrainSmem {
+  alignas(8) uint64_t mbar;
+  uint32_t tmem;
+  float bias[44];                                  // b1 | b2 | b3
+  alignas(128) uint8_t x[TC_ROWS * 32 * 2];        // layer 1 A: rows x 32 (20 features, zero padded), kcore 4
+  alignas(128) uint8_t h[TC_ROWS * 16 * 2];        // layer 2 / 3 and delta-product A: rows x 16, kcore 2
+  alignas(128) uint8_t w1[16 * 32 * 2];            // B: W1 (n = output, k = input), kcore 4
+  alignas(128) uint8_t w2[16 * 16 * 2];            // B: W2
+  alignas(128) uint8_t w3[16 * 16 * 2];            // B: W3 (outputs 12..15 zero)
+  alignas(128) uint8_t w3t[16 * 16 * 2];           // B of d2 = d3 W3: W3^T (k = 12..15 zero)
+  alignas(128) uint8_t w2t[16 * 16 * 2];           // B of d1 = d2 W2: W2^T
+  alignas(128) uint8_t ag[128 * TC_ROWS * 2];      // weight-gradient A: deltas (m) x rows (k), kcore 16
+  alignas(128) uint8_t bg[64 * TC_ROWS * 2];       // weight-gradient B: activations (n) x rows (k), kcore 16
+};
+constexpr size_t TC_SMEM_FWD = offsetof(TcTrainSmem, ag) + 128, TC_SMEM_BWD = sizeof(TcTrainSmem) + 128;
+
+template <bool BF16>
+HD_INL uint16_t tc_op(float v) {
+  if constexpr (BF16) return __bfloat16_as_ushort(__float2bfloat16_rn(v));
+  else return __half_as_ushort(__float2half_rn(v));
+}
+template <bool BF16>
+HD_INL uint4 tc_pack8(const float *v) {
+  uint4 q;
+  q.x = (uint32_t)tc_op<BF16>(v[0]) | ((uint32_t)tc_op<BF16>(v[1]) << 16);
+  q.y = (uint32_t)tc_op<BF16>(v[2]) | ((uint32_t)tc_op<BF16>(v[3]) << 16);
+  q.z = (uint32_t)tc_op<BF16>(v[4]) | ((uint32_t)tc_op<BF16>(v[5]) << 16);
+  q.w = (uint32_t)tc_op<BF16>(v[6]) | ((uint32_t)tc_op<BF16>(v[7]) << 16);
+  return q;
+}
+HD_INL TcTrainSmem &tc_smem(unsigned char *raw) {  // 128-byte aligned view of the dynamic shared memory
+  return *reinterpret_cast<TcTrainSmem *>((reinterpret_cast<uintptr_t>(raw) + 127) & ~(uintptr_t)127);
+}
+template <bool BF16>
+HD_INL void tc_put(uint8_t *base, int row, int k, int kcore, float v) {
+  *reinterpret_cast<uint16_t *>(base + umma::kmajor_off(row, k, kcore)) = tc_op<BF16>(v);
+}
+
+// Set-up shared by both kernels: TMEM (ncols), the mbarrier, the weight operands and FP32 biases from theta.
+template <bool BF16>
+__device__ void tc_setup(TcTrainSmem &S, const float *theta, uint32_t ncols) {
+  const int li = threadIdx.x;
+  if (li < 32) {
+    umma::tmem_alloc(umma::smem_u32(&S.tmem), ncols);
+    umma::tmem_relinquish();
+  }
+  if (li == 0) umma::mbar_init(umma::smem_u32(&S.mbar), 1);
+  for (int e = li; e < 16 * 32; e += TC_ROWS) {
+    const int n = e / 32, k = e % 32;
+    tc_put<BF16>(S.w1, n, k, 4, k < 20 ? theta[W1o + n * 20 + k] : 0.0f);
+  }
+  for (int e = li; e < 16 * 16; e += TC_ROWS) {
+    const int n = e / 16, k = e % 16;
+    tc_put<BF16>(S.w2, n, k, 2, theta[W2o + n * 16 + k]);
+    tc_put<BF16>(S.w3, n, k, 2, n < 12 ? theta[W3o + n * 16 + k] : 0.0f);
+    tc_put<BF16>(S.w3t, n, k, 2, k < 12 ? theta[W3o + k * 16 + n] : 0.0f);
+    tc_put<BF16>(S.w2t, n, k, 2, theta[W2o + k * 16 + n]);
+  }
+  if (li < 16) { S.bias[li] = theta[B1o + li]; S.bias[16 + li] = theta[B2o + li]; }
+  if (li < 12) S.bias[32 + li] = theta[B3o + li];
+}
+
+// One product D[row][n] = sum_k A[row][k] B[n][k] into TMEM columns [0, N); waits (bounded) and loads this thread's
+// first 16 columns into d. Returns false if the wait gave up.
+HD_INL bool tc_product(TcTrainSmem &S, const uint8_t *a, int kcore_a, const uint8_t *b, int kcore_b, int kblocks,
+                       uint32_t idesc, uint32_t &phase, float *d) {
+  umma::fence_proxy_async();
+  umma::fence_before_sync();
+  __syncthreads();
+  const uint32_t mbar = umma::smem_u32(&S.mbar);
+  if (threadIdx.x == 0) {
+    umma::fence_after_sync();
+    const uint32_t a0 = umma::smem_u32(a), b0 = umma::smem_u32(b);
+    for (int kb = 0; kb < kblocks; kb++)
+      umma::mma_f16(S.tmem, umma::sdesc(a0 + 256u * kb, 128, 128 * kcore_a),
+                    umma::sdesc(b0 + 256u * kb, 128, 128 * kcore_b), idesc, kb > 0 ? 1u : 0u);
+    umma::commit(mbar);
+  }
+  const bool ok = umma::mbar_wait_bounded(mbar, phase, TC_POLLS);
+  phase ^= 1u;
+  umma::fence_after_sync();
+  if (d) umma::ld16(S.tmem + ((uint32_t)(32 * (threadIdx.x >> 5)) << 16), d);
+  return ok;
+}
+
+// The three layers for this thread's row: fe (zeros for a dead row) -> h1, h2 (post-ReLU, FP32) and out (FP32).
+template <bool BF16>
+__device__ bool tc_forward(TcTrainSmem &S, const float *fe, float *h1, float *h2, float *out, uint32_t &phase) {
+  constexpr uint32_t ID = umma::idesc_f16(BF16 ? 1 : 0, 128, 16);
+  const int li = threadIdx.x;
+  float v[8];
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+#pragma unroll
+    for (int e = 0; e < 8; e++) v[e] = 8 * c + e < 20 ? fe[8 * c + e] : 0.0f;
+    *reinterpret_cast<uint4 *>(S.x + umma::kmajor_off(li, 8 * c, 4)) = tc_pack8<BF16>(v);
+  }
+  float d[16];
+  bool ok = tc_product(S, S.x, 4, S.w1, 4, 2, ID, phase, d);
+#pragma unroll
+  for (int j = 0; j < 16; j++) h1[j] = fmaxf(d[j] + S.bias[j], 0.0f);
+  *reinterpret_cast<uint4 *>(S.h + umma::kmajor_off(li, 0, 2)) = tc_pack8<BF16>(h1);
+  *reinterpret_cast<uint4 *>(S.h + umma::kmajor_off(li, 8, 2)) = tc_pack8<BF16>(h1 + 8);
+  ok &= tc_product(S, S.h, 2, S.w2, 2, 1, ID, phase, d);
+#pragma unroll
+  for (int j = 0; j < 16; j++) h2[j] = fmaxf(d[j] + S.bias[16 + j], 0.0f);
+  *reinterpret_cast<uint4 *>(S.h + umma::kmajor_off(li, 0, 2)) = tc_pack8<BF16>(h2);
+  *reinterpret_cast<uint4 *>(S.h + umma::kmajor_off(li, 8, 2)) = tc_pack8<BF16>(h2 + 8);
+  ok &= tc_product(S, S.h, 2, S.w3, 2, 1, ID, phase, d);
+#pragma unroll
+  for (int j = 0; j < 12; j++) out[j] = d[j] + S.bias[32 + j];
+  return ok;
+}
+
+HD_INL void tc_release(TcTrainSmem &S, uint32_t ncols) {
+  umma::fence_before_sync();
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(S.tmem, ncols);
+  }
+}
+
+template <bool BF16>
+__global__ void __launch_bounds__(TC_ROWS) k_mlp_fwd_tc(const TwinFrame T) {
+  extern __shared__ unsigned char tc_raw[];
+  TcTrainSmem &S = tc_smem(tc_raw);
+  tc_setup<BF16>(S, T.theta, 32);
+  const HushFrame &f = T.f;
+  const int o = blockIdx.x * TC_ROWS + threadIdx.x;
+  const bool in = o < f.W2 * f.H2;
+  const bool live = in && f3_guide_tw(f.F3, o).w >= 0.0f;
+  float fe[20], h1[16], h2[16], out[12];
+  if (live) load_features(f, o, fe);
+  else
+#pragma unroll
+    for (int i = 0; i < 20; i++) fe[i] = 0.0f;
+  uint32_t phase = 0;
+  const bool ok = tc_forward<BF16>(S, fe, h1, h2, out, phase);
+  tc_release(S, 32);
+  if (!ok) atomicOr(f.err, 2u);
+  if (!in) return;
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (T.zero_adj) { T.dpar[3 * o] = z4; T.dpar[3 * o + 1] = z4; T.dpar[3 * o + 2] = z4; }
+  if (!live) {
+    T.par[3 * o] = z4; T.par[3 * o + 1] = z4; T.par[3 * o + 2] = z4;
+    sth(f.par0, o, z4); sth(f.par1, o, z4); sth(f.par2, o, z4);
+    return;
+  }
+  float4 p0, p1, p2;
+  mlp_heads(out, p0, p1, p2);
+  T.par[3 * o] = p0; T.par[3 * o + 1] = p1; T.par[3 * o + 2] = p2;
+  sth(f.par0, o, p0); sth(f.par1, o, p1); sth(f.par2, o, p2);
+}
+
+template <bool BF16>
+__global__ void __launch_bounds__(TC_ROWS) k_mlp_bwd_tc(const TwinFrame T) {
+  extern __shared__ unsigned char tc_raw[];
+  TcTrainSmem &S = tc_smem(tc_raw);
+  tc_setup<BF16>(S, T.theta, 64);
+  const HushFrame &f = T.f;
+  const int li = threadIdx.x;
+  const int o = blockIdx.x * TC_ROWS + li;
+  const bool live = o < f.W2 * f.H2 && f3_guide_tw(f.F3, o).w >= 0.0f;
+  float fe[20], h1[16], h2[16], out[12];
+  if (live) load_features(f, o, fe);
+  else
+#pragma unroll
+    for (int i = 0; i < 20; i++) fe[i] = 0.0f;
+  uint32_t phase = 0;
+  bool ok = tc_forward<BF16>(S, fe, h1, h2, out, phase);
+  // heads adjoint (hush.js:357-362), FP32; dead rows carry zero deltas
+  float d3[16];
+#pragma unroll
+  for (int j = 0; j < 16; j++) d3[j] = 0.0f;
+  if (live) {
+    const float4 q0 = T.dpar[3 * o], q1 = T.dpar[3 * o + 1], q2 = T.dpar[3 * o + 2];
+    const float4 p0 = T.par[3 * o], p1 = T.par[3 * o + 1], p2 = T.par[3 * o + 2];
+    const float sa = sigmoidf_(out[0]), sg = sigmoidf_(out[1]);
+    d3[0] = q0.x * (31.0f / 32.0f) * sa * (1.0f - sa);
+    d3[1] = q0.y * 7.5f * sg * (1.0f - sg);
+    d3[2] = q0.z * p0.z * (1.0f - p0.z);
+    d3[3] = q0.w * p0.w * (1.0f - p0.w);
+    const float ps[4] = {p1.x, p1.y, p1.z, p1.w}, pc[4] = {p2.x, p2.y, p2.z, p2.w};
+    const float gs[4] = {q1.x, q1.y, q1.z, q1.w}, gc[4] = {q2.x, q2.y, q2.z, q2.w};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      d3[4 + k] = fabsf(out[4 + k]) < 5.0f ? gs[k] * ps[k] : 0.0f;
+      d3[8 + k] = fabsf(out[8 + k]) < 4.0f ? gc[k] * pc[k] : 0.0f;
+    }
+  }
+  // d2 = relu'(h2) (d3 W3), d1 = relu'(h1) (d2 W2)
+  constexpr uint32_t ID = umma::idesc_f16(BF16 ? 1 : 0, 128, 16);
+  *reinterpret_cast<uint4 *>(S.h + umma::kmajor_off(li, 0, 2)) = tc_pack8<BF16>(d3);
+  *reinterpret_cast<uint4 *>(S.h + umma::kmajor_off(li, 8, 2)) = tc_pack8<BF16>(d3 + 8);
+  float d[16], d2[16], d1[16];
+  ok &= tc_product(S, S.h, 2, S.w3t, 2, 1, ID, phase, d);
+#pragma unroll
+  for (int i = 0; i < 16; i++) d2[i] = h2[i] > 0.0f ? d[i] : 0.0f;
+  *reinterpret_cast<uint4 *>(S.h + umma::kmajor_off(li, 0, 2)) = tc_pack8<BF16>(d2);
+  *reinterpret_cast<uint4 *>(S.h + umma::kmajor_off(li, 8, 2)) = tc_pack8<BF16>(d2 + 8);
+  ok &= tc_product(S, S.h, 2, S.w2t, 2, 1, ID, phase, d);
+#pragma unroll
+  for (int i = 0; i < 16; i++) d1[i] = h1[i] > 0.0f ? d[i] : 0.0f;
+  // the weight-gradient operands: column k = this row
+#pragma unroll
+  for (int m = 0; m < 16; m++) {
+    tc_put<BF16>(S.ag, m, li, 16, d1[m]);
+    tc_put<BF16>(S.ag, 16 + m, li, 16, d2[m]);
+  }
+#pragma unroll
+  for (int m = 0; m < 12; m++) tc_put<BF16>(S.ag, 32 + m, li, 16, d3[m]);
+#pragma unroll
+  for (int n = 0; n < 20; n++) tc_put<BF16>(S.bg, n, li, 16, fe[n]);
+#pragma unroll
+  for (int n = 0; n < 16; n++) {
+    tc_put<BF16>(S.bg, 20 + n, li, 16, h1[n]);
+    tc_put<BF16>(S.bg, 36 + n, li, 16, h2[n]);
+  }
+  tc_put<BF16>(S.bg, 52, li, 16, 1.0f);
+  // G[m][n] = sum over rows: rows m >= 44 of A and n >= 53 of B are never written; they only reach entries of G
+  // that are not read
+  ok &= tc_product(S, S.ag, 16, S.bg, 16, TC_ROWS / 16, umma::idesc_f16(BF16 ? 1 : 0, 128, 64), phase, nullptr);
+  float *part = T.partials + (size_t)blockIdx.x * NW;
+  if (li < 64) {  // warps 0 and 1 hold lanes (delta rows m) 0..63
+    float g[64];
+    const uint32_t ta = S.tmem + ((uint32_t)(32 * (li >> 5)) << 16);
+    umma::ld16(ta, g);
+    umma::ld16(ta + 16, g + 16);
+    umma::ld16(ta + 32, g + 32);
+    umma::ld16(ta + 48, g + 48);
+    const int m = li;
+    if (m < 16) {
+      for (int i = 0; i < 20; i++) part[W1o + m * 20 + i] = g[i];
+      part[B1o + m] = g[52];
+    } else if (m < 32) {
+      for (int i = 0; i < 16; i++) part[W2o + (m - 16) * 16 + i] = g[20 + i];
+      part[B2o + m - 16] = g[52];
+    } else if (m < 44) {
+      for (int i = 0; i < 16; i++) part[W3o + (m - 32) * 16 + i] = g[36 + i];
+      part[B3o + m - 32] = g[52];
+    }
+  }
+  tc_release(S, 64);
+  if (!ok) atomicOr(f.err, 2u);
+}
+
 // Adam on the FP32 master weights (gradient in FP64, optionally clipped by global norm scale `scale`).
 __global__ void k_adam(float *theta, float *m, float *v, const double *grad, float lr, float b1, float b2, float eps,
                        float bc1, float bc2, float scale) {
@@ -859,8 +1119,9 @@ struct hush_trainer_s {
   int win_frames = 0;
   // hush_trainer_windows replays a window's training frames as a CUDA graph, one per (frame parity, output slot) at
   // the window's start; captured for one (frame count, lambda, exposure) and re-captured when those change
+  int mlp_mode = HUSH_MLP_FP32;  // the twin's MLP: FP32 per thread, or bf16 / f16 tensor-core tiles
   cudaGraphExec_t win_graph[4] = {};
-  int wg_frames = 0;
+  int wg_frames = 0, wg_mode = -1;
   float wg_lambda = 0.f, wg_exposure = 0.f;
   cudaStream_t cap = nullptr;
   // hush_trainer_windows runs windows concurrently on lanes: lane 0 is this trainer, lanes 1.. are helper trainers on
@@ -907,6 +1168,8 @@ extern "C" int hush_trainer_create(hush_t *h, const float *theta, hush_trainer_t
   e = cudaMemcpy(t->theta, theta ? theta : h->wf.data(), NW * 4, theta ? cudaMemcpyHostToDevice : cudaMemcpyHostToDevice);
   if (e != cudaSuccess) { cudaFree(t->pool); delete t; return hush_cuda_fail(h, e, "cudaMemcpy of the weights"); }
   cudaFuncSetAttribute(k_mlp_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MB_SMEM);
+  cudaFuncSetAttribute(k_mlp_bwd_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_BWD);
+  cudaFuncSetAttribute(k_mlp_bwd_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_BWD);
   *out = t;
   return HUSH_OK;
 }
@@ -929,6 +1192,20 @@ extern "C" void hush_trainer_destroy(hush_trainer_t *t) {
   cudaFree(t->pool);
   cudaFree(t->win_pool);
   delete t;
+}
+
+// The twin's MLP forward / adjoint (the adjoint includes the FP64 reduction into the gradient) in the trainer's form.
+static void launch_mlp_fwd(const hush_trainer_t *t, const TwinFrame &T, cudaStream_t st) {
+  const int half = T.f.W2 * T.f.H2;
+  if (t->mlp_mode == HUSH_MLP_BF16) k_mlp_fwd_tc<true><<<(half + TC_ROWS - 1) / TC_ROWS, TC_ROWS, TC_SMEM_FWD, st>>>(T);
+  else if (t->mlp_mode == HUSH_MLP_F16) k_mlp_fwd_tc<false><<<(half + TC_ROWS - 1) / TC_ROWS, TC_ROWS, TC_SMEM_FWD, st>>>(T);
+  else k_mlp_fwd<<<(half + 127) / 128, 128, 0, st>>>(T);
+}
+static void launch_mlp_bwd(const hush_trainer_t *t, const TwinFrame &T, cudaStream_t st) {
+  if (t->mlp_mode == HUSH_MLP_BF16) k_mlp_bwd_tc<true><<<t->n_mlp_ctas, TC_ROWS, TC_SMEM_BWD, st>>>(T);
+  else if (t->mlp_mode == HUSH_MLP_F16) k_mlp_bwd_tc<false><<<t->n_mlp_ctas, TC_ROWS, TC_SMEM_BWD, st>>>(T);
+  else k_mlp_bwd<<<t->n_mlp_ctas, MB_ROWS, MB_SMEM, st>>>(T);
+  k_reduce_partials<<<RP_BLOCKS, RP_THREADS, 0, st>>>(t->partials, t->n_mlp_ctas, t->grad);
 }
 
 static TwinFrame make_twin(hush_trainer_t *t, const hush_inputs *in, const float *clean, const float *clean_prev,
@@ -979,7 +1256,7 @@ extern "C" int hush_trainer_frame(hush_trainer_t *t, const hush_inputs *in, cons
   if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "trainer pass launch");
   const int half = f.W2 * f.H2, full = f.W * f.H;
   const dim3 blk(TW, TH), gh((f.W2 + TW - 1) / TW, (f.H2 + TH - 1) / TH), gf((f.W + TW - 1) / TW, (f.H + TH - 1) / TH);
-  k_mlp_fwd<<<(half + 127) / 128, 128, 0, st>>>(T);
+  launch_mlp_fwd(t, T, st);
   k_mid_fwd<1><<<gh, blk, 0, st>>>(T);
   k_mid_fwd<2><<<gh, blk, 0, st>>>(T);
   k_mid_fwd<3><<<gh, blk, 0, st>>>(T);
@@ -993,8 +1270,7 @@ extern "C" int hush_trainer_frame(hush_trainer_t *t, const hush_inputs *in, cons
     k_mid_bwd<3><<<gh, blk, 0, st>>>(T);
     k_mid_bwd<2><<<gh, blk, 0, st>>>(T);
     k_mid_bwd<1><<<gh, blk, 0, st>>>(T);
-    k_mlp_bwd<<<t->n_mlp_ctas, MB_ROWS, MB_SMEM, st>>>(T);
-    k_reduce_partials<<<RP_BLOCKS, RP_THREADS, 0, st>>>(t->partials, t->n_mlp_ctas, t->grad);
+    launch_mlp_bwd(t, T, st);
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "trainer kernel launch");
@@ -1160,11 +1436,13 @@ static int windows_serial(hush_trainer_t *t, const hush_scene *sc, const uint32_
     if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "cudaMalloc of the window buffers");
     t->win_frames = n_frames;
   }
-  if (t->wg_frames != n_frames || t->wg_lambda != lambda_t || t->wg_exposure != t->h->exposure) {
+  if (t->wg_frames != n_frames || t->wg_lambda != lambda_t || t->wg_exposure != t->h->exposure ||
+      t->wg_mode != t->mlp_mode) {
     drop_window_graphs(t);
     t->wg_frames = n_frames;
     t->wg_lambda = lambda_t;
     t->wg_exposure = t->h->exposure;
+    t->wg_mode = t->mlp_mode;
   }
   if (!t->cap) {
     cudaError_t e = cudaStreamCreateWithFlags(&t->cap, cudaStreamNonBlocking);
@@ -1287,6 +1565,7 @@ extern "C" int hush_trainer_windows(hush_trainer_t *t, const hush_scene *sc, con
     hush_trainer_t *lt = t->lane[l];
     if (l > 0) {
       hush_set_exposure(lt->h, t->h->exposure);
+      lt->mlp_mode = t->mlp_mode;
       rc = windows_serial(lt, sc, seeds + l, n_windows - l, n, n_frames, lambda_t, t->lane_st[l]);
       if (rc != HUSH_OK) rc = hush_fail(t->h, rc, std::string("training lane: ") + hush_last_error(lt->h));
     } else {
@@ -1304,6 +1583,14 @@ extern "C" int hush_trainer_windows(hush_trainer_t *t, const hush_scene *sc, con
   k_sum_lanes<<<(NW + 255) / 256, 256, 0, st>>>(t->grad, t->loss_acc, la);
   e = cudaGetLastError();
   return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, "summing the training lanes");
+}
+
+extern "C" int hush_trainer_set_mlp(hush_trainer_t *t, int mode) {
+  if (!t) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_trainer_set_mlp: NULL trainer");
+  if (mode != HUSH_MLP_FP32 && mode != HUSH_MLP_BF16 && mode != HUSH_MLP_F16)
+    return tr_fail(t, "hush_trainer_set_mlp: unknown MLP form");
+  t->mlp_mode = mode;
+  return HUSH_OK;
 }
 
 // ------------------------------------------------------------------------------------------------ per-pass pairs
@@ -1355,12 +1642,8 @@ static int run_twin_pass(hush_trainer_t *t, int pass, int backward, void *stream
   cudaError_t e = cudaSuccess;
   switch (pass) {
     case HUSH_TWIN_MLP:
-      if (!backward) {
-        k_mlp_fwd<<<(half + 127) / 128, 128, 0, st>>>(T);
-      } else {
-        k_mlp_bwd<<<t->n_mlp_ctas, MB_ROWS, MB_SMEM, st>>>(T);
-        k_reduce_partials<<<RP_BLOCKS, RP_THREADS, 0, st>>>(t->partials, t->n_mlp_ctas, t->grad);
-      }
+      if (!backward) launch_mlp_fwd(t, T, st);
+      else launch_mlp_bwd(t, T, st);
       break;
     case HUSH_TWIN_MID1:
       if (backward) k_mid_bwd<1><<<gh, blk, 0, st>>>(T); else k_mid_fwd<1><<<gh, blk, 0, st>>>(T);

@@ -256,6 +256,13 @@ class Hush:
         """Drops the temporal history (hush.js:801)."""
         _check(L.lib().hush_reset(self._h), self._h)
 
+    def kernel_status(self) -> int:
+        """The kernels' error word (a bounded wait that gave up sets a bit; synchronises, then clears it): raises
+        HushError if any bit was set."""
+        w = C.c_uint()
+        _check(L.lib().hush_kernel_status(self._h, C.byref(w)), self._h)
+        return w.value
+
     def set_weights(self, weights):
         self._wbuf = np.ascontiguousarray(decode_weights(weights))
         _check(L.lib().hush_set_weights(self._h, self._wbuf.ctypes.data_as(C.POINTER(C.c_uint16)),

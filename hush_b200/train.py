@@ -66,6 +66,11 @@ class Trainer:
                                                C.c_void_p(_stream_handle(stream)), C.byref(loss) if sync else None))
         return loss.value if sync else None
 
+    def set_mlp(self, mlp: str):
+        """The twin's MLP arithmetic: "fp32" (per-thread FP32) or "bf16" / "f16" (tensor-core GEMM tiles)."""
+        self._check(L.lib().hush_trainer_set_mlp(self._t, {"fp32": L.MLP_FP32, "bf16": L.MLP_BF16,
+                                                           "f16": L.MLP_F16}[mlp]))
+
     def windows(self, scene_cfg: SceneConfig, seeds, n_frames: int, lambda_t: float = 0.0, stream=None):
         """hush_trainer_windows: for each seed, the n_frames frames of scene_cfg with that seed generated on the
         device and run forward + backward (history reset per window); gradient and loss accumulate, no step."""
@@ -213,6 +218,7 @@ class TrainConfig:
     lambda_t: float = 0.5
     clip: float = 1.0
     init_seed: int = 0
+    mlp: str = "fp32"  # the twin's MLP: "fp32", or "bf16" / "f16" tensor-core tiles
 
 
 def window_scene(cfg: TrainConfig, seed: int = 0) -> SceneConfig:
@@ -239,6 +245,7 @@ def train(cfg: TrainConfig, log_every: int = 100, on_log=None, time_budget_s: fl
     dp = dp or DataParallel()
     hush = Hush(device, {"width": cfg.size, "height": cfg.size, "schedule": "passes"})
     tr = Trainer(hush, xavier_init(cfg.init_seed))
+    tr.set_mlp(cfg.mlp)
     if dp.world > 1:  # every rank starts from rank 0's weights
         th = torch.from_numpy(tr.theta).cuda(device)
         dp.broadcast_(th)
@@ -324,6 +331,7 @@ def main(argv=None):
     ap.add_argument("--frames", type=int, default=8)
     ap.add_argument("--seeds", type=int, default=2048)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--mlp", default="fp32", choices=["fp32", "bf16", "f16"], help="the twin's MLP arithmetic")
     ap.add_argument("--time-budget", type=float, default=None, help="stop after this many seconds of training")
     ap.add_argument("--eval-seeds", type=int, default=64)
     ap.add_argument("--out", default=None, help="write the summary JSON here")
@@ -335,7 +343,7 @@ def main(argv=None):
     if world > 1:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dp = DataParallel()
-    cfg = TrainConfig(size=a.size, frames=a.frames, seeds=a.seeds, batch=a.batch, steps=a.steps, lr=a.lr)
+    cfg = TrainConfig(size=a.size, frames=a.frames, seeds=a.seeds, batch=a.batch, steps=a.steps, lr=a.lr, mlp=a.mlp)
     log = []
 
     def on_log(rec):

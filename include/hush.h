@@ -114,6 +114,14 @@ int hush_timer_read(hush_t *h, hush_timing *out, int max);
 /* CUDA-graph replay of whole frames (config-5 style): capture the frame once per input-pointer set and replay it. */
 int hush_set_graph(hush_t *h, int enable);
 
+/* The kernels' error word: a bounded wait that gave up (tensor-core MLP of stage 0: bit 0; the trainer's tensor-core
+ * MLP: bit 1; hush_selftest_wait: bit 2) sets a bit instead of hanging. Reads the word into *word (may be NULL),
+ * synchronising the device, clears it, and returns HUSH_ERR_KERNEL with a message if any bit was set. */
+int hush_kernel_status(hush_t *h, unsigned *word);
+/* Enqueues one thread that waits `polls` times on a barrier nothing arrives at and then sets bit 2 of the error
+ * word: the failure path of every bounded wait, exercised without a fault. No counterpart in the reference. */
+int hush_selftest_wait(hush_t *h, uint32_t polls, void *stream);
+
 /* Last error message of the instance / of the calling thread (for hush_create failures). */
 const char *hush_last_error(const hush_t *h);
 const char *hush_global_error(void);
@@ -176,6 +184,12 @@ int hush_trainer_step(hush_trainer_t *t, float lr, float beta1, float beta2, flo
                       double *grad_norm);
 /* Round the master weights to the f16 blob, install it in the denoiser and copy it to blob (if not NULL). */
 int hush_trainer_export(hush_trainer_t *t, uint16_t *blob);
+/* Arithmetic of the twin's MLP forward and adjoint: HUSH_MLP_FP32 (default; per-thread FP32, the form the gradient
+ * checks hold to 1e-3) or HUSH_MLP_BF16 / HUSH_MLP_F16: tcgen05 GEMM tiles on bf16 / f16 operands with FP32
+ * accumulation (the three layers, the delta products and the weight gradient as one 128 x 64 x 128 product per CTA),
+ * FP32 master weights, bias / ReLU / heads in FP32. A bounded wait that gives up sets bit 1 of the instance's kernel
+ * error word. */
+int hush_trainer_set_mlp(hush_trainer_t *t, int mode);
 
 /* One optimiser step over a batch, as a one-GPU training loop runs it: for each of n_windows windows of n_frames
  * frames (frames[] and cleans[] window-major; cleans[] holds device pointers to dense f32 rgb images) a history

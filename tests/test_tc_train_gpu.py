@@ -1,0 +1,104 @@
+"""The trainer's tensor-core MLP forms (bf16 / f16 GEMM tiles with FP32 accumulation) against its FP32 form on a
+B200, through the per-pass C ABI and the fused frame; and the bounded-wait failure path through the kernel error
+word (a wait on a barrier nothing arrives at, no fault)."""
+import numpy as np
+import pytest
+
+import oracle
+from hush_b200 import Hush, HushError, scene
+from hush_b200 import _lib as L
+from hush_b200.train import Trainer, xavier_init
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _dev(f):
+    return {k: torch.from_numpy(np.ascontiguousarray(f[k])).cuda() for k in oracle.INPUTS}
+
+
+def _frame_state(W=96, H=64, seed=7):
+    cfg = scene.SceneConfig(W, H, 3, n_moving=2, pan_min=1.0, pan_max=3.0, seed=seed)
+    host = [scene.frame_host(cfg, i, clean=True) for i in range(3)]
+    g = Hush(0, {"width": W, "height": H, "schedule": "passes"})
+    tr = Trainer(g, xavier_init(seed))
+    cleans = [torch.from_numpy(h["clean"]).cuda() for h in host]
+    for t in range(2):
+        tr.frame(_dev(host[t]), cleans[t], cleans[t - 1] if t else None, 0.5, backward=False)
+        tr.end_frame()
+    return g, tr, _dev(host[2]), cleans
+
+
+@pytest.mark.parametrize("mlp,tol", [("f16", 5e-3), ("bf16", 3e-2)])
+def test_tensor_core_mlp_pass_matches_fp32(mlp, tol):
+    g, tr, inp, cleans = _frame_state()
+    tr.begin(inp, cleans[2], cleans[1], 0.5)
+    tr.fwd("mlp")
+    torch.cuda.synchronize()
+    par32 = tr.buffer("PAR").clone()
+    seed = torch.randn(par32.shape, generator=torch.Generator().manual_seed(1)).cuda()
+    tr.zero_adjoints()
+    tr.zero_grad()
+    tr.buffer("DPAR").copy_(seed)
+    tr.bwd("mlp")
+    g32 = tr.grad()
+    tr.set_mlp(mlp)
+    tr.fwd("mlp")
+    torch.cuda.synchronize()
+    par_tc = tr.buffer("PAR").clone()
+    # parameters: relative to each value (the heads keep them away from 0 except on sky rows, which are 0 in both)
+    rel = ((par_tc - par32).abs() / (par32.abs() + 1e-3)).cpu().numpy()
+    assert rel.mean() < tol / 5 and np.quantile(rel, 0.999) < tol * 5, (mlp, rel.mean(), rel.max())
+    # the adjoint from the FP32 parameters' seed: same DPAR, PAR restored to the FP32 values so both see one input
+    tr.buffer("PAR").copy_(par32)
+    tr.zero_grad()
+    tr.buffer("DPAR").copy_(seed)
+    tr.bwd("mlp")
+    gtc = tr.grad()
+    scale = np.abs(g32).max()
+    err = np.abs(gtc - g32)
+    assert err.max() <= tol * scale, (mlp, err.max() / scale)
+    cos = float(gtc @ g32 / (np.linalg.norm(gtc) * np.linalg.norm(g32)))
+    assert cos > 1 - tol, (mlp, cos)
+    assert g.kernel_status() == 0
+
+
+def test_bf16_frame_gradient_tracks_fp32():
+    g, tr, inp, cleans = _frame_state(seed=8)
+    tr.zero_grad()
+    l32 = tr.frame(inp, cleans[2], cleans[1], 0.5, backward=True)
+    g32 = tr.grad()
+    tr.set_mlp("bf16")
+    tr.zero_grad()
+    lbf = tr.frame(inp, cleans[2], cleans[1], 0.5, backward=True)
+    gbf = tr.grad()
+    assert abs(lbf - l32) <= 1e-2 * abs(l32)
+    cos = float(gbf @ g32 / (np.linalg.norm(gbf) * np.linalg.norm(g32)))
+    assert cos > 0.99, cos
+    assert np.abs(gbf - g32).max() <= 0.1 * np.abs(g32).max()
+    assert g.kernel_status() == 0
+
+
+def test_bf16_training_reduces_the_loss():
+    from hush_b200.train import TrainConfig, train
+
+    cfg = TrainConfig(size=64, frames=4, seeds=8, batch=4, steps=60, lr=1e-3, lambda_t=0.25, mlp="bf16")
+    tr, hush, hist = train(cfg)
+    first = np.mean([h["loss"] for h in hist[:10]])
+    last = np.mean([h["loss"] for h in hist[-10:]])
+    assert np.isfinite(last) and last < first, (first, last)
+    assert hush.kernel_status() == 0
+
+
+def test_a_wait_that_runs_out_is_reported_not_hung():
+    g = Hush(0, {"width": 32, "height": 32})
+    assert g.kernel_status() == 0
+    assert L.lib().hush_selftest_wait(g._h, 1000, None) == L.HUSH_OK
+    with pytest.raises(HushError, match="bounded wait gave up"):
+        g.kernel_status()
+    assert g.kernel_status() == 0  # cleared by the read
+    # the context stays usable
+    cfg = scene.SceneConfig(32, 32, 1, seed=2)
+    out = g.denoise(_dev(scene.frame_host(cfg, 0)))
+    torch.cuda.synchronize()
+    assert torch.isfinite(out.float()).all()
