@@ -317,7 +317,10 @@ def run_ours(args):
     hush_alt.destroy()
 
     # ---- one training step of the parameter MLP (data-parallel over the ranks when N > 1)
-    train_ms = None if args.no_train else _train_step_ms(local, stream, barrier, max_over_ranks)
+    train_ms = None
+    if not args.no_train:  # the BF16 tensor-core form (the training configuration's), the FP32 form beside it
+        train_ms = _train_step_ms(local, stream, barrier, max_over_ranks, mlp="bf16")
+        train_ms["fp32_step_ms"] = _train_step_ms(local, stream, barrier, max_over_ranks, mlp="fp32")["step_ms"]
 
     if rank != 0:
         hush.destroy()
@@ -384,19 +387,21 @@ def run_ours(args):
     return 0
 
 
-def _train_step_ms(local, stream, barrier, max_over_ranks, warmup=2, steps=5):
+def _train_step_ms(local, stream, barrier, max_over_ranks, warmup=2, steps=5, mlp="bf16"):
     """Device time of one training step: 16 windows x 8 frames of 384x384 generated on the device, the twin's
-    forward + adjoint per frame, the gradient / loss all-reduce across ranks (N > 1) and the Adam step."""
+    forward + adjoint per frame (MLP as bf16 tensor-core GEMM tiles, or FP32), the gradient / loss all-reduce across
+    ranks (N > 1) and the Adam step."""
     import torch
 
     from hush_b200 import Hush
     from hush_b200.dp import DataParallel, finish_step
     from hush_b200.train import TrainConfig, Trainer, window_scene, xavier_init
 
-    cfg = TrainConfig()
+    cfg = TrainConfig(mlp=mlp)
     dp = DataParallel()
     th = Hush(local, {"width": cfg.size, "height": cfg.size, "schedule": "passes"})
     tr = Trainer(th, xavier_init(cfg.init_seed))
+    tr.set_mlp(cfg.mlp)
     rng = dp.seed_rng(cfg.init_seed + 1)
     sc = window_scene(cfg)
 
@@ -416,7 +421,7 @@ def _train_step_ms(local, stream, barrier, max_over_ranks, warmup=2, steps=5):
     ms = max_over_ranks(e0.elapsed_time(e1)) / steps
     tr.destroy()
     th.destroy()
-    return {"step_ms": round(ms, 3), "steps": steps, "warmup": warmup, "world": dp.world,
+    return {"step_ms": round(ms, 3), "mlp": cfg.mlp, "steps": steps, "warmup": warmup, "world": dp.world,
             "windows_per_step": cfg.batch * dp.world, "frames_per_step": cfg.batch * cfg.frames * dp.world,
             "size": f"{cfg.size}x{cfg.size}", "loss_last": round(losses[-1], 5),
             "note": "window generation, twin forward + adjoint of every frame, gradient all-reduce (N > 1), Adam"}
