@@ -373,6 +373,7 @@ def run_ours(args):
         "e2e": {"value": round(e2e_ms / world, 4), "unit": "ms/frame", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": n_kernels * args.steps,
+        "kernel_status": hush.kernel_status(),  # the error word of the bounded waits after the run (0 = none gave up)
         "mlp_forms": {args.mlp: {"ms_per_frame": round(ms_frame, 4)},
                       alt: {"ms_per_frame": round(alt_ms, 4), "frames": n_alt}},
     }

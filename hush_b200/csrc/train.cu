@@ -1165,7 +1165,7 @@ extern "C" int hush_trainer_create(hush_t *h, const float *theta, hush_trainer_t
   t->out[0] = (float4 *)take(full * 16); t->out[1] = (float4 *)take(full * 16);
   t->gT = (float4 *)take(full * 16); t->gT2 = (float4 *)take(full * 16); t->dX = (float4 *)take(full * 16);
   t->partials = (float *)take((size_t)t->n_mlp_ctas * NW * 4);
-  e = cudaMemcpy(t->theta, theta ? theta : h->wf.data(), NW * 4, theta ? cudaMemcpyHostToDevice : cudaMemcpyHostToDevice);
+  e = cudaMemcpy(t->theta, theta ? theta : h->wf.data(), NW * 4, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) { cudaFree(t->pool); delete t; return hush_cuda_fail(h, e, "cudaMemcpy of the weights"); }
   cudaFuncSetAttribute(k_mlp_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MB_SMEM);
   cudaFuncSetAttribute(k_mlp_bwd_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_BWD);
