@@ -13,8 +13,11 @@
 // Levels with a neighbourhood (the a-trous levels, TAA) stay separate launches: fusing them needs recomputed halos,
 // and on B200 these passes are bound by instruction issue rather than HBM, so recomputation costs more than the
 // L2-resident round trip of a half-res image.
+#include <cuda.h>  // CUtensorMap and its enums (types only: the encoder is fetched from the driver)
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
+#include <cstring>
 #include <type_traits>
 
 #include "hush_device.cuh"
@@ -593,15 +596,60 @@ HD_INL void tile_mid1(const HushFrame &f, int tileX, int tileY, float4 *sA, floa
   sth(f.Bh0, o, filt<1, 1, true, SW>(sA, sG, lx, ly, X, Y, f.W2, f.H2, s, c));
 }
 
+// TMA staging of a mid level's halo tile (interior tiles): the guide Gd (float4 per texel, a 3-d FLOAT32 map
+// {4, W2, H2}) lands in sG as is, the level (8-byte texels, a 2-d UINT64 map {W2, H2}) in a staging array that is
+// widened to float4 afterwards. Both copies start at x = bx - STEP, even for STEP = 2 / 4, so the 8-byte map's
+// innermost coordinate is 16-byte aligned; the boxes are (16 + 2 STEP) x (8 + 2 STEP) texels.
+struct HalfMaps {
+  CUtensorMap gd2, gd4, bh0, bh1;  // Gd with the step-2 / step-4 box; Bh0 (mid2's source) and Bh1 (mid3's)
+  int ok;                          // 0: every tile loads with plain loads (odd W2, or no encoder)
+};
+constexpr uint32_t TMA_POLLS = 1u << 22;
+
+HD_INL void tma_expect(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+HD_INL void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(mbar)
+      : "memory");
+}
+HD_INL void tma_load_3d(uint32_t dst, const CUtensorMap *map, int c, int x, int y, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
+          "r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c), "r"(x), "r"(y), "r"(mbar)
+      : "memory");
+}
+
 template <int STEP, int COMP>
-HD_INL void tile_mid(const HushFrame &f, int tileX, int tileY, const uint2 *src, uint2 *dst, float4 *sA, float4 *sG) {
+HD_INL void tile_mid(const HushFrame &f, int tileX, int tileY, const uint2 *src, uint2 *dst, float4 *sA, float4 *sG,
+                     const CUtensorMap *mg, const CUtensorMap *ms) {
   constexpr int AP = STEP, SW = HT_W + 2 * AP, SH = HT_H + 2 * AP;
+  __shared__ alignas(128) uint2 stage[SW * SH];
+  __shared__ alignas(8) uint64_t mbar;
   const int li = threadIdx.x;
   const int bx = tileX * HT_W, by = tileY * HT_H;
-  for (int i = li; i < SW * SH; i += HT_W * HT_H) {
-    const int q = clampi(by - AP + i / SW, 0, f.H2 - 1) * f.W2 + clampi(bx - AP + i % SW, 0, f.W2 - 1);
-    sA[i] = ldh(src, q);
-    sG[i] = __ldg(f.Gd + q);
+  const bool inner = mg && bx - AP >= 0 && by - AP >= 0 && bx + HT_W + AP <= f.W2 && by + HT_H + AP <= f.H2;
+  if (inner) {
+    const uint32_t mb = umma::smem_u32(&mbar);
+    if (li == 0) umma::mbar_init(mb, 1);
+    __syncthreads();
+    if (li == 0) {
+      tma_expect(mb, SW * SH * (8 + 16));
+      tma_load_2d(umma::smem_u32(stage), ms, bx - AP, by - AP, mb);
+      tma_load_3d(umma::smem_u32(sG), mg, 0, bx - AP, by - AP, mb);
+    }
+    if (!umma::mbar_wait_bounded(mb, 0, TMA_POLLS)) atomicOr(f.err, 8u);
+    for (int i = li; i < SW * SH; i += HT_W * HT_H) sA[i] = h4_to_f4(stage[i]);
+  } else {
+    for (int i = li; i < SW * SH; i += HT_W * HT_H) {
+      const int q = clampi(by - AP + i / SW, 0, f.H2 - 1) * f.W2 + clampi(bx - AP + i % SW, 0, f.W2 - 1);
+      sA[i] = ldh(src, q);
+      sG[i] = __ldg(f.Gd + q);
+    }
   }
   __syncthreads();
   const int X = bx + li % HT_W, Y = by + li / HT_W;
@@ -687,15 +735,16 @@ HD_INL void tile_coarse2(const HushFrame &f, int tileX, int tileY, float4 *sA, f
 // stage 1: mid1 tiles then coarse1 tiles; stage 2: mid2 tiles then coarse2 tiles; stage 3: mid3 tiles.
 template <int STAGE>
 __global__ void __launch_bounds__(HT_W *HT_H) k_half_stage(const __grid_constant__ HushFrame f, int nAx, int nA,
-                                                           int nBx) {
+                                                           int nBx, const __grid_constant__ HalfMaps M) {
   constexpr int SMAX = (HT_W + 8) * (HT_H + 8);
-  __shared__ float4 sA[SMAX], sG[SMAX];
+  __shared__ alignas(128) float4 sA[SMAX];
+  __shared__ alignas(128) float4 sG[SMAX];
   const int b = blockIdx.x;
   if (b < nA) {
     const int tX = b % nAx, tY = b / nAx;
     if (STAGE == 1) tile_mid1(f, tX, tY, sA, sG);
-    else if (STAGE == 2) tile_mid<2, 2>(f, tX, tY, f.Bh0, f.Bh1, sA, sG);
-    else tile_mid<4, 3>(f, tX, tY, f.Bh1, f.Bh0, sA, sG);
+    else if (STAGE == 2) tile_mid<2, 2>(f, tX, tY, f.Bh0, f.Bh1, sA, sG, M.ok ? &M.gd2 : nullptr, &M.bh0);
+    else tile_mid<4, 3>(f, tX, tY, f.Bh1, f.Bh0, sA, sG, M.ok ? &M.gd4 : nullptr, &M.bh1);
   } else {
     const int t = b - nA, tX = t % nBx, tY = t / nBx;
     if (STAGE == 1) tile_coarse1(f, tX, tY, sA, sG);
@@ -897,6 +946,53 @@ static const char *STAGE_LABELS[6] = {"temporal+mlp", "mid1+coarse1", "mid2+coar
 int fused_stage_count() { return 6; }
 const char *fused_stage_label(int s) { return (s >= 0 && s < 6) ? STAGE_LABELS[s] : "?"; }
 
+// The half stages' tensor maps for the frame's buffers, encoded when the buffers or sizes change (per host thread).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+static const HalfMaps &half_maps(const HushFrame &f) {
+  struct Cache {
+    const void *gd = nullptr, *b0 = nullptr, *b1 = nullptr;
+    int w = -1, h = -1;
+    HalfMaps m{};
+  };
+  static thread_local Cache c;
+  if (c.gd == f.Gd && c.b0 == f.Bh0 && c.b1 == f.Bh1 && c.w == f.W2 && c.h == f.H2) return c.m;
+  c.gd = f.Gd; c.b0 = f.Bh0; c.b1 = f.Bh1; c.w = f.W2; c.h = f.H2;
+  std::memset(&c.m, 0, sizeof(c.m));
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  // the 8-byte level map needs a row pitch that is a multiple of 16 bytes
+  if (!enc || (f.W2 & 1) || f.W2 < HT_W + 8 || f.H2 < HT_H + 8) return c.m;
+  const cuuint32_t one[3] = {1, 1, 1};
+  auto gd = [&](CUtensorMap *m, int ap) {
+    const cuuint64_t dim[3] = {4, (cuuint64_t)f.W2, (cuuint64_t)f.H2};
+    const cuuint64_t str[2] = {16, (cuuint64_t)f.W2 * 16};
+    const cuuint32_t box[3] = {4, (cuuint32_t)(HT_W + 2 * ap), (cuuint32_t)(HT_H + 2 * ap)};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)f.Gd, dim, str, box, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  };
+  auto lv = [&](CUtensorMap *m, const uint2 *p, int ap) {
+    const cuuint64_t dim[2] = {(cuuint64_t)f.W2, (cuuint64_t)f.H2};
+    const cuuint64_t str[1] = {(cuuint64_t)f.W2 * 8};
+    const cuuint32_t box[2] = {(cuuint32_t)(HT_W + 2 * ap), (cuuint32_t)(HT_H + 2 * ap)};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, (void *)p, dim, str, box, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  };
+  const bool ok = gd(&c.m.gd2, 2) == CUDA_SUCCESS && gd(&c.m.gd4, 4) == CUDA_SUCCESS &&
+                  lv(&c.m.bh0, f.Bh0, 2) == CUDA_SUCCESS && lv(&c.m.bh1, f.Bh1, 4) == CUDA_SUCCESS;
+  c.m.ok = ok ? 1 : 0;
+  return c.m;
+}
+
 cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpW16 &w16, int mlp_mode, const void *mlp_tc,
                                cudaStream_t st) {
   const int hx = (f.W2 + HT_W - 1) / HT_W, hy = (f.H2 + HT_H - 1) / HT_H;
@@ -927,9 +1023,9 @@ cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpW16 &w16,
       }
       break;
     }
-    case 1: k_half_stage<1><<<hx * hy + qx * qy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx); break;
-    case 2: k_half_stage<2><<<hx * hy + qx * qy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx); break;
-    case 3: k_half_stage<3><<<hx * hy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx); break;
+    case 1: k_half_stage<1><<<hx * hy + qx * qy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx, half_maps(f)); break;
+    case 2: k_half_stage<2><<<hx * hy + qx * qy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx, half_maps(f)); break;
+    case 3: k_half_stage<3><<<hx * hy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx, half_maps(f)); break;
     case 4: k_fine_final_fused<<<dim3((f.W + FT_W - 1) / FT_W, (f.H + FT_H - 1) / FT_H), FT_W * FT_H, 0, st>>>(f); break;
     case 5: k_taa_fused<<<dim3((f.W + FT_W - 1) / FT_W, (f.H + FT_H - 1) / FT_H), FT_W * FT_H, 0, st>>>(f); break;
     default: return cudaErrorInvalidValue;
