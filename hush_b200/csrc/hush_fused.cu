@@ -605,6 +605,12 @@ struct HalfMaps {
   int ok;                          // 0: every tile loads with plain loads (odd W2, or no encoder)
 };
 constexpr uint32_t TMA_POLLS = 1u << 22;
+// FINE_FINAL's A0 / key tiles (8-byte texels, 2-d UINT64 maps {W, H}) on interior tiles: the copies start at
+// x = bx - 2 (even, so 16-byte aligned) with a 36 x 10 box; the tile's column c is the box's column c + 1.
+struct FineMaps {
+  CUtensorMap a0, key;
+  int ok;
+};
 
 HD_INL void tma_expect(uint32_t mbar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
@@ -761,13 +767,28 @@ constexpr int FT_W = 32, FT_H = 8;
 // parameters (s0, c0, beta, kappa; 16 x 4). Each texel is then read from shared memory by the 16 or so taps that use
 // it instead of being fetched and decoded per tap.
 constexpr int FH_W = FT_W / 2 + 2, FH_H = FT_H / 2 + 2, FQ_W = FT_W / 4 + 2, FQ_H = FT_H / 4 + 2;
-__global__ void __launch_bounds__(FT_W *FT_H, 3) k_fine_final_fused(const __grid_constant__ HushFrame f) {
+constexpr int FB_W = FT_W + 4, FB_H = FT_H + 2;  // the TMA box of the A0 / key tiles
+__global__ void __launch_bounds__(FT_W *FT_H, 3) k_fine_final_fused(const __grid_constant__ HushFrame f,
+                                                                     const __grid_constant__ FineMaps M) {
   constexpr int AP = 1, SW = FT_W + 2, SH = FT_H + 2;
   constexpr int NH = FH_W * FH_H, NQ = FQ_W * FQ_H, NP = (FT_W / 2) * (FT_H / 2);
   __shared__ float4 sA[SW * SH], sG[SW * SH];
   __shared__ float4 sHG[NH], sHA[NH], sHB[NH], sQG[NQ], sQC[NQ], sPar[NP];
+  __shared__ alignas(128) uint2 stA[FB_W * FB_H];
+  __shared__ alignas(128) uint2 stK[FB_W * FB_H];
+  __shared__ alignas(8) uint64_t mbar;
   const int li = threadIdx.x;
   const int bx = blockIdx.x * FT_W, by = blockIdx.y * FT_H;
+  const bool inner = M.ok && bx - 2 >= 0 && by - 1 >= 0 && bx + FT_W + 2 <= f.W && by + FT_H + 1 <= f.H;
+  const uint32_t mb = umma::smem_u32(&mbar);
+  if (inner) {
+    if (li == 0) {
+      umma::mbar_init(mb, 1);
+      tma_expect(mb, FB_W * FB_H * 16);
+      tma_load_2d(umma::smem_u32(stA), &M.a0, bx - 2, by - 1, mb);
+      tma_load_2d(umma::smem_u32(stK), &M.key, bx - 2, by - 1, mb);
+    }
+  }
   const int hx0 = bx / 2 - 1, hy0 = by / 2 - 1, qx0 = bx / 4 - 1, qy0 = by / 4 - 1;
   if (li < NH) {
     const int q = clampi(hy0 + li / FH_W, 0, f.H2 - 1) * f.W2 + clampi(hx0 + li % FH_W, 0, f.W2 - 1);
@@ -785,13 +806,26 @@ __global__ void __launch_bounds__(FT_W *FT_H, 3) k_fine_final_fused(const __grid
     const float4 p0 = ldh(f.par0, hq);
     sPar[i] = make_float4(ldh(f.par1, hq).x, ldh(f.par2, hq).x, p0.z, p0.w);  // s0, c0, beta, kappa
   }
-  for (int i = li; i < SW * SH; i += FT_W * FT_H) {
-    const int q = clampi(by - AP + i / SW, 0, f.H - 1) * f.W + clampi(bx - AP + i % SW, 0, f.W - 1);
-    sA[i] = ldh(f.A0, q);
-    const float4 k = ldh(f.key, q);
-    float4 g = oct_dec(k.x, k.y);
-    g.w = k.z;
-    sG[i] = g;
+  if (inner) {
+    __syncthreads();  // the mbarrier's initialisation, before anyone waits on it
+    if (!umma::mbar_wait_bounded(mb, 0, TMA_POLLS)) atomicOr(f.err, 8u);
+    for (int i = li; i < SW * SH; i += FT_W * FT_H) {
+      const int t = (i / SW) * FB_W + i % SW + 1;
+      sA[i] = h4_to_f4(stA[t]);
+      const float4 k = h4_to_f4(stK[t]);
+      float4 g = oct_dec(k.x, k.y);
+      g.w = k.z;
+      sG[i] = g;
+    }
+  } else {
+    for (int i = li; i < SW * SH; i += FT_W * FT_H) {
+      const int q = clampi(by - AP + i / SW, 0, f.H - 1) * f.W + clampi(bx - AP + i % SW, 0, f.W - 1);
+      sA[i] = ldh(f.A0, q);
+      const float4 k = ldh(f.key, q);
+      float4 g = oct_dec(k.x, k.y);
+      g.w = k.z;
+      sG[i] = g;
+    }
   }
   __syncthreads();
   const int px = bx + li % FT_W, py = by + li / FT_W;
@@ -993,6 +1027,36 @@ static const HalfMaps &half_maps(const HushFrame &f) {
   return c.m;
 }
 
+// FINE_FINAL's maps for the frame's A0 and key (which alternates with the frame parity: two cached entries).
+static const FineMaps &fine_maps(const HushFrame &f) {
+  struct Entry {
+    const void *a0 = nullptr, *key = nullptr;
+    int w = -1, h = -1;
+    FineMaps m{};
+  };
+  static thread_local Entry c[2];
+  static thread_local int next = 0;
+  for (Entry &e : c)
+    if (e.a0 == f.A0 && e.key == f.key && e.w == f.W && e.h == f.H) return e.m;
+  Entry &e = c[next];
+  next ^= 1;
+  e.a0 = f.A0; e.key = f.key; e.w = f.W; e.h = f.H;
+  std::memset(&e.m, 0, sizeof(e.m));
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || (f.W & 1) || f.W < FB_W || f.H < FB_H) return e.m;
+  const cuuint32_t one[2] = {1, 1};
+  const cuuint64_t dim[2] = {(cuuint64_t)f.W, (cuuint64_t)f.H};
+  const cuuint64_t str[1] = {(cuuint64_t)f.W * 8};
+  const cuuint32_t box[2] = {(cuuint32_t)FB_W, (cuuint32_t)FB_H};
+  auto lv = [&](CUtensorMap *m, const void *p) {
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, const_cast<void *>(p), dim, str, box, one,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  };
+  e.m.ok = (lv(&e.m.a0, f.A0) == CUDA_SUCCESS && lv(&e.m.key, f.key) == CUDA_SUCCESS) ? 1 : 0;
+  return e.m;
+}
+
 cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpW16 &w16, int mlp_mode, const void *mlp_tc,
                                cudaStream_t st) {
   const int hx = (f.W2 + HT_W - 1) / HT_W, hy = (f.H2 + HT_H - 1) / HT_H;
@@ -1026,7 +1090,9 @@ cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpW16 &w16,
     case 1: k_half_stage<1><<<hx * hy + qx * qy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx, half_maps(f)); break;
     case 2: k_half_stage<2><<<hx * hy + qx * qy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx, half_maps(f)); break;
     case 3: k_half_stage<3><<<hx * hy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx, half_maps(f)); break;
-    case 4: k_fine_final_fused<<<dim3((f.W + FT_W - 1) / FT_W, (f.H + FT_H - 1) / FT_H), FT_W * FT_H, 0, st>>>(f); break;
+    case 4:
+      k_fine_final_fused<<<dim3((f.W + FT_W - 1) / FT_W, (f.H + FT_H - 1) / FT_H), FT_W * FT_H, 0, st>>>(f, fine_maps(f));
+      break;
     case 5: k_taa_fused<<<dim3((f.W + FT_W - 1) / FT_W, (f.H + FT_H - 1) / FT_H), FT_W * FT_H, 0, st>>>(f); break;
     default: return cudaErrorInvalidValue;
   }
