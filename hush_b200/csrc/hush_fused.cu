@@ -577,31 +577,13 @@ constexpr int HT_W = 16, HT_H = 8;
 
 // mid1 (hush.js:326, 366): 3x3 step 1 with prefilter on the block means, learned s_1 / c_1 (stored par1.y / par2.y
 // are the qf16 values INFER passes).
-HD_INL void tile_mid1(const HushFrame &f, int tileX, int tileY, float4 *sA, float4 *sG) {
-  constexpr int AP = 1, SW = HT_W + 2, SH = HT_H + 2;
-  const int li = threadIdx.x;
-  const int bx = tileX * HT_W, by = tileY * HT_H;
-  for (int i = li; i < SW * SH; i += HT_W * HT_H) {
-    const int q = clampi(by - AP + i / SW, 0, f.H2 - 1) * f.W2 + clampi(bx - AP + i % SW, 0, f.W2 - 1);
-    sA[i] = ldh(f.Ah, q);
-    sG[i] = __ldg(f.Gd + q);
-  }
-  __syncthreads();
-  const int X = bx + li % HT_W, Y = by + li / HT_W;
-  if (X >= f.W2 || Y >= f.H2) return;
-  const int lx = li % HT_W + AP, ly = li / HT_W + AP;
-  const int o = Y * f.W2 + X;
-  if (sG[ly * SW + lx].w < 0.0f) { sth(f.Bh0, o, make_float4(0.f, 0.f, 0.f, 0.f)); return; }
-  const float s = ldh(f.par1, o).y, c = ldh(f.par2, o).y;
-  sth(f.Bh0, o, filt<1, 1, true, SW>(sA, sG, lx, ly, X, Y, f.W2, f.H2, s, c));
-}
-
 // TMA staging of a mid level's halo tile (interior tiles): the guide Gd (float4 per texel, a 3-d FLOAT32 map
 // {4, W2, H2}) lands in sG as is, the level (8-byte texels, a 2-d UINT64 map {W2, H2}) in a staging array that is
 // widened to float4 afterwards. Both copies start at x = bx - STEP, even for STEP = 2 / 4, so the 8-byte map's
 // innermost coordinate is 16-byte aligned; the boxes are (16 + 2 STEP) x (8 + 2 STEP) texels.
 struct HalfMaps {
   CUtensorMap gd2, gd4, bh0, bh1;  // Gd with the step-2 / step-4 box; Bh0 (mid2's source) and Bh1 (mid3's)
+  CUtensorMap gd1, ah;             // mid1: Gd with an 18 x 10 box at x = bx - 1; Ah with a 20 x 10 box at x = bx - 2
   int ok;                          // 0: every tile loads with plain loads (odd W2, or no encoder)
 };
 constexpr uint32_t TMA_POLLS = 1u << 22;
@@ -628,6 +610,44 @@ HD_INL void tma_load_3d(uint32_t dst, const CUtensorMap *map, int c, int x, int 
           "r"(dst),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(c), "r"(x), "r"(y), "r"(mbar)
       : "memory");
+}
+
+// mid1 (hush.js:326, 366): the block means Ah and the guide, apron 1. On interior tiles the guide lands in sG by TMA
+// (3-d map, no alignment rule on x) and Ah in a staging array from x = bx - 2 (the 8-byte map's x must be even), the
+// tile's column c being the staged column c + 1.
+HD_INL void tile_mid1(const HushFrame &f, int tileX, int tileY, float4 *sA, float4 *sG, const HalfMaps *M) {
+  constexpr int AP = 1, SW = HT_W + 2, SH = HT_H + 2, BW = HT_W + 4;
+  __shared__ alignas(128) uint2 stage[BW * SH];
+  __shared__ alignas(8) uint64_t mbar;
+  const int li = threadIdx.x;
+  const int bx = tileX * HT_W, by = tileY * HT_H;
+  const bool inner = M && bx - 2 >= 0 && by - 1 >= 0 && bx + HT_W + 2 <= f.W2 && by + HT_H + 1 <= f.H2;
+  if (inner) {
+    const uint32_t mb = umma::smem_u32(&mbar);
+    if (li == 0) umma::mbar_init(mb, 1);
+    __syncthreads();
+    if (li == 0) {
+      tma_expect(mb, BW * SH * 8 + SW * SH * 16);
+      tma_load_2d(umma::smem_u32(stage), &M->ah, bx - 2, by - 1, mb);
+      tma_load_3d(umma::smem_u32(sG), &M->gd1, 0, bx - 1, by - 1, mb);
+    }
+    if (!umma::mbar_wait_bounded(mb, 0, TMA_POLLS)) atomicOr(f.err, 8u);
+    for (int i = li; i < SW * SH; i += HT_W * HT_H) sA[i] = h4_to_f4(stage[(i / SW) * BW + i % SW + 1]);
+  } else {
+    for (int i = li; i < SW * SH; i += HT_W * HT_H) {
+      const int q = clampi(by - AP + i / SW, 0, f.H2 - 1) * f.W2 + clampi(bx - AP + i % SW, 0, f.W2 - 1);
+      sA[i] = ldh(f.Ah, q);
+      sG[i] = __ldg(f.Gd + q);
+    }
+  }
+  __syncthreads();
+  const int X = bx + li % HT_W, Y = by + li / HT_W;
+  if (X >= f.W2 || Y >= f.H2) return;
+  const int lx = li % HT_W + AP, ly = li / HT_W + AP;
+  const int o = Y * f.W2 + X;
+  if (sG[ly * SW + lx].w < 0.0f) { sth(f.Bh0, o, make_float4(0.f, 0.f, 0.f, 0.f)); return; }
+  const float s = ldh(f.par1, o).y, c = ldh(f.par2, o).y;
+  sth(f.Bh0, o, filt<1, 1, true, SW>(sA, sG, lx, ly, X, Y, f.W2, f.H2, s, c));
 }
 
 template <int STEP, int COMP>
@@ -748,7 +768,7 @@ __global__ void __launch_bounds__(HT_W *HT_H) k_half_stage(const __grid_constant
   const int b = blockIdx.x;
   if (b < nA) {
     const int tX = b % nAx, tY = b / nAx;
-    if (STAGE == 1) tile_mid1(f, tX, tY, sA, sG);
+    if (STAGE == 1) tile_mid1(f, tX, tY, sA, sG, M.ok ? &M : nullptr);
     else if (STAGE == 2) tile_mid<2, 2>(f, tX, tY, f.Bh0, f.Bh1, sA, sG, M.ok ? &M.gd2 : nullptr, &M.bh0);
     else tile_mid<4, 3>(f, tX, tY, f.Bh1, f.Bh0, sA, sG, M.ok ? &M.gd4 : nullptr, &M.bh1);
   } else {
@@ -995,13 +1015,13 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 static const HalfMaps &half_maps(const HushFrame &f) {
   struct Cache {
-    const void *gd = nullptr, *b0 = nullptr, *b1 = nullptr;
+    const void *gd = nullptr, *b0 = nullptr, *b1 = nullptr, *ah = nullptr;
     int w = -1, h = -1;
     HalfMaps m{};
   };
   static thread_local Cache c;
-  if (c.gd == f.Gd && c.b0 == f.Bh0 && c.b1 == f.Bh1 && c.w == f.W2 && c.h == f.H2) return c.m;
-  c.gd = f.Gd; c.b0 = f.Bh0; c.b1 = f.Bh1; c.w = f.W2; c.h = f.H2;
+  if (c.gd == f.Gd && c.b0 == f.Bh0 && c.b1 == f.Bh1 && c.ah == f.Ah && c.w == f.W2 && c.h == f.H2) return c.m;
+  c.gd = f.Gd; c.b0 = f.Bh0; c.b1 = f.Bh1; c.ah = f.Ah; c.w = f.W2; c.h = f.H2;
   std::memset(&c.m, 0, sizeof(c.m));
   const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
   // the 8-byte level map needs a row pitch that is a multiple of 16 bytes
@@ -1021,8 +1041,16 @@ static const HalfMaps &half_maps(const HushFrame &f) {
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, (void *)p, dim, str, box, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   };
-  const bool ok = gd(&c.m.gd2, 2) == CUDA_SUCCESS && gd(&c.m.gd4, 4) == CUDA_SUCCESS &&
-                  lv(&c.m.bh0, f.Bh0, 2) == CUDA_SUCCESS && lv(&c.m.bh1, f.Bh1, 4) == CUDA_SUCCESS;
+  bool ok = gd(&c.m.gd2, 2) == CUDA_SUCCESS && gd(&c.m.gd4, 4) == CUDA_SUCCESS && gd(&c.m.gd1, 1) == CUDA_SUCCESS &&
+            lv(&c.m.bh0, f.Bh0, 2) == CUDA_SUCCESS && lv(&c.m.bh1, f.Bh1, 4) == CUDA_SUCCESS;
+  {  // Ah: box (16 + 4) x (8 + 2) from an even x
+    const cuuint64_t dim[2] = {(cuuint64_t)f.W2, (cuuint64_t)f.H2};
+    const cuuint64_t str[1] = {(cuuint64_t)f.W2 * 8};
+    const cuuint32_t box[2] = {(cuuint32_t)(HT_W + 4), (cuuint32_t)(HT_H + 2)};
+    ok = ok && enc(&c.m.ah, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, (void *)f.Ah, dim, str, box, one,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  }
   c.m.ok = ok ? 1 : 0;
   return c.m;
 }
