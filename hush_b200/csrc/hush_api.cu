@@ -559,7 +559,7 @@ extern "C" int hush_run_pass(hush_t *h, int pass, const hush_inputs *in, void *s
 
 // ------------------------------------------------------------------------------------------------ kernel status
 // The kernels' error word: bits are set where a bounded wait gave up (1: the tensor-core MLP of stage 0, 2: the
-// trainer's tensor-core MLP, 4: the wait self-test). Reading it synchronises the device.
+// trainer's tensor-core MLP, 4: the wait self-test, 8: a TMA halo-tile copy). Reading it synchronises the device.
 extern "C" int hush_kernel_status(hush_t *h, unsigned *word) {
   if (!h) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_kernel_status: NULL instance");
   cudaSetDevice(h->dev);

@@ -115,7 +115,8 @@ int hush_timer_read(hush_t *h, hush_timing *out, int max);
 int hush_set_graph(hush_t *h, int enable);
 
 /* The kernels' error word: a bounded wait that gave up (tensor-core MLP of stage 0: bit 0; the trainer's tensor-core
- * MLP: bit 1; hush_selftest_wait: bit 2) sets a bit instead of hanging. Reads the word into *word (may be NULL),
+ * MLP: bit 1; hush_selftest_wait: bit 2; a TMA halo-tile copy of the a-trous stages: bit 3) sets a bit instead of
+ * hanging. Reads the word into *word (may be NULL),
  * synchronising the device, clears it, and returns HUSH_ERR_KERNEL with a message if any bit was set. */
 int hush_kernel_status(hush_t *h, unsigned *word);
 /* Enqueues one thread that waits `polls` times on a barrier nothing arrives at and then sets bit 2 of the error
