@@ -305,3 +305,91 @@ def test_train_step_is_the_training_loop():
     d = np.abs(a.theta - b.theta)
     assert np.mean(d <= 1e-6) >= 0.99 and d.max() <= 2.1e-3, (np.mean(d <= 1e-6), d.max())
     assert not np.array_equal(a.theta, theta)
+
+
+@pytest.mark.parametrize("name", ORDER)
+def test_pass_adjoint_matches_fp64_central_differences(frame, name):
+    """The CUDA adjoint of each pass against central differences (h = 1e-3) of the same pass evaluated in FP64 at the
+    CUDA pass's inputs: free of the FP32 rounding of the forward. Every entry whose +-h interval is smooth agrees to
+    1e-3 relative where the entry is at least 1e-2 of the largest gradient; smaller entries, whose FP32 accumulation
+    over the rows can cancel, to 1e-5 of the largest gradient in absolute terms."""
+    seed = _seed(frame, name, torch.Generator().manual_seed(5))
+    got = _run_bwd(frame, name, seed)
+    sd = None if seed is None else seed.double().cpu()
+
+    def objective(inputs):
+        with torch.no_grad():
+            if name == "mlp":
+                _, y = twin.mlp(frame.feats, inputs["THETA"], frame.sky_h)
+            elif name.startswith("mid"):
+                k = int(name[-1])
+                src = frame.Ah if k == 1 else inputs[f"B{k - 1}"]
+                y = twin.mid(k, src, frame.Gh, frame.sky_h, inputs["PAR"])
+            elif name == "fine":
+                _, y = twin.fine(frame.st, inputs["PAR"], inputs["B3"], frame.Gh, frame.sky_h, frame.Ah)
+            elif name == "taa":
+                y = twin.taa(frame.st, inputs["X"][..., :3])
+            else:
+                y = twin.loss_of(frame.st, inputs["OUT"][..., :3], frame.lam)
+            return y.sum().item() if sd is None else (sd[..., :y.shape[-1]] * y).sum().item()
+
+    def mlp_pattern(theta):
+        """The MLP's piecewise-linear switches over the non-sky rows: both ReLU masks and the heads' clamps. A weight
+        perturbation that flips any of them crosses a kink in one row of many, which the one-sided test misses."""
+        w = theta
+        live = ~frame.sky_h
+        x = frame.feats[live]
+        a1 = x @ w[twin.W1o:twin.B1o].view(16, 20).T + w[twin.B1o:twin.W2o]
+        h1 = torch.relu(a1)
+        a2 = h1 @ w[twin.W2o:twin.B2o].view(16, 16).T + w[twin.B2o:twin.W3o]
+        o = torch.relu(a2) @ w[twin.W3o:twin.B3o].view(12, 16).T + w[twin.B3o:twin.B3o + 12]
+        return torch.cat([a1 > 0, a2 > 0, o[:, 4:8].abs() < 5, o[:, 8:12].abs() < 4], 1)
+
+    base = {inp: frame.b(inp).double().cpu().clone() for inp in SPEC[name][3]}
+    rng = np.random.default_rng(6)
+    rels, kinks = [], 0
+    f0 = objective(base)
+    for inp, gname in SPEC[name][3].items():
+        g = got[gname].reshape(-1)
+        gmax = g.abs().max().item()
+        if inp == "PAR":
+            mask = torch.zeros(got[gname].shape, dtype=torch.bool)
+            mask[..., list(PAR_USED[name])] = True
+            g = torch.where(mask.reshape(-1), g, torch.zeros_like(g))
+        if inp in ("X", "OUT"):
+            mask = torch.zeros(got[gname].shape, dtype=torch.bool)
+            mask[..., :3] = True
+            g = torch.where(mask.reshape(-1), g, torch.zeros_like(g))
+        top = torch.argsort(-g.abs())[:16].numpy()
+        nz = torch.nonzero(g.abs() > 1e-3 * g.abs().max()).view(-1).numpy()
+        pick = np.unique(np.concatenate([top, rng.choice(nz, size=min(16, nz.size), replace=False)]))
+        for i in pick:
+            xs = {k: v.clone() for k, v in base.items()}
+            flat = xs[inp].view(-1)
+            v0 = flat[i].item()
+            flat[i] = v0 + H_FD
+            fp = objective(xs)
+            flat[i] = v0 - H_FD
+            fm = objective(xs)
+            up, down = (fp - f0) / H_FD, (f0 - fm) / H_FD
+            switched = False
+            if name == "mlp":
+                with torch.no_grad():
+                    p0 = mlp_pattern(base["THETA"])
+                    for dv in (H_FD, -H_FD):
+                        t = base["THETA"].clone()
+                        t[i] += dv
+                        switched |= bool((mlp_pattern(t) != p0).any())
+            if switched or abs(up - down) > 0.05 * max(abs(up), abs(down)):
+                kinks += 1
+                continue
+            fd = (fp - fm) / (2 * H_FD)
+            gi = g[i].item()
+            # the error in units of the bound: 1e-3 of the entry, or 1e-5 of the largest gradient for small entries
+            bound = 1e-3 * abs(gi) if abs(gi) >= 1e-2 * gmax else 1e-5 * gmax
+            rels.append((abs(fd - gi) / abs(gi), abs(fd - gi) / bound))
+    rels = np.array(rels)
+    print(f"{name}: {len(rels)} entries against FP64 differences, {kinks} across a kink, relative error median "
+          f"{np.median(rels[:, 0]):.2e} max {rels[:, 0].max():.2e}, worst / bound {rels[:, 1].max():.2f}")
+    assert len(rels) >= 8, (name, len(rels), kinks)
+    assert rels[:, 1].max() <= 1.0, (name, rels)
