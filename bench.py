@@ -42,12 +42,14 @@ def _scene_cfg():
 # Algorithmic bytes per launch of each fused stage at this build's formats (8 B per rgba16float texel), per
 # full-res pixel (P), half-res pixel (h) and quarter-res pixel (q): unique global reads + writes.
 STAGE_BYTES = {
-    "temporal+mlp": lambda P, h, q: P * (32 + 24 + 24) + h * (8 + 40),  # 4 inputs, 3 history gathers, A0/mom/key;
-                                                                        # prev par0, par0..2 + Ah + Gh
-    "mid1+coarse1": lambda P, h, q: h * (32 + 8) + q * 16,               # Ah Gh par1 par2 -> Bh0; -> C1, CG
-    "mid2+coarse2": lambda P, h, q: h * (32 + 8) + q * 24,               # Bh0 Gh par1 par2 -> Bh1; C1 CG -> C0
-    "mid3": lambda P, h, q: h * (32 + 8),                                # Bh1 Gh par1 par2 -> Bh0
-    "fine+final": lambda P, h, q: P * (32 + 16) + h * 48 + q * 16,       # A0 key mat emi -> hist X; 6 half, 2 quarter
+    # unique global bytes per launch at this build's formats: P full, h half, q quarter pixels
+    "temporal+mlp": lambda P, h, q: P * (32 + 24 + 24) + h * (8 + 56),  # rad nd mv mat; key hist mom gathers; A0 mom
+                                                                        # key | prev par0; par0..2 Ah Gh Gd
+    "mid1+coarse1": lambda P, h, q: h * (40 + 8 + 8) + q * 32,           # Ah Gd par1 par2 -> Bh0, Gh | -> C1 CG CGd
+    "mid2+coarse2": lambda P, h, q: h * (40 + 8) + q * 32,               # Bh0 Gd par1 par2 -> Bh1 | C1 CGd -> C0
+    "mid3": lambda P, h, q: h * (40 + 8),                                # Bh1 Gd par1 par2 -> Bh0
+    "fine+final": lambda P, h, q: P * (32 + 16) + h * 56 + q * 24,       # A0 key mat emi -> hist X | Gd Ah Bh0 par0..2
+                                                                        # | CGd C0
     "taa": lambda P, h, q: P * 32,                                       # X motion prevTaa -> taa
 }
 
