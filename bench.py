@@ -381,7 +381,7 @@ def run_ours(args):
     }
     if train_ms is not None:
         line["train"] = train_ms
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:  # the CPU baseline is timed on rank 0 of single-GPU runs only
         line["cpu_baseline"] = _cpu_baseline_sample()
     print(json.dumps(line), flush=True)
     hush.destroy()
