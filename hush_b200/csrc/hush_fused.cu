@@ -584,7 +584,9 @@ constexpr int HT_W = 16, HT_H = 8;
 struct HalfMaps {
   CUtensorMap gd2, gd4, bh0, bh1;  // Gd with the step-2 / step-4 box; Bh0 (mid2's source) and Bh1 (mid3's)
   CUtensorMap gd1, ah;             // mid1: Gd with an 18 x 10 box at x = bx - 1; Ah with a 20 x 10 box at x = bx - 2
+  CUtensorMap cgd, c1;             // coarse2 (quarter resolution): CGd and C1 with 24 x 16 boxes at x = bx - 4
   int ok;                          // 0: every tile loads with plain loads (odd W2, or no encoder)
+  int qok;                         // the same for the quarter-resolution maps (odd W4)
 };
 constexpr uint32_t TMA_POLLS = 1u << 22;
 // FINE_FINAL's A0 / key tiles (8-byte texels, 2-d UINT64 maps {W, H}) on interior tiles: the copies start at
@@ -741,14 +743,32 @@ HD_INL void tile_coarse1(const HushFrame &f, int tileX, int tileY, float4 *sA, f
   sth(f.C1, Y * f.W4 + X, filt<2, 1, true, SW>(sA, sG, lx, ly, X, Y, f.W4, f.H4, COARSE_S, 1.0f));
 }
 
-HD_INL void tile_coarse2(const HushFrame &f, int tileX, int tileY, float4 *sA, float4 *sG) {
+// coarse2 (hush.js:482-525, kind coarse): C1 and the decoded quarter-res guide, apron 4; interior tiles by TMA as
+// the mid levels (x = bx - 4 is even).
+HD_INL void tile_coarse2(const HushFrame &f, int tileX, int tileY, float4 *sA, float4 *sG, const HalfMaps *M) {
   constexpr int AP = 4, SW = HT_W + 2 * AP, SH = HT_H + 2 * AP;
+  __shared__ alignas(128) uint2 stage[SW * SH];
+  __shared__ alignas(8) uint64_t mbar;
   const int li = threadIdx.x;
   const int bx = tileX * HT_W, by = tileY * HT_H;
-  for (int i = li; i < SW * SH; i += HT_W * HT_H) {
-    const int q = clampi(by - AP + i / SW, 0, f.H4 - 1) * f.W4 + clampi(bx - AP + i % SW, 0, f.W4 - 1);
-    sA[i] = ldh(f.C1, q);
-    sG[i] = __ldg(f.CGd + q);
+  const bool inner = M && bx - AP >= 0 && by - AP >= 0 && bx + HT_W + AP <= f.W4 && by + HT_H + AP <= f.H4;
+  if (inner) {
+    const uint32_t mb = umma::smem_u32(&mbar);
+    if (li == 0) umma::mbar_init(mb, 1);
+    __syncthreads();
+    if (li == 0) {
+      tma_expect(mb, SW * SH * (8 + 16));
+      tma_load_2d(umma::smem_u32(stage), &M->c1, bx - AP, by - AP, mb);
+      tma_load_3d(umma::smem_u32(sG), &M->cgd, 0, bx - AP, by - AP, mb);
+    }
+    if (!umma::mbar_wait_bounded(mb, 0, TMA_POLLS)) atomicOr(f.err, 8u);
+    for (int i = li; i < SW * SH; i += HT_W * HT_H) sA[i] = h4_to_f4(stage[i]);
+  } else {
+    for (int i = li; i < SW * SH; i += HT_W * HT_H) {
+      const int q = clampi(by - AP + i / SW, 0, f.H4 - 1) * f.W4 + clampi(bx - AP + i % SW, 0, f.W4 - 1);
+      sA[i] = ldh(f.C1, q);
+      sG[i] = __ldg(f.CGd + q);
+    }
   }
   __syncthreads();
   const int X = bx + li % HT_W, Y = by + li / HT_W;
@@ -774,7 +794,7 @@ __global__ void __launch_bounds__(HT_W *HT_H) k_half_stage(const __grid_constant
   } else {
     const int t = b - nA, tX = t % nBx, tY = t / nBx;
     if (STAGE == 1) tile_coarse1(f, tX, tY, sA, sG);
-    else if (STAGE == 2) tile_coarse2(f, tX, tY, sA, sG);
+    else if (STAGE == 2) tile_coarse2(f, tX, tY, sA, sG, M.qok ? &M : nullptr);
   }
 }
 
@@ -1015,15 +1035,34 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 static const HalfMaps &half_maps(const HushFrame &f) {
   struct Cache {
-    const void *gd = nullptr, *b0 = nullptr, *b1 = nullptr, *ah = nullptr;
+    const void *gd = nullptr, *b0 = nullptr, *b1 = nullptr, *ah = nullptr, *cgd = nullptr, *c1 = nullptr;
     int w = -1, h = -1;
     HalfMaps m{};
   };
   static thread_local Cache c;
-  if (c.gd == f.Gd && c.b0 == f.Bh0 && c.b1 == f.Bh1 && c.ah == f.Ah && c.w == f.W2 && c.h == f.H2) return c.m;
-  c.gd = f.Gd; c.b0 = f.Bh0; c.b1 = f.Bh1; c.ah = f.Ah; c.w = f.W2; c.h = f.H2;
+  if (c.gd == f.Gd && c.b0 == f.Bh0 && c.b1 == f.Bh1 && c.ah == f.Ah && c.cgd == f.CGd && c.c1 == f.C1 &&
+      c.w == f.W2 && c.h == f.H2)
+    return c.m;
+  c.gd = f.Gd; c.b0 = f.Bh0; c.b1 = f.Bh1; c.ah = f.Ah; c.cgd = f.CGd; c.c1 = f.C1; c.w = f.W2; c.h = f.H2;
   std::memset(&c.m, 0, sizeof(c.m));
   const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (enc && !(f.W4 & 1) && f.W4 >= HT_W + 8 && f.H4 >= HT_H + 8) {  // coarse2's quarter-resolution maps
+    const cuuint32_t one3[3] = {1, 1, 1};
+    const cuuint64_t gdim[3] = {4, (cuuint64_t)f.W4, (cuuint64_t)f.H4};
+    const cuuint64_t gstr[2] = {16, (cuuint64_t)f.W4 * 16};
+    const cuuint32_t gbox[3] = {4, (cuuint32_t)(HT_W + 8), (cuuint32_t)(HT_H + 8)};
+    const cuuint64_t ldim[2] = {(cuuint64_t)f.W4, (cuuint64_t)f.H4};
+    const cuuint64_t lstr[1] = {(cuuint64_t)f.W4 * 8};
+    const cuuint32_t lbox[2] = {(cuuint32_t)(HT_W + 8), (cuuint32_t)(HT_H + 8)};
+    c.m.qok = enc(&c.m.cgd, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)f.CGd, gdim, gstr, gbox, one3,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
+              enc(&c.m.c1, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, (void *)f.C1, ldim, lstr, lbox, one3,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS
+                  ? 1
+                  : 0;
+  }
   // the 8-byte level map needs a row pitch that is a multiple of 16 bytes
   if (!enc || (f.W2 & 1) || f.W2 < HT_W + 8 || f.H2 < HT_H + 8) return c.m;
   const cuuint32_t one[3] = {1, 1, 1};
