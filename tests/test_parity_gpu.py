@@ -1,6 +1,6 @@
 """Parity of the CUDA path (through the C ABI) with the CPU oracle, on a B200.
 
-Bound (north star): |cuda - oracle| <= 2e-3 * max(|oracle|, floor) per channel with floor = 1e-2 of the frame's
+Bound: |cuda - oracle| <= 2e-3 * max(|oracle|, floor) per channel with floor = 1e-2 of the frame's
 mean |value|. Pass-level tests start every pass from the oracle's exact state, so differences cannot accumulate;
 sequence tests run both sides independently over whole sequences, where the f16 history feeds rounding differences
 back frame after frame.

@@ -1,7 +1,7 @@
 """Shared helpers of the tests: tolerance checks and oracle <-> CUDA state transfer."""
 import numpy as np
 
-# Parity bound (north star): |cuda - oracle| <= 2e-3 * max(|oracle|, floor) per channel, floor = 1e-2 of the
+# Parity bound: |cuda - oracle| <= 2e-3 * max(|oracle|, floor) per channel, floor = 1e-2 of the
 # frame's mean absolute value (relative error on near-zero values is meaningless).
 REL_TOL = 2e-3
 FLOOR_FRAC = 1e-2
