@@ -381,6 +381,8 @@ def run_ours(args):
     }
     if train_ms is not None:
         line["train"] = train_ms
+    if not args.no_extras:
+        line["extras"] = _extras_ms(frames, stream)
     if not args.no_cpu_baseline and world == 1:  # the CPU baseline is timed on rank 0 of single-GPU runs only
         line["cpu_baseline"] = _cpu_baseline_sample()
     print(json.dumps(line), flush=True)
@@ -388,6 +390,73 @@ def run_ours(args):
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def _extras_ms(frames, stream, n=32, warmup=4):
+    """Per-frame device time of the pieces around the denoiser at the workload's size, each timed alone with CUDA
+    events on the launching stream: plain SVGF (the fallback and judge, 5 a-trous iterations + TAA) on the same
+    frames, the path tracer (1 spp, 3 bounces, the demo scene) and the display post (bloom, vignette, AgX, sRGB into
+    an rgba8 target). A failure is reported in place of the time."""
+    import torch
+
+    from hush_b200 import SVGF, Post, pt
+
+    H, W = frames[0]["radiance"].shape[:2]
+    out = {}
+
+    def timed(step):
+        for i in range(warmup):
+            step(i)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(n):
+            step(warmup + i)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return round(e0.elapsed_time(e1) / n, 4)
+
+    try:
+        sv = SVGF(0, W, H)
+
+        def svgf_step(i):
+            k = i % len(frames)
+            g = dict(frames[k])
+            g["prevNormalDepth"] = frames[k - 1]["normalDepth"] if k else frames[k]["normalDepth"]
+            g["prevMotion"] = frames[k - 1]["motion"] if k else frames[k]["motion"]
+            sv.encode(g, stream=stream)
+
+        out["svgf_ms_per_frame"] = timed(svgf_step)
+        sv.destroy()
+    except Exception as e:  # pragma: no cover - reported, not fatal
+        out["svgf_ms_per_frame"] = f"failed: {e}"
+    try:
+        sc, env, mover = pt.demo_scene(0, seed=0, n_objects=32)
+        tracer = pt.PathTracer(0, sc, W, H)
+        cam = pt.Camera(position=(0.0, 4.0, 13.0), target=(0.0, 0.8, 0.0), fov=50, aspect=W / H)
+        state = {"vp": None}
+
+        def pt_step(i):
+            state["vp"] = tracer.write_uniforms(camera=cam, prev_view_proj=state["vp"], frame=i, mode=0,
+                                                jitter=pt.JITTER[i % 16], env=env)
+            tracer.encode(i & 1, stream=stream)
+
+        out["pt_ms_per_frame"] = timed(pt_step)
+        out["pt_config"] = "demo scene, 32 objects, 1 spp, 3 bounces, NEE + MIS, env map"
+        tracer.destroy()
+    except Exception as e:  # pragma: no cover
+        out["pt_ms_per_frame"] = f"failed: {e}"
+    try:
+        post = Post(0, "rgba8unorm")
+        den = frames[0]["radiance"]
+
+        def post_step(i):
+            post.encode(frames[i % len(frames)]["radiance"], den, split=0.5, stream=stream)
+
+        out["post_ms_per_frame"] = timed(post_step)
+        post.destroy()
+    except Exception as e:  # pragma: no cover
+        out["post_ms_per_frame"] = f"failed: {e}"
+    return out
 
 
 def _train_step_ms(local, stream, barrier, max_over_ranks, warmup=2, steps=5, mlp="bf16"):
@@ -442,6 +511,7 @@ def main(argv=None):
                     help="launch the six kernels of each frame directly instead of replaying the frame as a CUDA graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-train", action="store_true", help="skip the training-step timing")
+    ap.add_argument("--no-extras", action="store_true", help="skip the SVGF / path tracer / post timings")
     ap.add_argument("--workload", default="1080p", choices=["1080p", "4k"],
                     help="4k: the 3840x2160 workload (32 objects, 8 moving, 20%% sky, pan U[0,6], 2%% fireflies x100) "
                          "with the BF16 MLP and each frame replayed as one CUDA graph")

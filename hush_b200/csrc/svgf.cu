@@ -170,6 +170,15 @@ __global__ void k_svgf_atrous(const SvgfFrame f, const uint2 *in, uint2 *out, in
   const float gy = fminf(zd > 0.0f ? fabsf(zd - z) : 1e9f, zu > 0.0f ? fabsf(zu - z) : 1e9f);
   const float zg = fminf(fmaxf(gx, gy), z);
   const float h[5] = {1.0f / 16.0f, 1.0f / 4.0f, 3.0f / 8.0f, 1.0f / 4.0f, 1.0f / 16.0f};
+  // the tap distances sqrt(dx^2 + dy^2) (correctly rounded: 1, sqrt 2, 2, sqrt 5, sqrt 8) and one reciprocal per
+  // distance class and for the luminance scale instead of a division per tap; the weights' exp and pow run as the
+  // hardware approximations, which WGSL's own accuracy rules allow (exp: 3 + 2|x| ULP; pow via exp2(y log2 x)). The
+  // temporal pass, whose history-length test flips on an ulp, keeps IEEE arithmetic.
+  const float dcls[5] = {1.0f, 1.41421356237f, 2.0f, 2.2360679775f, 2.82842712475f};
+  float izd[5];
+#pragma unroll
+  for (int c = 0; c < 5; c++) izd[c] = 1.0f / (f.sigma_z * zg * (dcls[c] * (float)step) + 1e-3f);
+  const float ilum = 1.0f / denomL;
   float sw = h[2] * h[2];
   float scx = center.x * sw, scy = center.y * sw, scz = center.z * sw;
   float sv = center.w * sw * sw;
@@ -183,11 +192,12 @@ __global__ void k_svgf_atrous(const SvgfFrame f, const uint2 *in, uint2 *out, in
       const float4 ndq = ldh(f.nd, qy * f.p_nd + qx);
       if (ndq.w < 0.0f) continue;
       const float4 cq = ldh(in, qy * f.W + qx);
-      const float dist = sqrtf((float)dx * (float)dx + (float)dy * (float)dy) * (float)step;
-      const float wz = fabsf(ndq.w - nd.w) / (f.sigma_z * zg * dist + 1e-3f);
-      const float wn = powf(fmaxf(0.0f, dot3(ndq, nd)), f.sigma_n);
-      const float wl = fabsf(lum(cq) - lp) / denomL;
-      const float w = h[dx + 2] * h[dy + 2] * wn * expf(-wz - wl);
+      const int d2 = dx * dx + dy * dy;  // 1, 2, 4, 5, 8
+      const int cls = d2 == 1 ? 0 : (d2 == 2 ? 1 : (d2 == 4 ? 2 : (d2 == 5 ? 3 : 4)));
+      const float wz = fabsf(ndq.w - nd.w) * izd[cls];
+      const float wn = f.sigma_n != 0.0f ? __powf(fmaxf(0.0f, dot3(ndq, nd)), f.sigma_n) : 1.0f;  // pow(x, 0) = 1
+      const float wl = fabsf(lum(cq) - lp) * ilum;
+      const float w = h[dx + 2] * h[dy + 2] * wn * __expf(-wz - wl);
       sw += w;
       scx += w * cq.x; scy += w * cq.y; scz += w * cq.z;
       sv += w * w * cq.w;
