@@ -140,6 +140,17 @@ __global__ void k_svgf_variance(const SvgfFrame f, uint2 *out) {
   sth(out, o, make_float4(scx, scy, scz, v));
 }
 
+// The normal weight pow(max(n . n_q, 0), sigma_n): by seven squarings for the default sigma_n = 128 (no special-function
+// unit), else as the hardware exp2(sigma_n log2 x); pow(x, 0) = 1.
+HD_INL float svgf_wn(float x, float sigma_n) {
+  if (sigma_n == 128.0f) {
+#pragma unroll
+    for (int i = 0; i < 7; i++) x *= x;
+    return x;
+  }
+  return sigma_n != 0.0f ? __powf(x, sigma_n) : 1.0f;
+}
+
 // ATROUS iteration (svgf.js:157-216); iteration 0 also writes the colour history.
 __global__ void k_svgf_atrous(const SvgfFrame f, const uint2 *in, uint2 *out, int iter, int step) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -195,8 +206,86 @@ __global__ void k_svgf_atrous(const SvgfFrame f, const uint2 *in, uint2 *out, in
       const int d2 = dx * dx + dy * dy;  // 1, 2, 4, 5, 8
       const int cls = d2 == 1 ? 0 : (d2 == 2 ? 1 : (d2 == 4 ? 2 : (d2 == 5 ? 3 : 4)));
       const float wz = fabsf(ndq.w - nd.w) * izd[cls];
-      const float wn = f.sigma_n != 0.0f ? __powf(fmaxf(0.0f, dot3(ndq, nd)), f.sigma_n) : 1.0f;  // pow(x, 0) = 1
+      const float wn = svgf_wn(fmaxf(0.0f, dot3(ndq, nd)), f.sigma_n);
       const float wl = fabsf(lum(cq) - lp) * ilum;
+      const float w = h[dx + 2] * h[dy + 2] * wn * __expf(-wz - wl);
+      sw += w;
+      scx += w * cq.x; scy += w * cq.y; scz += w * cq.z;
+      sv += w * w * cq.w;
+    }
+  }
+  const float4 r = make_float4(scx / sw, scy / sw, scz / sw, sv / (sw * sw));
+  sth(out, o, r);
+  if (iter == 0) sth(f.hist, o, make_float4(r.x, r.y, r.z, 0.f));
+}
+
+// The same iteration for steps 1, 2 and 4 with the 5 x 5 footprint staged in shared memory: a 16 x 16 tile with an
+// apron of 2 step texels (clamped to the image, as the centre's 3 x 3 variance blur and depth gradient read them),
+// each texel converted once and its luminance formed once. The arithmetic per tap is the kernel's above.
+template <int STEP>
+__global__ void __launch_bounds__(256) k_svgf_atrous_tile(const SvgfFrame f, const uint2 *in, uint2 *out, int iter) {
+  constexpr int TS = 16, A = 2 * STEP, T = TS + 2 * A;
+  __shared__ float4 sC[T * T], sN[T * T];
+  __shared__ float sL[T * T];
+  const int li = threadIdx.y * TS + threadIdx.x;
+  const int bx = blockIdx.x * TS, by = blockIdx.y * TS;
+  for (int i = li; i < T * T; i += TS * TS) {
+    const int gx = clampi(bx - A + i % T, 0, f.W - 1), gy = clampi(by - A + i / T, 0, f.H - 1);
+    const float4 c = ldh(in, gy * f.W + gx);
+    sC[i] = c;
+    sN[i] = ldh(f.nd, gy * f.p_nd + gx);
+    sL[i] = lum(c);
+  }
+  __syncthreads();
+  const int x = bx + threadIdx.x, y = by + threadIdx.y;
+  if (x >= f.W || y >= f.H) return;
+  const int o = y * f.W + x;
+  const int lx = threadIdx.x + A, ly = threadIdx.y + A, tc = ly * T + lx;
+  const float4 nd = sN[tc];
+  if (nd.w < 0.0f) {
+    sth(out, o, make_float4(0.f, 0.f, 0.f, 0.f));
+    if (iter == 0) sth(f.hist, o, make_float4(0.f, 0.f, 0.f, 0.f));
+    return;
+  }
+  const float4 center = sC[tc];
+  const float k3[3] = {0.25f, 0.5f, 0.25f};
+  float gv = 0.f;
+#pragma unroll
+  for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+    for (int dx = -1; dx <= 1; dx++) gv += k3[dx + 1] * k3[dy + 1] * sC[tc + dy * T + dx].w;
+  const float lp = sL[tc];
+  const float denomL = f.sigma_l * sqrtf(fmaxf(gv, 0.0f)) + 1e-6f;
+  const float z = nd.w;
+  const float zl = sN[tc - 1].w, zr = sN[tc + 1].w, zu = sN[tc - T].w, zd = sN[tc + T].w;
+  const float gx = fminf(zr > 0.0f ? fabsf(zr - z) : 1e9f, zl > 0.0f ? fabsf(zl - z) : 1e9f);
+  const float gy = fminf(zd > 0.0f ? fabsf(zd - z) : 1e9f, zu > 0.0f ? fabsf(zu - z) : 1e9f);
+  const float zg = fminf(fmaxf(gx, gy), z);
+  const float h[5] = {1.0f / 16.0f, 1.0f / 4.0f, 3.0f / 8.0f, 1.0f / 4.0f, 1.0f / 16.0f};
+  const float dcls[5] = {1.0f, 1.41421356237f, 2.0f, 2.2360679775f, 2.82842712475f};
+  float izd[5];
+#pragma unroll
+  for (int c = 0; c < 5; c++) izd[c] = 1.0f / (f.sigma_z * zg * (dcls[c] * (float)STEP) + 1e-3f);
+  const float ilum = 1.0f / denomL;
+  float sw = h[2] * h[2];
+  float scx = center.x * sw, scy = center.y * sw, scz = center.z * sw;
+  float sv = center.w * sw * sw;
+#pragma unroll
+  for (int dy = -2; dy <= 2; dy++) {
+#pragma unroll
+    for (int dx = -2; dx <= 2; dx++) {
+      if (dx == 0 && dy == 0) continue;
+      const int qx = x + dx * STEP, qy = y + dy * STEP;
+      if (qx < 0 || qy < 0 || qx >= f.W || qy >= f.H) continue;
+      const int t = tc + dy * STEP * T + dx * STEP;
+      const float4 ndq = sN[t];
+      if (ndq.w < 0.0f) continue;
+      const float4 cq = sC[t];
+      const int d2 = dx * dx + dy * dy;
+      const int cls = d2 == 1 ? 0 : (d2 == 2 ? 1 : (d2 == 4 ? 2 : (d2 == 5 ? 3 : 4)));
+      const float wz = fabsf(ndq.w - nd.w) * izd[cls];
+      const float wn = svgf_wn(fmaxf(0.0f, dot3(ndq, nd)), f.sigma_n);
+      const float wl = fabsf(sL[t] - lp) * ilum;
       const float w = h[dx + 2] * h[dy + 2] * wn * __expf(-wz - wl);
       sw += w;
       scx += w * cq.x; scy += w * cq.y; scz += w * cq.z;
@@ -388,8 +477,14 @@ extern "C" int svgf_encode(svgf_t *s, const svgf_inputs *in, void *stream, const
   k_svgf_temporal<<<grd, blk, 0, st>>>(f);
   k_svgf_variance<<<grd, blk, 0, st>>>(f, s->atrous[0]);
   int src = 0;
+  const dim3 tblk(16, 16), tgrd((s->W + 15) / 16, (s->H + 15) / 16);
   for (int i = 0; i < s->o.iterations; i++) {
-    k_svgf_atrous<<<grd, blk, 0, st>>>(f, s->atrous[src], s->atrous[src ^ 1], i, 1 << i);
+    const uint2 *a = s->atrous[src];
+    uint2 *b = s->atrous[src ^ 1];
+    if (i == 0) k_svgf_atrous_tile<1><<<tgrd, tblk, 0, st>>>(f, a, b, i);
+    else if (i == 1) k_svgf_atrous_tile<2><<<tgrd, tblk, 0, st>>>(f, a, b, i);
+    else if (i == 2) k_svgf_atrous_tile<4><<<tgrd, tblk, 0, st>>>(f, a, b, i);
+    else k_svgf_atrous<<<grd, blk, 0, st>>>(f, a, b, i, 1 << i);
     src ^= 1;
   }
   k_svgf_resolve<<<grd, blk, 0, st>>>(f, s->atrous[src]);
