@@ -1101,6 +1101,12 @@ __global__ void k_adam(float *theta, float *m, float *v, const double *grad, flo
 using namespace hush;
 using namespace hush::twin;
 
+#ifndef HUSH_TRAIN_LANES
+#define HUSH_TRAIN_LANES 8
+#endif
+// windows hush_trainer_windows runs at once (this trainer and HUSH_TRAIN_LANES - 1 helpers)
+constexpr int TRAIN_LANES = HUSH_TRAIN_LANES;
+
 struct hush_trainer_s {
   hush_t *h = nullptr;
   int W = 0, H = 0, W2 = 0, H2 = 0;
@@ -1127,10 +1133,10 @@ struct hush_trainer_s {
   // hush_trainer_windows runs windows concurrently on lanes: lane 0 is this trainer, lanes 1.. are helper trainers on
   // private Hush instances of the same size (their own history), reading this trainer's weights and accumulating
   // into their own gradient / loss, which are added into this trainer's after the batch
-  hush_trainer_t *lane[4] = {};
-  hush_t *lane_h[4] = {};
-  cudaStream_t lane_st[4] = {};
-  cudaEvent_t lane_ev[4] = {};
+  hush_trainer_t *lane[TRAIN_LANES] = {};
+  hush_t *lane_h[TRAIN_LANES] = {};
+  cudaStream_t lane_st[TRAIN_LANES] = {};
+  cudaEvent_t lane_ev[TRAIN_LANES] = {};
   cudaEvent_t fork_ev = nullptr;
   bool is_lane = false;
 };
@@ -1177,11 +1183,11 @@ extern "C" int hush_trainer_create(hush_t *h, const float *theta, hush_trainer_t
 extern "C" void hush_trainer_destroy(hush_trainer_t *t) {
   if (!t) return;
   cudaSetDevice(t->h->dev);
-  for (int l = 1; l < 4; l++) {
+  for (int l = 1; l < TRAIN_LANES; l++) {
     if (t->lane[l]) hush_trainer_destroy(t->lane[l]);
     if (t->lane_h[l]) hush_destroy(t->lane_h[l]);
   }
-  for (int l = 0; l < 4; l++) {
+  for (int l = 0; l < TRAIN_LANES; l++) {
     if (t->lane_st[l]) cudaStreamDestroy(t->lane_st[l]);
     if (t->lane_ev[l]) cudaEventDestroy(t->lane_ev[l]);
   }
@@ -1254,7 +1260,6 @@ extern "C" int hush_trainer_frame(hush_trainer_t *t, const hush_inputs *in, cons
   if (e == cudaSuccess) e = launch_pass(PASS_COARSE1, f, t->h->w16, st);
   if (e == cudaSuccess) e = launch_pass(PASS_COARSE2, f, t->h->w16, st);
   if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "trainer pass launch");
-  const int half = f.W2 * f.H2, full = f.W * f.H;
   const dim3 blk(TW, TH), gh((f.W2 + TW - 1) / TW, (f.H2 + TH - 1) / TH), gf((f.W + TW - 1) / TW, (f.H + TH - 1) / TH);
   launch_mlp_fwd(t, T, st);
   k_mid_fwd<1><<<gh, blk, 0, st>>>(T);
@@ -1493,7 +1498,7 @@ static int windows_serial(hush_trainer_t *t, const hush_scene *sc, const uint32_
 
 // this trainer's accumulators += the helper lanes' (in lane order), which are cleared
 struct LaneAcc {
-  double *grad[4], *loss[4];
+  double *grad[TRAIN_LANES], *loss[TRAIN_LANES];
   int n;
 };
 __global__ void k_sum_lanes(double *grad, double *loss, LaneAcc la) {
@@ -1510,7 +1515,6 @@ __global__ void k_sum_lanes(double *grad, double *loss, LaneAcc la) {
   }
 }
 
-constexpr int TRAIN_LANES = 4;
 
 static int make_lanes(hush_trainer_t *t, int n) {
   hush_t *h = t->h;
@@ -1637,7 +1641,7 @@ static int run_twin_pass(hush_trainer_t *t, int pass, int backward, void *stream
   cudaStream_t st = (cudaStream_t)stream;
   const TwinFrame &T = t->T;
   const HushFrame &f = T.f;
-  const int half = f.W2 * f.H2, full = f.W * f.H;
+  const int full = f.W * f.H;
   const dim3 blk(TW, TH), gh((f.W2 + TW - 1) / TW, (f.H2 + TH - 1) / TH), gf((f.W + TW - 1) / TW, (f.H + TH - 1) / TH);
   cudaError_t e = cudaSuccess;
   switch (pass) {

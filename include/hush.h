@@ -207,7 +207,7 @@ int hush_train_step(hush_trainer_t *t, const hush_inputs *frames, const float *c
  * generated on the device into trainer-owned buffers (allocated on first use) and run as hush_train_step runs a
  * window (history reset, then per frame forward + backward with the temporal term from the second frame on, and
  * end-of-frame). Adds into the gradient and loss accumulators; no optimiser step (the caller all-reduces across ranks
- * if it trains data-parallel, then calls hush_trainer_step). sc's size must be the trainer's. Up to four windows run
+ * if it trains data-parallel, then calls hush_trainer_step). sc's size must be the trainer's. Up to eight windows run
  * concurrently on lanes forked from and joined back to `stream` (helper trainers on private Hush instances, created
  * on first use, own history and accumulators, summed into this trainer's in lane order); each window's training
  * frames replay as a cached CUDA graph. The trainer's own Hush instance ends in the state of the windows it ran. */
