@@ -625,54 +625,70 @@ __global__ void __launch_bounds__(TW *TH) k_fine_bwd(const TwinFrame T, const fl
   }
   __syncthreads();
   const int px = bx + threadIdx.x, py = by + threadIdx.y;
-  if (px >= f.W || py >= f.H) return;
-  const int o = py * f.W + px, ti = (threadIdx.y + AP) * SW + threadIdx.x + AP;
+  const bool in = px < f.W && py < f.H;
+  const int hp = (min(py, f.H - 1) >> 1) * f.W2 + (min(px, f.W - 1) >> 1);
+  float q4[4] = {0.f, 0.f, 0.f, 0.f};  // this pixel's dL/d(beta, kappa, s0, c0)
+  const int ti = (threadIdx.y + AP) * SW + threadIdx.x + AP;
   const float4 gp = sG[ti];
-  if (gp.w < 0.0f) return;  // X = emission: no dependence on the parameters
-  const float4 gt = gT[o];
-  const float3 gX = SEED_TM ? tm_adjoint(T.X[o], gt) : make_float3(gt.x, gt.y, gt.z);
-  const float4 alb = ldh(f.mat, py * f.p_mat + px);
-  const int hp = (py >> 1) * f.W2 + (px >> 1);
-  const float4 p0 = T.par[3 * hp], p1 = T.par[3 * hp + 1], p2 = T.par[3 * hp + 2];
-  Filt1<1, true, SW> F;
-  F.run(sA, sG, ti, px, py, f.W, f.H, p1.x, p2.x);
-  const float4 A1 = F.out();
-  Recomb R;
-  recomb_fwd(T, px, py, A1, gp, R);
-  float ix = R.fx, iy = R.fy, iz = R.fz;
-  const bool mid = R.swh > 1e-4f;
-  if (mid) {
-    ix = R.uBx / R.swh + p0.w * (R.fx - R.uAx / R.swh);
-    iy = R.uBy / R.swh + p0.w * (R.fy - R.uAy / R.swh);
-    iz = R.uBz / R.swh + p0.w * (R.fz - R.uAz / R.swh);
-  }
-  // X = ill2 * alb + emi, ill2 = ill + (up - ill) beta
-  const float3 g2 = make_float3(gX.x * alb.x, gX.y * alb.y, gX.z * alb.z);
-  float3 gill = g2;
-  float gbeta = 0.0f;
-  if (R.swq > 1e-4f) {
-    const float upx = R.uCx / R.swq, upy = R.uCy / R.swq, upz = R.uCz / R.swq;
-    gbeta = g2.x * (upx - ix) + g2.y * (upy - iy) + g2.z * (upz - iz);
-    gill = make_float3(g2.x * (1.0f - p0.z), g2.y * (1.0f - p0.z), g2.z * (1.0f - p0.z));
-  }
-  float3 gf = gill;
-  float gkappa = 0.0f;
-  if (mid) {
-    gkappa = gill.x * (R.fx - R.uAx / R.swh) + gill.y * (R.fy - R.uAy / R.swh) + gill.z * (R.fz - R.uAz / R.swh);
-    gf = make_float3(gill.x * p0.w, gill.y * p0.w, gill.z * p0.w);
-    for (int j = 0; j < 4; j++) {
-      if (!R.vh[j]) continue;
-      const float w = R.wh[j] / R.swh;
-      atomic_add4(T.dB3 + R.qh[j], make_float4(gill.x * w, gill.y * w, gill.z * w, 0.f));
+  if (in && gp.w >= 0.0f) {  // sky: X = emission, no dependence on the parameters
+    const int o = py * f.W + px;
+    const float4 gt = gT[o];
+    const float3 gX = SEED_TM ? tm_adjoint(T.X[o], gt) : make_float3(gt.x, gt.y, gt.z);
+    const float4 alb = ldh(f.mat, py * f.p_mat + px);
+    const float4 p0 = T.par[3 * hp], p1 = T.par[3 * hp + 1], p2 = T.par[3 * hp + 2];
+    Filt1<1, true, SW> F;
+    F.run(sA, sG, ti, px, py, f.W, f.H, p1.x, p2.x);
+    const float4 A1 = F.out();
+    Recomb R;
+    recomb_fwd(T, px, py, A1, gp, R);
+    float ix = R.fx, iy = R.fy, iz = R.fz;
+    const bool mid = R.swh > 1e-4f;
+    if (mid) {
+      ix = R.uBx / R.swh + p0.w * (R.fx - R.uAx / R.swh);
+      iy = R.uBy / R.swh + p0.w * (R.fy - R.uAy / R.swh);
+      iz = R.uBz / R.swh + p0.w * (R.fz - R.uAz / R.swh);
     }
+    // X = ill2 * alb + emi, ill2 = ill + (up - ill) beta
+    const float3 g2 = make_float3(gX.x * alb.x, gX.y * alb.y, gX.z * alb.z);
+    float3 gill = g2;
+    float gbeta = 0.0f;
+    if (R.swq > 1e-4f) {
+      const float upx = R.uCx / R.swq, upy = R.uCy / R.swq, upz = R.uCz / R.swq;
+      gbeta = g2.x * (upx - ix) + g2.y * (upy - iy) + g2.z * (upz - iz);
+      gill = make_float3(g2.x * (1.0f - p0.z), g2.y * (1.0f - p0.z), g2.z * (1.0f - p0.z));
+    }
+    float3 gf = gill;
+    float gkappa = 0.0f;
+    if (mid) {
+      gkappa = gill.x * (R.fx - R.uAx / R.swh) + gill.y * (R.fy - R.uAy / R.swh) + gill.z * (R.fz - R.uAz / R.swh);
+      gf = make_float3(gill.x * p0.w, gill.y * p0.w, gill.z * p0.w);
+      for (int j = 0; j < 4; j++) {
+        if (!R.vh[j]) continue;
+        const float w = R.wh[j] / R.swh;
+        float *d = &T.dB3[R.qh[j]].x;  // the level's variance gets no gradient from the recombination
+        atomicAdd(d, gill.x * w);
+        atomicAdd(d + 1, gill.y * w);
+        atomicAdd(d + 2, gill.z * w);
+      }
+    }
+    float ds, dc;
+    F.adjoint(sA, ti, gf, 0.0f, p1.x, ds, dc, nullptr, 0, 0);
+    q4[0] = gbeta; q4[1] = gkappa; q4[2] = ds; q4[3] = dc;
   }
-  float ds, dc;
-  F.adjoint(sA, ti, gf, 0.0f, p1.x, ds, dc, nullptr, 0, 0);
-  float *d0 = &T.dpar[3 * hp].x, *d1 = &T.dpar[3 * hp + 1].x, *d2 = &T.dpar[3 * hp + 2].x;
-  atomicAdd(d0 + 2, gbeta);
-  atomicAdd(d0 + 3, gkappa);
-  atomicAdd(d1 + 0, ds);
-  atomicAdd(d2 + 0, dc);
+  // the 2 x 2 pixels of a half-res block are lanes l, l ^ 1, l ^ 16 and l ^ 17 of one warp (16-pixel rows, even
+  // tile origin): their parameter gradients are summed in the warp and added once
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    q4[k] += __shfl_xor_sync(0xffffffffu, q4[k], 1);
+    q4[k] += __shfl_xor_sync(0xffffffffu, q4[k], 16);
+  }
+  if (in && !(threadIdx.x & 1) && !(threadIdx.y & 1) && (q4[0] != 0.f || q4[1] != 0.f || q4[2] != 0.f || q4[3] != 0.f)) {
+    float *d0 = &T.dpar[3 * hp].x, *d1 = &T.dpar[3 * hp + 1].x, *d2 = &T.dpar[3 * hp + 2].x;
+    atomicAdd(d0 + 2, q4[0]);
+    atomicAdd(d0 + 3, q4[1]);
+    atomicAdd(d1 + 0, q4[2]);
+    atomicAdd(d2 + 0, q4[3]);
+  }
 }
 
 // ------------------------------------------------------------------------------------------------ MLP adjoint
