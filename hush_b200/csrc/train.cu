@@ -51,8 +51,7 @@ struct TwinFrame {
   float lambda_t;         // weight of the temporal term
   int has_prev;
   float inv_n;            // 1 / (3 * pixels)
-  float4 *gtm;            // full: gradient scratch of the tone-mapped colour (TAA adjoint, scattered)
-  int zero_adj;           // forward kernels clear the adjoint accumulators (dpar, dB1..dB3, gtm) they precede
+  int zero_adj;           // forward kernels clear the adjoint accumulators (dpar, dB1..dB3) they precede
 };
 
 HD_INL float4 f3_guide_tw(const uint4 *F3, int i) {
@@ -471,7 +470,6 @@ __global__ void k_taa_fwd(const TwinFrame T) {
   TaaF A;
   taa_fwd(T, px, py, A);
   const int o = py * f.W + px;
-  if (T.zero_adj) T.gtm[o] = make_float4(0.f, 0.f, 0.f, 0.f);
   T.out[o] = make_float4(A.out.x, A.out.y, A.out.z, 1.0f);
   sth(f.taa, o, make_float4(A.out.x, A.out.y, A.out.z, 1.0f));
 }
@@ -537,8 +535,11 @@ __global__ void k_reduce_f64(const double *partials, int n, double *out, double 
 }
 
 // ------------------------------------------------------------------------------------------------ TAA adjoint
-// Pass 1 (per pixel p): from dL/dout (in gT[p], overwritten) to the gradients of tm(X) at the 3x3 window (clip box)
-// and at p (current colour); scattered into gT2.
+// In two gathers, without atomics. Pass 1 (per pixel p): from dL/dout to the per-pixel coefficients of the clip box's
+// adjoint, dL/d(window mean) gm and dL/d(window variance) gs per YCoCg channel, with the window mean m1, and the
+// gradient of the current colour tm(X_p) itself. Pass 2 (per pixel q): dL/d tm(X_q) as that own term plus, for every
+// pixel p whose clamped 3 x 3 window holds q (with the window's multiplicity at the image border), the YCoCg-adjoint
+// of gm_p / 9 + gs_p 2 (y_q - m1_p) / 9.
 HD_INL float3 itm_adjoint(const TaaF &A, float3 g) {
   const float inv = 1.0f / A.d;
   float3 r = make_float3(g.x * inv, g.y * inv, g.z * inv);
@@ -558,7 +559,8 @@ HD_INL float3 ycocg_adjoint(float3 g) {  // transpose of to_ycocg
   return make_float3(0.25f * g.x + 0.5f * g.y - 0.25f * g.z, 0.5f * g.x + 0.5f * g.z, 0.25f * g.x - 0.5f * g.y - 0.25f * g.z);
 }
 
-__global__ void k_taa_bwd(const TwinFrame T, const float4 *gout, float4 *gT) {
+// coef[3p .. 3p + 2] = (gm, gcur.x), (gs, gcur.y), (m1, gcur.z)
+__global__ void k_taa_bwd_coef(const TwinFrame T, const float4 *gout, float4 *coef) {
   const HushFrame &f = T.f;
   const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
   if (px >= f.W || py >= f.H) return;
@@ -568,30 +570,56 @@ __global__ void k_taa_bwd(const TwinFrame T, const float4 *gout, float4 *gT) {
   const float4 go = gout[o];
   const float3 gres = itm_adjoint(A, make_float3(go.x, go.y, go.z));
   float3 gcur = gres;
+  float gm[3] = {0.f, 0.f, 0.f}, gs[3] = {0.f, 0.f, 0.f};
   if (A.inside) {
     gcur = make_float3(0.1f * gres.x, 0.1f * gres.y, 0.1f * gres.z);
     const float3 ghr = make_float3(0.9f * gres.x, 0.9f * gres.y, 0.9f * gres.z);
     // from_ycocg transpose
     const float gh[3] = {ghr.x + ghr.y + ghr.z, ghr.x - ghr.z, -ghr.x + ghr.y - ghr.z};
-    float gm[3], gs[3];
-    const float v3[3] = {A.v3.x, A.v3.y, A.v3.z}, sd[3] = {A.sd.x, A.sd.y, A.sd.z}, m1[3] = {A.m1.x, A.m1.y, A.m1.z};
+    const float v3[3] = {A.v3.x, A.v3.y, A.v3.z}, sd[3] = {A.sd.x, A.sd.y, A.sd.z};
     for (int c = 0; c < 3; c++) {
       const float glo = A.lo_act[c] ? gh[c] : 0.0f, ghi = A.hi_act[c] ? gh[c] : 0.0f;
       gm[c] = glo + ghi;
       gs[c] = 1.25f * (ghi - glo);
       gs[c] = v3[c] > 1e-12f ? gs[c] / (2.0f * sd[c]) : 0.0f;  // d sd / d v3
     }
-    for (int j = 0; j < 9; j++) {
-      const float yy[3] = {A.y[j].x, A.y[j].y, A.y[j].z};
-      float3 gy;
-      gy.x = gm[0] / 9.0f + gs[0] * 2.0f * (yy[0] - m1[0]) / 9.0f;
-      gy.y = gm[1] / 9.0f + gs[1] * 2.0f * (yy[1] - m1[1]) / 9.0f;
-      gy.z = gm[2] / 9.0f + gs[2] * 2.0f * (yy[2] - m1[2]) / 9.0f;
-      const float3 gt = ycocg_adjoint(gy);
-      if (gt.x != 0.f || gt.y != 0.f || gt.z != 0.f) atomic_add4(gT + A.q[j], make_float4(gt.x, gt.y, gt.z, 0.f));
+  }
+  coef[3 * o] = make_float4(gm[0], gm[1], gm[2], gcur.x);
+  coef[3 * o + 1] = make_float4(gs[0], gs[1], gs[2], gcur.y);
+  coef[3 * o + 2] = make_float4(A.m1.x, A.m1.y, A.m1.z, gcur.z);
+}
+
+// how many of the clamped offsets p + d (d = -1, 0, 1) land on q
+HD_INL int window_hits(int p, int q, int n) {
+  return (clampi(p - 1, 0, n - 1) == q) + (p == q) + (clampi(p + 1, 0, n - 1) == q);
+}
+
+// gT[q] = dL/d tm(X_q) (set, not added)
+__global__ void k_taa_bwd_gather(const TwinFrame T, const float4 *coef, float4 *gT) {
+  const HushFrame &f = T.f;
+  const int qx = blockIdx.x * blockDim.x + threadIdx.x, qy = blockIdx.y * blockDim.y + threadIdx.y;
+  if (qx >= f.W || qy >= f.H) return;
+  const int o = qy * f.W + qx;
+  const float3 y = to_ycocg(tm3(T.X[o]));
+  float gx = coef[3 * o].w, gyy = coef[3 * o + 1].w, gz = coef[3 * o + 2].w;
+  for (int py = max(qy - 1, 0); py <= min(qy + 1, f.H - 1); py++) {
+    const int my = window_hits(py, qy, f.H);
+    if (!my) continue;
+    for (int px = max(qx - 1, 0); px <= min(qx + 1, f.W - 1); px++) {
+      const int m = my * window_hits(px, qx, f.W);
+      if (!m) continue;
+      const int p = py * f.W + px;
+      const float4 a = coef[3 * p], b = coef[3 * p + 1], c = coef[3 * p + 2];
+      float3 g;
+      g.x = a.x / 9.0f + b.x * 2.0f * (y.x - c.x) / 9.0f;
+      g.y = a.y / 9.0f + b.y * 2.0f * (y.y - c.y) / 9.0f;
+      g.z = a.z / 9.0f + b.z * 2.0f * (y.z - c.z) / 9.0f;
+      const float3 t = ycocg_adjoint(g);
+      const float k = (float)m;
+      gx += k * t.x; gyy += k * t.y; gz += k * t.z;
     }
   }
-  atomic_add4(gT + o, make_float4(gcur.x, gcur.y, gcur.z, 0.f));
+  gT[o] = make_float4(gx, gyy, gz, 0.f);
 }
 
 // dX += tm adjoint of the tone-mapped-colour gradient at every pixel (the per-pass TAA adjoint's second step; the fused
@@ -1129,7 +1157,7 @@ struct hush_trainer_s {
   float *theta = nullptr, *m = nullptr, *v = nullptr;
   double *grad = nullptr, *loss = nullptr, *loss_acc = nullptr, *loss_partials = nullptr;
   float4 *par = nullptr, *B[3] = {}, *A1 = nullptr, *X = nullptr, *out[2] = {}, *gT = nullptr, *gT2 = nullptr,
-         *dB[3] = {}, *dpar = nullptr, *dX = nullptr;
+         *dB[3] = {}, *dpar = nullptr, *dX = nullptr, *tcoef = nullptr;
   float *partials = nullptr;
   int n_mlp_ctas = 0, n_loss_ctas = 0;
   int cur = 0, has_prev = 0;
@@ -1172,7 +1200,7 @@ extern "C" int hush_trainer_create(hush_t *h, const float *theta, hush_trainer_t
   t->n_loss_ctas = (int)((full + 255) / 256);
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
   const size_t bytes = al(NW * 4) * 3 + al(NW * 8) + al(8) * 2 + al(t->n_loss_ctas * 8) + al(half * 48) * 2 +
-                       al(half * 16) * 6 + al(full * 16) * 7 + al((size_t)t->n_mlp_ctas * NW * 4);
+                       al(half * 16) * 6 + al(full * 16) * 7 + al(full * 48) + al((size_t)t->n_mlp_ctas * NW * 4);
   cudaError_t e = cudaMalloc(&t->pool, bytes);
   if (e != cudaSuccess) { delete t; return hush_cuda_fail(h, e, "cudaMalloc of the trainer"); }
   cudaMemset(t->pool, 0, bytes);
@@ -1186,6 +1214,7 @@ extern "C" int hush_trainer_create(hush_t *h, const float *theta, hush_trainer_t
   t->A1 = (float4 *)take(full * 16); t->X = (float4 *)take(full * 16);
   t->out[0] = (float4 *)take(full * 16); t->out[1] = (float4 *)take(full * 16);
   t->gT = (float4 *)take(full * 16); t->gT2 = (float4 *)take(full * 16); t->dX = (float4 *)take(full * 16);
+  t->tcoef = (float4 *)take(full * 48);
   t->partials = (float *)take((size_t)t->n_mlp_ctas * NW * 4);
   e = cudaMemcpy(t->theta, theta ? theta : h->wf.data(), NW * 4, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) { cudaFree(t->pool); delete t; return hush_cuda_fail(h, e, "cudaMemcpy of the weights"); }
@@ -1244,7 +1273,6 @@ static TwinFrame make_twin(hush_trainer_t *t, const hush_inputs *in, const float
   T.clean = clean;
   T.clean_prev = clean_prev;
   T.gT = t->gT;
-  T.gtm = t->gT2;
   T.zero_adj = 0;
   T.dB1 = t->dB[0]; T.dB2 = t->dB[1]; T.dB3 = t->dB[2];
   T.dpar = t->dpar;
@@ -1286,7 +1314,8 @@ extern "C" int hush_trainer_frame(hush_trainer_t *t, const hush_inputs *in, cons
   k_loss<<<t->n_loss_ctas, 256, 0, st>>>(T, backward);
   k_reduce_f64<<<1, 256, 0, st>>>(t->loss_partials, t->n_loss_ctas, t->loss, t->loss_acc);
   if (backward) {
-    k_taa_bwd<<<gf, blk, 0, st>>>(T, t->gT, t->gT2);
+    k_taa_bwd_coef<<<gf, blk, 0, st>>>(T, t->gT, t->tcoef);
+    k_taa_bwd_gather<<<gf, blk, 0, st>>>(T, t->tcoef, t->gT2);
     k_fine_bwd<true><<<gf, blk, 0, st>>>(T, t->gT2);
     k_mid_bwd<3><<<gh, blk, 0, st>>>(T);
     k_mid_bwd<2><<<gh, blk, 0, st>>>(T);
@@ -1681,8 +1710,8 @@ static int run_twin_pass(hush_trainer_t *t, int pass, int backward, void *stream
       if (!backward) {
         k_taa_fwd<<<gf, blk, 0, st>>>(T);
       } else {
-        e = cudaMemsetAsync(t->gT2, 0, (size_t)full * 16, st);
-        k_taa_bwd<<<gf, blk, 0, st>>>(T, t->gT, t->gT2);
+        k_taa_bwd_coef<<<gf, blk, 0, st>>>(T, t->gT, t->tcoef);
+        k_taa_bwd_gather<<<gf, blk, 0, st>>>(T, t->tcoef, t->gT2);
         k_tm_bwd<<<(full + 255) / 256, 256, 0, st>>>(T, t->gT2, t->dX);
       }
       break;
