@@ -156,7 +156,38 @@ def _cpu_baseline_sample(frames: int = 3):
         times.append(time.perf_counter() - t)
     ms = 1000.0 * statistics.mean(times[1:] if len(times) > 1 else times)
     return {"value": round(ms, 3), "unit": "ms/frame", "cores": cores, "kind": "port",
-            "sample": f"{frames} frames of the {W}x{H} sequence (frame 0 untimed), oracle f32, {cores} threads"}
+            "sample": f"{frames} frames of the {W}x{H} sequence (frame 0 untimed), oracle f32, {cores} threads",
+            "per_pass_ms": _cpu_per_pass_sizes()}
+
+
+def _cpu_per_pass_sizes():
+    out = {}
+    for w, h in ((W, H), (640, 360)):
+        try:
+            out[f"{w}x{h}"] = _cpu_per_pass(w, h)
+        except Exception as e:  # pragma: no cover - reported, not fatal
+            out[f"{w}x{h}"] = f"failed: {e}"
+    return out
+
+
+def _cpu_per_pass(w, h, warm=2, timed=5):
+    """The oracle's passes one by one (f32, all host threads): the median ms per pass over `timed` frames of the
+    sequence at w x h after `warm` frames."""
+    import oracle
+    from hush_b200 import builtin_weights, scene
+
+    cfg = scene.SceneConfig(w, h, warm + timed, n_moving=3, pan_min=0.0, pan_max=4.0, seed=_scene_cfg().seed)
+    o = oracle.OracleHush(w, h, builtin_weights())
+    per = {p: [] for p in oracle.PASS_NAMES}
+    for i in range(warm + timed):
+        f = scene.frame_host(cfg, i)
+        for p in oracle.PASS_NAMES:
+            t = time.perf_counter()
+            o.run_pass(p, f)
+            if i >= warm:
+                per[p].append(1000.0 * (time.perf_counter() - t))
+        o.end_frame()
+    return {p: round(statistics.median(v), 3) for p, v in per.items()}
 
 
 def run_reference(args):
