@@ -83,6 +83,8 @@ int hush_set_exposure(hush_t *h, float exposure);
 float hush_get_exposure(const hush_t *h);
 /* Replaces the MLP weights (same blob format as the constructor option). */
 int hush_set_weights(hush_t *h, const uint16_t *weights, size_t n);
+/* HUSH_MLP_*: the tensor-core forms run in the fused schedule's stage 0; the pass-by-pass schedule's INFER always
+ * computes the reference's FP32 form. */
 int hush_set_mlp_mode(hush_t *h, int mode);
 int hush_set_schedule(hush_t *h, int schedule);
 int hush_get_size(const hush_t *h, int *width, int *height);
