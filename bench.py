@@ -376,7 +376,12 @@ def run_ours(args):
         ach = per_stage[dominant]["gbs"]
         roof = {"kernel": dominant, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                 "frac": round(ach / peak, 4), "peak_source": peak_kind,
-                "traffic": (tr or {}).get("bytes_per_launch"),
+                # the captures are of 1920 x 1080 launches; other sizes scale them by the pixels processed (the
+                # kernels stream their images, so DRAM bytes grow in proportion)
+                "traffic": (round(tr["bytes_per_launch"] * P / (1920 * 1080)) if tr and "bytes_per_launch" in tr
+                            else None),
+                "traffic_source": (("ncu capture at 1920x1080" if P == 1920 * 1080
+                                    else "ncu capture at 1920x1080 scaled by the pixel count") if tr else None),
                 "algorithmic_bytes_per_launch": per_stage[dominant]["bytes"]}
     filt_bytes = sum(v["bytes"] for v in per_stage.values() if v["bytes"])
     filt_ms = sum(v["ms"] for v in per_stage.values())

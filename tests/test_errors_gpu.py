@@ -113,3 +113,39 @@ def test_mlp_forms_at_1080p_against_fp64_and_clean():
     assert np.mean(rows["bf16"]) <= np.mean(rows["fp32"]) * 1.01
     assert abs(np.mean(rows["fp32"]) - np.mean(rows["oracle_f64"])) <= 1e-3
     assert stats["fp32"][0].max() <= 1e-3 and stats["f16"][0].max() <= 5e-3 and stats["bf16"][0].max() <= 5e-2
+
+
+def test_4k_bf16_against_fp32_and_clean():
+    """The 3840x2160 configuration (32 objects, 8 moving, 20% sky, pan U[0,6] px/frame, 2% fireflies x100), every
+    frame replayed as one CUDA graph: the BF16 tensor-core form against the FP32 plain form and both against the
+    noise-free radiance over 6 frames."""
+    cfg = scene.CONFIG_4K
+    W, H = cfg.width, cfg.height
+    forms = {m: Hush(0, {"width": W, "height": H, "mlp": m, "graph": True}) for m in ("fp32", "bf16")}
+    rel = {m: [] for m in forms}
+    flick = {m: [] for m in forms}
+    diff = []
+    prev, prev_clean = {}, None
+    for i in range(6):
+        fr = scene.frame_device(cfg, i, clean=True)
+        outs = {m: g.denoise(fr).float()[..., :3].clone() for m, g in forms.items()}
+        torch.cuda.synchronize()
+        a, b = outs["bf16"].cpu().numpy(), outs["fp32"].cpu().numpy()
+        diff.append((mismatch(a, b)[0], mismatch(a, b, rel=5e-2)[0]))
+        if i > 0:
+            for m in forms:
+                rel[m].append(_clipped_rel(outs[m], fr["clean"]))
+                flick[m].append(_flicker(outs[m], prev[m], fr["clean"], prev_clean))
+        prev, prev_clean = outs, fr["clean"]
+    print(f"\n3840x2160, frames 1..5")
+    print("| form | clipped rel-L1 to clean | temporal flicker |")
+    print("|---|---|---|")
+    for m in forms:
+        print(f"| {m} | {np.mean(rel[m]):.4f} | {np.mean(flick[m]):.4f} |")
+    print(f"BF16 against FP32: values beyond 2e-3 rel. {np.mean([d[0] for d in diff]):.2e} (mean over frames), "
+          f"beyond 5e-2 {np.mean([d[1] for d in diff]):.2e}")
+    for g in forms.values():
+        assert g.kernel_status() == 0
+        g.destroy()
+    assert np.mean(rel["bf16"]) <= np.mean(rel["fp32"]) * 1.01
+    assert max(d[1] for d in diff) <= 1e-2
