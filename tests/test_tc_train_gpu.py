@@ -102,3 +102,17 @@ def test_a_wait_that_runs_out_is_reported_not_hung():
     out = g.denoise(_dev(scene.frame_host(cfg, 0)))
     torch.cuda.synchronize()
     assert torch.isfinite(out.float()).all()
+
+
+def test_window_and_form_arguments_are_checked():
+    from hush_b200.train import TrainConfig, window_scene
+
+    g = Hush(0, {"width": 64, "height": 64, "schedule": "passes"})
+    tr = Trainer(g, xavier_init(0))
+    with pytest.raises(HushError, match="scene size differs"):
+        tr.windows(window_scene(TrainConfig(size=32, frames=2)), [1], 2, 0.5)
+    with pytest.raises(HushError, match="empty batch"):
+        tr.windows(window_scene(TrainConfig(size=64, frames=2)), [], 2, 0.5)
+    assert L.lib().hush_trainer_set_mlp(tr._t, 7) == L.HUSH_ERR_ARG
+    tr.windows(window_scene(TrainConfig(size=64, frames=2)), [3, 4], 2, 0.5)  # still usable
+    assert np.isfinite(tr.loss_sum()) and np.abs(tr.grad()).max() > 0
