@@ -11,8 +11,9 @@ before timing, so the timed region starts with them resident in HBM; every frame
 ~230 MB of state, more than the 126 MB L2, so no L2 flush is needed between frames. --workload 4k runs the 3840x2160
 workload instead (BF16 MLP, one graph per frame).
 
-Prints one JSON line (rank 0). For N > 1 (torchrun), every rank denoises its own independent sequence on its own GPU
-(replicas: the path has no cross-GPU exchange); value = total frames / max-over-ranks time.
+Prints one JSON line (rank 0). For N > 1 every rank denoises its own independent sequence on its own GPU (replicas:
+the path has no cross-GPU exchange); value = max-over-ranks time / total frames. `--gpus N` under torchrun uses its
+ranks; without one, bench.py starts the N ranks itself through torch.distributed.run.
 """
 from __future__ import annotations
 
@@ -30,8 +31,14 @@ sys.path.insert(0, ROOT)
 
 METRIC = "1080p ms/frame + %HBM roofline, BF16-MLP vs FP32 plain; train-step ms at equal error"
 W, H, SEQ = 1920, 1080, 64
-WORKLOAD = ("1920x1080 64-frame sequence, 3 moving objects, pan U[0,4] px/frame, cut at 32 (reset); inputs generated "
-            "on the device")
+WORKLOAD = "1920x1080 64-frame sequence, 3 moving objects, pan U[0,4] px/frame, cut at 32 (reset)"
+L2_NOTE = "no flush: each frame reads 83 MB of fresh inputs + ~230 MB of state (> 126 MB L2)"
+
+
+def _config(mlp: str, world: int) -> dict:
+    """The workload as both arms print it (implementation details such as the schedule go in "setup")."""
+    return {"workload": WORKLOAD, "width": W, "height": H, "mlp": mlp, "l2": L2_NOTE,
+            "parallelism": f"replicas x{world}"}
 
 
 def _scene_cfg():
@@ -142,15 +149,14 @@ def _cpu_baseline_sample(frames: int = 3):
     import numpy as np  # noqa: F401
 
     import oracle
-    from hush_b200 import builtin_weights, scene
 
     oracle.set_threads(0)
     cores = os.cpu_count() or 1
     cfg = _scene_cfg()
-    o = oracle.OracleHush(W, H, builtin_weights())
+    o = oracle.OracleHush(W, H, oracle.builtin_weights())
     times = []
     for i in range(frames):
-        f = scene.frame_host(cfg, i)
+        f = oracle.scene_frame(cfg, i)
         t = time.perf_counter()
         o.denoise(f)
         times.append(time.perf_counter() - t)
@@ -174,13 +180,12 @@ def _cpu_per_pass(w, h, warm=2, timed=5):
     """The oracle's passes one by one (f32, all host threads): the median ms per pass over `timed` frames of the
     sequence at w x h after `warm` frames."""
     import oracle
-    from hush_b200 import builtin_weights, scene
 
-    cfg = scene.SceneConfig(w, h, warm + timed, n_moving=3, pan_min=0.0, pan_max=4.0, seed=_scene_cfg().seed)
-    o = oracle.OracleHush(w, h, builtin_weights())
+    cfg = _scene_cfg().with_(width=w, height=h, frames=warm + timed, cut_frame=-1)
+    o = oracle.OracleHush(w, h, oracle.builtin_weights())
     per = {p: [] for p in oracle.PASS_NAMES}
     for i in range(warm + timed):
-        f = scene.frame_host(cfg, i)
+        f = oracle.scene_frame(cfg, i)
         for p in oracle.PASS_NAMES:
             t = time.perf_counter()
             o.run_pass(p, f)
@@ -194,13 +199,12 @@ def run_reference(args):
     rank, _, world = _env_rank()
     if rank != 0:
         return 0
-    import oracle
-    from hush_b200 import builtin_weights, scene
+    import oracle  # the CPU arm loads only the oracle library: frames, weights and passes all come from it
 
     oracle.set_threads(0)
     cores = os.cpu_count() or 1
     cfg = _scene_cfg()
-    o = oracle.OracleHush(W, H, builtin_weights())
+    o = oracle.OracleHush(W, H, oracle.builtin_weights())
     # bounded sample: the CPU takes ~0.3 s per 1080p frame, so at most 2 warm-up and 24 timed frames
     warm, steps = min(args.warmup, 2), min(args.steps, 24)
     n = warm + steps
@@ -209,7 +213,7 @@ def run_reference(args):
     for i in range(n):
         k = i % SEQ
         if k not in frames:
-            frames[k] = scene.frame_host(cfg, k)
+            frames[k] = oracle.scene_frame(cfg, k)
         if k == 32 or (k == 0 and i > 0):
             o.reset()
         t = time.perf_counter()
@@ -223,10 +227,11 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": round(ms, 3), "unit": "ms/frame", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "1920x1080 64-frame sequence, 3 moving objects, pan U[0,4] px/frame, cut at 32",
-                   "width": W, "height": H, "mlp": "fp32"},
+        "config": _config(args.mlp, world),
+        "setup": {"inputs": "generated on the host by the oracle library before each frame's timing",
+                  "arithmetic": "f32 oracle, OpenMP over rows"},
         "cpu_baseline": {"value": round(ms, 3), "unit": "ms/frame", "cores": cores, "kind": "port",
-                         "sample": f"{steps} full 1920x1080 frames of the sequence after {warm} warm-up frames; the "
+                         "sample": f"{steps} full {W}x{H} frames of the sequence after {warm} warm-up frames; the "
                                    "reference's WGSL cannot run here (no WebGPU / Dawn / node), its scalar "
                                    "restatement (oracle/) stands in"},
         "e2e": {"value": round(ms, 3), "unit": "ms/frame", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -393,10 +398,9 @@ def run_ours(args):
         "metric": METRIC, "value": round(ms_frame / world, 4), "unit": "ms/frame", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_frame, 4), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD,
-                   "width": W, "height": H, "mlp": args.mlp, "schedule": args.schedule, "graph": bool(args.graph),
-                   "l2": "no flush: each frame reads 83 MB of fresh inputs + ~230 MB of state (> 126 MB L2)",
-                   "parallelism": f"replicas x{world}"},
+        "config": _config(args.mlp, world),
+        "setup": {"inputs": "generated on the device before timing", "schedule": args.schedule,
+                  "graph": bool(args.graph)},
         "roofline": roof,
         "frame_hbm": {"bytes_per_frame": filt_bytes, "sum_stage_ms": round(filt_ms, 4),
                       "gbs": round(filt_bytes / (filt_ms * 1e-3) / 1e9, 1) if filt_ms else None,
@@ -548,6 +552,8 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-train", action="store_true", help="skip the training-step timing")
     ap.add_argument("--no-extras", action="store_true", help="skip the SVGF / path tracer / post timings")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="run only the rank plumbing on the CPU (gloo) and print the rank fields of the line")
     ap.add_argument("--workload", default="1080p", choices=["1080p", "4k"],
                     help="4k: the 3840x2160 workload (32 objects, 8 moving, 20%% sky, pan U[0,6], 2%% fireflies x100) "
                          "with the BF16 MLP and each frame replayed as one CUDA graph")
@@ -562,9 +568,49 @@ def main(argv=None):
             args.mlp = "bf16"
         args.graph = True
         args.no_train = True
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return _launch_ranks(args.gpus, list(sys.argv[1:] if argv is None else argv))
+    if args.dry_run:
+        return run_dry(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
+
+
+def _launch_ranks(n: int, argv) -> int:
+    """`bench.py --gpus N` without an outer torchrun: re-run this script as N ranks on this node (one process per GPU,
+    rendezvous on 127.0.0.1), bounded by `timeout -k 60` well above the run's own process-group timeouts."""
+    import socket
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = ["timeout", "-k", "60", "3600", sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={n}", "--master-addr", "127.0.0.1", f"--master-port={port}",
+           os.path.abspath(__file__)] + argv
+    return subprocess.call(cmd)
+
+
+def run_dry(args) -> int:
+    """--dry-run: the rank plumbing alone, on the CPU (gloo): every rank joins, one all-reduce counts them, rank 0
+    prints the line's rank fields. No GPU work."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    rank, _, world = _env_rank()
+    if world > 1:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    t = torch.ones(1)
+    if world > 1:
+        dist.all_reduce(t)
+    if rank == 0:
+        print(json.dumps({"dry_run": True, "impl": args.impl, "metric": METRIC, "n_gpus": world,
+                          "ranks_joined": int(t.item()), "config": _config(args.mlp, world)}), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
 
 
 if __name__ == "__main__":

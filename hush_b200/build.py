@@ -76,7 +76,7 @@ def _run(cmd, verbose):
 
 def build_oracle(force: bool = False, verbose: bool = False) -> str:
     src = [os.path.join(ORACLE_DIR, f) for f in os.listdir(ORACLE_DIR) if f.endswith((".cpp", ".h"))]
-    src.append(os.path.join(ORACLE_DIR, "Makefile"))
+    src += [os.path.join(ORACLE_DIR, "Makefile"), os.path.join(CSRC, "scene.h")]
     if force or not os.path.exists(ORACLE_LIB) or _newest(src) > os.path.getmtime(ORACLE_LIB):
         _run(["make", "-C", ORACLE_DIR, "-B" if force else "-s", "liboracle_hush.so"], verbose)
     return ORACLE_LIB

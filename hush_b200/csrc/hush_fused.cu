@@ -589,6 +589,14 @@ struct HalfMaps {
   int qok;                         // the same for the quarter-resolution maps (odd W4)
 };
 constexpr uint32_t TMA_POLLS = 1u << 22;
+// Waits (bounded) for a halo tile's TMA copies. On giving up it sets bit 3 of the error word and returns false: the
+// caller then fills its tile with the plain clamped loads, so the output stays defined. Interior tiles need no
+// clamping, so a copy that still lands later writes the very values those loads wrote.
+HD_INL bool tma_wait_or_flag(const HushFrame &f, uint32_t mb) {
+  if (umma::mbar_wait_bounded(mb, 0, TMA_POLLS)) return true;
+  atomicOr(f.err, 8u);
+  return false;
+}
 // FINE_FINAL's A0 / key tiles (8-byte texels, 2-d UINT64 maps {W, H}) on interior tiles: the copies start at
 // x = bx - 2 (even, so 16-byte aligned) with a 36 x 10 box; the tile's column c is the box's column c + 1.
 struct FineMaps {
@@ -624,6 +632,7 @@ HD_INL void tile_mid1(const HushFrame &f, int tileX, int tileY, float4 *sA, floa
   const int li = threadIdx.x;
   const int bx = tileX * HT_W, by = tileY * HT_H;
   const bool inner = M && bx - 2 >= 0 && by - 1 >= 0 && bx + HT_W + 2 <= f.W2 && by + HT_H + 1 <= f.H2;
+  bool staged = false;
   if (inner) {
     const uint32_t mb = umma::smem_u32(&mbar);
     if (li == 0) umma::mbar_init(mb, 1);
@@ -633,9 +642,11 @@ HD_INL void tile_mid1(const HushFrame &f, int tileX, int tileY, float4 *sA, floa
       tma_load_2d(umma::smem_u32(stage), &M->ah, bx - 2, by - 1, mb);
       tma_load_3d(umma::smem_u32(sG), &M->gd1, 0, bx - 1, by - 1, mb);
     }
-    if (!umma::mbar_wait_bounded(mb, 0, TMA_POLLS)) atomicOr(f.err, 8u);
-    for (int i = li; i < SW * SH; i += HT_W * HT_H) sA[i] = h4_to_f4(stage[(i / SW) * BW + i % SW + 1]);
-  } else {
+    staged = tma_wait_or_flag(f, mb);
+    if (staged)
+      for (int i = li; i < SW * SH; i += HT_W * HT_H) sA[i] = h4_to_f4(stage[(i / SW) * BW + i % SW + 1]);
+  }
+  if (!staged) {
     for (int i = li; i < SW * SH; i += HT_W * HT_H) {
       const int q = clampi(by - AP + i / SW, 0, f.H2 - 1) * f.W2 + clampi(bx - AP + i % SW, 0, f.W2 - 1);
       sA[i] = ldh(f.Ah, q);
@@ -661,6 +672,7 @@ HD_INL void tile_mid(const HushFrame &f, int tileX, int tileY, const uint2 *src,
   const int li = threadIdx.x;
   const int bx = tileX * HT_W, by = tileY * HT_H;
   const bool inner = mg && bx - AP >= 0 && by - AP >= 0 && bx + HT_W + AP <= f.W2 && by + HT_H + AP <= f.H2;
+  bool staged = false;
   if (inner) {
     const uint32_t mb = umma::smem_u32(&mbar);
     if (li == 0) umma::mbar_init(mb, 1);
@@ -670,9 +682,11 @@ HD_INL void tile_mid(const HushFrame &f, int tileX, int tileY, const uint2 *src,
       tma_load_2d(umma::smem_u32(stage), ms, bx - AP, by - AP, mb);
       tma_load_3d(umma::smem_u32(sG), mg, 0, bx - AP, by - AP, mb);
     }
-    if (!umma::mbar_wait_bounded(mb, 0, TMA_POLLS)) atomicOr(f.err, 8u);
-    for (int i = li; i < SW * SH; i += HT_W * HT_H) sA[i] = h4_to_f4(stage[i]);
-  } else {
+    staged = tma_wait_or_flag(f, mb);
+    if (staged)
+      for (int i = li; i < SW * SH; i += HT_W * HT_H) sA[i] = h4_to_f4(stage[i]);
+  }
+  if (!staged) {
     for (int i = li; i < SW * SH; i += HT_W * HT_H) {
       const int q = clampi(by - AP + i / SW, 0, f.H2 - 1) * f.W2 + clampi(bx - AP + i % SW, 0, f.W2 - 1);
       sA[i] = ldh(src, q);
@@ -752,6 +766,7 @@ HD_INL void tile_coarse2(const HushFrame &f, int tileX, int tileY, float4 *sA, f
   const int li = threadIdx.x;
   const int bx = tileX * HT_W, by = tileY * HT_H;
   const bool inner = M && bx - AP >= 0 && by - AP >= 0 && bx + HT_W + AP <= f.W4 && by + HT_H + AP <= f.H4;
+  bool staged = false;
   if (inner) {
     const uint32_t mb = umma::smem_u32(&mbar);
     if (li == 0) umma::mbar_init(mb, 1);
@@ -761,9 +776,11 @@ HD_INL void tile_coarse2(const HushFrame &f, int tileX, int tileY, float4 *sA, f
       tma_load_2d(umma::smem_u32(stage), &M->c1, bx - AP, by - AP, mb);
       tma_load_3d(umma::smem_u32(sG), &M->cgd, 0, bx - AP, by - AP, mb);
     }
-    if (!umma::mbar_wait_bounded(mb, 0, TMA_POLLS)) atomicOr(f.err, 8u);
-    for (int i = li; i < SW * SH; i += HT_W * HT_H) sA[i] = h4_to_f4(stage[i]);
-  } else {
+    staged = tma_wait_or_flag(f, mb);
+    if (staged)
+      for (int i = li; i < SW * SH; i += HT_W * HT_H) sA[i] = h4_to_f4(stage[i]);
+  }
+  if (!staged) {
     for (int i = li; i < SW * SH; i += HT_W * HT_H) {
       const int q = clampi(by - AP + i / SW, 0, f.H4 - 1) * f.W4 + clampi(bx - AP + i % SW, 0, f.W4 - 1);
       sA[i] = ldh(f.C1, q);
@@ -846,18 +863,21 @@ __global__ void __launch_bounds__(FT_W *FT_H, 3) k_fine_final_fused(const __grid
     const float4 p0 = ldh(f.par0, hq);
     sPar[i] = make_float4(ldh(f.par1, hq).x, ldh(f.par2, hq).x, p0.z, p0.w);  // s0, c0, beta, kappa
   }
+  bool staged = false;
   if (inner) {
     __syncthreads();  // the mbarrier's initialisation, before anyone waits on it
-    if (!umma::mbar_wait_bounded(mb, 0, TMA_POLLS)) atomicOr(f.err, 8u);
-    for (int i = li; i < SW * SH; i += FT_W * FT_H) {
-      const int t = (i / SW) * FB_W + i % SW + 1;
-      sA[i] = h4_to_f4(stA[t]);
-      const float4 k = h4_to_f4(stK[t]);
-      float4 g = oct_dec(k.x, k.y);
-      g.w = k.z;
-      sG[i] = g;
-    }
-  } else {
+    staged = tma_wait_or_flag(f, mb);
+    if (staged)
+      for (int i = li; i < SW * SH; i += FT_W * FT_H) {
+        const int t = (i / SW) * FB_W + i % SW + 1;
+        sA[i] = h4_to_f4(stA[t]);
+        const float4 k = h4_to_f4(stK[t]);
+        float4 g = oct_dec(k.x, k.y);
+        g.w = k.z;
+        sG[i] = g;
+      }
+  }
+  if (!staged) {
     for (int i = li; i < SW * SH; i += FT_W * FT_H) {
       const int q = clampi(by - AP + i / SW, 0, f.H - 1) * f.W + clampi(bx - AP + i % SW, 0, f.W - 1);
       sA[i] = ldh(f.A0, q);

@@ -1809,23 +1809,24 @@ constexpr int NA_ROWS = 64;                 // rows per chunk (one thread per ro
 constexpr int NA_MAX_CTAS = 512;            // CTAs, hence partial sums, at most
 constexpr long NA_MAX_ROWS = 16L << 20;     // 16,777,216 rows: a 4096 x 4096 half-resolution image
 
-// 512 partial sums x 812 floats = 1.66 MB, shared by every call on the device.
-static __device__ __align__(256) float g_noalloc_partials[NA_MAX_CTAS * NW];
+// 512 partial sums x 812 doubles = 3.33 MB, shared by every call on the device.
+static __device__ __align__(256) double g_noalloc_partials[NA_MAX_CTAS * NW];
 
 // Grid-stride over chunks of NA_ROWS rows; each CTA keeps its parameter sums in registers (thread t owns parameters
 // t, t + 64, ...) and writes them once to partials[blockIdx.x]: every slot the reduction reads is overwritten first,
-// so nothing has to start at zero.
+// so nothing has to start at zero. A chunk's 64 rows are summed in FP32 (as the trainer sums its 128-row CTAs), the
+// chunks of a CTA in FP64, so the error does not grow with the number of chunks a CTA takes.
 __global__ void __launch_bounds__(NA_ROWS) k_mlp_grad_noalloc(const uint4 *F0, const uint4 *F1, const uint4 *F2,
                                                               const uint4 *F3, const float4 *dpar, const float *theta,
-                                                              int rows, float *partials) {
+                                                              int rows, double *partials) {
   __shared__ float th[NW];
   __shared__ float sd3[12][NA_ROWS], sd2[16][NA_ROWS], sd1[16][NA_ROWS], sf[20][NA_ROWS], sh1[16][NA_ROWS],
       sh2[16][NA_ROWS];
   for (int i = threadIdx.x; i < NW; i += NA_ROWS) th[i] = theta[i];
   constexpr int PER = (NW + NA_ROWS - 1) / NA_ROWS;  // 13 parameters per thread
-  float acc[PER];
+  double acc[PER];
 #pragma unroll
-  for (int k = 0; k < PER; k++) acc[k] = 0.0f;
+  for (int k = 0; k < PER; k++) acc[k] = 0.0;
   HushFrame f;
   f.F0 = const_cast<uint4 *>(F0); f.F1 = const_cast<uint4 *>(F1); f.F2 = const_cast<uint4 *>(F2);
   __syncthreads();
@@ -1845,6 +1846,10 @@ __global__ void __launch_bounds__(NA_ROWS) k_mlp_grad_noalloc(const uint4 *F0, c
       const float4 q0 = dpar[3 * o], q1 = dpar[3 * o + 1], q2 = dpar[3 * o + 2];
       float4 p0, p1, p2;
       mlp_heads(out, p0, p1, p2);
+      // the heads' adjoint as k_mlp_bwd forms it, alpha and gamma seeds included
+      const float sa = sigmoidf_(out[0]), sg = sigmoidf_(out[1]);
+      d3[0] = q0.x * (31.0f / 32.0f) * sa * (1.0f - sa);
+      d3[1] = q0.y * 7.5f * sg * (1.0f - sg);
       d3[2] = q0.z * p0.z * (1.0f - p0.z);
       d3[3] = q0.w * p0.w * (1.0f - p0.w);
       const float ps[4] = {p1.x, p1.y, p1.z, p1.w}, pc[4] = {p2.x, p2.y, p2.z, p2.w};
@@ -1890,7 +1895,7 @@ __global__ void __launch_bounds__(NA_ROWS) k_mlp_grad_noalloc(const uint4 *F0, c
       float a = 0.f;
       if (xv) for (int j = 0; j < NA_ROWS; j++) a += dv[j] * xv[j];
       else for (int j = 0; j < NA_ROWS; j++) a += dv[j];
-      acc[k] += a;
+      acc[k] += (double)a;
     }
     __syncthreads();
   }
@@ -1902,11 +1907,11 @@ __global__ void __launch_bounds__(NA_ROWS) k_mlp_grad_noalloc(const uint4 *F0, c
 }
 
 // dtheta = sum over the grid's partials, in FP64 (overwrites dtheta)
-__global__ void k_mlp_grad_noalloc_reduce(const float *partials, int nparts, double *dtheta) {
+__global__ void k_mlp_grad_noalloc_reduce(const double *partials, int nparts, double *dtheta) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= NW) return;
   double a = 0.0;
-  for (int c = 0; c < nparts; c++) a += (double)partials[(size_t)c * NW + p];
+  for (int c = 0; c < nparts; c++) a += partials[(size_t)c * NW + p];
   dtheta[p] = a;
 }
 
@@ -1918,7 +1923,7 @@ __global__ void k_mlp_grad_noalloc_reduce(const float *partials, int nparts, dou
 // Host-side address of g_noalloc_partials per device: the symbol's name in host code is only a stand-in, so the
 // device address is looked up once per device (with that device current) and cached.
 static std::mutex g_noalloc_mu;
-static float *g_noalloc_ptr[64] = {};
+static double *g_noalloc_ptr[64] = {};
 
 extern "C" int hush_mlp_grad_noalloc(const void *F0, const void *F1, const void *F2, const void *F3,
                                      const float *dpar, const float *theta, int width2, int height2, double *dtheta,
@@ -1939,14 +1944,14 @@ extern "C" int hush_mlp_grad_noalloc(const void *F0, const void *F1, const void 
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return hush_cuda_fail(nullptr, e, "cudaGetDevice");
   if (dev < 0 || dev >= 64) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_mlp_grad_noalloc: device ordinal >= 64");
-  float *partials = nullptr;
+  double *partials = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     if (!g_noalloc_ptr[dev]) {
       void *p = nullptr;
       e = cudaGetSymbolAddress(&p, g_noalloc_partials);
       if (e != cudaSuccess) return hush_cuda_fail(nullptr, e, "cudaGetSymbolAddress of the fixed scratch");
-      g_noalloc_ptr[dev] = (float *)p;
+      g_noalloc_ptr[dev] = (double *)p;
     }
     partials = g_noalloc_ptr[dev];
   }

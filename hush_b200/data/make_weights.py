@@ -26,4 +26,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python hush_b200/data/make_weights.py <path to the reference checkout>")
+    main(sys.argv[1])

@@ -28,8 +28,11 @@ class DataParallel:
         return np.random.default_rng([int(base_seed), self.rank])
 
     def window_seed(self, rng: np.random.Generator, n_seeds: int) -> int:
-        """A seed in [0, n_seeds) congruent to this rank modulo world."""
-        per = max(n_seeds // self.world, 1)
+        """A seed in [0, n_seeds) congruent to this rank modulo world. Needs n_seeds >= world: with fewer seeds than
+        ranks some rank would have no seed of its own."""
+        if n_seeds < self.world:
+            raise ValueError(f"window_seed: {n_seeds} seeds cannot give each of {self.world} ranks its own")
+        per = (n_seeds - self.rank + self.world - 1) // self.world  # seeds congruent to rank in [0, n_seeds)
         return int(rng.integers(0, per)) * self.world + self.rank
 
     def average_(self, *tensors) -> None:

@@ -283,11 +283,13 @@ int hush_loss_bwd(hush_trainer_t *t, void *stream);
 
 /* Weight gradient of the parameter MLP (812 doubles in dtheta, overwritten) from a half-resolution image of rows:
  * packed features F0..F3 (16-byte texels, width2 x height2, as hush_buffer returns them), dL/dpar (12 floats per
- * row, as hush_trainer_par lays them out) and FP32 weights theta (812). The same computation as the weight-gradient
- * part of hush_trainer_frame, but it allocates nothing: no counterpart in the reference. It exists for callers that
- * cannot allocate device memory after start-up (a render or training loop with a fixed memory budget, where an
- * allocation would synchronise the device or fail mid-frame) or that only lend the library buffers they own. Its
- * scratch is a fixed 1.66 MB device array (512 partial sums) that every GPU loading the library holds until exit;
+ * row, as hush_trainer_par lays them out, all 12 channels honoured) and FP32 weights theta (812). The same
+ * computation as hush_mlp_bwd's weight gradient, but it allocates nothing: no counterpart in the reference. It
+ * exists for callers that cannot allocate device memory after start-up (a render or training loop with a fixed
+ * memory budget, where an allocation would synchronise the device or fail mid-frame) or that only lend the library
+ * buffers they own. Rows are summed in FP32 over chunks of 64 and the chunks in FP64, so the rounding error stays
+ * that of a 64-row FP32 sum at every size. Its scratch is a fixed 3.33 MB device array (512 FP64 partial sums) that
+ * every GPU loading the library holds until exit;
  * at most 16,777,216 rows (4096 x 4096) are accepted, larger sizes fail with HUSH_ERR_ARG. The first call on a device
  * looks up that array's device address, so make it before any stream capture. Calls share the array: calls that
  * overlap on the GPU (different streams, or different threads) race. Errors: hush_global_error(). */

@@ -42,7 +42,15 @@ class _PostArgs(C.Structure):
                 ("vignette", C.c_float), ("same", C.c_int)]
 
 
+class _SceneDesc(C.Structure):  # hs_desc of hush_b200/csrc/scene.h
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("n_objects", C.c_int), ("n_moving", C.c_int),
+                ("sky_frac", C.c_float), ("pan_min", C.c_float), ("pan_max", C.c_float), ("yaw_deg", C.c_float),
+                ("firefly_rate", C.c_float), ("firefly_scale", C.c_float), ("cut_frame", C.c_int),
+                ("seed", C.c_uint32)]
+
+
 POST_LEVELS = 6
+WEIGHTS_PATH = os.path.join(os.path.dirname(HERE), "hush_b200", "data", "hush-weights.bin")
 _lib = None
 
 
@@ -75,6 +83,8 @@ def lib():
             "ho_svgf_encode": (P, [P, C.POINTER(_SvgfInputs)]),
             "ho_post_level_size": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
             "ho_post": (C.c_int, [C.POINTER(_PostArgs), P, P, P, P]),
+            "ho_f2h_rne": (C.c_uint16, [C.c_float]),
+            "ho_scene_frame": (C.c_int, [C.POINTER(_SceneDesc), C.c_int, P, P, P, P, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -174,6 +184,31 @@ class OracleSVGF:
                 self._h = None
         except Exception:  # interpreter shutdown
             pass
+
+
+def builtin_weights() -> np.ndarray:
+    """The reference's built-in weight blob (812 f16 values), read from the data file."""
+    return np.fromfile(WEIGHTS_PATH, dtype="<u2")
+
+
+def scene_frame(cfg, frame: int, clean: bool = False) -> dict:
+    """One frame of a synthetic G-buffer sequence (cfg: any object with SceneConfig's fields), generated on the host
+    by the oracle library's build of the generator: five (H, W, 4) float16 arrays (+ 'clean' (H, W, 3) float32)."""
+    H, W = cfg.height, cfg.width
+    bufs = {n: np.empty((H, W, 4), dtype=np.float16) for n in INPUTS}
+    cl = np.empty((H, W, 3), dtype=np.float32) if clean else None
+    d = _SceneDesc(W, H, cfg.n_objects, cfg.n_moving, cfg.sky_frac, cfg.pan_min, cfg.pan_max, cfg.yaw_deg,
+                   cfg.firefly_rate, cfg.firefly_scale, cfg.cut_frame, cfg.seed & 0xFFFFFFFF)
+    if lib().ho_scene_frame(C.byref(d), int(frame), *[bufs[n].ctypes.data for n in INPUTS],
+                            cl.ctypes.data if clean else None) != 0:
+        raise RuntimeError("scene generation failed")
+    if clean:
+        bufs["clean"] = cl
+    return bufs
+
+
+def f2h_rne(x: float) -> int:
+    return int(lib().ho_f2h_rne(float(x)))
 
 
 def f2h_rz(x: float) -> int:

@@ -137,3 +137,15 @@ def test_single_process_is_a_no_op():
     assert dp.max_divergence(t) == 0.0
     rng = dp.seed_rng(3)
     assert all(0 <= dp.window_seed(rng, 10) < 10 for _ in range(50))
+
+
+def test_window_seeds_cover_each_residue_class_and_need_one_seed_per_rank():
+    dp = DataParallel()
+    for rank, world, n in ((0, 3, 10), (1, 3, 10), (2, 3, 10), (3, 4, 4)):
+        dp.rank, dp.world = rank, world
+        rng = np.random.default_rng(rank)
+        got = {dp.window_seed(rng, n) for _ in range(400)}
+        assert got == {s for s in range(n) if s % world == rank}
+    dp.rank, dp.world = 2, 4
+    with pytest.raises(ValueError, match="cannot give each of 4 ranks"):
+        dp.window_seed(np.random.default_rng(0), 3)

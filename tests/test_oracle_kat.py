@@ -209,3 +209,29 @@ def test_svgf_oracle_runs_and_resets():
         assert np.isfinite(out).all()
         assert np.all(out[..., 3] == 1.0)
         prev = f
+
+
+def test_f2h_rne_matches_numpy_round_to_nearest_even():
+    rng = np.random.default_rng(7)
+    xs = np.concatenate([
+        rng.normal(scale=s, size=2000).astype(np.float32) for s in (1e-7, 1e-5, 1e-2, 1.0, 1e3, 6e4)
+    ] + [np.array([0.0, -0.0, 65504.0, 65519.99, 65520.0, 1e9, -1e9, 2.0 ** -24, 2.0 ** -25, 3 * 2.0 ** -26,
+                   np.inf, -np.inf], np.float32)])
+    got = np.array([oracle.f2h_rne(float(x)) for x in xs], np.uint16)
+    np.testing.assert_array_equal(got, xs.astype(np.float16).view(np.uint16))
+
+
+def test_oracle_scene_generator_is_the_product_generator_bit_for_bit():
+    """The CPU timing arm generates its frames with the oracle library's build of scene.h; they must be the frames
+    the product's generator makes (the device generator is checked against the host one in the GPU tests)."""
+    from hush_b200 import scene
+
+    for cfg, frames in ((scene.SceneConfig(96, 64, 3, n_moving=2, pan_min=0.0, pan_max=4.0, cut_frame=2, seed=3),
+                         (0, 1, 2)),
+                        (scene.CONFIG_1080P.with_(width=160, height=90), (0, 31, 32))):
+        for i in frames:
+            a = oracle.scene_frame(cfg, i, clean=True)
+            b = scene.frame_host(cfg, i, clean=True)
+            for k in oracle.INPUTS:
+                np.testing.assert_array_equal(a[k].view(np.uint16), b[k].view(np.uint16), err_msg=f"{k} frame {i}")
+            np.testing.assert_array_equal(a["clean"], b["clean"])

@@ -61,6 +61,63 @@ def test_noalloc_weight_gradient_matches_the_trainer():
         assert np.abs(got - ref).max() <= 1e-3 * scale, np.abs(got - ref).max() / scale
 
 
+def test_noalloc_matches_the_mlp_adjoint_on_all_seeds_and_many_chunks():
+    """At 640 x 360 (320 x 180 = 57,600 half-res rows: 900 chunks of 64 on 512 CTAs, so CTAs sum two chunks) with a
+    random dL/dpar on all 12 channels, alpha and gamma included, against hush_mlp_bwd's weight gradient; then a
+    smaller call on the same scratch (the first 10 half-res rows) against the adjoint of the seed cut to those rows,
+    so partial sums left by the larger call cannot leak into it."""
+    W, H = 640, 360
+    cfg = scene.SceneConfig(W, H, 3, n_moving=2, pan_min=1.0, pan_max=3.0, seed=5)
+    host = [scene.frame_host(cfg, i, clean=True) for i in range(3)]
+    cleans = [torch.from_numpy(h["clean"]).cuda() for h in host]
+    g = Hush(0, {"width": W, "height": H, "schedule": "passes"})
+    tr = Trainer(g, xavier_init(5))
+    for t in range(2):
+        tr.frame(_dev(host[t]), cleans[t], cleans[t - 1] if t else None, 0.5, backward=False)
+        tr.end_frame()
+    inputs = _dev(host[2])
+    tr.begin(inputs, cleans[2], cleans[1], 0.5)
+    tr.fwd("mlp")
+    dpar = tr.buffer("DPAR")
+    H2, W2 = dpar.shape[0], dpar.shape[1]
+    assert H2 * W2 > 512 * 64
+    seed = torch.randn(dpar.shape, generator=torch.Generator().manual_seed(9), dtype=torch.float64).float().cuda()
+    theta = tr.buffer("THETA")
+
+    def adjoint(sd):
+        tr.zero_adjoints()
+        tr.zero_grad()
+        dpar.copy_(sd)
+        tr.bwd("mlp")
+        torch.cuda.synchronize()
+        return tr.grad()
+
+    ref = adjoint(seed)
+    b3 = 16 * 20 + 16 + 16 * 16 + 16 + 12 * 16  # offset of b3 in the blob
+    assert ref[b3] != 0.0 and ref[b3 + 1] != 0.0, "the alpha / gamma seeds must reach their biases"
+    out = torch.full((812,), float("nan"), dtype=torch.float64, device="cuda")
+    scale = np.abs(ref).max()
+    for _ in range(2):
+        got = _noalloc(g, seed, theta, out)
+        assert np.isfinite(got).all()
+        assert np.abs(got - ref).max() <= 1e-3 * scale, np.abs(got - ref).max() / scale
+    # a smaller call after the larger one: 10 half-res rows
+    cut = seed.clone()
+    cut[10:] = 0.0
+    ref_small = adjoint(cut)
+    ptrs = [g.buffer(n).data_ptr() for n in ("F0", "F1", "F2", "F3")]
+    rc = L.lib().hush_mlp_grad_noalloc(*ptrs, seed.data_ptr(), theta.data_ptr(), W2, 10, out.data_ptr(),
+                                       C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == L.HUSH_OK, L.lib().hush_global_error()
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    s_small = np.abs(ref_small).max()
+    assert s_small > 0
+    assert np.abs(got - ref_small).max() <= 1e-3 * s_small, np.abs(got - ref_small).max() / s_small
+    tr.destroy()
+    g.destroy()
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch():
     t = torch.zeros(16, dtype=torch.float32, device="cuda")
     d = torch.zeros(812, dtype=torch.float64, device="cuda")
