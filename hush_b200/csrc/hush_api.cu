@@ -141,11 +141,12 @@ static int set_weights(hush_t *h, const uint16_t *weights, size_t n) {
   std::memset(&h->w16, 0, sizeof(h->w16));
   if (hd == 16) {
     std::memcpy(h->w16.w, wf.data(), sizeof(h->w16.w));
-    // tensor-core operands (bf16, then f16), then the FP32 weights of the 4-lane MLP
-    alignas(16) uint8_t blob[2 * MLP_TC_BLOB_BYTES + MLP_FP32_BLOB_BYTES];
-    mlp_tc_build_blob(wf.data(), 1, blob);
-    mlp_tc_build_blob(wf.data(), 0, blob + MLP_TC_BLOB_BYTES);
-    mlp_fp32_build_blob(wf.data(), reinterpret_cast<float *>(blob + 2 * MLP_TC_BLOB_BYTES));
+    // tensor-core operands (bf16 hi, bf16 lo, f16), then the FP32 weights of the per-thread MLP
+    alignas(16) uint8_t blob[MLP_BLOB_FP32 + MLP_FP32_BLOB_BYTES];
+    mlp_tc_build_blob(wf.data(), 1, 0, blob + MLP_BLOB_BF16);
+    mlp_tc_build_blob(wf.data(), 1, 1, blob + MLP_BLOB_BF16 + MLP_TC_BLOB_BYTES);
+    mlp_tc_build_blob(wf.data(), 0, 0, blob + MLP_BLOB_F16);
+    mlp_fp32_build_blob(wf.data(), reinterpret_cast<float *>(blob + MLP_BLOB_FP32));
     if (!h->tc_blob_dev) {
       e = cudaMalloc(&h->tc_blob_dev, sizeof(blob));
       if (e != cudaSuccess) return hush_cuda_fail(h, e, "cudaMalloc of the tensor-core weights");

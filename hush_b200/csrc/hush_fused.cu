@@ -47,13 +47,22 @@ HD_INL uint16_t to_op(float v) {
   else return __half_as_ushort(__float2half_rn(v));
 }
 template <bool BF16>
-HD_INL uint4 pack8(const float *v) {
-  uint4 q;
-  q.x = (uint32_t)to_op<BF16>(v[0]) | ((uint32_t)to_op<BF16>(v[1]) << 16);
-  q.y = (uint32_t)to_op<BF16>(v[2]) | ((uint32_t)to_op<BF16>(v[3]) << 16);
-  q.z = (uint32_t)to_op<BF16>(v[4]) | ((uint32_t)to_op<BF16>(v[5]) << 16);
-  q.w = (uint32_t)to_op<BF16>(v[6]) | ((uint32_t)to_op<BF16>(v[7]) << 16);
-  return q;
+HD_INL float from_op(uint16_t h) {
+  if constexpr (BF16) return __bfloat162float(__ushort_as_bfloat16(h));
+  else return __half2float(__ushort_as_half(h));
+}
+// Eight values as one 16-byte operand row segment (hi), and the rounding residuals v - hi rounded again (lo): a
+// split-precision operand, hi + lo carrying 16 (bf16) or 22 (f16) significant bits of v.
+template <bool BF16>
+HD_INL void pack8_split(const float *v, uint4 &hi, uint4 &lo) {
+  uint32_t h[8], l[8];
+#pragma unroll
+  for (int e = 0; e < 8; e++) {
+    h[e] = to_op<BF16>(v[e]);
+    l[e] = to_op<BF16>(v[e] - from_op<BF16>((uint16_t)h[e]));
+  }
+  hi = make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16), h[4] | (h[5] << 16), h[6] | (h[7] << 16));
+  lo = make_uint4(l[0] | (l[1] << 16), l[2] | (l[3] << 16), l[4] | (l[5] << 16), l[6] | (l[7] << 16));
 }
 
 // pixel()'s inputs to block(): P0..P4 as block() reads them and the decoded normal (Ns.w = 1 with a surface).
@@ -260,23 +269,28 @@ struct KbSmem {
   float4 w[MLP_FP32_BLOB_BYTES / 16];
 };
 // Tensor-core forms: the same tile plus the MMA operands of the CTA's 256 rows (one per block) in the K-major
-// no-swizzle layout: A1 256 x 32 (features, zero padded), A2 256 x 16 (hidden layers), B1 / B2 / B3.
+// no-swizzle layout, each as a split-precision pair (hi, lo): A1 256 x 32 (features, zero padded), A2 256 x 16
+// (hidden layers), then the weights B1 / B2 / B3 (hi, and for bf16 lo).
 struct KbTcSmem {
   float4 I[2 * KB_HW * KB_SH];
   float2 Lq[2 * KB_HW * KB_SH];
   alignas(128) uint8_t a1[KB_NT * 32 * 2];
+  alignas(128) uint8_t a1lo[KB_NT * 32 * 2];
   alignas(128) uint8_t a2[KB_NT * 16 * 2];
-  alignas(128) uint8_t b[MLP_TC_BLOB_BYTES];
+  alignas(128) uint8_t a2lo[KB_NT * 16 * 2];
+  alignas(128) uint8_t b[2 * MLP_TC_BLOB_BYTES];
   alignas(8) uint64_t mbar;
   uint32_t tmem;
 };
 
 // One MMA layer over the CTA's 256 rows: rows 0-127 and 128-255 go to TMEM columns [0, 16) and [16, 32) of the
-// 128 lanes. Every thread of the CTA takes part (the operand rows were written by all of them); thread 0 issues and
-// commits, all wait on the mbarrier (bounded) and load their own row: warp w reads lanes 32 (w % 4) of column block
-// w / 4. Returns false if the wait gave up.
-HD_INL bool tc_layer_256(KbTcSmem &S, int li, const uint8_t *a, uint32_t kcore_a, int kblocks, uint32_t b_off,
-                         uint32_t kcore_b, uint32_t idesc, uint32_t phase, float *d) {
+// 128 lanes. Per K block the products A_hi B_hi, A_lo B_hi and (with lo weights, bf16) A_hi B_lo accumulate into the
+// same FP32 accumulator; the dropped A_lo B_lo term is 2^-16 (bf16) / 2^-22 (f16) of the product. Every thread of the
+// CTA takes part (the operand rows were written by all of them); thread 0 issues and commits, all wait on the
+// mbarrier (bounded) and load their own row: warp w reads lanes 32 (w % 4) of column block w / 4. Returns false if
+// the wait gave up.
+HD_INL bool tc_layer_256(KbTcSmem &S, int li, const uint8_t *a, const uint8_t *alo, uint32_t kcore_a, int kblocks,
+                         uint32_t b_off, bool b_lo, uint32_t kcore_b, uint32_t idesc, uint32_t phase, float *d) {
   umma::fence_proxy_async();
   umma::fence_before_sync();
   __syncthreads();
@@ -286,10 +300,17 @@ HD_INL bool tc_layer_256(KbTcSmem &S, int li, const uint8_t *a, uint32_t kcore_a
     const uint32_t b = umma::smem_u32(S.b) + b_off;
 #pragma unroll
     for (int half = 0; half < 2; half++) {
-      const uint32_t a0 = umma::smem_u32(a) + (uint32_t)half * 16u * 128u * kcore_a;
-      for (int kb = 0; kb < kblocks; kb++)
-        umma::mma_f16(S.tmem + 16u * half, umma::sdesc(a0 + 256u * kb, 128, 128 * kcore_a),
-                      umma::sdesc(b + 256u * kb, 128, 128 * kcore_b), idesc, kb > 0 ? 1u : 0u);
+      const uint32_t ah = umma::smem_u32(a) + (uint32_t)half * 16u * 128u * kcore_a;
+      const uint32_t al = umma::smem_u32(alo) + (uint32_t)half * 16u * 128u * kcore_a;
+      for (int kb = 0; kb < kblocks; kb++) {
+        const uint64_t bh = umma::sdesc(b + 256u * kb, 128, 128 * kcore_b);
+        umma::mma_f16(S.tmem + 16u * half, umma::sdesc(ah + 256u * kb, 128, 128 * kcore_a), bh, idesc,
+                      kb > 0 ? 1u : 0u);
+        umma::mma_f16(S.tmem + 16u * half, umma::sdesc(al + 256u * kb, 128, 128 * kcore_a), bh, idesc, 1u);
+        if (b_lo)
+          umma::mma_f16(S.tmem + 16u * half, umma::sdesc(ah + 256u * kb, 128, 128 * kcore_a),
+                        umma::sdesc(b + MLP_TC_BLOB_BYTES + 256u * kb, 128, 128 * kcore_b), idesc, 1u);
+      }
     }
     umma::commit(mbar);
   }
@@ -323,7 +344,8 @@ __global__ void __launch_bounds__(KB_NT, 2)
       umma::tmem_relinquish();
     }
     if (li == 0) umma::mbar_init(umma::smem_u32(&S.mbar), 1);
-    if (li < MLP_TC_BLOB_BYTES / 16) reinterpret_cast<uint4 *>(S.b)[li] = __ldg(blob + li);
+    constexpr int NB = (MODE == 1 ? 2 : 1) * MLP_TC_BLOB_BYTES / 16;  // bf16: hi and lo weights
+    for (int i = li; i < NB; i += KB_NT) reinterpret_cast<uint4 *>(S.b)[i] = __ldg(blob + i);
     umma::fence_proxy_async();
     umma::fence_before_sync();
   } else {
@@ -471,26 +493,32 @@ __global__ void __launch_bounds__(KB_NT, 2)
     constexpr bool BF16 = MODE == 1;
     constexpr int B1 = 16 * N_FEAT, B2 = B1 + 16 + 16 * 16, B3 = B2 + 16 + N_OUT * 16;
     constexpr uint32_t ID = umma::idesc_f16(BF16 ? 1 : 0, 128, 16);
+    auto put_row = [&](uint8_t *hi, uint8_t *lo, int k0, int kcore, const float *v) {
+      uint4 h, l;
+      pack8_split<BF16>(v, h, l);
+      *reinterpret_cast<uint4 *>(hi + umma::kmajor_off(li, k0, kcore)) = h;
+      *reinterpret_cast<uint4 *>(lo + umma::kmajor_off(li, k0, kcore)) = l;
+    };
 #pragma unroll
     for (int c = 0; c < 4; c++) {
       float v8[8];
 #pragma unroll
       for (int e = 0; e < 8; e++)
         v8[e] = (8 * c + e < N_FEAT && valid && ok) ? __half2float(__ushort_as_half(f2h(qf16(fe[8 * c + e])))) : 0.f;
-      *reinterpret_cast<uint4 *>(S.a1 + umma::kmajor_off(li, 8 * c, 4)) = pack8<BF16>(v8);
+      put_row(S.a1, S.a1lo, 8 * c, 4, v8);
     }
     float row[16], d[16];
-    bool good = tc_layer_256(S, li, S.a1, 4, 2, 0, 4, ID, 0, d);
+    bool good = tc_layer_256(S, li, S.a1, S.a1lo, 4, 2, 0, BF16, 4, ID, 0, d);
 #pragma unroll
     for (int j = 0; j < 16; j++) row[j] = fmaxf(d[j] + wts.w[B1 + j], 0.0f);
-    *reinterpret_cast<uint4 *>(S.a2 + umma::kmajor_off(li, 0, 2)) = pack8<BF16>(row);
-    *reinterpret_cast<uint4 *>(S.a2 + umma::kmajor_off(li, 8, 2)) = pack8<BF16>(row + 8);
-    good &= tc_layer_256(S, li, S.a2, 2, 1, 1024, 2, ID, 1, d);
+    put_row(S.a2, S.a2lo, 0, 2, row);
+    put_row(S.a2, S.a2lo, 8, 2, row + 8);
+    good &= tc_layer_256(S, li, S.a2, S.a2lo, 2, 1, 1024, BF16, 2, ID, 1, d);
 #pragma unroll
     for (int j = 0; j < 16; j++) row[j] = fmaxf(d[j] + wts.w[B2 + j], 0.0f);
-    *reinterpret_cast<uint4 *>(S.a2 + umma::kmajor_off(li, 0, 2)) = pack8<BF16>(row);
-    *reinterpret_cast<uint4 *>(S.a2 + umma::kmajor_off(li, 8, 2)) = pack8<BF16>(row + 8);
-    good &= tc_layer_256(S, li, S.a2, 2, 1, 1536, 2, ID, 0, d);
+    put_row(S.a2, S.a2lo, 0, 2, row);
+    put_row(S.a2, S.a2lo, 8, 2, row + 8);
+    good &= tc_layer_256(S, li, S.a2, S.a2lo, 2, 1, 1536, BF16, 2, ID, 0, d);
     float out[N_OUT];
 #pragma unroll
     for (int j = 0; j < N_OUT; j++) out[j] = d[j] + wts.w[B3 + j];
@@ -1150,14 +1178,14 @@ cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpW16 &w16,
   const int qx = (f.W4 + HT_W - 1) / HT_W, qy = (f.H4 + HT_H - 1) / HT_H;
   switch (stage) {
     case 0: {
-      // blob: bf16 operands, f16 operands, then the transposed FP32 weights
+      // blob: bf16 hi / lo operands, f16 operands, then the transposed FP32 weights
       const uint4 *blob = (const uint4 *)mlp_tc;
       int dev = 0;
       cudaGetDevice(&dev);
       if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
       const dim3 g((f.W + KB_TW - 1) / KB_TW, (f.H + KB_TH - 1) / KB_TH);
       if (mlp_mode == 0) {
-        k_temporal_block<0><<<g, KB_NT, sizeof(KbSmem), st>>>(f, w16, blob + 2 * MLP_TC_BLOB_BYTES / 16);
+        k_temporal_block<0><<<g, KB_NT, sizeof(KbSmem), st>>>(f, w16, blob + MLP_BLOB_FP32 / 16);
       } else {
         // the tensor-core forms need more than 48 KB of dynamic shared memory: opt in once per device
         static bool opted[2][64] = {};
@@ -1169,8 +1197,8 @@ cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpW16 &w16,
           if (e != cudaSuccess) return e;
           opted[m][dev] = true;
         }
-        if (m == 0) k_temporal_block<1><<<g, KB_NT, sizeof(KbTcSmem), st>>>(f, w16, blob);
-        else k_temporal_block<2><<<g, KB_NT, sizeof(KbTcSmem), st>>>(f, w16, blob + MLP_TC_BLOB_BYTES / 16);
+        if (m == 0) k_temporal_block<1><<<g, KB_NT, sizeof(KbTcSmem), st>>>(f, w16, blob + MLP_BLOB_BF16 / 16);
+        else k_temporal_block<2><<<g, KB_NT, sizeof(KbTcSmem), st>>>(f, w16, blob + MLP_BLOB_F16 / 16);
       }
       break;
     }

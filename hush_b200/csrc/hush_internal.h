@@ -27,9 +27,12 @@ const char *fused_stage_label(int stage);
 size_t fused_scratch_bytes(int W, int H);
 
 // Tensor-core MLP weight operands for h = 16 in the UMMA K-major no-swizzle shared-memory layout: B1 (16 x 32, W1
-// zero-padded along K), B2 (16 x 16), B3 (16 x 16, W3 zero-padded along N), in bf16 or f16 (mlp_tc.cu).
+// zero-padded along K), B2 (16 x 16), B3 (16 x 16, W3 zero-padded along N), in bf16 or f16 (mlp_tc.cu). lo = 1
+// (bf16): the bf16 residuals w - bf16(w) instead, the low half of a split-precision operand.
 constexpr int MLP_TC_BLOB_BYTES = 2048;
-void mlp_tc_build_blob(const float *w812, int bf16, uint8_t *blob);
+void mlp_tc_build_blob(const float *w812, int bf16, int lo, uint8_t *blob);
+// The instance's weight blob on the device: bf16 hi | bf16 lo | f16 (tensor-core operands), then the FP32 weights.
+constexpr int MLP_BLOB_BF16 = 0, MLP_BLOB_F16 = 2 * MLP_TC_BLOB_BYTES, MLP_BLOB_FP32 = 3 * MLP_TC_BLOB_BYTES;
 // FP32 weights of the h = 16 network for the 4-lane MLP: per input i and lane k the float4 of the units lane k owns
 // (layer 1 / 2: units 4k..4k+3; layer 3: outputs k, 4+k, 8+k), then the biases in the same grouping.
 constexpr int MLP_FP32_W1 = 0, MLP_FP32_W2 = 80, MLP_FP32_W3 = 144, MLP_FP32_B1 = 208, MLP_FP32_B2 = 212,

@@ -32,10 +32,19 @@ static uint16_t f32_to_f16_rn(float x) {
   return (uint16_t)(s | q);
 }
 
-void mlp_tc_build_blob(const float *w, int bf16, uint8_t *blob) {
+static float bf16_to_f32(uint16_t h) {
+  const uint32_t u = (uint32_t)h << 16;
+  float x;
+  std::memcpy(&x, &u, 4);
+  return x;
+}
+
+void mlp_tc_build_blob(const float *w, int bf16, int lo, uint8_t *blob) {
   std::memset(blob, 0, MLP_TC_BLOB_BYTES);
   auto put = [&](uint8_t *base, int n, int k, int kcore, float v) {
-    const uint16_t h = bf16 ? f32_to_bf16_rn(v) : f32_to_f16_rn(v);
+    // lo (bf16 only): the rounding residual v - bf16(v), itself rounded to bf16; hi + lo holds any f16 value exactly
+    uint16_t h = bf16 ? f32_to_bf16_rn(v) : f32_to_f16_rn(v);
+    if (bf16 && lo) h = f32_to_bf16_rn(v - bf16_to_f32(h));
     std::memcpy(base + umma::kmajor_off(n, k, kcore), &h, 2);
   };
   const int W1 = 0, B1 = 16 * 20, W2 = B1 + 16, B2 = W2 + 256, W3 = B2 + 16;

@@ -105,14 +105,15 @@ def test_mlp_forms_at_1080p_against_fp64_and_clean():
     for j, p in enumerate(PARAMS):
         print(f"| {p} | " + " | ".join(f"{stats[m][0][j]:.1e} / {stats[m][1][j]:.1e}" for m in FORMS) + " |")
 
-    # bounds: the FP32 and F16 forms inside the per-channel 2e-3 bound on all but 1e-2 of values; BF16 (features
-    # rounded to 8 bits) inside 5e-2; BF16 no worse than FP32 against the noise-free image
-    for m in ("fp32", "f16"):
-        assert max(x[0] for x in beyond[m]) <= 1e-2, (m, beyond[m])
-    assert max(x[1] for x in beyond["bf16"]) <= 1e-2, beyond["bf16"]
+    # bounds: every form (FP32, and the split-precision F16 / BF16 tensor-core forms) inside the per-channel 2e-3
+    # bound of the FP64 oracle on all but 1e-3 of values; BF16 no worse than FP32 against the noise-free image; the
+    # 12 MLP outputs of every form within 1e-3 (mean) of the FP64 oracle's
+    for m in ("fp32", "f16", "bf16"):
+        assert max(x[0] for x in beyond[m]) <= 1e-3, (m, beyond[m])
     assert np.mean(rows["bf16"]) <= np.mean(rows["fp32"]) * 1.01
     assert abs(np.mean(rows["fp32"]) - np.mean(rows["oracle_f64"])) <= 1e-3
-    assert stats["fp32"][0].max() <= 1e-3 and stats["f16"][0].max() <= 5e-3 and stats["bf16"][0].max() <= 5e-2
+    for m in FORMS:
+        assert stats[m][0].max() <= 1e-3, (m, stats[m][0])
 
 
 def test_4k_bf16_against_fp32_and_clean():
@@ -148,4 +149,4 @@ def test_4k_bf16_against_fp32_and_clean():
         assert g.kernel_status() == 0
         g.destroy()
     assert np.mean(rel["bf16"]) <= np.mean(rel["fp32"]) * 1.01
-    assert max(d[1] for d in diff) <= 1e-2
+    assert max(d[0] for d in diff) <= 1e-3

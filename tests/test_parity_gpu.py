@@ -22,7 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 # per-pass: fraction of values allowed outside the bound (f16 round-toward-zero boundary flips of a last-ulp f32
 # difference); sequences: the same differences fed back through the temporal history and TAA
 PASS_FRAC = 2e-3
-SEQ_FRAC = 1e-2
+SEQ_FRAC = 5e-3  # ~4x the worst fraction measured on any frame of the 1080p sequences (1.3e-3)
 
 PASS_OUTPUTS = {
     "temporal": ["A0", "MOM{c}", "KEY{c}", "F0", "F1", "F2", "F3"],
@@ -271,27 +271,37 @@ def test_device_generator_matches_host():
             assert np.mean(np.abs(a - b) <= 1e-2 * np.maximum(np.abs(b), 1)) > 0.99, k
 
 
-@pytest.mark.parametrize("mlp,rel,frac", [("f16", 2e-3, 1e-2), ("bf16", 5e-2, 1e-2)])
-def test_tensor_core_mlp_forms(mlp, rel, frac):
-    """The tcgen05 MLP forms against the FP32 oracle: f16 operands keep the features exact (only the hidden
-    activations round), so they stay within the FP32 bound on nearly every value; bf16 operands round the features
-    to 8 bits and move the parameters by ~0.3 % on average, so they are held to a 5e-2 bound."""
-    cfg = scene.CONFIG_360P
-    frames = [scene.frame_host(cfg, i) for i in range(4)]
+# fraction of output values beyond 2e-3 of the f32 oracle that every MLP form must stay under: the FP32 form
+# measures ~1.5e-4 at 360p and 1080p; the split-precision tensor-core forms must meet the same bar
+FORM_FRAC = 1e-3
+
+
+@pytest.mark.parametrize("mlp", ["fp32", "f16", "bf16"])
+@pytest.mark.parametrize("cfg,n", [(scene.CONFIG_360P, 4), (scene.CONFIG_1080P, 3)], ids=["360p", "1080p"])
+def test_tensor_core_mlp_forms(mlp, cfg, n):
+    """The MLP forms against the f32 oracle at the north-star bound of 2e-3: each tcgen05 layer runs on split-
+    precision operands (hi + lo, the residual of the rounding in a second operand) with FP32 accumulation in TMEM,
+    so the features and weights (f16 values) are exact and the hidden activations carry 16 (bf16) or 22 (f16)
+    bits; the forms are held to the FP32 form's fraction."""
+    frames = [scene.frame_host(cfg, i) for i in range(n)]
     o = oracle.OracleHush(cfg.width, cfg.height, builtin_weights())
     g = Hush(0, {"width": cfg.width, "height": cfg.height, "mlp": mlp})
     for i, f in enumerate(frames):
         ref = o.denoise(f).astype(np.float32)
         got = to_f32(g.denoise(_dev(f)))
-        fr, worst, _ = mismatch(got, ref, rel=rel)
-        assert fr <= frac, (mlp, i, fr, worst)
+        fr, worst, _ = mismatch(got, ref, rel=2e-3)
+        print(f"{mlp} {cfg.width}x{cfg.height} frame {i}: {fr:.2e} beyond 2e-3 (worst {worst:.3g})")
+        assert fr <= FORM_FRAC, (mlp, i, fr, worst)
 
 
-def test_tensor_core_parameters_match_fp32_parameters():
+@pytest.mark.parametrize("mlp", ["f16", "bf16"])
+def test_tensor_core_parameters_match_fp32_parameters(mlp):
+    """The stored filter parameters (f16, rounded toward zero) of the split-precision forms equal the FP32 form's
+    but for last-ulp flips of the storage rounding."""
     cfg = scene.SceneConfig(256, 144, 3, n_moving=2, seed=41)
     frames = [_dev(scene.frame_host(cfg, i)) for i in range(cfg.frames)]
     a = Hush(0, {"width": cfg.width, "height": cfg.height, "mlp": "fp32"})
-    b = Hush(0, {"width": cfg.width, "height": cfg.height, "mlp": "f16"})
+    b = Hush(0, {"width": cfg.width, "height": cfg.height, "mlp": mlp})
     for f in frames:
         a.denoise(f)
         b.denoise(f)
@@ -300,7 +310,77 @@ def test_tensor_core_parameters_match_fp32_parameters():
     for name in (f"PAR0_{c}", "PAR1", "PAR2"):
         pa, pb = _download(a, name), _download(b, name)
         rel = np.abs(pb - pa) / (np.abs(pa) + 1e-3)
-        assert rel.mean() < 1e-3 and rel.max() < 5e-2, (name, rel.mean(), rel.max())
+        print(f"{mlp} {name}: rel. diff mean {rel.mean():.2e} max {rel.max():.2e}, "
+              f"{np.mean(pa != pb):.2e} of values differ")
+        assert rel.mean() < 1e-4 and rel.max() < 4e-3, (name, rel.mean(), rel.max())
+
+
+def test_config2_full_sequence_with_cut():
+    """The 1080p workload in full: 64 frames (3 moving objects, pan U[0,4] px/frame, camera cut at frame 32 with
+    reset()) through the FP32 and the BF16 forms against the f32 oracle on every frame. Frame 32 must equal what a
+    fresh instance makes of the same inputs, bit for bit (reset drops all history), and frames 32-33 carry no
+    drift from before the cut."""
+    cfg = scene.CONFIG_1080P
+    W, H = cfg.width, cfg.height
+    o = oracle.OracleHush(W, H, builtin_weights())
+    forms = {m: Hush(0, {"width": W, "height": H, "mlp": m}) for m in ("fp32", "bf16")}
+    worst_frac = {m: 0.0 for m in forms}
+    for i in range(cfg.frames):
+        f = scene.frame_host(cfg, i)
+        if i == cfg.cut_frame:
+            o.reset()
+            for g in forms.values():
+                g.reset()
+        ref = o.denoise(f).astype(np.float32)
+        dev = _dev(f)
+        for m, g in forms.items():
+            out = g.denoise(dev)
+            if i == cfg.cut_frame:
+                fresh = Hush(0, {"width": W, "height": H, "mlp": m})
+                same = torch.equal(out, fresh.denoise(dev))
+                fresh.destroy()
+                assert same, f"{m}: frame {i} after reset differs from a fresh instance"
+            fr, worst, _ = mismatch(to_f32(out), ref)
+            worst_frac[m] = max(worst_frac[m], fr)
+            bound = PASS_FRAC if i in (cfg.cut_frame, cfg.cut_frame + 1) else SEQ_FRAC
+            assert fr <= bound, f"{m}: frame {i}: {fr:.2e} beyond 2e-3 (worst {worst:.3g})"
+    print("worst fraction per form:", worst_frac)
+    for g in forms.values():
+        assert g.kernel_status() == 0
+        g.destroy()
+
+
+def test_exported_weights_load_and_match_the_oracle():
+    """hush_trainer_export -> Hush(weights=blob) against the oracle running the same blob: the trained FP32 master
+    weights round to f16 (nearest) once, and the drop-in instance then follows the oracle like the built-in
+    weights do."""
+    from hush_b200.train import Trainer, xavier_init
+
+    cfg = scene.SceneConfig(160, 96, 4, n_moving=2, pan_min=1.0, pan_max=3.0, seed=23)
+    th = Hush(0, {"width": cfg.width, "height": cfg.height, "schedule": "passes"})
+    tr = Trainer(th, xavier_init(23))
+    host = [scene.frame_host(cfg, i, clean=True) for i in range(cfg.frames)]
+    devs = [_dev(h) for h in host]
+    cleans = [torch.from_numpy(h["clean"]).cuda() for h in host]
+    tr.zero_grad()
+    for i in range(cfg.frames):  # one optimiser step so the exported weights are trained ones, not the init
+        tr.frame(devs[i], cleans[i], cleans[i - 1] if i else None, 0.5, backward=True)
+        tr.end_frame()
+    tr.step(lr=1e-2)
+    theta = tr.theta
+    blob = tr.export()
+    assert blob.dtype == np.uint16 and blob.size == 812
+    np.testing.assert_array_equal(blob, theta.astype(np.float16).view(np.uint16))
+    assert not np.array_equal(blob, builtin_weights())
+    tr.destroy()
+    th.destroy()
+    for sched in ("fused", "passes"):
+        g = Hush(0, {"width": cfg.width, "height": cfg.height, "weights": blob.tobytes(), "schedule": sched})
+        o = oracle.OracleHush(cfg.width, cfg.height, blob)
+        for i, f in enumerate(host):
+            frac, worst, _ = mismatch(to_f32(g.denoise(devs[i])), o.denoise(f).astype(np.float32))
+            assert frac <= SEQ_FRAC, (sched, i, frac, worst)
+        g.destroy()
 
 
 def test_config5_4k_graph_bf16_and_fp32():
