@@ -87,3 +87,17 @@ def test_scene_generator_is_deterministic_and_well_formed():
     alb = a["material"][..., :3].astype(np.float32)[~sky]
     assert alb.min() >= 0.05 * 0.6 - 1e-3 and alb.max() <= 0.9 + 1e-3
     assert np.all(a["clean"] >= 0)
+
+
+def test_node_addon_calls_only_exported_symbols():
+    """node/hush_node.c cannot be compiled here (no node / node_api.h); every library function it calls must at
+    least be one the library exports."""
+    import re
+
+    src = open(os.path.join(ROOT, "node", "hush_node.c")).read()
+    called = set(re.findall(r"\b((?:hush|svgf)_[a-z0-9_]+)\s*\(", src))
+    defined = set(re.findall(r"\b(?:static\s+)?[a-z_ ]+\*?\s*((?:hush|svgf)_[a-z0-9_]+)\s*\([^;]*\)\s*\{", src))
+    lib = L.lib()
+    missing = sorted(n for n in called - defined if not hasattr(lib, n))
+    assert not missing, missing
+    assert {"hush_create", "hush_denoise", "svgf_encode", "hush_required_limits"} <= called
