@@ -8,7 +8,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libhush_b200.so")
 
 HUSH_OK, HUSH_ERR_ARG, HUSH_ERR_DEVICE, HUSH_ERR_CUDA, HUSH_ERR_KERNEL = 0, 1, 2, 3, 4
-MLP_FP32, MLP_BF16, MLP_F16 = 0, 1, 2
+MLP_FP32, MLP_BF16, MLP_F16, MLP_HALF = 0, 1, 2, 3
 SCHED_FUSED, SCHED_PASSES = 0, 1
 PASS_NAMES = ["temporal", "infer", "mid2", "mid3", "coarse1", "coarse2", "fine_final", "taa"]
 BUF_NAMES = ["A0", "X", "BH0", "BH1", "MOM0", "MOM1", "KEY0", "KEY1", "HIST0", "HIST1", "TAA0", "TAA1",

@@ -141,12 +141,14 @@ static int set_weights(hush_t *h, const uint16_t *weights, size_t n) {
   std::memset(&h->w16, 0, sizeof(h->w16));
   if (hd == 16) {
     std::memcpy(h->w16.w, wf.data(), sizeof(h->w16.w));
-    // tensor-core operands (bf16 hi, bf16 lo, f16), then the FP32 weights of the per-thread MLP
-    alignas(16) uint8_t blob[MLP_BLOB_FP32 + MLP_FP32_BLOB_BYTES];
+    // tensor-core operands (bf16 hi, bf16 lo, f16), the FP32 weights of the per-thread MLP, the f16x2 weights
+    static_assert(MLP_BLOB_HALF == MLP_BLOB_FP32 + MLP_FP32_BLOB_BYTES, "blob layout");
+    alignas(16) uint8_t blob[MLP_BLOB_BYTES];
     mlp_tc_build_blob(wf.data(), 1, 0, blob + MLP_BLOB_BF16);
     mlp_tc_build_blob(wf.data(), 1, 1, blob + MLP_BLOB_BF16 + MLP_TC_BLOB_BYTES);
     mlp_tc_build_blob(wf.data(), 0, 0, blob + MLP_BLOB_F16);
     mlp_fp32_build_blob(wf.data(), reinterpret_cast<float *>(blob + MLP_BLOB_FP32));
+    mlp_half_build_blob(wf.data(), reinterpret_cast<uint32_t *>(blob + MLP_BLOB_HALF));
     if (!h->tc_blob_dev) {
       e = cudaMalloc(&h->tc_blob_dev, sizeof(blob));
       if (e != cudaSuccess) return hush_cuda_fail(h, e, "cudaMalloc of the tensor-core weights");
@@ -184,7 +186,7 @@ extern "C" int hush_create(const hush_desc *desc, hush_t **out) {
   if (!(desc->width > 0 && desc->height > 0))
     return hush_fail(nullptr, HUSH_ERR_ARG,
                 "Hush: bad size " + std::to_string(desc->width) + "x" + std::to_string(desc->height));
-  if (desc->mlp_mode < HUSH_MLP_FP32 || desc->mlp_mode > HUSH_MLP_F16)
+  if (desc->mlp_mode < HUSH_MLP_FP32 || desc->mlp_mode > HUSH_MLP_HALF)
     return hush_fail(nullptr, HUSH_ERR_ARG, "Hush: unknown mlp_mode " + std::to_string(desc->mlp_mode));
   if (desc->schedule != HUSH_SCHED_FUSED && desc->schedule != HUSH_SCHED_PASSES)
     return hush_fail(nullptr, HUSH_ERR_ARG, "Hush: unknown schedule " + std::to_string(desc->schedule));
@@ -194,7 +196,7 @@ extern "C" int hush_create(const hush_desc *desc, hush_t **out) {
   h->dev = dev;
   h->exposure = desc->exposure;
   h->mlp_mode = desc->mlp_mode;
-  if (desc->f16 && h->mlp_mode == HUSH_MLP_FP32) h->mlp_mode = HUSH_MLP_F16;
+  if (desc->f16 && h->mlp_mode == HUSH_MLP_FP32) h->mlp_mode = HUSH_MLP_HALF;  // the reference's f16 arithmetic
   h->schedule = desc->schedule;
   const uint16_t *w = desc->weights ? desc->weights : HUSH_BUILTIN_WEIGHTS;
   const size_t n = desc->weights ? desc->n_weights : HUSH_BUILTIN_WEIGHT_COUNT;
@@ -259,7 +261,7 @@ extern "C" int hush_set_weights(hush_t *h, const uint16_t *w, size_t n) {
 }
 extern "C" int hush_set_mlp_mode(hush_t *h, int mode) {
   if (!h) return hush_fail(nullptr, HUSH_ERR_ARG, "hush_set_mlp_mode: NULL instance");
-  if (mode < HUSH_MLP_FP32 || mode > HUSH_MLP_F16) return hush_fail(h, HUSH_ERR_ARG, "Hush: unknown mlp_mode");
+  if (mode < HUSH_MLP_FP32 || mode > HUSH_MLP_HALF) return hush_fail(h, HUSH_ERR_ARG, "Hush: unknown mlp_mode");
   h->mlp_mode = mode;
   drop_graphs(h);
   return HUSH_OK;
@@ -330,6 +332,7 @@ HushFrame hush_make_frame(hush_t *h, const hush_inputs *in) {
   f.Ah = h->Ah; f.Gh = h->Gh; f.Gd = h->Gd; f.CGd = h->CGd;
   f.w_glob = h->w_dev;
   f.hidden = h->hidden;
+  f.mlp_half = h->mlp_mode == HUSH_MLP_HALF ? 1 : 0;
   f.err = h->err;
   return f;
 }

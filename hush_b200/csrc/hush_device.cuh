@@ -22,6 +22,7 @@ struct HushFrame {
   float4 *Gd, *CGd;
   const float *w_glob;  // decoded f32 weights in device memory (any hidden width)
   int hidden;
+  int mlp_half;         // the reference's `f16` option: INFER's MLP in f16 arithmetic (mlp_fwd_half)
   unsigned int *err;    // device error word (bounded waits in the tensor-core MLP)
 };
 
@@ -81,6 +82,56 @@ HD_INL void mlp_fwd_dyn(const float *__restrict__ w, int hd, const float *f, flo
     for (int i = 0; i < hd; i++) a = a + h2[i] * __ldg(w + W3 + j * hd + i);
     o[j] = a;
   }
+}
+
+// mlpCode with f16 = true (hush.js:683-703, chosen by the `f16` option at hush.js:740, 750): inputs, weights and
+// biases are f16 values; every product input * weight and every running sum bias + p0 + p1 + ... is rounded to f16
+// (round to nearest even) in that left-to-right order, ReLU is max(., 0h), and the outputs widen to f32. Two units per
+// f16x2 instruction; `mul.rn` / `add.rn` carry an explicit rounding mode, so they are never contracted into an FMA.
+HD_INL uint32_t hmul2_rn(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm("mul.rn.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+HD_INL uint32_t hadd2_rn(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm("add.rn.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+HD_INL uint32_t hrelu2(uint32_t a) {  // max(a, 0) per half; a NaN half gives 0
+  uint32_t r;
+  asm("max.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(0u));
+  return r;
+}
+HD_INL uint32_t h2pack(float a, float b) {  // (a, b) as f16 bits, low half first
+  return (uint32_t)__half_as_ushort(__float2half_rn(a)) | ((uint32_t)__half_as_ushort(__float2half_rn(b)) << 16);
+}
+HD_INL uint32_t hdup(uint32_t h16) { return (h16 & 0xffffu) * 0x10001u; }
+HD_INL float hlo(uint32_t a) { return __half2float(__ushort_as_half((uint16_t)(a & 0xffffu))); }
+HD_INL float hhi(uint32_t a) { return __half2float(__ushort_as_half((uint16_t)(a >> 16))); }
+
+// One f16 layer from decoded f32 weights (row-major (out, in)); in / out hold f16 bits per unit.
+HD_INL void mlp_layer_half(const float *__restrict__ w, int wo, int bo, int nin, int nout, const uint16_t *in,
+                           bool relu, uint16_t *out) {
+  for (int j = 0; j < nout; j += 2) {
+    const bool two = j + 1 < nout;
+    uint32_t a = h2pack(w[bo + j], two ? w[bo + j + 1] : 0.0f);
+    for (int i = 0; i < nin; i++)
+      a = hadd2_rn(a, hmul2_rn(hdup(in[i]), h2pack(w[wo + j * nin + i], two ? w[wo + (j + 1) * nin + i] : 0.0f)));
+    if (relu) a = hrelu2(a);
+    out[j] = (uint16_t)(a & 0xffffu);
+    if (two) out[j + 1] = (uint16_t)(a >> 16);
+  }
+}
+// Any hidden width (<= 256) from decoded weights, as the per-pass INFER runs it.
+HD_INL void mlp_fwd_half(const float *__restrict__ w, int hd, const float *f, float *o) {
+  const int W1 = 0, B1 = hd * N_FEAT, W2 = B1 + hd, B2 = W2 + hd * hd, W3 = B2 + hd, B3 = W3 + N_OUT * hd;
+  uint16_t x[N_FEAT], h1[256], h2[256], oh[N_OUT];
+  for (int i = 0; i < N_FEAT; i++) x[i] = __half_as_ushort(__float2half_rn(f[i]));
+  mlp_layer_half(w, W1, B1, N_FEAT, hd, x, true, h1);
+  mlp_layer_half(w, W2, B2, hd, hd, h1, true, h2);
+  mlp_layer_half(w, W3, B3, hd, N_OUT, h2, false, oh);
+  for (int j = 0; j < N_OUT; j++) o[j] = __half2float(__ushort_as_half(oh[j]));
 }
 
 // Output heads (hush.js:357-362): par0 = (alpha, gamma, beta, kappa), par1 = s, par2 = c.

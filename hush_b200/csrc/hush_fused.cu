@@ -327,12 +327,13 @@ struct ParityTile {
   HD_INL float4 operator()(int dx, int dy) const { return I[kb_tix(r + dy, c + dx)]; }
 };
 
-// MODE 0: FP32 MLP per thread; 1 / 2: tensor-core MLP on bf16 / f16 operands (dynamic shared memory).
+// MODE 0: FP32 MLP per thread; 1 / 2: tensor-core MLP on split bf16 / f16 operands (dynamic shared memory);
+// 3: the reference's f16-arithmetic MLP per thread (the `f16` option).
 template <int MODE>
 __global__ void __launch_bounds__(KB_NT, 2)
     k_temporal_block(const __grid_constant__ HushFrame f, const __grid_constant__ MlpW16 wts,
                      const uint4 *__restrict__ blob) {
-  constexpr bool TC = MODE != 0;
+  constexpr bool TC = MODE == 1 || MODE == 2;
   using Smem = std::conditional_t<TC, KbTcSmem, KbSmem>;
   extern __shared__ __align__(128) unsigned char kb_smem[];
   Smem &S = *reinterpret_cast<Smem *>(kb_smem);
@@ -349,7 +350,9 @@ __global__ void __launch_bounds__(KB_NT, 2)
     umma::fence_proxy_async();
     umma::fence_before_sync();
   } else {
-    for (int i = li; i < MLP_FP32_BLOB_BYTES / 16; i += KB_NT) reinterpret_cast<uint4 *>(S.w)[i] = __ldg(blob + i);
+    constexpr int NB = (MODE == 3 ? MLP_HALF_BLOB_BYTES : MLP_FP32_BLOB_BYTES) / 16;
+    static_assert(MLP_HALF_BLOB_BYTES <= MLP_FP32_BLOB_BYTES, "the f16x2 weights share the FP32 weights' space");
+    for (int i = li; i < NB; i += KB_NT) reinterpret_cast<uint4 *>(S.w)[i] = __ldg(blob + i);
   }
   const int lbx = li % (KB_TW / 2), lby = li / (KB_TW / 2);
   const int px0 = blockIdx.x * KB_TW + 2 * lbx, py0 = blockIdx.y * KB_TH + 2 * lby;
@@ -547,6 +550,48 @@ __global__ void __launch_bounds__(KB_NT, 2)
   if (!valid) return;
   if (!ok) {  // INFER on a block without valid pixels writes zeros (hush.js:343-346)
     sth(f.par0, o, z4); sth(f.par1, o, z4); sth(f.par2, o, z4);
+    return;
+  }
+  if constexpr (MODE == 3) {
+    // phase 4 (the `f16` option, hush.js:683-703): f16 products and running sums per unit in the WGSL's order (bias,
+    // then the inputs in increasing index), two units per f16x2 instruction, weights as f16x2 unit pairs in shared
+    // memory; the features enter as stored (packed f16, hush.js:278-280)
+    const uint32_t *Wh = reinterpret_cast<const uint32_t *>(S.w);
+    uint32_t a[8], b[8];
+#pragma unroll
+    for (int p = 0; p < 8; p++) a[p] = Wh[MLP_HALF_B1 + p];
+#pragma unroll
+    for (int i = 0; i < N_FEAT; i++) {
+      const uint32_t x = hdup(f2h(qf16(fe[i])));
+#pragma unroll
+      for (int p = 0; p < 8; p++) a[p] = hadd2_rn(a[p], hmul2_rn(x, Wh[MLP_HALF_W1 + i * 8 + p]));
+    }
+#pragma unroll
+    for (int p = 0; p < 8; p++) { a[p] = hrelu2(a[p]); b[p] = Wh[MLP_HALF_B2 + p]; }
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      const uint32_t x = hdup((i & 1) ? a[i >> 1] >> 16 : a[i >> 1]);
+#pragma unroll
+      for (int p = 0; p < 8; p++) b[p] = hadd2_rn(b[p], hmul2_rn(x, Wh[MLP_HALF_W2 + i * 8 + p]));
+    }
+#pragma unroll
+    for (int p = 0; p < 8; p++) b[p] = hrelu2(b[p]);
+#pragma unroll
+    for (int p = 0; p < 6; p++) a[p] = Wh[MLP_HALF_B3 + p];
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      const uint32_t x = hdup((i & 1) ? b[i >> 1] >> 16 : b[i >> 1]);
+#pragma unroll
+      for (int p = 0; p < 6; p++) a[p] = hadd2_rn(a[p], hmul2_rn(x, Wh[MLP_HALF_W3 + i * 6 + p]));
+    }
+    float out[N_OUT];
+#pragma unroll
+    for (int p = 0; p < 6; p++) { out[2 * p] = hlo(a[p]); out[2 * p + 1] = hhi(a[p]); }
+    float4 p0, p1, p2;
+    mlp_heads(out, p0, p1, p2);
+    sth(f.par0, o, p0);
+    sth(f.par1, o, p1);
+    sth(f.par2, o, p2);
     return;
   }
   // phase 4: the MLP (hush.js:681-704) on the features as stored (packed f16, hush.js:278-280, 348-353); each unit
@@ -1186,6 +1231,8 @@ cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpW16 &w16,
       const dim3 g((f.W + KB_TW - 1) / KB_TW, (f.H + KB_TH - 1) / KB_TH);
       if (mlp_mode == 0) {
         k_temporal_block<0><<<g, KB_NT, sizeof(KbSmem), st>>>(f, w16, blob + MLP_BLOB_FP32 / 16);
+      } else if (mlp_mode == 3) {
+        k_temporal_block<3><<<g, KB_NT, sizeof(KbSmem), st>>>(f, w16, blob + MLP_BLOB_HALF / 16);
       } else {
         // the tensor-core forms need more than 48 KB of dynamic shared memory: opt in once per device
         static bool opted[2][64] = {};

@@ -15,7 +15,7 @@ enum {
 // One reference pass (hush_passes.cu).
 cudaError_t launch_pass(int pass, const HushFrame &f, const MlpW16 &w16, cudaStream_t st);
 
-// Fused frame kernels (hush_fused.cu). mlp_mode: 0 FP32, 1 BF16 tensor cores, 2 F16 tensor cores.
+// Fused frame kernels (hush_fused.cu). mlp_mode: 0 FP32, 1 BF16 tensor cores, 2 F16 tensor cores, 3 f16 arithmetic.
 struct FusedPlan {
   int n_kernels;
   const char *labels[8];
@@ -31,8 +31,16 @@ size_t fused_scratch_bytes(int W, int H);
 // (bf16): the bf16 residuals w - bf16(w) instead, the low half of a split-precision operand.
 constexpr int MLP_TC_BLOB_BYTES = 2048;
 void mlp_tc_build_blob(const float *w812, int bf16, int lo, uint8_t *blob);
-// The instance's weight blob on the device: bf16 hi | bf16 lo | f16 (tensor-core operands), then the FP32 weights.
-constexpr int MLP_BLOB_BF16 = 0, MLP_BLOB_F16 = 2 * MLP_TC_BLOB_BYTES, MLP_BLOB_FP32 = 3 * MLP_TC_BLOB_BYTES;
+// f16 weights of the h = 16 network for the f16-arithmetic MLP, as f16x2 unit pairs (low half = the even unit): per
+// layer, for input i and pair p the word (w[2p][i], w[2p+1][i]) at i * (units / 2) + p, then the bias pairs.
+constexpr int MLP_HALF_W1 = 0, MLP_HALF_B1 = 160, MLP_HALF_W2 = 168, MLP_HALF_B2 = 296, MLP_HALF_W3 = 304,
+              MLP_HALF_B3 = 400;  // offsets in 32-bit words
+constexpr int MLP_HALF_BLOB_BYTES = 416 * 4;  // 406 words, padded to a multiple of 16 bytes
+void mlp_half_build_blob(const float *w812, uint32_t *blob);
+// The instance's weight blob on the device: bf16 hi | bf16 lo | f16 (tensor-core operands), the FP32 weights, then
+// the f16x2 weights.
+constexpr int MLP_BLOB_BF16 = 0, MLP_BLOB_F16 = 2 * MLP_TC_BLOB_BYTES, MLP_BLOB_FP32 = 3 * MLP_TC_BLOB_BYTES,
+              MLP_BLOB_HALF = MLP_BLOB_FP32 + 220 * 16, MLP_BLOB_BYTES = MLP_BLOB_HALF + MLP_HALF_BLOB_BYTES;
 // FP32 weights of the h = 16 network for the 4-lane MLP: per input i and lane k the float4 of the units lane k owns
 // (layer 1 / 2: units 4k..4k+3; layer 3: outputs k, 4+k, 8+k), then the biases in the same grouping.
 constexpr int MLP_FP32_W1 = 0, MLP_FP32_W2 = 80, MLP_FP32_W3 = 144, MLP_FP32_B1 = 208, MLP_FP32_B2 = 212,

@@ -106,7 +106,8 @@ __global__ void __launch_bounds__(TW *TH) k_infer(const __grid_constant__ HushFr
       fe[2 * i + 1] = t.y;
     }
   }
-  if constexpr (HD > 0) mlp_fwd<HD>(w.w, fe, out);
+  if (f.mlp_half) mlp_fwd_half(HD > 0 ? w.w : f.w_glob, f.hidden, fe, out);
+  else if constexpr (HD > 0) mlp_fwd<HD>(w.w, fe, out);
   else mlp_fwd_dyn(f.w_glob, f.hidden, fe, out);
   float4 p0, p1, p2;
   mlp_heads(out, p0, p1, p2);

@@ -56,6 +56,23 @@ void mlp_tc_build_blob(const float *w, int bf16, int lo, uint8_t *blob) {
     for (int k = 0; k < 16; k++) put(blob + 1536, n, k, 2, w[W3 + n * 16 + k]);
 }
 
+void mlp_half_build_blob(const float *w, uint32_t *blob) {
+  std::memset(blob, 0, MLP_HALF_BLOB_BYTES);
+  const int W1 = 0, B1 = 16 * 20, W2 = B1 + 16, B2 = W2 + 256, W3 = B2 + 16, B3 = W3 + 12 * 16;
+  auto pair = [](float a, float b) { return (uint32_t)f32_to_f16_rn(a) | ((uint32_t)f32_to_f16_rn(b) << 16); };
+  for (int i = 0; i < 20; i++)
+    for (int p = 0; p < 8; p++) blob[MLP_HALF_W1 + i * 8 + p] = pair(w[W1 + 2 * p * 20 + i], w[W1 + (2 * p + 1) * 20 + i]);
+  for (int i = 0; i < 16; i++)
+    for (int p = 0; p < 8; p++) blob[MLP_HALF_W2 + i * 8 + p] = pair(w[W2 + 2 * p * 16 + i], w[W2 + (2 * p + 1) * 16 + i]);
+  for (int i = 0; i < 16; i++)
+    for (int p = 0; p < 6; p++) blob[MLP_HALF_W3 + i * 6 + p] = pair(w[W3 + 2 * p * 16 + i], w[W3 + (2 * p + 1) * 16 + i]);
+  for (int p = 0; p < 8; p++) {
+    blob[MLP_HALF_B1 + p] = pair(w[B1 + 2 * p], w[B1 + 2 * p + 1]);
+    blob[MLP_HALF_B2 + p] = pair(w[B2 + 2 * p], w[B2 + 2 * p + 1]);
+    if (p < 6) blob[MLP_HALF_B3 + p] = pair(w[B3 + 2 * p], w[B3 + 2 * p + 1]);
+  }
+}
+
 void mlp_fp32_build_blob(const float *w, float *blob) {
   std::memset(blob, 0, MLP_FP32_BLOB_BYTES);
   const int W1 = 0, B1 = 16 * 20, W2 = B1 + 16, B2 = W2 + 256, W3 = B2 + 16, B3 = W3 + 12 * 16;

@@ -105,6 +105,8 @@ def _fill_inputs(inp: "L.HushInputs", tensors: dict, names=INPUTS):
         inp.pitch[k] = t.stride(0) * 2
 
 
+MLP_MODES = {"fp32": L.MLP_FP32, "bf16": L.MLP_BF16, "f16": L.MLP_F16, "half": L.MLP_HALF}
+
 _FIELD = {"radiance": "radiance", "normalDepth": "normal_depth", "motion": "motion", "material": "material",
           "emission": "emission", "prevNormalDepth": "prev_normal_depth", "prevMotion": "prev_motion"}
 
@@ -112,7 +114,9 @@ _FIELD = {"radiance": "radiance", "normalDepth": "normal_depth", "motion": "moti
 class Hush:
     """Drop-in ``Hush``: ``Hush(device, {"width", "height", "exposure", "weights", "f16"})``.
 
-    Extra options of this implementation: ``mlp`` ("fp32" | "bf16" | "f16"; the reference's form is fp32),
+    ``f16=True`` is the reference's option: the MLP in f16 arithmetic (``mlp="half"``). Extra options of this
+    implementation: ``mlp`` ("fp32" | "bf16" | "f16" | "half"; "bf16" / "f16" are the split-precision tensor-core
+    forms, "half" the reference's f16 arithmetic, "fp32" the reference's default),
     ``schedule`` ("fused" | "passes"), ``graph`` (replay whole frames as CUDA graphs).
     """
 
@@ -142,7 +146,7 @@ class Hush:
             d.weights = self._wbuf.ctypes.data_as(C.POINTER(C.c_uint16))
             d.n_weights = self._wbuf.size
         d.f16 = 1 if opts.get("f16", False) else 0
-        d.mlp_mode = {"fp32": L.MLP_FP32, "bf16": L.MLP_BF16, "f16": L.MLP_F16}[opts.get("mlp", "fp32")]
+        d.mlp_mode = MLP_MODES[opts.get("mlp", "fp32")]
         d.schedule = {"fused": L.SCHED_FUSED, "passes": L.SCHED_PASSES}[opts.get("schedule", "fused")]
         h = C.c_void_p()
         _check(L.lib().hush_create(C.byref(d), C.byref(h)))
@@ -269,7 +273,7 @@ class Hush:
                                          self._wbuf.size), self._h)
 
     def set_mlp(self, mode: str):
-        _check(L.lib().hush_set_mlp_mode(self._h, {"fp32": 0, "bf16": 1, "f16": 2}[mode]), self._h)
+        _check(L.lib().hush_set_mlp_mode(self._h, MLP_MODES[mode]), self._h)
 
     def set_schedule(self, schedule: str):
         _check(L.lib().hush_set_schedule(self._h, {"fused": 0, "passes": 1}[schedule]), self._h)

@@ -26,9 +26,11 @@ extern "C" {
 typedef struct hush_s hush_t;
 typedef struct svgf_s svgf_t;
 
-/* MLP arithmetic. FP32 is the reference's form (f32 FMA chain, hush.js:683-704); BF16 / F16 run the three layers
- * as tcgen05 tensor-core MMAs with FP32 accumulation (operands rounded to bf16 / f16). */
-enum { HUSH_MLP_FP32 = 0, HUSH_MLP_BF16 = 1, HUSH_MLP_F16 = 2 };
+/* MLP arithmetic. FP32 is the reference's default form (f32 chain, hush.js:683-704); BF16 / F16 run the three
+ * layers as tcgen05 tensor-core MMAs with FP32 accumulation on split-precision operands (each operand as a rounded
+ * hi part plus its rounded residual, so f16 inputs and weights stay exact); HALF is the reference's `f16` option
+ * (hush.js:683-703, 740): f16 products and f16 running sums in the WGSL's order. */
+enum { HUSH_MLP_FP32 = 0, HUSH_MLP_BF16 = 1, HUSH_MLP_F16 = 2, HUSH_MLP_HALF = 3 };
 
 /* Kernel schedule: FUSED (default) = the B200 frame (fused temporal+features+MLP, half-res pyramid, fine+final+TAA);
  * PASSES = one kernel per reference dispatch (hush.js:858-870). Both give the same results. */
@@ -40,7 +42,7 @@ typedef struct {
   float exposure;            /* default 1 when the descriptor comes from hush_desc_default() */
   const uint16_t *weights;   /* f16 blob W1 b1 W2 b2 W3 b3 (hush.js:20-21); NULL = built-in weights */
   size_t n_weights;          /* number of f16 values; the MLP width follows (hiddenOf) */
-  int f16;                   /* reference option `f16` (hush.js:740): selects HUSH_MLP_F16 when mlp_mode is FP32 */
+  int f16;                   /* reference option `f16` (hush.js:740): selects HUSH_MLP_HALF when mlp_mode is FP32 */
   int mlp_mode;              /* HUSH_MLP_* */
   int schedule;              /* HUSH_SCHED_* */
   int device;                /* CUDA device ordinal; -1 = current device */

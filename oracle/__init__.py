@@ -84,6 +84,7 @@ def lib():
             "ho_post_level_size": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
             "ho_post": (C.c_int, [C.POINTER(_PostArgs), P, P, P, P]),
             "ho_f2h_rne": (C.c_uint16, [C.c_float]),
+            "ho_hush_set_mlp_half": (None, [P, C.c_int]),
             "ho_scene_frame": (C.c_int, [C.POINTER(_SceneDesc), C.c_int, P, P, P, P, P, P]),
         }
         for name, (res, args) in sig.items():
@@ -104,15 +105,18 @@ def _as_u16(a: np.ndarray) -> np.ndarray:
 
 
 class OracleHush:
-    """The oracle's Hush instance (mode 0: f32 like the WGSL, mode 1: f64 arithmetic)."""
+    """The oracle's Hush instance (mode 0: f32 like the WGSL, mode 1: f64 arithmetic). f16=True is the reference's
+    `f16` option: INFER's MLP in f16 arithmetic (hush.js:683-703, 740)."""
 
-    def __init__(self, width, height, weights: np.ndarray, exposure=1.0, fp64=False):
+    def __init__(self, width, height, weights: np.ndarray, exposure=1.0, fp64=False, f16=False):
         self.w16 = np.ascontiguousarray(weights.astype(np.uint16))
         self.W, self.H = int(width), int(height)
         self._h = lib().ho_hush_create(self.W, self.H, float(exposure), self.w16.ctypes.data, self.w16.size,
                                        1 if fp64 else 0)
         if not self._h:
             raise ValueError("oracle: bad weights or size")
+        if f16:
+            lib().ho_hush_set_mlp_half(self._h, 1)
         self._keep = None
 
     def _inputs(self, inputs: dict) -> _Inputs:
@@ -223,11 +227,12 @@ def qf16(x: float) -> float:
     return float(lib().ho_qf16(float(x)))
 
 
-def mlp(weights: np.ndarray, features: np.ndarray, fp64=False) -> np.ndarray:
+def mlp(weights: np.ndarray, features: np.ndarray, fp64=False, half=False) -> np.ndarray:
+    """One MLP row: f32 (the default), f64, or half=True for the reference's f16 arithmetic (the `f16` option)."""
     w = np.ascontiguousarray(weights.astype(np.uint16))
     f = np.ascontiguousarray(features.astype(np.float32))
     o = np.zeros(12, dtype=np.float32)
-    lib().ho_mlp(w.ctypes.data, w.size, f.ctypes.data, o.ctypes.data, 1 if fp64 else 0)
+    lib().ho_mlp(w.ctypes.data, w.size, f.ctypes.data, o.ctypes.data, 2 if half else (1 if fp64 else 0))
     return o
 
 

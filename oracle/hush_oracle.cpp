@@ -150,6 +150,7 @@ struct ho_hush {
   float exposure = 1.0f;
   int hidden = 16;
   int fp64 = 0;
+  int mlp_half = 0;  // the `f16` option: the MLP in f16 arithmetic (hush.js:683-703, 740)
   std::vector<float> wf;  // decoded weights (exact f16 values)
   Img A0, X, Bh[2], mom[2], key[2], hist[2], taa[2], par0[2], par1, par2, F[4], C[2], CG;
   Img *buf(int id) {
@@ -190,6 +191,41 @@ template <class T> void mlp(const float *w, int Hd, const T *f, T *o) {
     for (int i = 0; i < Hd; i++) a = a + h2[i] * T(w[W3 + j * Hd + i]);
     o[j] = a;
   }
+}
+
+// mlpCode with f16 = true (hush.js:683-703, selected by the `f16` option at hush.js:740, 750): every value is an f16
+// (features converted with f16(), weights and biases f16 literals), each product input * weight and each running sum
+// bias + p0 + p1 + ... rounds to f16 in that left-to-right order (vec4h arithmetic: a multiply and an add per term,
+// each correctly rounded, round to nearest even), ReLU as max(., 0h); the outputs widen to f32 (vec4f(oh_k)). Every
+// f16 product and every sum of two f16 values is exact in double, so rounding the double once gives the correctly
+// rounded f16 result.
+double h16(double x) {  // round to the nearest f16 value (ties to even), overflow to infinity
+  if (std::isnan(x)) return x;
+  const double ax = std::fabs(x);
+  if (ax >= 65520.0) return std::copysign(INFINITY, x);
+  int e;
+  std::frexp(ax, &e);                      // ax = m * 2^e, m in [0.5, 1)
+  const int q = std::max(e - 11, -24);     // f16 spacing: 2^(e - 11) for normal values, 2^-24 below 2^-14
+  const double u = std::ldexp(1.0, q);
+  return std::copysign(std::nearbyint(ax / u) * u, x);  // default rounding mode: to nearest, ties to even
+}
+void mlp_half(const float *w, int Hd, const float *f, float *o) {
+  const int NF = 20, NO = 12;
+  const int W1 = 0, B1 = Hd * NF, W2 = B1 + Hd, B2 = W2 + Hd * Hd, W3 = B2 + Hd, B3 = W3 + NO * Hd;
+  std::vector<double> x(NF), h1(Hd), h2(Hd);
+  for (int i = 0; i < NF; i++) x[i] = h16(f[i]);
+  auto layer = [&](const std::vector<double> &in, int nin, int wo, int bo, int nout, bool relu, double *out) {
+    for (int j = 0; j < nout; j++) {
+      double a = w[bo + j];  // f16 values already
+      for (int i = 0; i < nin; i++) a = h16(a + h16(in[i] * (double)w[wo + j * nin + i]));
+      out[j] = relu ? (a > 0.0 ? a : 0.0) : a;  // max(., 0h); a NaN sum gives 0, as the GPU's max.f16x2 does
+    }
+  };
+  layer(x, NF, W1, B1, Hd, true, h1.data());
+  layer(h1, Hd, W2, B2, Hd, true, h2.data());
+  std::vector<double> oo(NO);
+  layer(h2, Hd, W3, B3, NO, false, oo.data());
+  for (int j = 0; j < NO; j++) o[j] = (float)oo[j];
 }
 
 // ------------------------------------------------------------------------------------------------ a-trous
@@ -517,7 +553,14 @@ template <class T> void pass_infer(ho_hush *S) {
             e = F2.ld<T>(x, y, 0);
       v4<T> q[5] = {a, b, c, d, e};
       for (int i = 0; i < 5; i++) { f[4 * i] = q[i].x; f[4 * i + 1] = q[i].y; f[4 * i + 2] = q[i].z; f[4 * i + 3] = q[i].w; }
-      mlp<T>(S->wf.data(), S->hidden, f, o);
+      if (S->mlp_half) {
+        float ff[20], oh[12];
+        for (int i = 0; i < 20; i++) ff[i] = (float)f[i];
+        mlp_half(S->wf.data(), S->hidden, ff, oh);
+        for (int i = 0; i < 12; i++) o[i] = T(oh[i]);
+      } else {
+        mlp<T>(S->wf.data(), S->hidden, f, o);
+      }
       T alpha = T(1.0f / 32.0f) + T(31.0f / 32.0f) * sigmoid(o[0]);
       T gamma = T(0.5f) + T(7.5f) * sigmoid(o[1]);
       T beta = sigmoid(o[2]);
@@ -850,11 +893,15 @@ uint16_t *ho_hush_buffer(ho_hush *h, int id, int *w, int *hgt, int *channels) {
   return b->d.data();
 }
 
+void ho_hush_set_mlp_half(ho_hush *h, int on) { h->mlp_half = on ? 1 : 0; }
+
 void ho_mlp(const uint16_t *weights, long n_weights, const float *features, float *out, int fp64) {
   int hd = ho_hidden_of(n_weights);
   std::vector<float> wf(n_weights);
   for (long i = 0; i < n_weights; i++) wf[i] = h2f(weights[i]);
-  if (fp64) {
+  if (fp64 == 2) {
+    mlp_half(wf.data(), hd, features, out);
+  } else if (fp64) {
     double f[20], o[12];
     for (int i = 0; i < 20; i++) f[i] = features[i];
     mlp<double>(wf.data(), hd, f, o);

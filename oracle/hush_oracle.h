@@ -67,8 +67,11 @@ uint16_t ho_f2h_rz(float f);
 float ho_h2f(uint16_t h);
 float ho_qf16(float x);
 
-/* MLP on one feature row (20 inputs) with f16 weights, outputs 12 raw values (mode 0 f32, 1 f64). */
+/* MLP on one feature row (20 inputs) with f16 weights, outputs 12 raw values (mode 0 f32, 1 f64, 2 the reference's
+ * f16 arithmetic of the `f16` option, hush.js:683-703). */
 void ho_mlp(const uint16_t *weights, long n_weights, const float *features, float *out, int fp64);
+/* The `f16` option (hush.js:740): INFER's MLP in f16 arithmetic (mode 2 of ho_mlp); the rest of the frame unchanged. */
+void ho_hush_set_mlp_half(ho_hush *h, int on);
 
 /* SVGF baseline (svgf.js). */
 typedef struct {

@@ -235,3 +235,40 @@ def test_oracle_scene_generator_is_the_product_generator_bit_for_bit():
             for k in oracle.INPUTS:
                 np.testing.assert_array_equal(a[k].view(np.uint16), b[k].view(np.uint16), err_msg=f"{k} frame {i}")
             np.testing.assert_array_equal(a["clean"], b["clean"])
+
+
+def _mlp_half_numpy(w16: np.ndarray, f: np.ndarray) -> np.ndarray:
+    """mlpCode with f16 = true (hush.js:683-703) restated with numpy's correctly rounded float64 -> float16
+    conversion: each product and each running sum rounds to f16 (ties to even) in the WGSL's order."""
+    w = w16.view(np.float16).astype(np.float64)
+    h = int(round((-34 + np.sqrt(34 * 34 - 4 * (12 - w.size))) / 2))
+    W1, B1 = 0, 20 * h
+    W2, B2 = B1 + h, B1 + h + h * h
+    W3, B3 = B2 + h, B2 + h + 12 * h
+    r = lambda v: float(np.float16(v))  # noqa: E731
+
+    def layer(x, nin, wo, bo, nout, relu):
+        out = []
+        for j in range(nout):
+            a = w[bo + j]
+            for i in range(nin):
+                a = r(a + r(x[i] * w[wo + j * nin + i]))
+            out.append(max(a, 0.0) if relu else a)
+        return out
+
+    x = [r(v) for v in f]
+    h1 = layer(x, 20, W1, B1, h, True)
+    h2 = layer(h1, h, W2, B2, h, True)
+    return np.array(layer(h2, h, W3, B3, 12, False), np.float32)
+
+
+def test_f16_arithmetic_mlp_matches_a_numpy_restatement():
+    w = builtin_weights()
+    rng = np.random.default_rng(11)
+    for scale in (0.5, 2.0, 8.0):
+        f = (rng.normal(size=20) * scale).astype(np.float16).astype(np.float32)
+        got = oracle.mlp(w, f, half=True)
+        np.testing.assert_array_equal(got, _mlp_half_numpy(w, f))
+        # f16 arithmetic stays near the f32 form (the hidden sums carry 11 bits)
+        ref = oracle.mlp(w, f)
+        assert np.max(np.abs(got - ref)) <= 2e-2 * max(1.0, np.max(np.abs(ref)))

@@ -294,6 +294,51 @@ def test_tensor_core_mlp_forms(mlp, cfg, n):
         assert fr <= FORM_FRAC, (mlp, i, fr, worst)
 
 
+@pytest.mark.parametrize("sched", ["fused", "passes"])
+def test_f16_option_matches_the_f16_oracle(sched):
+    """The reference's `f16: true` (hush.js:683-703, 740): INFER's MLP in f16 arithmetic (f16 products and running
+    sums in the WGSL's order) against the oracle's f16 mode over the 360p sequence at the 2e-3 bound. The f16 MLP
+    really runs: its stored parameters differ from the FP32 form's."""
+    cfg = scene.CONFIG_360P
+    frames = [scene.frame_host(cfg, i) for i in range(cfg.frames)]
+    o = oracle.OracleHush(cfg.width, cfg.height, builtin_weights(), f16=True)
+    g = Hush(0, {"width": cfg.width, "height": cfg.height, "f16": True, "schedule": sched})
+    a = Hush(0, {"width": cfg.width, "height": cfg.height, "schedule": sched})
+    for i, f in enumerate(frames):
+        dev = _dev(f)
+        ref = o.denoise(f).astype(np.float32)
+        got = to_f32(g.denoise(dev))
+        a.denoise(dev)
+        fr, worst, _ = mismatch(got, ref)
+        print(f"f16 option ({sched}) frame {i}: {fr:.2e} beyond 2e-3 of the f16 oracle (worst {worst:.3g})")
+        assert fr <= FORM_FRAC, (sched, i, fr, worst)
+    torch.cuda.synchronize()
+    assert np.mean(_download(g, "PAR1") != _download(a, "PAR1")) > 1e-2
+
+
+def test_f16_option_infer_pass_matches_the_f16_oracle(seq_small):
+    """INFER alone in f16 arithmetic, started from the f16 oracle's exact state: the parameters and mid1 level."""
+    cfg, frames = seq_small
+    o = oracle.OracleHush(cfg.width, cfg.height, builtin_weights(), f16=True)
+    for f in frames[:3]:
+        o.denoise(f)
+    g = Hush(0, {"width": cfg.width, "height": cfg.height, "schedule": "passes", "f16": True})
+    for _ in range(3):
+        g.end_frame()
+    f = frames[3]
+    fd = _dev(f)
+    c = o.frame & 1
+    for p in oracle.PASS_NAMES[:2]:
+        _upload(o, g)
+        o.run_pass(p, f)
+        g.run_pass(p, fd)
+    torch.cuda.synchronize()
+    for name in PASS_OUTPUTS["infer"]:
+        name = name.format(c=c)
+        frac, worst, _ = mismatch(_download(g, name), o.buffer(name).astype(np.float32))
+        assert frac <= PASS_FRAC, (name, frac, worst)
+
+
 @pytest.mark.parametrize("mlp", ["f16", "bf16"])
 def test_tensor_core_parameters_match_fp32_parameters(mlp):
     """The stored filter parameters (f16, rounded toward zero) of the split-precision forms equal the FP32 form's
