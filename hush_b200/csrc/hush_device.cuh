@@ -153,8 +153,9 @@ HD_INL void mlp_heads(const float *o, float4 &p0, float4 &p1, float4 &p2) {
 // ------------------------------------------------------------------------------------------------ a-trous
 // atrousFn (hush.js:431-476) over shared-memory tiles sA (colour, variance) and sG (decoded normal, depth) of row
 // stride SW. (lx, ly) is the centre's tile position, (qx, qy) its image position, (w, h) the image size for the
-// inside() test. The tiles hold clamp-to-edge loads.
-template <int R, int STEP, bool PREF, int SW>
+// inside() test. The tiles hold clamp-to-edge loads. CHECK = false: the caller knows every tap lies inside the image
+// (an interior tile), so the inside() test is always true and is left out.
+template <int R, int STEP, bool PREF, int SW, bool CHECK = true>
 HD_INL float4 filt(const float4 *sA, const float4 *sG, int lx, int ly, int qx, int qy, int w, int h, float s,
                    float c) {
   const int ti = ly * SW + lx;
@@ -200,10 +201,85 @@ HD_INL float4 filt(const float4 *sA, const float4 *sG, int lx, int ly, int qx, i
       const int o = dy * STEP * SW + dx * STEP;
       const float4 gq = sG[ti + o];
       const int tx = qx + dx * STEP, ty = qy + dy * STEP;
-      if (tx >= 0 && ty >= 0 && tx < w && ty < h && gq.w >= 0.0f) {
+      if ((!CHECK || (tx >= 0 && ty >= 0 && tx < w && ty < h)) && gq.w >= 0.0f) {
         const float4 cq = sA[ti + o];
         const float wt = (hx * hy) * pow128(fmaxf(dot3(gq, gp), 0.0f)) *
                          expf(-fabsf(gq.w - gp.w) * iz[dx * dx + dy * dy] - sl * fabsf(lum(cq) - lc));
+        sw += wt;
+        scx += wt * cq.x;
+        scy += wt * cq.y;
+        scz += wt * cq.z;
+        sv += wt * wt * cq.w;
+      }
+    }
+  }
+  return make_float4(scx / sw, scy / sw, scz / sw, sv / (sw * sw));
+}
+
+// 2^x on the special-function unit (the hardware approximation WGSL's exp may use as well).
+HD_INL float ex2_approx(float x) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+constexpr float LOG2E = 1.4426950408889634f;
+// log2 of the B-spline tap weights h: 1/4, 1/2 (R = 1) and 1/16, 1/4, 3/8 (R = 2)
+HD_INL constexpr float lg_h(int R, int d) {
+  return R == 1 ? (d == 0 ? -1.0f : -2.0f) : (d == 0 ? -1.4150374992788438f : (d == 1 || d == -1) ? -2.0f : -4.0f);
+}
+
+// The fused schedule's atrousFn: the weights of filt() with exp(x) taken as 2^(x log2 e), log2 e folded into the
+// per-centre factors (1 / (zg dist step + 1e-3) and s / sd) and the tap's B-spline weight h_x h_y folded into the
+// exponent as log2(h_x) + log2(h_y); CHECK = false leaves out the inside() test on interior tiles. Same operation
+// order as filt() otherwise; the differences are last-place roundings of the weights.
+template <int R, int STEP, bool PREF, int SW, bool CHECK>
+HD_INL float4 filt_x(const float4 *sA, const float4 *sG, int lx, int ly, int qx, int qy, int w, int h, float s,
+                     float c) {
+  const int ti = ly * SW + lx;
+  const float4 gp = sG[ti];
+  const float4 center = sA[ti];
+  float gv;
+  if (PREF) {
+    gv = 0.0625f * (sA[ti - SW - 1].w + sA[ti - SW + 1].w + sA[ti + SW - 1].w + sA[ti + SW + 1].w) +
+         0.125f * (sA[ti - SW].w + sA[ti - 1].w + sA[ti + 1].w + sA[ti + SW].w) + 0.25f * center.w;
+  } else {
+    gv = center.w;
+  }
+  const float lc = lum(center);
+  const float sll = LOG2E * s / (sqrtf(fmaxf(gv, 1e-12f)) + 1e-6f);
+  const float zl = sG[ti - 1].w, zr = sG[ti + 1].w, zu = sG[ti - SW].w, zd = sG[ti + SW].w;
+  const float gx = fminf(zr > 0.0f ? fabsf(zr - gp.w) : 1e9f, zl > 0.0f ? fabsf(zl - gp.w) : 1e9f);
+  const float gy = fminf(zd > 0.0f ? fabsf(zd - gp.w) : 1e9f, zu > 0.0f ? fabsf(zu - gp.w) : 1e9f);
+  const float zg = fminf(fmaxf(gx, gy), gp.w);
+  float izl[9];
+#pragma unroll
+  for (int d = 1; d <= 2 * R * R; d++) {
+    const float k = d == 1 ? 1.0f * STEP
+                    : d == 2 ? 1.41421356237309515f * STEP
+                    : d == 4 ? 2.0f * STEP
+                    : d == 5 ? 2.23606797749978981f * STEP
+                    : d == 8 ? 2.82842712474619029f * STEP
+                             : 0.0f;
+    izl[d] = LOG2E / (zg * k + 1e-3f);
+  }
+  constexpr float hc = R == 1 ? 0.5f : 0.375f;
+  const float cw = (hc * hc) * c;
+  float sw = cw;
+  float scx = center.x * cw, scy = center.y * cw, scz = center.z * cw;
+  float sv = center.w * cw * cw;
+#pragma unroll
+  for (int dy = -R; dy <= R; dy++) {
+#pragma unroll
+    for (int dx = -R; dx <= R; dx++) {
+      if (dx == 0 && dy == 0) continue;
+      const int o = dy * STEP * SW + dx * STEP;
+      const float4 gq = sG[ti + o];
+      const int tx = qx + dx * STEP, ty = qy + dy * STEP;
+      if ((!CHECK || (tx >= 0 && ty >= 0 && tx < w && ty < h)) && gq.w >= 0.0f) {
+        const float4 cq = sA[ti + o];
+        const float arg = fmaf(-fabsf(gq.w - gp.w), izl[dx * dx + dy * dy],
+                               fmaf(-sll, fabsf(lum(cq) - lc), lg_h(R, dx) + lg_h(R, dy)));
+        const float wt = pow128(fmaxf(dot3(gq, gp), 0.0f)) * ex2_approx(arg);
         sw += wt;
         scx += wt * cq.x;
         scy += wt * cq.y;
@@ -462,6 +538,14 @@ HD_INL bool block_features(const PixP *P, const float4 *sI, int t0, float E, flo
 }
 
 // ------------------------------------------------------------------------------------------------ FINE_FINAL
+// jbw() for the fused schedule: rzl = log2(e) / (0.05 z + 1e-3), formed once per pixel; exp as 2^(x log2 e).
+HD_INL float jbw_x(float frx, float fry, int j, float4 nq, float zq, float4 n, float z, float rzl) {
+  const float wb = ((j & 1) == 1 ? frx : 1.0f - frx) * ((j >> 1) == 1 ? fry : 1.0f - fry);
+  const float dn = fmaxf(dot3(nq, n), 0.0f);
+  const float dn2 = dn * dn;
+  const float dn4 = dn2 * dn2;
+  return wb * ex2_approx(-fabsf(zq - z) * rzl) * dn4 * dn4;
+}
 HD_INL float jbw(float frx, float fry, int j, float4 nq, float zq, float4 n, float z) {  // hush.js:552-558
   const float wb = ((j & 1) == 1 ? frx : 1.0f - frx) * ((j >> 1) == 1 ? fry : 1.0f - fry);
   const float dn = fmaxf(dot3(nq, n), 0.0f);

@@ -704,7 +704,14 @@ HD_INL void tile_mid1(const HushFrame &f, int tileX, int tileY, float4 *sA, floa
   __shared__ alignas(8) uint64_t mbar;
   const int li = threadIdx.x;
   const int bx = tileX * HT_W, by = tileY * HT_H;
-  const bool inner = M && bx - 2 >= 0 && by - 1 >= 0 && bx + HT_W + 2 <= f.W2 && by + HT_H + 1 <= f.H2;
+  const bool interior = bx - 2 >= 0 && by - 1 >= 0 && bx + HT_W + 2 <= f.W2 && by + HT_H + 1 <= f.H2;
+  const bool inner = M && interior;
+  const int X = bx + li % HT_W, Y = by + li / HT_W;
+  const bool in_img = X < f.W2 && Y < f.H2;
+  const int o = Y * f.W2 + X;
+  // this pixel's parameters, in flight while the tile arrives
+  uint2 p1 = make_uint2(0, 0), p2 = make_uint2(0, 0);
+  if (in_img) { p1 = __ldg(f.par1 + o); p2 = __ldg(f.par2 + o); }
   bool staged = false;
   if (inner) {
     const uint32_t mb = umma::smem_u32(&mbar);
@@ -727,13 +734,12 @@ HD_INL void tile_mid1(const HushFrame &f, int tileX, int tileY, float4 *sA, floa
     }
   }
   __syncthreads();
-  const int X = bx + li % HT_W, Y = by + li / HT_W;
-  if (X >= f.W2 || Y >= f.H2) return;
+  if (!in_img) return;
   const int lx = li % HT_W + AP, ly = li / HT_W + AP;
-  const int o = Y * f.W2 + X;
   if (sG[ly * SW + lx].w < 0.0f) { sth(f.Bh0, o, make_float4(0.f, 0.f, 0.f, 0.f)); return; }
-  const float s = ldh(f.par1, o).y, c = ldh(f.par2, o).y;
-  sth(f.Bh0, o, filt<1, 1, true, SW>(sA, sG, lx, ly, X, Y, f.W2, f.H2, s, c));
+  const float s = h4_to_f4(p1).y, c = h4_to_f4(p2).y;
+  sth(f.Bh0, o, interior ? filt_x<1, 1, true, SW, false>(sA, sG, lx, ly, X, Y, f.W2, f.H2, s, c)
+                         : filt_x<1, 1, true, SW, true>(sA, sG, lx, ly, X, Y, f.W2, f.H2, s, c));
 }
 
 template <int STEP, int COMP>
@@ -744,7 +750,13 @@ HD_INL void tile_mid(const HushFrame &f, int tileX, int tileY, const uint2 *src,
   __shared__ alignas(8) uint64_t mbar;
   const int li = threadIdx.x;
   const int bx = tileX * HT_W, by = tileY * HT_H;
-  const bool inner = mg && bx - AP >= 0 && by - AP >= 0 && bx + HT_W + AP <= f.W2 && by + HT_H + AP <= f.H2;
+  const bool interior = bx - AP >= 0 && by - AP >= 0 && bx + HT_W + AP <= f.W2 && by + HT_H + AP <= f.H2;
+  const bool inner = mg && interior;
+  const int X = bx + li % HT_W, Y = by + li / HT_W;
+  const bool in_img = X < f.W2 && Y < f.H2;
+  const int o = Y * f.W2 + X;
+  uint2 p1 = make_uint2(0, 0), p2 = make_uint2(0, 0);  // this pixel's parameters, in flight with the tile
+  if (in_img) { p1 = __ldg(f.par1 + o); p2 = __ldg(f.par2 + o); }
   bool staged = false;
   if (inner) {
     const uint32_t mb = umma::smem_u32(&mbar);
@@ -767,14 +779,13 @@ HD_INL void tile_mid(const HushFrame &f, int tileX, int tileY, const uint2 *src,
     }
   }
   __syncthreads();
-  const int X = bx + li % HT_W, Y = by + li / HT_W;
-  if (X >= f.W2 || Y >= f.H2) return;
+  if (!in_img) return;
   const int lx = li % HT_W + AP, ly = li / HT_W + AP;
-  const int o = Y * f.W2 + X;
   if (sG[ly * SW + lx].w < 0.0f) { sth(dst, o, make_float4(0.f, 0.f, 0.f, 0.f)); return; }
-  const float4 a = ldh(f.par1, o), b = ldh(f.par2, o);
+  const float4 a = h4_to_f4(p1), b = h4_to_f4(p2);
   const float s = COMP == 2 ? a.z : a.w, c = COMP == 2 ? b.z : b.w;
-  sth(dst, o, filt<1, STEP, false, SW>(sA, sG, lx, ly, X, Y, f.W2, f.H2, s, c));
+  sth(dst, o, interior ? filt_x<1, STEP, false, SW, false>(sA, sG, lx, ly, X, Y, f.W2, f.H2, s, c)
+                       : filt_x<1, STEP, false, SW, true>(sA, sG, lx, ly, X, Y, f.W2, f.H2, s, c));
 }
 
 // down() (hush.js:385-402) from the half-res planes.
@@ -827,7 +838,9 @@ HD_INL void tile_coarse1(const HushFrame &f, int tileX, int tileY, float4 *sA, f
   if (X >= f.W4 || Y >= f.H4) return;
   const int lx = li % HT_W + AP, ly = li / HT_W + AP;
   if (sG[ly * SW + lx].w < 0.0f) { sth(f.C1, Y * f.W4 + X, make_float4(0.f, 0.f, 0.f, 0.f)); return; }
-  sth(f.C1, Y * f.W4 + X, filt<2, 1, true, SW>(sA, sG, lx, ly, X, Y, f.W4, f.H4, COARSE_S, 1.0f));
+  const bool interior = bx - AP >= 0 && by - AP >= 0 && bx + HT_W + AP <= f.W4 && by + HT_H + AP <= f.H4;
+  sth(f.C1, Y * f.W4 + X, interior ? filt_x<2, 1, true, SW, false>(sA, sG, lx, ly, X, Y, f.W4, f.H4, COARSE_S, 1.0f)
+                                   : filt_x<2, 1, true, SW, true>(sA, sG, lx, ly, X, Y, f.W4, f.H4, COARSE_S, 1.0f));
 }
 
 // coarse2 (hush.js:482-525, kind coarse): C1 and the decoded quarter-res guide, apron 4; interior tiles by TMA as
@@ -865,7 +878,9 @@ HD_INL void tile_coarse2(const HushFrame &f, int tileX, int tileY, float4 *sA, f
   if (X >= f.W4 || Y >= f.H4) return;
   const int lx = li % HT_W + AP, ly = li / HT_W + AP;
   if (sG[ly * SW + lx].w < 0.0f) { sth(f.C0, Y * f.W4 + X, make_float4(0.f, 0.f, 0.f, 0.f)); return; }
-  sth(f.C0, Y * f.W4 + X, filt<2, 2, true, SW>(sA, sG, lx, ly, X, Y, f.W4, f.H4, COARSE_S, 1.0f));
+  const bool interior = bx - AP >= 0 && by - AP >= 0 && bx + HT_W + AP <= f.W4 && by + HT_H + AP <= f.H4;
+  sth(f.C0, Y * f.W4 + X, interior ? filt_x<2, 2, true, SW, false>(sA, sG, lx, ly, X, Y, f.W4, f.H4, COARSE_S, 1.0f)
+                                   : filt_x<2, 2, true, SW, true>(sA, sG, lx, ly, X, Y, f.W4, f.H4, COARSE_S, 1.0f));
 }
 
 // stage 1: mid1 tiles then coarse1 tiles; stage 2: mid2 tiles then coarse2 tiles; stage 3: mid3 tiles.
@@ -909,8 +924,17 @@ __global__ void __launch_bounds__(FT_W *FT_H, 3) k_fine_final_fused(const __grid
   __shared__ alignas(8) uint64_t mbar;
   const int li = threadIdx.x;
   const int bx = blockIdx.x * FT_W, by = blockIdx.y * FT_H;
-  const bool inner = M.ok && bx - 2 >= 0 && by - 1 >= 0 && bx + FT_W + 2 <= f.W && by + FT_H + 1 <= f.H;
+  const bool interior = bx - 2 >= 0 && by - 1 >= 0 && bx + FT_W + 2 <= f.W && by + FT_H + 1 <= f.H;
+  const bool inner = M.ok && interior;
   const uint32_t mb = umma::smem_u32(&mbar);
+  // this pixel's material and emission, in flight while the tiles arrive
+  const int px = bx + li % FT_W, py = by + li / FT_W;
+  const bool in_img = px < f.W && py < f.H;
+  uint2 mat_r = make_uint2(0, 0), emi_r = make_uint2(0, 0);
+  if (in_img) {
+    mat_r = __ldg(f.mat + py * f.p_mat + px);
+    emi_r = __ldg(f.emi + py * f.p_emi + px);
+  }
   if (inner) {
     if (li == 0) {
       umma::mbar_init(mb, 1);
@@ -961,10 +985,9 @@ __global__ void __launch_bounds__(FT_W *FT_H, 3) k_fine_final_fused(const __grid
     }
   }
   __syncthreads();
-  const int px = bx + li % FT_W, py = by + li / FT_W;
-  if (px >= f.W || py >= f.H) return;
+  if (!in_img) return;
   const int lx = li % FT_W + AP, ly = li / FT_W + AP;
-  const float4 alb = ldh(f.mat, py * f.p_mat + px), emi = ldh(f.emi, py * f.p_emi + px);
+  const float4 alb = h4_to_f4(mat_r), emi = h4_to_f4(emi_r);
   const float4 gp = sG[ly * SW + lx];
   const int o = py * f.W + px;
   if (gp.w < 0.0f) {
@@ -973,11 +996,13 @@ __global__ void __launch_bounds__(FT_W *FT_H, 3) k_fine_final_fused(const __grid
     return;
   }
   const float4 pr = sPar[((py - by) >> 1) * (FT_W / 2) + ((px - bx) >> 1)];
-  const float4 A1 = filt<1, 1, true, SW>(sA, sG, lx, ly, px, py, f.W, f.H, pr.x, pr.y);
+  const float4 A1 = interior ? filt_x<1, 1, true, SW, false>(sA, sG, lx, ly, px, py, f.W, f.H, pr.x, pr.y)
+                             : filt_x<1, 1, true, SW, true>(sA, sG, lx, ly, px, py, f.W, f.H, pr.x, pr.y);
   sth(f.hist, o, A1);
   // recombination (hush.js:580-620) with the half-res block means (Ah) and decoded guides (Gd, CGd)
   const float fx = qf16(A1.x), fy = qf16(A1.y), fz = qf16(A1.z);
   const float z = gp.w;
+  const float rzl = LOG2E / (0.05f * z + 1e-3f);
   const int hsx = (f.W + 1) / 2, hsy = (f.H + 1) / 2;
   const float hposx = ((float)px + 0.5f) / 2.0f - 0.5f, hposy = ((float)py + 0.5f) / 2.0f - 0.5f;
   const float hbx = floorf(hposx), hby = floorf(hposy);
@@ -991,7 +1016,7 @@ __global__ void __launch_bounds__(FT_W *FT_H, 3) k_fine_final_fused(const __grid
     const int t = (qy - hy0) * FH_W + (qx - hx0);
     const float4 gh = sHG[t];
     if (!(qx >= 0 && qy >= 0 && qx < hsx && qy < hsy) || gh.w < 0.0f) continue;
-    const float w = jbw(hposx - hbx, hposy - hby, j, gh, gh.w, gp, z);
+    const float w = jbw_x(hposx - hbx, hposy - hby, j, gh, gh.w, gp, z, rzl);
     const float4 a = sHA[t], m = sHB[t];
     swh += w;
     uBx += w * m.x; uBy += w * m.y; uBz += w * m.z;
@@ -1010,7 +1035,7 @@ __global__ void __launch_bounds__(FT_W *FT_H, 3) k_fine_final_fused(const __grid
     const int t = (ry - qy0) * FQ_W + (rx - qx0);
     const float4 cg = sQG[t];
     if (!(rx >= 0 && ry >= 0 && rx < qsx && ry < qsy) || cg.w < 0.0f) continue;
-    const float w = jbw(cposx - cbx, cposy - cby, j, cg, cg.w, gp, z);
+    const float w = jbw_x(cposx - cbx, cposy - cby, j, cg, cg.w, gp, z, rzl);
     const float4 c = sQC[t];
     swq += w;
     uCx += w * c.x; uCy += w * c.y; uCz += w * c.z;
