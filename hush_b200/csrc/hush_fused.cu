@@ -21,6 +21,7 @@
 #include <type_traits>
 
 #include "hush_device.cuh"
+#include "hush_pair.cuh"
 #include "hush_internal.h"
 #include "umma.cuh"
 
@@ -883,6 +884,78 @@ HD_INL void tile_coarse2(const HushFrame &f, int tileX, int tileY, float4 *sA, f
                                    : filt_x<2, 2, true, SW, true>(sA, sG, lx, ly, X, Y, f.W4, f.H4, COARSE_S, 1.0f));
 }
 
+// mid2 / mid3 (hush.js:482-525, 753-754) on 32 x 8 tiles in two-pixel lanes (filt_pair): the level and the decoded
+// guide of the (32 + 2 STEP) x (8 + 2 STEP) window are loaded as texel pairs (one 16-byte load for the two 8-byte
+// level texels of an even column pair when the row pitch allows it, clamped single loads at the image border), every
+// load of the thread issued before the first is unpacked, and stored in the even-column pair layout.
+constexpr int MP_W = 32;  // tile width of the two-pixel mid tiles (16 lanes x 8 rows)
+template <int STEP>
+constexpr int mid_pair_smem() {
+  return 4 * ((MP_W + 2 * STEP) / 2) * (HT_H + 2 * STEP) * 16;
+}
+template <int STEP, int COMP>
+HD_INL void tile_mid_pair(const HushFrame &f, int tileX, int tileY, const uint2 *src, uint2 *dst, float4 *smem) {
+  constexpr int AP = STEP, SW = MP_W + 2 * AP, SH = HT_H + 2 * AP, EW = SW / 2, NE = EW * SH;
+  constexpr int NT = HT_W * HT_H, NIT = (NE + NT - 1) / NT;
+  const PairTile T{smem, smem + NE, smem + 2 * NE, smem + 3 * NE};
+  const int li = threadIdx.x;
+  const int bx = tileX * MP_W, by = tileY * HT_H;
+  const bool interior = bx - AP >= 0 && by - AP >= 0 && bx + MP_W + AP <= f.W2 && by + HT_H + AP <= f.H2;
+  const int tx = li % (MP_W / 2), ty = li / (MP_W / 2);
+  const int X = bx + 2 * tx, Y = by + ty;
+  const bool in0 = X < f.W2 && Y < f.H2, in1 = in0 && X + 1 < f.W2;
+  const int o = Y * f.W2 + X;
+  // this pair's parameters, in flight with the tile
+  uint2 pa1 = make_uint2(0, 0), pa2 = pa1, pb1 = pa1, pb2 = pa1;
+  if (in0) { pa1 = __ldg(f.par1 + o); pa2 = __ldg(f.par2 + o); }
+  if (in1) { pb1 = __ldg(f.par1 + o + 1); pb2 = __ldg(f.par2 + o + 1); }
+  const bool even_w = !(f.W2 & 1);
+  uint4 lv[NIT];
+  float4 qa[NIT], qb[NIT];
+#pragma unroll
+  for (int i = 0; i < NIT; i++) {
+    const int e = li + i * NT;
+    const int r = e / EW, k = e % EW;
+    const int gy = clampi(by - AP + r, 0, f.H2 - 1), gx = bx - AP + 2 * k;
+    const int x0 = clampi(gx, 0, f.W2 - 1), x1 = clampi(gx + 1, 0, f.W2 - 1);
+    if (e < NE) {
+      if (even_w && gx >= 0 && gx + 1 < f.W2) {
+        lv[i] = __ldg(reinterpret_cast<const uint4 *>(src + gy * f.W2 + gx));
+      } else {
+        const uint2 a = __ldg(src + gy * f.W2 + x0), b = __ldg(src + gy * f.W2 + x1);
+        lv[i] = make_uint4(a.x, a.y, b.x, b.y);
+      }
+      qa[i] = __ldg(f.Gd + gy * f.W2 + x0);
+      qb[i] = __ldg(f.Gd + gy * f.W2 + x1);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < NIT; i++) {
+    const int e = li + i * NT;
+    if (e < NE)
+      pair_put(T, e, h4_to_f4(make_uint2(lv[i].x, lv[i].y)), h4_to_f4(make_uint2(lv[i].z, lv[i].w)), qa[i], qb[i]);
+  }
+  __syncthreads();
+  if (!in0) return;
+  const float4 a0 = h4_to_f4(pa1), b0 = h4_to_f4(pa2), a1 = h4_to_f4(pb1), b1 = h4_to_f4(pb2);
+  const float2 s = COMP == 2 ? f2(a0.z, a1.z) : f2(a0.w, a1.w), c = COMP == 2 ? f2(b0.z, b1.z) : f2(b0.w, b1.w);
+  const int row = ty + AP, col = 2 * tx + AP;
+  float4 r0, r1;
+  if (interior) filt_pair<1, STEP, false, false, false, EW>(T, row, col, X, Y, f.W2, f.H2, s, c, r0, r1);
+  else filt_pair<1, STEP, false, false, true, EW>(T, row, col, X, Y, f.W2, f.H2, s, c, r0, r1);
+  const float4 zc = T.g1[pe<false, EW>(row, col)];  // centre depths (z, z') in .z / .w
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (zc.z < 0.0f) r0 = z4;  // sky centres write zeros (hush.js:505)
+  if (zc.w < 0.0f) r1 = z4;
+  if (in1 && even_w) {
+    const uint2 u0 = f4_to_h4(r0), u1 = f4_to_h4(r1);
+    *reinterpret_cast<uint4 *>(dst + o) = make_uint4(u0.x, u0.y, u1.x, u1.y);
+  } else {
+    sth(dst, o, r0);
+    if (in1) sth(dst, o + 1, r1);
+  }
+}
+
 // stage 1: mid1 tiles then coarse1 tiles; stage 2: mid2 tiles then coarse2 tiles; stage 3: mid3 tiles.
 template <int STAGE>
 __global__ void __launch_bounds__(HT_W *HT_H) k_half_stage(const __grid_constant__ HushFrame f, int nAx, int nA,
@@ -900,6 +973,23 @@ __global__ void __launch_bounds__(HT_W *HT_H) k_half_stage(const __grid_constant
     const int t = b - nA, tX = t % nBx, tY = t / nBx;
     if (STAGE == 1) tile_coarse1(f, tX, tY, sA, sG);
     else if (STAGE == 2) tile_coarse2(f, tX, tY, sA, sG, M.qok ? &M : nullptr);
+  }
+}
+
+// stages 2 and 3 with the two-pixel mid tiles: 32 x 8 mid2 / mid3 tiles (blockIdx.x < nA), then stage 2's coarse2
+// tiles (16 x 8, quarter resolution). Dynamic shared memory: the pair tile, or coarse2's two float4 tiles.
+template <int STAGE>
+__global__ void __launch_bounds__(HT_W *HT_H) k_half_pair(const __grid_constant__ HushFrame f, int nAx, int nA,
+                                                          int nBx, const __grid_constant__ HalfMaps M) {
+  extern __shared__ __align__(128) float4 hp_smem[];  // 128-byte aligned: coarse2 stages its guide by TMA
+  const int b = blockIdx.x;
+  if (b < nA) {
+    if (STAGE == 2) tile_mid_pair<2, 2>(f, b % nAx, b / nAx, f.Bh0, f.Bh1, hp_smem);
+    else tile_mid_pair<4, 3>(f, b % nAx, b / nAx, f.Bh1, f.Bh0, hp_smem);
+  } else if (STAGE == 2) {
+    constexpr int SMAX = (HT_W + 8) * (HT_H + 8);
+    const int t = b - nA;
+    tile_coarse2(f, t % nBx, t / nBx, hp_smem, hp_smem + SMAX, M.qok ? &M : nullptr);
   }
 }
 
@@ -1246,6 +1336,7 @@ cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpW16 &w16,
                                cudaStream_t st) {
   const int hx = (f.W2 + HT_W - 1) / HT_W, hy = (f.H2 + HT_H - 1) / HT_H;
   const int qx = (f.W4 + HT_W - 1) / HT_W, qy = (f.H4 + HT_H - 1) / HT_H;
+  const int hpx = (f.W2 + MP_W - 1) / MP_W;  // two-pixel mid tiles per row
   switch (stage) {
     case 0: {
       // blob: bf16 hi / lo operands, f16 operands, then the transposed FP32 weights
@@ -1275,8 +1366,13 @@ cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpW16 &w16,
       break;
     }
     case 1: k_half_stage<1><<<hx * hy + qx * qy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx, half_maps(f)); break;
-    case 2: k_half_stage<2><<<hx * hy + qx * qy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx, half_maps(f)); break;
-    case 3: k_half_stage<3><<<hx * hy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx, half_maps(f)); break;
+    case 2: {
+      constexpr int sm = mid_pair_smem<2>() > 2 * (HT_W + 8) * (HT_H + 8) * 16 ? mid_pair_smem<2>()
+                                                                               : 2 * (HT_W + 8) * (HT_H + 8) * 16;
+      k_half_pair<2><<<hpx * hy + qx * qy, HT_W * HT_H, sm, st>>>(f, hpx, hpx * hy, qx, half_maps(f));
+      break;
+    }
+    case 3: k_half_pair<3><<<hpx * hy, HT_W * HT_H, mid_pair_smem<4>(), st>>>(f, hpx, hpx * hy, qx, half_maps(f)); break;
     case 4:
       k_fine_final_fused<<<dim3((f.W + FT_W - 1) / FT_W, (f.H + FT_H - 1) / FT_H), FT_W * FT_H, 0, st>>>(f, fine_maps(f));
       break;
