@@ -62,9 +62,9 @@ class HushPostInputs(C.Structure):
 
 
 # the training twin's passes (hush_twin_pass) and buffers (hush_trainer_buf)
-TWIN_PASSES = ["mlp", "mid1", "mid2", "mid3", "fine", "taa", "loss"]
+TWIN_PASSES = ["mlp", "mid1", "mid2", "mid3", "fine", "taa", "loss", "temporal"]
 TWIN_BUF_NAMES = ["THETA", "GRAD", "LOSS", "PAR", "DPAR", "B1", "B2", "B3", "DB1", "DB2", "DB3", "A1", "X", "DX", "OUT",
-                  "OUT_PREV", "DOUT"]
+                  "OUT_PREV", "DOUT", "DA0", "DA1", "DMOM", "DHIST", "DMOM_PREV", "DAG"]
 
 POST_LEVELS = 6
 POST_RGBA8, POST_BGRA8, POST_RGBA32F = 0, 1, 2
@@ -123,6 +123,8 @@ _SIGS = {
     "hush_trainer_set_mlp": (C.c_int, [_P, C.c_int]),
     "hush_trainer_windows": (C.c_int, [_P, C.POINTER(HushScene), C.POINTER(C.c_uint32), C.c_int, C.c_int,
                                        C.c_float, _P]),
+    "hush_trainer_window_bptt": (C.c_int, [_P, C.POINTER(HushInputs), C.POINTER(C.c_void_p), C.c_int, C.c_float,
+                                           _P]),
     "hush_trainer_begin": (C.c_int, [_P, C.POINTER(HushInputs), C.c_void_p, C.c_void_p, C.c_float, _P]),
     "hush_trainer_zero_adjoints": (C.c_int, [_P, _P]),
     "hush_trainer_buffer": (C.c_int, [_P, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int), C.POINTER(C.c_int),

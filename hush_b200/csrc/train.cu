@@ -45,6 +45,8 @@ struct TwinFrame {
   const float *clean, *clean_prev;  // full: noise-free rgb (f32, dense), previous frame's
   float4 *gT;             // full: gradient w.r.t. the tone-mapped colour tm(X)
   float4 *dB1, *dB2, *dB3;  // half: level gradients
+  const float4 *gA1;        // full: dL/d fine level through the colour history (the next frame's TEMPORAL), or NULL
+  float4 *dA0;              // full: dL/d TEMPORAL's colour + variance A0 (the fine level's input), or NULL
   float4 *dpar;           // half: 3 float4 per row
   float *partials;        // per-CTA weight-gradient partials (NW floats each)
   double *loss_partials;  // per-CTA loss partials
@@ -190,7 +192,7 @@ struct Filt1 {
   // Adjoint for output gradient (g_rgb, g_v): parameter gradients ds, dc and, if dIn != nullptr, the input-level
   // gradient scattered to the taps (image index of the tile centre pix, tap offsets STEP on a row pitch of `pitch`).
   HD_INL void adjoint(const float4 *sA, int ti, float3 g, float g_v, float s, float &ds, float &dc, float4 *dIn,
-                      int pix, int pitch) const {
+                      int pix, int pitch, float *dgv_out = nullptr) const {
     const float o_r = S.x / W, o_g = S.y / W, o_b = S.z / W, ov = V / (W * W);
     const float3 gS = make_float3(g.x / W, g.y / W, g.z / W);
     const float gV = g_v / (W * W);
@@ -222,8 +224,9 @@ struct Filt1 {
       }
     }
     ds = dsl / den;
+    const float dgv = gv > 1e-12f ? dsl * (-s / (den * den)) * (0.5f / sqrtf(gv)) : 0.0f;
+    if (dgv_out) *dgv_out = dgv;  // with the prefilter, the caller spreads it over the 3x3 variances
     if (dIn) {
-      const float dgv = gv > 1e-12f ? dsl * (-s / (den * den)) * (0.5f / sqrtf(gv)) : 0.0f;
       // centre: direct terms, luminance through every tap's weight, variance through sl (no prefilter here)
       atomic_add4(dIn + pix, make_float4(gS.x * cw + dlp * 0.2126f, gS.y * cw + dlp * 0.7152f, gS.z * cw + dlp * 0.0722f,
                                          gV * cw * cw + (PREF ? 0.0f : dgv)));
@@ -699,8 +702,23 @@ __global__ void __launch_bounds__(TW *TH) k_fine_bwd(const TwinFrame T, const fl
         atomicAdd(d + 2, gill.z * w);
       }
     }
-    float ds, dc;
-    F.adjoint(sA, ti, gf, 0.0f, p1.x, ds, dc, nullptr, 0, 0);
+    float gv1 = 0.0f;  // the fine level's variance reaches X through nothing; only the history may seed it
+    if (T.gA1) {       // the next frame reads this fine level as its colour history
+      const float4 h = T.gA1[o];
+      gf = make_float3(gf.x + h.x, gf.y + h.y, gf.z + h.z);
+      gv1 = h.w;
+    }
+    float ds, dc, dgv = 0.0f;
+    F.adjoint(sA, ti, gf, gv1, p1.x, ds, dc, T.dA0, o, f.W, &dgv);
+    if (T.dA0 && dgv != 0.0f) {  // the 3x3 variance prefilter (clamp-to-edge taps): 1/16 corners, 1/8 edges, 1/4 centre
+#pragma unroll
+      for (int j = 0; j < 9; j++) {
+        const int dx = j % 3 - 1, dy = j / 3 - 1;
+        const float k = (dx == 0 && dy == 0) ? 0.25f : ((dx == 0 || dy == 0) ? 0.125f : 0.0625f);
+        const int q = clampi(py + dy, 0, f.H - 1) * f.W + clampi(px + dx, 0, f.W - 1);
+        atomicAdd(&T.dA0[q].w, k * dgv);
+      }
+    }
     q4[0] = gbeta; q4[1] = gkappa; q4[2] = ds; q4[3] = dc;
   }
   // the 2 x 2 pixels of a half-res block are lanes l, l ^ 1, l ^ 16 and l ^ 17 of one warp (16-pixel rows, even
@@ -717,6 +735,184 @@ __global__ void __launch_bounds__(TW *TH) k_fine_bwd(const TwinFrame T, const fl
     atomicAdd(d1 + 0, q4[2]);
     atomicAdd(d2 + 0, q4[3]);
   }
+}
+
+// ------------------------------------------------------------------------------------------------ TEMPORAL adjoint
+// Adjoint of TEMPORAL's pixel() (hush.js:111-223) through the two outputs that carry gradient across frames: the
+// colour + variance A0 (the fine level's input) and the moments (m1, m2, fast mean, history length) that the next
+// frame reprojects. Seeds gA (dL/dA0) and gM (dL/d moments; may be NULL); it ADDS dL/d(previous colour history) into
+// dhist, dL/d(previous moments) into dmom and dL/d(previous frame's alpha, gamma) into dag (half-res, per pixel of
+// the previous par0). The f16 storage of A0, the moments, the history and par0 counts as the identity (a straight-
+// through gradient). The forward is recomputed from the frame's G-buffer and the previous frame's stored history
+// with temporal_pixel()'s arithmetic: the 3x3 statistics (no gradient: they depend on this frame's inputs only), the
+// bilinear reprojection with its key tests or the 3x3 fallback (the tap weights depend on the motion only, so the
+// history enters linearly), the anti-lag clamp mu +- gamma sd (hush.js:195), the blend a = max(alpha, 1 / len)
+// (hush.js:196-199), the moment updates (hush.js:200) and the variance lerp (hush.js:206-207). The lag metric and the
+// block features are not differentiated: the MLP's inputs are held fixed.
+__global__ void __launch_bounds__(TW *TH) k_temporal_bwd(const TwinFrame T, const float4 *gA, const float4 *gM,
+                                                         float4 *dhist, float4 *dmom, float2 *dag) {
+  constexpr int SW = TW + 2, SH = TH + 2;
+  __shared__ float4 sI[SW * SH];
+  const HushFrame &f = T.f;
+  const int li = threadIdx.y * TW + threadIdx.x;
+  const int ox = blockIdx.x * TW - 1, oy = blockIdx.y * TH - 1;
+  for (int i = li; i < SW * SH; i += TW * TH) {  // the illumination tile of k_temporal
+    const int qx = ox + i % SW, qy = oy + i / SW;
+    float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (qx >= 0 && qy >= 0 && qx < f.W && qy < f.H && ldh(f.nd, qy * f.p_nd + qx).w >= 0.0f) {
+      const float4 r = ldh(f.rad, qy * f.p_rad + qx), m = ldh(f.mat, qy * f.p_mat + qx);
+      e = make_float4(r.x / fmaxf(m.x, 1e-3f), r.y / fmaxf(m.y, 1e-3f), r.z / fmaxf(m.z, 1e-3f), 1.0f);
+    }
+    sI[i] = e;
+  }
+  __syncthreads();
+  const int px = blockIdx.x * TW + threadIdx.x, py = blockIdx.y * TH + threadIdx.y;
+  if (px >= f.W || py >= f.H || f.reset) return;
+  const int W = f.W, H = f.H;
+  const float4 nd = ldh(f.nd, py * f.p_nd + px);
+  if (nd.w < 0.0f) return;
+  const float4 mv = ldh(f.mv, py * f.p_mv + px);
+  const int o = py * W + px;
+  const int ti = (threadIdx.y + 1) * SW + threadIdx.x + 1;
+  const float4 illum = sI[ti];
+  const float l = lum(illum);
+  float s1x = 0.f, s1y = 0.f, s1z = 0.f, cnt = 0.f;
+  for (int j = 0; j < 9; j++) {
+    const float4 c = sI[ti + (j / 3 - 1) * SW + (j % 3 - 1)];
+    s1x += c.x * c.w; s1y += c.y * c.w; s1z += c.z * c.w;
+    cnt += c.w;
+  }
+  cnt = fmaxf(cnt, 1.0f);
+  const float mu[3] = {s1x / cnt, s1y / cnt, s1z / cnt};
+  const float slm = lum3(mu[0], mu[1], mu[2]);
+  float sv[3] = {0.f, 0.f, 0.f}, svar = 0.f;
+  for (int j = 0; j < 9; j++) {
+    const float4 c = sI[ti + (j / 3 - 1) * SW + (j % 3 - 1)];
+    const float dx = c.x - mu[0], dy = c.y - mu[1], dz = c.z - mu[2];
+    const float dl = lum(c) - slm;
+    sv[0] += c.w * dx * dx; sv[1] += c.w * dy * dy; sv[2] += c.w * dz * dz;
+    svar += c.w * dl * dl;
+  }
+  const float sd[3] = {sqrtf(fmaxf(sv[0] / cnt, 1e-12f)), sqrtf(fmaxf(sv[1] / cnt, 1e-12f)),
+                       sqrtf(fmaxf(sv[2] / cnt, 1e-12f))};
+  svar /= cnt;
+  // reprojection: the taps, their normalised weights and whether the history is used
+  const float ppx = (float)px + mv.x, ppy = (float)py + mv.y;
+  const float bxf = floorf(ppx), byf = floorf(ppy);
+  const float fx = ppx - bxf, fy = ppy - byf;
+  const int bix = __float2int_rz(bxf), biy = __float2int_rz(byf);
+  const int cx = __float2int_rz(floorf(ppx + 0.5f)), cy = __float2int_rz(floorf(ppy + 0.5f));
+  int tq[9];
+  float tw[9];
+  int nt = 0;
+  float hc[3] = {0.f, 0.f, 0.f};
+  float4 hm = make_float4(0.f, 0.f, 0.f, 0.f);
+  float sumW = 0.f;
+  const float wts[4] = {(1.0f - fx) * (1.0f - fy), fx * (1.0f - fy), (1.0f - fx) * fy, fx * fy};
+  for (int i = 0; i < 4; i++) {
+    const int qx = bix + (i & 1), qy = biy + (i >> 1);
+    if (wts[i] > 0.0f && qx >= 0 && qy >= 0 && qx < W && qy < H &&
+        check_key(ldh(f.key_prev, qy * W + qx), nd, mv.w, mv.z)) {
+      const int q = qy * W + qx;
+      const float4 c = ldh(f.hist_prev, q), m = ldh(f.mom_prev, q);
+      sumW += wts[i];
+      hc[0] += wts[i] * c.x; hc[1] += wts[i] * c.y; hc[2] += wts[i] * c.z;
+      hm.x += wts[i] * m.x; hm.y += wts[i] * m.y; hm.z += wts[i] * m.z; hm.w += wts[i] * m.w;
+      tq[nt] = q;
+      tw[nt] = wts[i];
+      nt++;
+    }
+  }
+  bool has = false;
+  if (sumW >= 0.01f) {
+    for (int c = 0; c < 3; c++) hc[c] /= sumW;
+    hm.x /= sumW; hm.y /= sumW; hm.z /= sumW; hm.w /= sumW;
+    for (int k = 0; k < nt; k++) tw[k] /= sumW;
+    has = true;
+  } else {
+    float n3 = 0.f;
+    hc[0] = hc[1] = hc[2] = 0.f;
+    hm = make_float4(0.f, 0.f, 0.f, 0.f);
+    nt = 0;
+    for (int j = 0; j < 9; j++) {
+      const int qx = cx + j % 3 - 1, qy = cy + j / 3 - 1;
+      if (qx >= 0 && qy >= 0 && qx < W && qy < H && check_key(ldh(f.key_prev, qy * W + qx), nd, mv.w, mv.z)) {
+        const int q = qy * W + qx;
+        const float4 c = ldh(f.hist_prev, q), m = ldh(f.mom_prev, q);
+        n3 += 1.0f;
+        hc[0] += c.x; hc[1] += c.y; hc[2] += c.z;
+        hm.x += m.x; hm.y += m.y; hm.z += m.z; hm.w += m.w;
+        tq[nt] = q;
+        nt++;
+      }
+    }
+    if (n3 > 0.0f) {
+      for (int c = 0; c < 3; c++) hc[c] /= n3;
+      hm.x /= n3; hm.y /= n3; hm.z /= n3; hm.w /= n3;
+      for (int k = 0; k < nt; k++) tw[k] = 1.0f / n3;
+      has = true;
+    }
+  }
+  has = has && hm.w > 0.0f;
+  if (!has) return;  // A0 and the moments come from this frame alone
+  const int hq = (clampi(cy, 0, H - 1) >> 1) * f.W2 + (clampi(cx, 0, W - 1) >> 1);
+  const float4 pq = ldh(f.par0_prev, hq);
+  const float alpha = pq.x, gamma = pq.y;
+  // forward of the blend
+  const float il[3] = {illum.x, illum.y, illum.z};
+  float hcl[3];
+  int clampside[3];  // -1 clamped to mu - gamma sd, +1 to mu + gamma sd, 0 not clamped
+  for (int c = 0; c < 3; c++) {
+    const float lo = mu[c] - gamma * sd[c], hi = mu[c] + gamma * sd[c];
+    hcl[c] = fminf(fmaxf(hc[c], lo), hi);
+    clampside[c] = hc[c] < lo ? -1 : (hc[c] > hi ? 1 : 0);
+  }
+  const float len1 = fminf(hm.w + 1.0f, HMAX);
+  const float inv = 1.0f / len1;
+  const bool a_is_alpha = alpha >= inv;
+  const float a = fmaxf(alpha, inv);
+  const float nmx = hm.x + (l - hm.x) * a, nmy = hm.y + (l * l - hm.y) * a;
+  const bool b_is_inv = inv > 1.0f / 6.0f;
+  const float b = fmaxf(1.0f / 6.0f, inv);
+  const float tv = nmy - nmx * nmx;
+  const float tvar = fmaxf(tv, 0.0f);
+  const float kk = fminf(len1 / 4.0f, 1.0f);
+  // seeds
+  const float4 gAo = gA ? gA[o] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 gMo = gM ? gM[o] : make_float4(0.f, 0.f, 0.f, 0.f);
+  float g_nmx = gMo.x, g_nmy = gMo.y, g_nf = gMo.z, g_len = gMo.w;
+  // A.w = svar + (tvar - svar) k
+  const float g_tvar = gAo.w * kk;
+  if (len1 < 4.0f) g_len += gAo.w * (tvar - svar) * 0.25f;
+  if (tv > 0.0f) { g_nmy += g_tvar; g_nmx += -2.0f * nmx * g_tvar; }
+  // nfast = hm.z + (l - hm.z) b
+  float g_hm[4] = {0.f, 0.f, g_nf * (1.0f - b), 0.f};
+  if (b_is_inv) g_len += g_nf * (l - hm.z) * (-inv * inv);
+  // moments m1 / m2 and the colour blend
+  float g_a = g_nmx * (l - hm.x) + g_nmy * (l * l - hm.y);
+  g_hm[0] = g_nmx * (1.0f - a);
+  g_hm[1] = g_nmy * (1.0f - a);
+  const float gcol[3] = {gAo.x, gAo.y, gAo.z};
+  float g_hc[3], g_gamma = 0.0f;
+  for (int c = 0; c < 3; c++) {
+    g_a += gcol[c] * (il[c] - hcl[c]);
+    const float g_hcl = gcol[c] * (1.0f - a);
+    g_hc[c] = clampside[c] == 0 ? g_hcl : 0.0f;
+    g_gamma += clampside[c] == 0 ? 0.0f : g_hcl * (float)clampside[c] * sd[c];
+  }
+  float g_alpha = 0.0f;
+  if (a_is_alpha) g_alpha = g_a;
+  else g_len += g_a * (-inv * inv);
+  if (hm.w + 1.0f < HMAX) g_hm[3] = g_len;
+  // the history taps (bilinear weights / sumW, or 1 / n3 in the fallback)
+  for (int k = 0; k < nt; k++) {
+    const float w = tw[k];
+    if (g_hc[0] != 0.f || g_hc[1] != 0.f || g_hc[2] != 0.f) atomic_add4(dhist + tq[k], make_float4(w * g_hc[0], w * g_hc[1], w * g_hc[2], 0.f));
+    if (g_hm[0] != 0.f || g_hm[1] != 0.f || g_hm[2] != 0.f || g_hm[3] != 0.f)
+      atomic_add4(dmom + tq[k], make_float4(w * g_hm[0], w * g_hm[1], w * g_hm[2], w * g_hm[3]));
+  }
+  if (g_alpha != 0.f) atomicAdd(&dag[hq].x, g_alpha);
+  if (g_gamma != 0.f) atomicAdd(&dag[hq].y, g_gamma);
 }
 
 // ------------------------------------------------------------------------------------------------ MLP adjoint
@@ -1159,6 +1355,21 @@ struct hush_trainer_s {
   float4 *par = nullptr, *B[3] = {}, *A1 = nullptr, *X = nullptr, *out[2] = {}, *gT = nullptr, *gT2 = nullptr,
          *dB[3] = {}, *dpar = nullptr, *dX = nullptr, *tcoef = nullptr;
   float *partials = nullptr;
+  // TEMPORAL's adjoint: seeds dA0 / dA1 (the fine level's input / output) and dmom (this frame's moments); outputs
+  // dhist / dmomp (the previous frame's colour history and moments) and dag (its alpha, gamma per half-res pixel)
+  float4 *dA0 = nullptr, *dA1 = nullptr, *dmom = nullptr, *dhist = nullptr, *dmomp = nullptr;
+  float2 *dag = nullptr;
+  // hush_trainer_window_bptt: the window's per-frame state records and the carried gradients (ping-pong)
+  struct Rec {
+    uint2 *A0, *key, *mom, *hist, *taa, *par0, *C0, *C1, *CG;
+    uint4 *F[4];
+    float4 *out;
+  };
+  std::vector<Rec> rec;
+  char *rec_pool = nullptr;
+  float4 *c_hist[2] = {}, *c_mom[2] = {};
+  float2 *c_ag[2] = {};
+  char *carry_pool = nullptr;
   int n_mlp_ctas = 0, n_loss_ctas = 0;
   int cur = 0, has_prev = 0;
   int adam_t = 0;
@@ -1200,7 +1411,8 @@ extern "C" int hush_trainer_create(hush_t *h, const float *theta, hush_trainer_t
   t->n_loss_ctas = (int)((full + 255) / 256);
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
   const size_t bytes = al(NW * 4) * 3 + al(NW * 8) + al(8) * 2 + al(t->n_loss_ctas * 8) + al(half * 48) * 2 +
-                       al(half * 16) * 6 + al(full * 16) * 7 + al(full * 48) + al((size_t)t->n_mlp_ctas * NW * 4);
+                       al(half * 16) * 6 + al(full * 16) * 12 + al(full * 48) + al((size_t)t->n_mlp_ctas * NW * 4) +
+                       al(half * 8);
   cudaError_t e = cudaMalloc(&t->pool, bytes);
   if (e != cudaSuccess) { delete t; return hush_cuda_fail(h, e, "cudaMalloc of the trainer"); }
   cudaMemset(t->pool, 0, bytes);
@@ -1216,6 +1428,9 @@ extern "C" int hush_trainer_create(hush_t *h, const float *theta, hush_trainer_t
   t->gT = (float4 *)take(full * 16); t->gT2 = (float4 *)take(full * 16); t->dX = (float4 *)take(full * 16);
   t->tcoef = (float4 *)take(full * 48);
   t->partials = (float *)take((size_t)t->n_mlp_ctas * NW * 4);
+  t->dA0 = (float4 *)take(full * 16); t->dA1 = (float4 *)take(full * 16); t->dmom = (float4 *)take(full * 16);
+  t->dhist = (float4 *)take(full * 16); t->dmomp = (float4 *)take(full * 16);
+  t->dag = (float2 *)take(half * 8);
   e = cudaMemcpy(t->theta, theta ? theta : h->wf.data(), NW * 4, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) { cudaFree(t->pool); delete t; return hush_cuda_fail(h, e, "cudaMemcpy of the weights"); }
   cudaFuncSetAttribute(k_mlp_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MB_SMEM);
@@ -1242,6 +1457,8 @@ extern "C" void hush_trainer_destroy(hush_trainer_t *t) {
   if (t->cap) cudaStreamDestroy(t->cap);
   cudaFree(t->pool);
   cudaFree(t->win_pool);
+  cudaFree(t->rec_pool);
+  cudaFree(t->carry_pool);
   delete t;
 }
 
@@ -1675,6 +1892,9 @@ extern "C" int hush_trainer_zero_adjoints(hush_trainer_t *t, void *stream) {
   if (e == cudaSuccess) e = cudaMemsetAsync(t->gT, 0, full * 16, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(t->dpar, 0, half * 48, st);
   for (int i = 0; i < 3 && e == cudaSuccess; i++) e = cudaMemsetAsync(t->dB[i], 0, half * 16, st);
+  float4 *tb[5] = {t->dA0, t->dA1, t->dmom, t->dhist, t->dmomp};
+  for (int i = 0; i < 5 && e == cudaSuccess; i++) e = cudaMemsetAsync(tb[i], 0, full * 16, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(t->dag, 0, half * 8, st);
   return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, "cudaMemsetAsync");
 }
 
@@ -1704,7 +1924,18 @@ static int run_twin_pass(hush_trainer_t *t, int pass, int backward, void *stream
       if (backward) k_mid_bwd<3><<<gh, blk, 0, st>>>(T); else k_mid_fwd<3><<<gh, blk, 0, st>>>(T);
       break;
     case HUSH_TWIN_FINE:
-      if (backward) k_fine_bwd<false><<<gf, blk, 0, st>>>(T, t->dX); else k_fine_fwd<<<gf, blk, 0, st>>>(T);
+      if (backward) {  // per pass: the history seed dA1 and the input gradient dA0 as well
+        TwinFrame Tb = T;
+        Tb.gA1 = t->dA1;
+        Tb.dA0 = t->dA0;
+        k_fine_bwd<false><<<gf, blk, 0, st>>>(Tb, t->dX);
+      } else {
+        k_fine_fwd<<<gf, blk, 0, st>>>(T);
+      }
+      break;
+    case HUSH_TWIN_TEMPORAL:
+      if (backward) k_temporal_bwd<<<gf, blk, 0, st>>>(T, t->dA0, t->dmom, t->dhist, t->dmomp, t->dag);
+      else e = launch_pass(PASS_TEMPORAL, f, t->h->w16, st);
       break;
     case HUSH_TWIN_TAA:
       if (!backward) {
@@ -1741,6 +1972,160 @@ extern "C" int hush_taa_fwd(hush_trainer_t *t, void *stream) { return run_twin_p
 extern "C" int hush_taa_bwd(hush_trainer_t *t, void *stream) { return run_twin_pass(t, HUSH_TWIN_TAA, 1, stream, "hush_taa_bwd"); }
 extern "C" int hush_loss_fwd(hush_trainer_t *t, void *stream) { return run_twin_pass(t, HUSH_TWIN_LOSS, 0, stream, "hush_loss_fwd"); }
 extern "C" int hush_loss_bwd(hush_trainer_t *t, void *stream) { return run_twin_pass(t, HUSH_TWIN_LOSS, 1, stream, "hush_loss_bwd"); }
+extern "C" int hush_temporal_fwd(hush_trainer_t *t, void *stream) {
+  return run_twin_pass(t, HUSH_TWIN_TEMPORAL, 0, stream, "hush_temporal_fwd");
+}
+extern "C" int hush_temporal_bwd(hush_trainer_t *t, void *stream) {
+  return run_twin_pass(t, HUSH_TWIN_TEMPORAL, 1, stream, "hush_temporal_bwd");
+}
+
+// ------------------------------------------------------------------------------------------------ window BPTT
+// dpar's alpha / gamma (components 0, 1 of its first float4) += the gradient carried back from the next frame.
+__global__ void k_add_ag(float4 *dpar, const float2 *ag, int n) {
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= n) return;
+  const float2 g = ag[o];
+  dpar[3 * o].x += g.x;
+  dpar[3 * o].y += g.y;
+}
+
+// The state of each frame of a window that the reverse sweep reads again: TEMPORAL's outputs and key, the features,
+// the coarse levels, the twin's stored history (colour, TAA, par0) and its FP32 TAA output (the next frame's temporal
+// loss term). Allocated for the longest window seen.
+static int ensure_records(hush_trainer_t *t, int n) {
+  if ((int)t->rec.size() >= n) return HUSH_OK;
+  const size_t full = (size_t)t->W * t->H, half = (size_t)t->W2 * t->H2;
+  const size_t quarter = (size_t)((t->W2 + 1) / 2) * ((t->H2 + 1) / 2);
+  auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t per = al(full * 8) * 5 + al(half * 8) + al(half * 16) * 4 + al(quarter * 8) * 3 + al(full * 16);
+  cudaFree(t->rec_pool);
+  t->rec.clear();
+  cudaError_t e = cudaMalloc(&t->rec_pool, per * n);
+  if (e != cudaSuccess) { t->rec_pool = nullptr; return hush_cuda_fail(t->h, e, "cudaMalloc of the window records"); }
+  e = cudaMemset(t->rec_pool, 0, per * n);
+  if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "cudaMemset of the window records");
+  if (!t->carry_pool) {
+    const size_t cb = al(full * 16) * 4 + al(half * 8) * 2;
+    e = cudaMalloc(&t->carry_pool, cb);
+    if (e != cudaSuccess) { t->carry_pool = nullptr; return hush_cuda_fail(t->h, e, "cudaMalloc of the carries"); }
+    char *c = t->carry_pool;
+    for (int k = 0; k < 2; k++) { t->c_hist[k] = (float4 *)c; c += al(full * 16); }
+    for (int k = 0; k < 2; k++) { t->c_mom[k] = (float4 *)c; c += al(full * 16); }
+    for (int k = 0; k < 2; k++) { t->c_ag[k] = (float2 *)c; c += al(half * 8); }
+  }
+  char *b = t->rec_pool;
+  for (int i = 0; i < n; i++) {
+    hush_trainer_t::Rec r;
+    auto take = [&](size_t sz) { char *q = b; b += al(sz); return q; };
+    r.A0 = (uint2 *)take(full * 8); r.key = (uint2 *)take(full * 8); r.mom = (uint2 *)take(full * 8);
+    r.hist = (uint2 *)take(full * 8); r.taa = (uint2 *)take(full * 8); r.par0 = (uint2 *)take(half * 8);
+    for (int k = 0; k < 4; k++) r.F[k] = (uint4 *)take(half * 16);
+    r.C0 = (uint2 *)take(quarter * 8); r.C1 = (uint2 *)take(quarter * 8); r.CG = (uint2 *)take(quarter * 8);
+    r.out = (float4 *)take(full * 16);
+    t->rec.push_back(r);
+  }
+  return HUSH_OK;
+}
+
+// The twin frame of window frame i, its state in record i and its history in record i - 1 (frame 0: a reset).
+static TwinFrame rec_twin(hush_trainer_t *t, const hush_inputs *in, const float *clean, const float *clean_prev, int i,
+                          float lambda_t) {
+  TwinFrame T = make_twin(t, in, clean, clean_prev, lambda_t);
+  const hush_trainer_t::Rec &r = t->rec[i], &p = t->rec[i > 0 ? i - 1 : 0];
+  HushFrame &f = T.f;
+  f.reset = i == 0 ? 1 : 0;
+  f.A0 = r.A0; f.key = r.key; f.mom = r.mom; f.hist = r.hist; f.taa = r.taa; f.par0 = r.par0;
+  f.F0 = r.F[0]; f.F1 = r.F[1]; f.F2 = r.F[2]; f.F3 = r.F[3];
+  f.C0 = r.C0; f.C1 = r.C1; f.CG = r.CG;
+  f.key_prev = p.key; f.hist_prev = p.hist; f.mom_prev = p.mom; f.par0_prev = p.par0; f.taa_prev = p.taa;
+  T.out = r.out;
+  T.out_prev = p.out;
+  T.has_prev = (i > 0 && clean_prev) ? 1 : 0;
+  return T;
+}
+
+// Backpropagation through time over one window (see include/hush.h): forward over the frames, keeping each frame's
+// state, then the reverse sweep, frame by frame from the last: the twin's forward again, the loss, TAA, fine (seeded
+// with the gradient the next frame sent to this frame's colour history, and giving dL/dA0), mid3..mid1, the MLP
+// (whose alpha / gamma seeds are the gradient the next frame sent to this frame's par0), then TEMPORAL's adjoint,
+// which sends this frame's gradient to the previous frame's colour history, moments and alpha / gamma.
+extern "C" int hush_trainer_window_bptt(hush_trainer_t *t, const hush_inputs *frames, const float *const *cleans,
+                                        int n_frames, float lambda_t, void *stream) {
+  if (!t || !frames || !cleans)
+    return hush_fail(t ? t->h : nullptr, HUSH_ERR_ARG, "hush_trainer_window_bptt: NULL argument");
+  if (n_frames < 1) return tr_fail(t, "hush_trainer_window_bptt: empty window");
+  if (t->W != t->h->W || t->H != t->h->H)
+    return tr_fail(t, "hush_trainer_window_bptt: the denoiser was resized after the trainer was created");
+  for (int i = 0; i < n_frames; i++) {
+    if (!cleans[i]) return tr_fail(t, "hush_trainer_window_bptt: missing clean image");
+    const int rc = hush_check_inputs(t->h, frames + i);
+    if (rc != HUSH_OK) return rc;
+  }
+  cudaSetDevice(t->h->dev);
+  int rc = ensure_records(t, n_frames);
+  if (rc != HUSH_OK) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int W = t->W, H = t->H, W2 = t->W2, H2 = t->H2;
+  const size_t full = (size_t)W * H, half = (size_t)W2 * H2;
+  const dim3 blk(TW, TH), gh((W2 + TW - 1) / TW, (H2 + TH - 1) / TH), gf((W + TW - 1) / TW, (H + TH - 1) / TH);
+  auto twin = [&](int i) {
+    return rec_twin(t, frames + i, cleans[i], i ? cleans[i - 1] : nullptr, i, lambda_t);
+  };
+  auto forward = [&](const TwinFrame &T) {
+    launch_mlp_fwd(t, T, st);
+    k_mid_fwd<1><<<gh, blk, 0, st>>>(T);
+    k_mid_fwd<2><<<gh, blk, 0, st>>>(T);
+    k_mid_fwd<3><<<gh, blk, 0, st>>>(T);
+    k_fine_fwd<<<gf, blk, 0, st>>>(T);
+    k_taa_fwd<<<gf, blk, 0, st>>>(T);
+  };
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < n_frames && e == cudaSuccess; i++) {
+    const TwinFrame T = twin(i);
+    e = launch_pass(PASS_TEMPORAL, T.f, t->h->w16, st);
+    if (e == cudaSuccess) e = launch_pass(PASS_COARSE1, T.f, t->h->w16, st);
+    if (e == cudaSuccess) e = launch_pass(PASS_COARSE2, T.f, t->h->w16, st);
+    if (e != cudaSuccess) break;
+    forward(T);
+    k_loss<<<t->n_loss_ctas, 256, 0, st>>>(T, 0);
+    k_reduce_f64<<<1, 256, 0, st>>>(t->loss_partials, t->n_loss_ctas, t->loss, t->loss_acc);
+  }
+  int c = 0;
+  for (int k = 0; k < 2 && e == cudaSuccess; k++) {
+    e = cudaMemsetAsync(t->c_hist[k], 0, full * 16, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(t->c_mom[k], 0, full * 16, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(t->c_ag[k], 0, half * 8, st);
+  }
+  for (int i = n_frames - 1; i >= 0 && e == cudaSuccess; i--) {
+    TwinFrame T = twin(i);
+    T.zero_adj = 1;
+    forward(T);
+    k_loss<<<t->n_loss_ctas, 256, 0, st>>>(T, 1);
+    k_add_ag<<<(unsigned)((half + 255) / 256), 256, 0, st>>>(t->dpar, t->c_ag[c], (int)half);
+    k_taa_bwd_coef<<<gf, blk, 0, st>>>(T, t->gT, t->tcoef);
+    k_taa_bwd_gather<<<gf, blk, 0, st>>>(T, t->tcoef, t->gT2);
+    e = cudaMemsetAsync(t->dA0, 0, full * 16, st);
+    if (e != cudaSuccess) break;
+    T.gA1 = t->c_hist[c];
+    T.dA0 = t->dA0;
+    k_fine_bwd<true><<<gf, blk, 0, st>>>(T, t->gT2);
+    k_mid_bwd<3><<<gh, blk, 0, st>>>(T);
+    k_mid_bwd<2><<<gh, blk, 0, st>>>(T);
+    k_mid_bwd<1><<<gh, blk, 0, st>>>(T);
+    launch_mlp_bwd(t, T, st);
+    if (i > 0) {
+      const int n = c ^ 1;
+      e = cudaMemsetAsync(t->c_hist[n], 0, full * 16, st);
+      if (e == cudaSuccess) e = cudaMemsetAsync(t->c_mom[n], 0, full * 16, st);
+      if (e == cudaSuccess) e = cudaMemsetAsync(t->c_ag[n], 0, half * 8, st);
+      if (e != cudaSuccess) break;
+      k_temporal_bwd<<<gf, blk, 0, st>>>(T, t->dA0, t->c_mom[c], t->c_hist[n], t->c_mom[n], t->c_ag[n]);
+      c = n;
+    }
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, "hush_trainer_window_bptt");
+}
 
 extern "C" int hush_trainer_buffer(hush_trainer_t *t, int which, void **ptr, int *width, int *height, int *channels) {
   if (!t || !ptr) return hush_fail(t ? t->h : nullptr, HUSH_ERR_ARG, "hush_trainer_buffer: NULL argument");
@@ -1762,6 +2147,12 @@ extern "C" int hush_trainer_buffer(hush_trainer_t *t, int which, void **ptr, int
     case HUSH_TB_OUT: p = t->out[t->cur]; break;
     case HUSH_TB_OUT_PREV: p = t->out[t->cur ^ 1]; break;
     case HUSH_TB_DOUT: p = t->gT; break;
+    case HUSH_TB_DA0: p = t->dA0; break;
+    case HUSH_TB_DA1: p = t->dA1; break;
+    case HUSH_TB_DMOM: p = t->dmom; break;
+    case HUSH_TB_DHIST: p = t->dhist; break;
+    case HUSH_TB_DMOM_PREV: p = t->dmomp; break;
+    case HUSH_TB_DAG: p = t->dag; w = t->W2; h = t->H2; c = 2; break;
     default: return tr_fail(t, "hush_trainer_buffer: unknown buffer");
   }
   *ptr = p;

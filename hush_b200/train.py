@@ -155,7 +155,7 @@ class Trainer:
                                                float(lambda_t), C.c_void_p(_stream_handle(stream))))
 
     def fwd(self, name: str, stream=None):
-        """Forward of one pass ("mlp", "mid1", "mid2", "mid3", "fine", "taa", "loss")."""
+        """Forward of one pass ("mlp", "mid1", "mid2", "mid3", "fine", "taa", "loss", "temporal")."""
         self._check(getattr(L.lib(), f"hush_{name}_fwd")(self._t, C.c_void_p(_stream_handle(stream))))
 
     def bwd(self, name: str, stream=None):
@@ -177,6 +177,18 @@ class Trainer:
         v = torch.as_tensor(_DevView(ptr.value, h.value, w.value, c.value, ts),
                             device=torch.device("cuda", self.hush.device))
         return v.view(-1) if h.value == 1 and c.value == 1 else v
+
+    def window_bptt(self, window, lambda_t: float = 0.5, stream=None):
+        """hush_trainer_window_bptt: backpropagation through time over one window, a list of input dicts each with a
+        "clean" (H, W, 3) float32 CUDA tensor. Adds into the gradient and loss accumulators (no optimiser step)."""
+        n = len(window)
+        ins = (L.HushInputs * n)()
+        cl = (C.c_void_p * n)()
+        for i, fr in enumerate(window):
+            _fill_inputs(ins[i], fr)
+            cl[i] = fr["clean"].data_ptr()
+        self._check(L.lib().hush_trainer_window_bptt(self._t, ins, cl, n, float(lambda_t),
+                                                     C.c_void_p(_stream_handle(stream))))
 
     def train_step(self, windows, lambda_t=0.5, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, clip=1.0, stream=None):
         """hush_train_step over a batch: windows = list of windows, each a list of input dicts with a "clean" (H, W, 3)

@@ -238,7 +238,9 @@ typedef enum {
   HUSH_TWIN_FINE = 4, /* A0, key, PAR, B3, C0, CG, G-buffer      -> A1, X    | dX   -> dB3, dPAR (s0 c0 beta kappa) */
   HUSH_TWIN_TAA = 5,  /* X, motion, previous TAA output          -> OUT      | dOUT -> dX                       */
   HUSH_TWIN_LOSS = 6, /* OUT, clean, clean_prev, OUT_PREV        -> LOSS     | 1    -> dOUT                     */
-  HUSH_TWIN_PASSES = 7
+  HUSH_TWIN_TEMPORAL = 7, /* G-buffer, previous history (colour, moments, key, par0) -> A0, moments, key, features |
+                           * dA0, dMOM -> dHIST, dMOM_PREV, dAG (the previous frame's colour, moments, alpha / gamma) */
+  HUSH_TWIN_PASSES = 8
 } hush_twin_pass;
 
 /* The trainer's buffers (device memory owned by the trainer, valid until hush_trainer_destroy; OUT / OUT_PREV swap at
@@ -257,7 +259,13 @@ typedef enum {
   HUSH_TB_OUT = 14,     /* W x H x 4: TAA output of this frame                                       */
   HUSH_TB_OUT_PREV = 15, /* W x H x 4: TAA output of the previous frame (the temporal loss term)     */
   HUSH_TB_DOUT = 16,    /* W x H x 4                                                                 */
-  HUSH_TB_COUNT = 17
+  HUSH_TB_DA0 = 17,     /* W x H x 4: dL/d TEMPORAL's colour + variance (the fine adjoint adds into it) */
+  HUSH_TB_DA1 = 18,     /* W x H x 4: dL/d the fine level through the colour history (a fine seed)    */
+  HUSH_TB_DMOM = 19,    /* W x H x 4: dL/d this frame's moments (a TEMPORAL seed)                     */
+  HUSH_TB_DHIST = 20,   /* W x H x 4: dL/d the previous frame's colour history (TEMPORAL adds into it) */
+  HUSH_TB_DMOM_PREV = 21, /* W x H x 4: dL/d the previous frame's moments                             */
+  HUSH_TB_DAG = 22,     /* W2 x H2 x 2: dL/d the previous frame's alpha, gamma per half-res pixel     */
+  HUSH_TB_COUNT = 23
 } hush_trainer_buf;
 
 /* TEMPORAL and the coarse levels for the frame's inputs, and the frame context for the pass calls (clean: dense f32
@@ -282,6 +290,24 @@ int hush_taa_fwd(hush_trainer_t *t, void *stream);
 int hush_taa_bwd(hush_trainer_t *t, void *stream);
 int hush_loss_fwd(hush_trainer_t *t, void *stream);
 int hush_loss_bwd(hush_trainer_t *t, void *stream);
+/* TEMPORAL (hush.js:111-223) as a pass: the forward reruns the reference pass on the begun frame; the adjoint takes
+ * dA0 and dMOM (the gradients of TEMPORAL's colour + variance and moments) back through the anti-lag clamp, the blend
+ * a = max(alpha, 1 / len), the moment updates, the variance lerp and the bilinear (or 3x3 fallback) reprojection,
+ * ADDING into dHIST, dMOM_PREV and dAG. The f16 storage of the history counts as the identity; the lag metric and the
+ * block features are not differentiated (the MLP's inputs are held fixed). */
+int hush_temporal_fwd(hush_trainer_t *t, void *stream);
+int hush_temporal_bwd(hush_trainer_t *t, void *stream);
+
+/* Backpropagation through time over one window of n_frames frames (frames[] / cleans[] as in hush_train_step): the
+ * window starts without history, every frame runs forward with its state kept, then the frames run backward from the
+ * last one. Besides each frame's own loss gradient (what hush_trainer_frame takes), the gradient flows across frames
+ * through TEMPORAL (hush_temporal_bwd): from a frame's colour + variance A0 and moments into the previous frame's
+ * colour history (its fine level), moments and alpha / gamma, so the alpha and gamma heads of the MLP train. The
+ * block features and the TAA history are held fixed (truncated there). Adds into the gradient and loss accumulators,
+ * like hush_trainer_windows; allocates the window's per-frame records (about 11 MB per frame at 384 x 384) on first
+ * use. The trainer's own Hush history is not touched. */
+int hush_trainer_window_bptt(hush_trainer_t *t, const hush_inputs *frames, const float *const *cleans, int n_frames,
+                             float lambda_t, void *stream);
 
 /* Weight gradient of the parameter MLP (812 doubles in dtheta, overwritten) from a half-resolution image of rows:
  * packed features F0..F3 (16-byte texels, width2 x height2, as hush_buffer returns them), dL/dpar (12 floats per

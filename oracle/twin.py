@@ -161,10 +161,11 @@ def mid(k: int, src, Gh, sky_h, par):
     return torch.where(sky_h[..., None], z4, filt(src, Gh, pf[..., 4 + k], pf[..., 8 + k], step, k == 1))
 
 
-def fine(st: dict, par, B3, Gh, sky_h, Ah):
-    """Fine level and recombination (hush.js:578-620): (A1, X), (H, W, 4) and (H, W, 3)."""
+def fine(st: dict, par, B3, Gh, sky_h, Ah, A0=None):
+    """Fine level and recombination (hush.js:578-620): (A1, X), (H, W, 4) and (H, W, 3). A0: TEMPORAL's colour +
+    variance as a tensor (to differentiate through it), else st["A0"]."""
     par_f = _par_f(par, sky_h)
-    A0 = _t(st["A0"])
+    A0 = _t(st["A0"]) if A0 is None else A0
     key = _t(st["key"])
     H, W = A0.shape[:2]
     G = torch.cat([oct_dec(key[..., 0], key[..., 1]), key[..., 2:3]], -1)
@@ -265,6 +266,133 @@ def loss_of(st: dict, out, lambda_t=0.0):
         cp = _t(st["clean_prev"])
         loss = loss + lambda_t * torch.clamp(((out - op) - (clean - cp)).abs() / den, max=1.0).sum() / N
     return loss
+
+
+def _nb(img, dy, dx, fill=0.0):
+    """img shifted so that out[y, x] = img[y + dy, x + dx], `fill` outside the image."""
+    H, W = img.shape[:2]
+    out = torch.full_like(img, fill)
+    ys0, ys1 = max(0, -dy), min(H, H - dy)
+    xs0, xs1 = max(0, -dx), min(W, W - dx)
+    if ys0 < ys1 and xs0 < xs1:
+        out[ys0:ys1, xs0:xs1] = img[ys0 + dy:ys1 + dy, xs0 + dx:xs1 + dx]
+    return out
+
+
+def _check_key(k, nd, z_prev, obj):
+    """The history key test (hush.js:103-105) on gathered keys k (..., 4) against the pixel's normal / depth."""
+    n = oct_dec(k[..., 0], k[..., 1])
+    return ((k[..., 2] >= 0) & (k[..., 3] == obj) & ((k[..., 2] - z_prev).abs() <= 0.05 * z_prev + 0.01)
+            & ((n * nd[..., :3]).sum(-1) >= 0.9))
+
+
+def temporal(st: dict, hist_prev, mom_prev, par0_prev):
+    """TEMPORAL's pixel() (hush.js:111-223) in float64 for the gradient through the history: (A0 (H, W, 4) colour +
+    variance, mom (H, W, 4) = m1, m2, fast mean, history length), differentiable in hist_prev (H, W, 4; rgb used),
+    mom_prev (H, W, 4) and par0_prev (h, w, 4; alpha = .x, gamma = .y). The G-buffer (st: radiance, normalDepth,
+    motion, material) and the previous keys (st["key_prev"]) fix the statistics, the reprojection taps and their
+    weights. For frames with history (st["reset"] false)."""
+    rad, nd, mv, mat = (_t(np.asarray(st[k], np.float32)) for k in ("radiance", "normalDepth", "motion", "material"))
+    keyp = _t(np.asarray(st["key_prev"], np.float32))
+    H, W = rad.shape[:2]
+    ys, xs = torch.meshgrid(torch.arange(H), torch.arange(W), indexing="ij")
+    valid = nd[..., 3] >= 0
+    illum = torch.where(valid[..., None], rad[..., :3] / torch.clamp(mat[..., :3], min=1e-3), torch.zeros(H, W, 3,
+                        dtype=torch.float64))
+    vf = valid.double()
+    win = [(dy, dx) for dy in (-1, 0, 1) for dx in (-1, 0, 1)]
+    cnt = torch.clamp(sum(_nb(vf, dy, dx) for dy, dx in win), min=1.0)
+    mu = sum(_nb(illum, dy, dx) * _nb(vf, dy, dx)[..., None] for dy, dx in win) / cnt[..., None]
+    slm = lum(mu)
+    sv = sum(_nb(vf, dy, dx)[..., None] * (_nb(illum, dy, dx) - mu) ** 2 for dy, dx in win)
+    svar = sum(_nb(vf, dy, dx) * (lum(_nb(illum, dy, dx)) - slm) ** 2 for dy, dx in win) / cnt
+    sd = torch.sqrt(torch.clamp(sv / cnt[..., None], min=1e-12))
+    l = lum(illum)
+    ppx, ppy = xs.double() + mv[..., 0], ys.double() + mv[..., 1]
+    bxf, byf = torch.floor(ppx), torch.floor(ppy)
+    fx, fy = ppx - bxf, ppy - byf
+    bix, biy = bxf.long(), byf.long()
+    wts = [(1 - fx) * (1 - fy), fx * (1 - fy), (1 - fx) * fy, fx * fy]
+    sumW = torch.zeros(H, W, dtype=torch.float64)
+    hc = torch.zeros(H, W, 3, dtype=torch.float64)
+    hm = torch.zeros(H, W, 4, dtype=torch.float64)
+    for i in range(4):
+        qx, qy = bix + (i & 1), biy + (i >> 1)
+        ok = (wts[i] > 0) & (qx >= 0) & (qy >= 0) & (qx < W) & (qy < H)
+        ok = ok & _check_key(gather(keyp, qy, qx), nd, mv[..., 3], mv[..., 2])
+        w = torch.where(ok, wts[i], torch.zeros_like(wts[i]))
+        sumW = sumW + w
+        hc = hc + w[..., None] * gather(hist_prev, qy, qx)[..., :3]
+        hm = hm + w[..., None] * gather(mom_prev, qy, qx)
+    bil = sumW >= 0.01
+    cx, cy = torch.floor(ppx + 0.5).long(), torch.floor(ppy + 0.5).long()
+    n3 = torch.zeros(H, W, dtype=torch.float64)
+    hc3 = torch.zeros(H, W, 3, dtype=torch.float64)
+    hm3 = torch.zeros(H, W, 4, dtype=torch.float64)
+    for j in range(9):
+        qx, qy = cx + j % 3 - 1, cy + j // 3 - 1
+        ok = (qx >= 0) & (qy >= 0) & (qx < W) & (qy < H) & _check_key(gather(keyp, qy, qx), nd, mv[..., 3], mv[..., 2])
+        okd = ok.double()
+        n3 = n3 + okd
+        hc3 = hc3 + okd[..., None] * gather(hist_prev, qy, qx)[..., :3]
+        hm3 = hm3 + okd[..., None] * gather(mom_prev, qy, qx)
+    one = torch.ones_like(sumW)
+    hc = torch.where(bil[..., None], hc / torch.where(bil, sumW, one)[..., None],
+                     hc3 / torch.where(n3 > 0, n3, one)[..., None])
+    hm = torch.where(bil[..., None], hm / torch.where(bil, sumW, one)[..., None],
+                     hm3 / torch.where(n3 > 0, n3, one)[..., None])
+    has = (bil | (n3 > 0)) & (hm[..., 3] > 0) & valid
+    hq = gather(par0_prev, torch.clamp(cy, 0, H - 1) >> 1, torch.clamp(cx, 0, W - 1) >> 1)
+    alpha, gamma = hq[..., 0], hq[..., 1]
+    hcl = torch.minimum(torch.maximum(hc, mu - gamma[..., None] * sd), mu + gamma[..., None] * sd)
+    len1 = torch.clamp(torch.where(has, hm[..., 3], one) + 1.0, max=32.0)
+    a = torch.maximum(alpha, 1.0 / len1)
+    col = hcl + (illum - hcl) * a[..., None]
+    nmx = hm[..., 0] + (l - hm[..., 0]) * a
+    nmy = hm[..., 1] + (l * l - hm[..., 1]) * a
+    nfast = hm[..., 2] + (l - hm[..., 2]) * torch.clamp(1.0 / len1, min=1.0 / 6.0)
+    col = torch.where(has[..., None], col, illum)
+    nmx, nmy = torch.where(has, nmx, l), torch.where(has, nmy, l * l)
+    nfast, len1 = torch.where(has, nfast, l), torch.where(has, len1, one)
+    tvar = torch.clamp(nmy - nmx * nmx, min=0.0)
+    Aw = svar + (tvar - svar) * torch.clamp(len1 / 4.0, max=1.0)
+    A0 = torch.cat([col, Aw[..., None]], -1)
+    mom = torch.stack([nmx, nmy, nfast, len1], -1)
+    z = torch.zeros_like(A0)
+    return torch.where(valid[..., None], A0, z), torch.where(valid[..., None], mom, z)
+
+
+def _st_value(x64, stored):
+    """x64 in the backward, the stored f16 value in the forward (the straight-through gradient of the storage)."""
+    return x64 + (_t(np.asarray(stored, np.float32)) - x64).detach()
+
+
+def window_loss(states, theta, lambda_t=0.0):
+    """The summed loss of a window with the gradient through time of hush_trainer_window_bptt: states[i] is frame i's
+    st (twin_loss's keys, plus the frame's stored mom / hist / par0 and the G-buffer, and key_prev), frame 0 a reset.
+    TEMPORAL runs in float64 on the previous frame's history, each stored value (A0, moments, colour history, par0)
+    entering with the straight-through gradient; the features, coarse levels and TAA history are constants."""
+    total = 0.0
+    hist_prev = mom_prev = par0_prev = None
+    for i, st in enumerate(states):
+        if i == 0:
+            A0 = _t(np.asarray(st["A0"], np.float32))
+            mom = _t(np.asarray(st["mom"], np.float32))
+        else:
+            A0_64, mom_64 = temporal(st, hist_prev, mom_prev, par0_prev)
+            A0, mom = _st_value(A0_64, st["A0"]), _st_value(mom_64, st["mom"])
+        feats, Gh, sky_h, Ah = half_inputs(st)
+        _, par = mlp(feats, theta, sky_h)
+        B1 = mid(1, Ah, Gh, sky_h, par)
+        B2 = mid(2, B1, Gh, sky_h, par)
+        B3 = mid(3, B2, Gh, sky_h, par)
+        A1, X = fine(st, par, B3, Gh, sky_h, Ah, A0=A0)
+        total = total + loss_of(st, taa(st, X), lambda_t)
+        sky = _t(np.asarray(st["key"], np.float32))[..., 2] < 0
+        A1 = torch.where(sky[..., None], torch.zeros_like(A1), A1)  # sky pixels store no history
+        hist_prev, mom_prev = _st_value(A1, st["hist"]), mom
+        par0_prev = _st_value(par[..., :4], st["par0"])
+    return total
 
 
 def twin_loss(st: dict, theta, lambda_t=0.0, return_all=False):
