@@ -359,6 +359,9 @@ def run_ours(args):
     if not args.no_train:  # the BF16 tensor-core form (the training configuration's), the FP32 form beside it
         train_ms = _train_step_ms(local, stream, barrier, max_over_ranks, mlp="bf16")
         train_ms["fp32_step_ms"] = _train_step_ms(local, stream, barrier, max_over_ranks, mlp="fp32")["step_ms"]
+        # backpropagation through time over each window (alpha / gamma heads trained), one window after another
+        train_ms["bptt_step_ms"] = _train_step_ms(local, stream, barrier, max_over_ranks, mlp="bf16",
+                                                  bptt=True)["step_ms"]
 
     if rank != 0:
         hush.destroy()
@@ -499,7 +502,7 @@ def _extras_ms(frames, stream, n=32, warmup=4):
     return out
 
 
-def _train_step_ms(local, stream, barrier, max_over_ranks, warmup=2, steps=5, mlp="bf16"):
+def _train_step_ms(local, stream, barrier, max_over_ranks, warmup=2, steps=5, mlp="bf16", bptt=False):
     """Device time of one training step: 16 windows x 8 frames of 384x384 generated on the device, the twin's
     forward + adjoint per frame (MLP as bf16 tensor-core GEMM tiles, or FP32), the gradient / loss all-reduce across
     ranks (N > 1) and the Adam step."""
@@ -507,9 +510,9 @@ def _train_step_ms(local, stream, barrier, max_over_ranks, warmup=2, steps=5, ml
 
     from hush_b200 import Hush
     from hush_b200.dp import DataParallel, finish_step
-    from hush_b200.train import TrainConfig, Trainer, window_scene, xavier_init
+    from hush_b200.train import TrainConfig, Trainer, window, window_scene, xavier_init
 
-    cfg = TrainConfig(mlp=mlp)
+    cfg = TrainConfig(mlp=mlp, bptt=bptt)
     dp = DataParallel()
     th = Hush(local, {"width": cfg.size, "height": cfg.size, "schedule": "passes"})
     tr = Trainer(th, xavier_init(cfg.init_seed))
@@ -517,9 +520,15 @@ def _train_step_ms(local, stream, barrier, max_over_ranks, warmup=2, steps=5, ml
     rng = dp.seed_rng(cfg.init_seed + 1)
     sc = window_scene(cfg)
 
+    buf = window(cfg, 0) if bptt else None
+
     def one():
-        tr.windows(sc, [dp.window_seed(rng, cfg.seeds) for _ in range(cfg.batch)], cfg.frames, cfg.lambda_t,
-                   stream=stream)
+        seeds = [dp.window_seed(rng, cfg.seeds) for _ in range(cfg.batch)]
+        if bptt:
+            for s in seeds:
+                tr.window_bptt(window(cfg, s, buf), cfg.lambda_t, stream=stream)
+        else:
+            tr.windows(sc, seeds, cfg.frames, cfg.lambda_t, stream=stream)
         return finish_step(tr, dp, cfg.batch * cfg.frames, cfg.lr, cfg.clip)
 
     for _ in range(warmup):

@@ -218,6 +218,10 @@ class Trainer:
             pass
 
 
+# W3 rows 0-1 and b3[0:2] in the weight blob (W1 b1 W2 b2 W3 b3, hush.js:20-21): the alpha and gamma heads' weights
+AG_IDX = list(range(608, 640)) + [800, 801]
+
+
 @dataclass
 class TrainConfig:
     """The training workload: windows of `frames` frames at `size`^2 from `seeds` generator seeds."""
@@ -231,6 +235,7 @@ class TrainConfig:
     clip: float = 1.0
     init_seed: int = 0
     mlp: str = "fp32"  # the twin's MLP: "fp32", or "bf16" / "f16" tensor-core tiles
+    bptt: bool = False  # gradient through time over each window (hush_trainer_window_bptt): alpha / gamma train
 
 
 def window_scene(cfg: TrainConfig, seed: int = 0) -> SceneConfig:
@@ -265,11 +270,16 @@ def train(cfg: TrainConfig, log_every: int = 100, on_log=None, time_budget_s: fl
     rng = dp.seed_rng(cfg.init_seed + 1)
     sc = window_scene(cfg)
     hist = []
+    buf = window(cfg, 0) if cfg.bptt else None  # device buffers of one window, reused
     t0 = time.time()
     for step in range(cfg.steps):
         ts = time.perf_counter()
         seeds = [dp.window_seed(rng, cfg.seeds) for _ in range(cfg.batch)]
-        tr.windows(sc, seeds, cfg.frames, cfg.lambda_t)  # generation + forward + adjoint of every frame, on device
+        if cfg.bptt:  # each window generated on the device, then forward and backward through time
+            for s in seeds:
+                tr.window_bptt(window(cfg, s, buf), cfg.lambda_t)
+        else:
+            tr.windows(sc, seeds, cfg.frames, cfg.lambda_t)  # generation + forward + adjoint of every frame
         loss, gn = finish_step(tr, dp, cfg.batch * cfg.frames, cfg.lr, cfg.clip)
         torch.cuda.synchronize()
         ms = (time.perf_counter() - ts) * 1e3
@@ -344,6 +354,8 @@ def main(argv=None):
     ap.add_argument("--seeds", type=int, default=2048)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--mlp", default="fp32", choices=["fp32", "bf16", "f16"], help="the twin's MLP arithmetic")
+    ap.add_argument("--bptt", action="store_true",
+                    help="backpropagate through time over each window (the alpha / gamma heads train)")
     ap.add_argument("--time-budget", type=float, default=None, help="stop after this many seconds of training")
     ap.add_argument("--eval-seeds", type=int, default=64)
     ap.add_argument("--out", default=None, help="write the summary JSON here")
@@ -355,7 +367,8 @@ def main(argv=None):
     if world > 1:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dp = DataParallel()
-    cfg = TrainConfig(size=a.size, frames=a.frames, seeds=a.seeds, batch=a.batch, steps=a.steps, lr=a.lr, mlp=a.mlp)
+    cfg = TrainConfig(size=a.size, frames=a.frames, seeds=a.seeds, batch=a.batch, steps=a.steps, lr=a.lr, mlp=a.mlp,
+                      bptt=a.bptt)
     log = []
 
     def on_log(rec):
@@ -384,6 +397,8 @@ def main(argv=None):
         "eval_trained": evaluate(blob, held_out, a.size, a.frames),
         "eval_builtin": evaluate(None, held_out, a.size, a.frames),
         "eval_svgf": evaluate(None, held_out, a.size, a.frames, svgf=True),
+        # the weights that feed only alpha and gamma (rows 0-1 of W3 and b3): they move only with --bptt
+        "alpha_gamma_weights_max_change": float(np.abs(tr.theta[AG_IDX] - xavier_init(cfg.init_seed)[AG_IDX]).max()),
         "log": log,
     }
     print(json.dumps({k: v for k, v in res.items() if k != "log"}), flush=True)

@@ -258,10 +258,10 @@ def test_pass_calls_check_their_arguments():
     tr = Trainer(g, xavier_init(0))
     with pytest.raises(HushError, match="hush_trainer_begin first"):
         tr.fwd("mlp")
-    assert L.lib().hush_trainer_pass(tr._t, 7, 0, None) == L.HUSH_ERR_ARG
+    assert L.lib().hush_trainer_pass(tr._t, len(L.TWIN_PASSES), 0, None) == L.HUSH_ERR_ARG
     assert L.lib().hush_trainer_pass(tr._t, -1, 1, None) == L.HUSH_ERR_ARG
     p = C.c_void_p()
-    assert L.lib().hush_trainer_buffer(tr._t, 17, C.byref(p), None, None, None) == L.HUSH_ERR_ARG
+    assert L.lib().hush_trainer_buffer(tr._t, len(L.TWIN_BUF_NAMES), C.byref(p), None, None, None) == L.HUSH_ERR_ARG
     cfg = scene.SceneConfig(32, 24, 1, seed=1)
     f = scene.frame_host(cfg, 0, clean=True)
     clean = torch.from_numpy(f["clean"]).cuda()
