@@ -280,38 +280,37 @@ struct KbTcSmem {
   alignas(128) uint8_t a2[KB_NT * 16 * 2];
   alignas(128) uint8_t a2lo[KB_NT * 16 * 2];
   alignas(128) uint8_t b[2 * MLP_TC_BLOB_BYTES];
-  alignas(8) uint64_t mbar;
+  alignas(8) uint64_t mbar[2];  // one per 128-row group
   uint32_t tmem;
 };
 
-// One MMA layer over the CTA's 256 rows: rows 0-127 and 128-255 go to TMEM columns [0, 16) and [16, 32) of the
-// 128 lanes. Per K block the products A_hi B_hi, A_lo B_hi and (with lo weights, bf16) A_hi B_lo accumulate into the
-// same FP32 accumulator; the dropped A_lo B_lo term is 2^-16 (bf16) / 2^-22 (f16) of the product. Every thread of the
-// CTA takes part (the operand rows were written by all of them); thread 0 issues and commits, all wait on the
-// mbarrier (bounded) and load their own row: warp w reads lanes 32 (w % 4) of column block w / 4. Returns false if
-// the wait gave up.
+// One MMA layer over the CTA's 256 rows, as two independent 128-row groups: warps 0-3 (rows 0-127, TMEM columns
+// [0, 16)) and warps 4-7 (rows 128-255, columns [16, 32)). A group waits only for its own four warps (a named barrier
+// of 128 threads), then its first thread issues the group's MMAs and commits them to the group's mbarrier, so one
+// group's MMAs run while the other group's warps are still forming their rows. Per K block the products A_hi B_hi,
+// A_lo B_hi and (with lo weights, bf16) A_hi B_lo accumulate into the same FP32 accumulator; the dropped A_lo B_lo
+// term is 2^-16 (bf16) / 2^-22 (f16) of the product. Every thread waits on its group's mbarrier (bounded) and loads
+// its own row: warp w reads lanes 32 (w % 4) of column block w / 4. Returns false if the wait gave up.
 HD_INL bool tc_layer_256(KbTcSmem &S, int li, const uint8_t *a, const uint8_t *alo, uint32_t kcore_a, int kblocks,
                          uint32_t b_off, bool b_lo, uint32_t kcore_b, uint32_t idesc, uint32_t phase, float *d) {
+  const int g = li >> 7;
   umma::fence_proxy_async();
   umma::fence_before_sync();
-  __syncthreads();
-  const uint32_t mbar = umma::smem_u32(&S.mbar);
-  if (li == 0) {
+  if (g == 0) asm volatile("bar.sync 1, 128;" ::: "memory");  // named barriers 1 / 2 (0 is __syncthreads)
+  else asm volatile("bar.sync 2, 128;" ::: "memory");
+  const uint32_t mbar = umma::smem_u32(&S.mbar[g]);
+  if ((li & 127) == 0) {
     umma::fence_after_sync();
     const uint32_t b = umma::smem_u32(S.b) + b_off;
-#pragma unroll
-    for (int half = 0; half < 2; half++) {
-      const uint32_t ah = umma::smem_u32(a) + (uint32_t)half * 16u * 128u * kcore_a;
-      const uint32_t al = umma::smem_u32(alo) + (uint32_t)half * 16u * 128u * kcore_a;
-      for (int kb = 0; kb < kblocks; kb++) {
-        const uint64_t bh = umma::sdesc(b + 256u * kb, 128, 128 * kcore_b);
-        umma::mma_f16(S.tmem + 16u * half, umma::sdesc(ah + 256u * kb, 128, 128 * kcore_a), bh, idesc,
-                      kb > 0 ? 1u : 0u);
-        umma::mma_f16(S.tmem + 16u * half, umma::sdesc(al + 256u * kb, 128, 128 * kcore_a), bh, idesc, 1u);
-        if (b_lo)
-          umma::mma_f16(S.tmem + 16u * half, umma::sdesc(ah + 256u * kb, 128, 128 * kcore_a),
-                        umma::sdesc(b + MLP_TC_BLOB_BYTES + 256u * kb, 128, 128 * kcore_b), idesc, 1u);
-      }
+    const uint32_t ah = umma::smem_u32(a) + (uint32_t)g * 16u * 128u * kcore_a;
+    const uint32_t al = umma::smem_u32(alo) + (uint32_t)g * 16u * 128u * kcore_a;
+    for (int kb = 0; kb < kblocks; kb++) {
+      const uint64_t bh = umma::sdesc(b + 256u * kb, 128, 128 * kcore_b);
+      umma::mma_f16(S.tmem + 16u * g, umma::sdesc(ah + 256u * kb, 128, 128 * kcore_a), bh, idesc, kb > 0 ? 1u : 0u);
+      umma::mma_f16(S.tmem + 16u * g, umma::sdesc(al + 256u * kb, 128, 128 * kcore_a), bh, idesc, 1u);
+      if (b_lo)
+        umma::mma_f16(S.tmem + 16u * g, umma::sdesc(ah + 256u * kb, 128, 128 * kcore_a),
+                      umma::sdesc(b + MLP_TC_BLOB_BYTES + 256u * kb, 128, 128 * kcore_b), idesc, 1u);
     }
     umma::commit(mbar);
   }
@@ -345,7 +344,10 @@ __global__ void __launch_bounds__(KB_NT, 2)
       umma::tmem_alloc(umma::smem_u32(&S.tmem), 32);
       umma::tmem_relinquish();
     }
-    if (li == 0) umma::mbar_init(umma::smem_u32(&S.mbar), 1);
+    if (li == 0) {
+      umma::mbar_init(umma::smem_u32(&S.mbar[0]), 1);
+      umma::mbar_init(umma::smem_u32(&S.mbar[1]), 1);
+    }
     constexpr int NB = (MODE == 1 ? 2 : 1) * MLP_TC_BLOB_BYTES / 16;  // bf16: hi and lo weights
     for (int i = li; i < NB; i += KB_NT) reinterpret_cast<uint4 *>(S.b)[i] = __ldg(blob + i);
     umma::fence_proxy_async();

@@ -116,3 +116,32 @@ def test_window_and_form_arguments_are_checked():
     assert L.lib().hush_trainer_set_mlp(tr._t, 7) == L.HUSH_ERR_ARG
     tr.windows(window_scene(TrainConfig(size=64, frames=2)), [3, 4], 2, 0.5)  # still usable
     assert np.isfinite(tr.loss_sum()) and np.abs(tr.grad()).max() > 0
+
+
+def test_twin_forward_tracks_the_inference_path_per_frame():
+    """The twin trains on a frame without the f16 storage rounding between its passes (parameters, mid levels, fine
+    level and recombined colour stay FP32 within a frame; the history between frames is stored as f16 like the
+    inference path's). Per frame of a sequence, its TAA output against the inference path's with the same weights:
+    the gap between what training sees and what is deployed."""
+    W, H = 160, 96
+    cfg = scene.SceneConfig(W, H, 6, n_moving=2, pan_min=1.0, pan_max=3.0, seed=17)
+    inf = Hush(0, {"width": W, "height": H, "schedule": "passes"})
+    tw = Hush(0, {"width": W, "height": H, "schedule": "passes"})
+    tr = Trainer(tw)  # the built-in weights, as the inference instance has them
+    prev = None
+    for i in range(cfg.frames):
+        h = scene.frame_host(cfg, i, clean=True)
+        d = _dev(h)
+        clean = torch.from_numpy(h["clean"]).cuda()
+        ref = inf.denoise(d).float()[..., :3].cpu().numpy()
+        tr.frame(d, clean, prev, 0.5, backward=False)
+        got = tr.output()[..., :3]
+        tr.end_frame()
+        prev = clean
+        rel = np.minimum(np.abs(got - ref) / (np.abs(ref) + 1e-2), 1.0)
+        print(f"twin vs inference, frame {i}: mean clipped rel. diff {rel.mean():.2e}, "
+              f"{np.mean(rel > 2e-3):.2e} beyond 2e-3, {np.mean(rel > 2e-2):.2e} beyond 2e-2")
+        assert rel.mean() <= 5e-3 and np.mean(rel > 2e-2) <= 2e-2, (i, rel.mean(), np.mean(rel > 2e-2))
+    tr.destroy()
+    tw.destroy()
+    inf.destroy()
