@@ -42,28 +42,38 @@ constexpr uint32_t MBAR_POLLS = 1u << 22;
 constexpr float L_INVALID = -1e30f;
 HD_INL bool l_valid(float L) { return L > -1e29f; }
 
-template <bool BF16>
-HD_INL uint16_t to_op(float v) {
-  if constexpr (BF16) return __bfloat16_as_ushort(__float2bfloat16_rn(v));
-  else return __half_as_ushort(__float2half_rn(v));
-}
-template <bool BF16>
-HD_INL float from_op(uint16_t h) {
-  if constexpr (BF16) return __bfloat162float(__ushort_as_bfloat16(h));
-  else return __half2float(__ushort_as_half(h));
-}
 // Eight values as one 16-byte operand row segment (hi), and the rounding residuals v - hi rounded again (lo): a
-// split-precision operand, hi + lo carrying 16 (bf16) or 22 (f16) significant bits of v.
+// split-precision operand, hi + lo carrying 16 (bf16) or 22 (f16) significant bits of v. Two values per conversion
+// (cvt.rn.bf16x2.f32 / cvt.rn.f16x2.f32) and per residual subtraction (FP32x2).
+HD_INL uint32_t cvt2(float a, float b, std::true_type) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t *>(&h);
+}
+HD_INL uint32_t cvt2(float a, float b, std::false_type) {
+  const __half2 h = __floats2half2_rn(a, b);
+  return *reinterpret_cast<const uint32_t *>(&h);
+}
+HD_INL float2 back2(uint32_t u, std::true_type) {
+  return make_float2(__uint_as_float(u << 16), __uint_as_float(u & 0xffff0000u));
+}
+HD_INL float2 back2(uint32_t u, std::false_type) {
+  return __half22float2(*reinterpret_cast<const __half2 *>(&u));
+}
 template <bool BF16>
 HD_INL void pack8_split(const float *v, uint4 &hi, uint4 &lo) {
-  uint32_t h[8], l[8];
+  using T = std::integral_constant<bool, BF16>;
+  uint32_t h[4], l[4];
 #pragma unroll
-  for (int e = 0; e < 8; e++) {
-    h[e] = to_op<BF16>(v[e]);
-    l[e] = to_op<BF16>(v[e] - from_op<BF16>((uint16_t)h[e]));
+  for (int k = 0; k < 4; k++) {
+    h[k] = cvt2(v[2 * k], v[2 * k + 1], T{});
+    const float2 r = __fadd2_rn(make_float2(v[2 * k], v[2 * k + 1]), [&] {
+      const float2 b = back2(h[k], T{});
+      return make_float2(-b.x, -b.y);
+    }());
+    l[k] = cvt2(r.x, r.y, T{});
   }
-  hi = make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16), h[4] | (h[5] << 16), h[6] | (h[7] << 16));
-  lo = make_uint4(l[0] | (l[1] << 16), l[2] | (l[3] << 16), l[4] | (l[5] << 16), l[6] | (l[7] << 16));
+  hi = make_uint4(h[0], h[1], h[2], h[3]);
+  lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
 // pixel()'s inputs to block(): P0..P4 as block() reads them and the decoded normal (Ns.w = 1 with a surface).

@@ -141,7 +141,8 @@ def test_twin_forward_tracks_the_inference_path_per_frame():
         rel = np.minimum(np.abs(got - ref) / (np.abs(ref) + 1e-2), 1.0)
         print(f"twin vs inference, frame {i}: mean clipped rel. diff {rel.mean():.2e}, "
               f"{np.mean(rel > 2e-3):.2e} beyond 2e-3, {np.mean(rel > 2e-2):.2e} beyond 2e-2")
-        assert rel.mean() <= 5e-3 and np.mean(rel > 2e-2) <= 2e-2, (i, rel.mean(), np.mean(rel > 2e-2))
+        # measured on a B200 (160 x 96, 6 frames): mean 1.6e-3 - 1.7e-3, 1.5e-4 - 5.0e-4 of values beyond 2e-2
+        assert rel.mean() <= 3e-3 and np.mean(rel > 2e-2) <= 3e-3, (i, rel.mean(), np.mean(rel > 2e-2))
     tr.destroy()
     tw.destroy()
     inf.destroy()
