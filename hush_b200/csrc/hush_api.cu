@@ -141,14 +141,12 @@ static int set_weights(hush_t *h, const uint16_t *weights, size_t n) {
   std::memset(&h->w16, 0, sizeof(h->w16));
   if (hd == 16) {
     std::memcpy(h->w16.w, wf.data(), sizeof(h->w16.w));
-    // tensor-core operands (bf16 hi, bf16 lo, f16), the FP32 weights of the per-thread MLP, the f16x2 weights
-    static_assert(MLP_BLOB_HALF == MLP_BLOB_FP32 + MLP_FP32_BLOB_BYTES, "blob layout");
+    // stage 0's constant-bank weights per MLP form, and the tensor-core operands (bf16 hi, bf16 lo, f16)
+    for (int m = 0; m < 4; m++) mlp_const_build(wf.data(), m, h->mconst[m]);
     alignas(16) uint8_t blob[MLP_BLOB_BYTES];
     mlp_tc_build_blob(wf.data(), 1, 0, blob + MLP_BLOB_BF16);
     mlp_tc_build_blob(wf.data(), 1, 1, blob + MLP_BLOB_BF16 + MLP_TC_BLOB_BYTES);
     mlp_tc_build_blob(wf.data(), 0, 0, blob + MLP_BLOB_F16);
-    mlp_fp32_build_blob(wf.data(), reinterpret_cast<float *>(blob + MLP_BLOB_FP32));
-    mlp_half_build_blob(wf.data(), reinterpret_cast<uint32_t *>(blob + MLP_BLOB_HALF));
     if (!h->tc_blob_dev) {
       e = cudaMalloc(&h->tc_blob_dev, sizeof(blob));
       if (e != cudaSuccess) return hush_cuda_fail(h, e, "cudaMalloc of the tensor-core weights");
@@ -362,7 +360,7 @@ static int encode_frame(hush_t *h, const HushFrame &f, cudaStream_t st, bool tim
     const int ns = fused_stage_count();
     for (int s = 0; s < ns && e == cudaSuccess; s++) {
       mark(fused_stage_label(s));
-      e = launch_fused_stage(s, f, h->w16, h->mlp_mode, h->tc_blob_dev, st);
+      e = launch_fused_stage(s, f, h->mconst[h->mlp_mode], h->mlp_mode, h->tc_blob_dev, st);
     }
   }
   if (timed) {

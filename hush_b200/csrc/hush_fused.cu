@@ -265,8 +265,8 @@ HD_INL float4 ffma4(float s, float4 w, float4 a) {  // a + s * w as two packed F
 // ------------------------------------------------------------------------------------------------ k_temporal_block
 // One thread per 2x2 block: tile 64 x 16 pixels = 32 x 8 blocks, 256 threads. Each thread runs pixel() for its four
 // pixels in block order, accumulates block()'s sums in registers in the WGSL's order (hush.js:226-282), forms the 20
-// features once and runs the whole FP32 MLP (weights read as shared-memory broadcasts), so after the tile barrier no
-// thread waits for another. The tile is stored column-parity-split (even and odd columns in separate rows of 33
+// features once and runs the whole FP32 MLP (weights in the constant bank, a kernel parameter: each FMA takes its
+// weight as a broadcast operand), so after the tile barrier no thread waits for another. The tile is stored column-parity-split (even and odd columns in separate rows of 33
 // entries): neighbouring threads, two pixel columns apart, then read consecutive 16-byte entries. The tensor-core
 // forms instead write each block's features as one operand row and run each layer as two tcgen05 MMAs (M = 128,
 // N = 16) over the CTA's 256 rows, FP32 accumulators in TMEM; bias, ReLU and the heads stay FP32.
@@ -277,7 +277,6 @@ HD_INL int kb_tix(int r, int c) { return (2 * r + (c & 1)) * KB_HW + (c >> 1); }
 struct KbSmem {
   float4 I[2 * KB_HW * KB_SH];   // illumination (r, g, b) and L (luminance or L_INVALID), apron 1
   float2 Lq[2 * KB_HW * KB_SH];  // (E * qf16(L), 1) for valid entries, (0, 0) otherwise
-  float4 w[MLP_FP32_BLOB_BYTES / 16];
 };
 // Tensor-core forms: the same tile plus the MMA operands of the CTA's 256 rows (one per block) in the K-major
 // no-swizzle layout, each as a split-precision pair (hi, lo): A1 256 x 32 (features, zero padded), A2 256 x 16
@@ -341,7 +340,7 @@ struct ParityTile {
 // 3: the reference's f16-arithmetic MLP per thread (the `f16` option).
 template <int MODE>
 __global__ void __launch_bounds__(KB_NT, 2)
-    k_temporal_block(const __grid_constant__ HushFrame f, const __grid_constant__ MlpW16 wts,
+    k_temporal_block(const __grid_constant__ HushFrame f, const __grid_constant__ MlpConst wp,
                      const uint4 *__restrict__ blob) {
   constexpr bool TC = MODE == 1 || MODE == 2;
   using Smem = std::conditional_t<TC, KbTcSmem, KbSmem>;
@@ -362,10 +361,6 @@ __global__ void __launch_bounds__(KB_NT, 2)
     for (int i = li; i < NB; i += KB_NT) reinterpret_cast<uint4 *>(S.b)[i] = __ldg(blob + i);
     umma::fence_proxy_async();
     umma::fence_before_sync();
-  } else {
-    constexpr int NB = (MODE == 3 ? MLP_HALF_BLOB_BYTES : MLP_FP32_BLOB_BYTES) / 16;
-    static_assert(MLP_HALF_BLOB_BYTES <= MLP_FP32_BLOB_BYTES, "the f16x2 weights share the FP32 weights' space");
-    for (int i = li; i < NB; i += KB_NT) reinterpret_cast<uint4 *>(S.w)[i] = __ldg(blob + i);
   }
   const int lbx = li % (KB_TW / 2), lby = li / (KB_TW / 2);
   const int px0 = blockIdx.x * KB_TW + 2 * lbx, py0 = blockIdx.y * KB_TH + 2 * lby;
@@ -508,6 +503,7 @@ __global__ void __launch_bounds__(KB_NT, 2)
     // without valid pixels) and takes part in all three layers
     constexpr bool BF16 = MODE == 1;
     constexpr int B1 = 16 * N_FEAT, B2 = B1 + 16 + 16 * 16, B3 = B2 + 16 + N_OUT * 16;
+    const float *wb = reinterpret_cast<const float *>(wp.w);  // the decoded weights (their biases)
     constexpr uint32_t ID = umma::idesc_f16(BF16 ? 1 : 0, 128, 16);
     auto put_row = [&](uint8_t *hi, uint8_t *lo, int k0, int kcore, const float *v) {
       uint4 h, l;
@@ -526,18 +522,18 @@ __global__ void __launch_bounds__(KB_NT, 2)
     float row[16], d[16];
     bool good = tc_layer_256(S, li, S.a1, S.a1lo, 4, 2, 0, BF16, 4, ID, 0, d);
 #pragma unroll
-    for (int j = 0; j < 16; j++) row[j] = fmaxf(d[j] + wts.w[B1 + j], 0.0f);
+    for (int j = 0; j < 16; j++) row[j] = fmaxf(d[j] + wb[B1 + j], 0.0f);
     put_row(S.a2, S.a2lo, 0, 2, row);
     put_row(S.a2, S.a2lo, 8, 2, row + 8);
     good &= tc_layer_256(S, li, S.a2, S.a2lo, 2, 1, 1024, BF16, 2, ID, 1, d);
 #pragma unroll
-    for (int j = 0; j < 16; j++) row[j] = fmaxf(d[j] + wts.w[B2 + j], 0.0f);
+    for (int j = 0; j < 16; j++) row[j] = fmaxf(d[j] + wb[B2 + j], 0.0f);
     put_row(S.a2, S.a2lo, 0, 2, row);
     put_row(S.a2, S.a2lo, 8, 2, row + 8);
     good &= tc_layer_256(S, li, S.a2, S.a2lo, 2, 1, 1536, BF16, 2, ID, 0, d);
     float out[N_OUT];
 #pragma unroll
-    for (int j = 0; j < N_OUT; j++) out[j] = d[j] + wts.w[B3 + j];
+    for (int j = 0; j < N_OUT; j++) out[j] = d[j] + wb[B3 + j];
     umma::fence_before_sync();
     __syncthreads();
     if (li < 32) {
@@ -567,9 +563,9 @@ __global__ void __launch_bounds__(KB_NT, 2)
   }
   if constexpr (MODE == 3) {
     // phase 4 (the `f16` option, hush.js:683-703): f16 products and running sums per unit in the WGSL's order (bias,
-    // then the inputs in increasing index), two units per f16x2 instruction, weights as f16x2 unit pairs in shared
-    // memory; the features enter as stored (packed f16, hush.js:278-280)
-    const uint32_t *Wh = reinterpret_cast<const uint32_t *>(S.w);
+    // then the inputs in increasing index), two units per f16x2 instruction, weights as f16x2 unit pairs in the
+    // constant bank; the features enter as stored (packed f16, hush.js:278-280)
+    const uint32_t *Wh = reinterpret_cast<const uint32_t *>(wp.w);
     uint32_t a[8], b[8];
 #pragma unroll
     for (int p = 0; p < 8; p++) a[p] = Wh[MLP_HALF_B1 + p];
@@ -612,7 +608,7 @@ __global__ void __launch_bounds__(KB_NT, 2)
 #pragma unroll
   for (int i = 0; i < N_FEAT; i++) fe[i] = __half2float(__ushort_as_half(f2h(qf16(fe[i]))));
   const float4 *Wt;
-  if constexpr (!TC) Wt = S.w;
+  if constexpr (!TC) Wt = wp.w;
   float4 a[4];
 #pragma unroll
   for (int q = 0; q < 4; q++) a[q] = Wt[MLP_FP32_B1 + q];
@@ -1344,23 +1340,23 @@ static const FineMaps &fine_maps(const HushFrame &f) {
   return e.m;
 }
 
-cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpW16 &w16, int mlp_mode, const void *mlp_tc,
+cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpConst &mc, int mlp_mode, const void *mlp_tc,
                                cudaStream_t st) {
   const int hx = (f.W2 + HT_W - 1) / HT_W, hy = (f.H2 + HT_H - 1) / HT_H;
   const int qx = (f.W4 + HT_W - 1) / HT_W, qy = (f.H4 + HT_H - 1) / HT_H;
   const int hpx = (f.W2 + MP_W - 1) / MP_W;  // two-pixel mid tiles per row
   switch (stage) {
     case 0: {
-      // blob: bf16 hi / lo operands, f16 operands, then the transposed FP32 weights
+      // blob: the tensor-core forms' bf16 hi / lo operands and f16 operands; mc: the weights as a kernel parameter
       const uint4 *blob = (const uint4 *)mlp_tc;
       int dev = 0;
       cudaGetDevice(&dev);
       if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
       const dim3 g((f.W + KB_TW - 1) / KB_TW, (f.H + KB_TH - 1) / KB_TH);
       if (mlp_mode == 0) {
-        k_temporal_block<0><<<g, KB_NT, sizeof(KbSmem), st>>>(f, w16, blob + MLP_BLOB_FP32 / 16);
+        k_temporal_block<0><<<g, KB_NT, sizeof(KbSmem), st>>>(f, mc, blob);
       } else if (mlp_mode == 3) {
-        k_temporal_block<3><<<g, KB_NT, sizeof(KbSmem), st>>>(f, w16, blob + MLP_BLOB_HALF / 16);
+        k_temporal_block<3><<<g, KB_NT, sizeof(KbSmem), st>>>(f, mc, blob);
       } else {
         // the tensor-core forms need more than 48 KB of dynamic shared memory: opt in once per device
         static bool opted[2][64] = {};
@@ -1372,8 +1368,8 @@ cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpW16 &w16,
           if (e != cudaSuccess) return e;
           opted[m][dev] = true;
         }
-        if (m == 0) k_temporal_block<1><<<g, KB_NT, sizeof(KbTcSmem), st>>>(f, w16, blob + MLP_BLOB_BF16 / 16);
-        else k_temporal_block<2><<<g, KB_NT, sizeof(KbTcSmem), st>>>(f, w16, blob + MLP_BLOB_F16 / 16);
+        if (m == 0) k_temporal_block<1><<<g, KB_NT, sizeof(KbTcSmem), st>>>(f, mc, blob + MLP_BLOB_BF16 / 16);
+        else k_temporal_block<2><<<g, KB_NT, sizeof(KbTcSmem), st>>>(f, mc, blob + MLP_BLOB_F16 / 16);
       }
       break;
     }

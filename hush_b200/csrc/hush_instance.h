@@ -19,6 +19,7 @@ struct hush_s {
   int schedule = HUSH_SCHED_FUSED;
   std::vector<float> wf;
   hush::MlpW16 w16;
+  hush::MlpConst mconst[4];  // stage 0's weights per MLP form (kernel parameter)
   float *w_dev = nullptr;
   void *tc_blob_dev = nullptr;
   // state images (hush.js:783-793) plus the fused path's half-res planes

@@ -20,7 +20,8 @@ struct FusedPlan {
   int n_kernels;
   const char *labels[8];
 };
-cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpW16 &w16, int mlp_mode, const void *mlp_tc,
+struct MlpConst;
+cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpConst &mc, int mlp_mode, const void *mlp_tc,
                                cudaStream_t st);
 int fused_stage_count();
 const char *fused_stage_label(int stage);
@@ -37,15 +38,23 @@ constexpr int MLP_HALF_W1 = 0, MLP_HALF_B1 = 160, MLP_HALF_W2 = 168, MLP_HALF_B2
               MLP_HALF_B3 = 400;  // offsets in 32-bit words
 constexpr int MLP_HALF_BLOB_BYTES = 416 * 4;  // 406 words, padded to a multiple of 16 bytes
 void mlp_half_build_blob(const float *w812, uint32_t *blob);
-// The instance's weight blob on the device: bf16 hi | bf16 lo | f16 (tensor-core operands), the FP32 weights, then
-// the f16x2 weights.
-constexpr int MLP_BLOB_BF16 = 0, MLP_BLOB_F16 = 2 * MLP_TC_BLOB_BYTES, MLP_BLOB_FP32 = 3 * MLP_TC_BLOB_BYTES,
-              MLP_BLOB_HALF = MLP_BLOB_FP32 + 220 * 16, MLP_BLOB_BYTES = MLP_BLOB_HALF + MLP_HALF_BLOB_BYTES;
+// The instance's tensor-core weight operands on the device: bf16 hi | bf16 lo | f16.
+constexpr int MLP_BLOB_BF16 = 0, MLP_BLOB_F16 = 2 * MLP_TC_BLOB_BYTES, MLP_BLOB_BYTES = 3 * MLP_TC_BLOB_BYTES;
 // FP32 weights of the h = 16 network for the 4-lane MLP: per input i and lane k the float4 of the units lane k owns
 // (layer 1 / 2: units 4k..4k+3; layer 3: outputs k, 4+k, 8+k), then the biases in the same grouping.
 constexpr int MLP_FP32_W1 = 0, MLP_FP32_W2 = 80, MLP_FP32_W3 = 144, MLP_FP32_B1 = 208, MLP_FP32_B2 = 212,
               MLP_FP32_B3 = 216;  // offsets in float4
 constexpr int MLP_FP32_BLOB_BYTES = 220 * 16;
 void mlp_fp32_build_blob(const float *w812, float *blob);
+
+// Stage 0's MLP weights as one kernel parameter, so that they sit in the constant bank: every lane of a warp reads
+// the same weight, which reaches the FMA as a broadcast operand, and no CTA copies them into shared memory. Mode 0
+// holds the FP32 blob, mode 3 the f16x2 blob, the tensor-core modes the decoded weights (they add the biases).
+struct MlpConst {
+  float4 w[MLP_FP32_BLOB_BYTES / 16];
+};
+static_assert(MLP_HALF_BLOB_BYTES <= sizeof(MlpConst) && sizeof(MlpW16) <= sizeof(MlpConst), "MlpConst size");
+// The parameter for one mode from the 812 decoded weights of the h = 16 network (mlp_tc.cu).
+void mlp_const_build(const float *w812, int mlp_mode, MlpConst &c);
 
 }  // namespace hush

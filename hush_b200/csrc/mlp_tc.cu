@@ -93,4 +93,11 @@ void mlp_fp32_build_blob(const float *w, float *blob) {
     }
 }
 
+void mlp_const_build(const float *w, int mlp_mode, MlpConst &c) {
+  std::memset(&c, 0, sizeof(c));
+  if (mlp_mode == 0) mlp_fp32_build_blob(w, reinterpret_cast<float *>(c.w));
+  else if (mlp_mode == 3) mlp_half_build_blob(w, reinterpret_cast<uint32_t *>(c.w));
+  else std::memcpy(c.w, w, sizeof(MlpW16));
+}
+
 }  // namespace hush
