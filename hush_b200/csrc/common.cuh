@@ -17,7 +17,12 @@ HD_INL float4 h4_to_f4(uint2 t) {
 }
 // f32 -> f16 rounded toward zero: the storage-write rounding the reference models (hush.js:98).
 HD_INL uint16_t f2h(float x) { return __half_as_ushort(__float2half_rz(x)); }
-HD_INL uint32_t pack2(float a, float b) { return (uint32_t)f2h(a) | ((uint32_t)f2h(b) << 16); }
+// Two values in one conversion (cvt.rz.f16x2.f32 puts its first source in the upper half): a in bits 0-15.
+HD_INL uint32_t pack2(float a, float b) {
+  uint32_t r;
+  asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+  return r;
+}
 HD_INL uint2 f4_to_h4(float4 v) { return make_uint2(pack2(v.x, v.y), pack2(v.z, v.w)); }
 HD_INL float2 unpack2(uint32_t u) {
   __half2 h = *reinterpret_cast<__half2 *>(&u);

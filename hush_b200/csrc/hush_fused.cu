@@ -92,10 +92,10 @@ struct PixLoads {
   uint2 nd, mv, mat, k4[4], c4[4], m4[4], pq;
 };
 
-HD_INL void pixel_issue(const HushFrame &f, int px, int py, PixLoads &L) {
+HD_INL void pixel_issue(const HushFrame &f, int px, int py, uint2 mvr, PixLoads &L) {
   const int W = f.W, H = f.H;
   L.nd = __ldg(f.nd + py * f.p_nd + px);
-  L.mv = __ldg(f.mv + py * f.p_mv + px);
+  L.mv = mvr;
   L.mat = __ldg(f.mat + py * f.p_mat + px);
   if (f.reset) return;
   const float4 mv = h4_to_f4(L.mv);
@@ -143,29 +143,33 @@ HD_INL PixOut temporal_pixel_fast(const HushFrame &f, int px, int py, const Tile
   // 3x3 statistics of the illumination (valid neighbours), two passes
   const float4 illum = T(0, 0);
   const float l = illum.w;
-  float s1x = 0.f, s1y = 0.f, s1z = 0.f, cnt = 0.f;
+  // (r, g) as one packed FP32x2 lane pair, b and (in the second pass) L as the other: the same arithmetic per lane
+  float2 s1xy = f2(0.f, 0.f);
+  float s1z = 0.f, cnt = 0.f;
 #pragma unroll
   for (int j = 0; j < 9; j++) {
     const float4 c = T(j % 3 - 1, j / 3 - 1);
-    s1x += c.x; s1y += c.y; s1z += c.z;  // invalid entries hold rgb = 0
+    s1xy = add2(s1xy, lo2(c));  // invalid entries hold rgb = 0
+    s1z += c.z;
     cnt += l_valid(c.w) ? 1.0f : 0.0f;
   }
   cnt = fmaxf(cnt, 1.0f);
-  const float mux = s1x / cnt, muy = s1y / cnt, muz = s1z / cnt;
+  const float mux = s1xy.x / cnt, muy = s1xy.y / cnt, muz = s1z / cnt;
   const float slm = lum3(mux, muy, muz);
-  float svx = 0.f, svy = 0.f, svz = 0.f, svar = 0.f;
+  const float2 nmu_xy = f2(-mux, -muy), nmu_zl = f2(-muz, -slm);
+  float2 svxy = f2(0.f, 0.f), svzl = f2(0.f, 0.f);
 #pragma unroll
   for (int j = 0; j < 9; j++) {
     const float4 c = T(j % 3 - 1, j / 3 - 1);
     if (l_valid(c.w)) {
-      const float dx = c.x - mux, dy = c.y - muy, dz = c.z - muz, dl = c.w - slm;
-      svx += dx * dx; svy += dy * dy; svz += dz * dz;
-      svar += dl * dl;
+      const float2 dxy = add2(lo2(c), nmu_xy), dzl = add2(hi2(c), nmu_zl);
+      svxy = fma2(dxy, dxy, svxy);
+      svzl = fma2(dzl, dzl, svzl);
     }
   }
-  const float sdx = sqrtf(fmaxf(svx / cnt, 1e-12f)), sdy = sqrtf(fmaxf(svy / cnt, 1e-12f)),
-              sdz = sqrtf(fmaxf(svz / cnt, 1e-12f));
-  svar /= cnt;
+  const float sdx = sqrtf(fmaxf(svxy.x / cnt, 1e-12f)), sdy = sqrtf(fmaxf(svxy.y / cnt, 1e-12f)),
+              sdz = sqrtf(fmaxf(svzl.x / cnt, 1e-12f));
+  float svar = svzl.y / cnt;
   bool has = false;
   float hcx = 0.f, hcy = 0.f, hcz = 0.f;
   float4 hm = z4;
@@ -178,9 +182,13 @@ HD_INL PixOut temporal_pixel_fast(const HushFrame &f, int px, int py, const Tile
       const int qx = bix + (i & 1), qy = biy + (i >> 1);
       if (wts[i] > 0.0f && qx >= 0 && qy >= 0 && qx < W && qy < H && check_key(h4_to_f4(k4[i]), nd, mv.w, mv.z)) {
         const float4 c = h4_to_f4(c4[i]), m = h4_to_f4(m4[i]);
+        const float2 w2 = bc2(wts[i]);
         sumW += wts[i];
-        hcx += wts[i] * c.x; hcy += wts[i] * c.y; hcz += wts[i] * c.z;
-        hm.x += wts[i] * m.x; hm.y += wts[i] * m.y; hm.z += wts[i] * m.z; hm.w += wts[i] * m.w;
+        const float2 hxy = fma2(w2, lo2(c), f2(hcx, hcy));
+        hcx = hxy.x; hcy = hxy.y;
+        hcz += wts[i] * c.z;
+        const float2 mxy = fma2(w2, lo2(m), f2(hm.x, hm.y)), mzw = fma2(w2, hi2(m), f2(hm.z, hm.w));
+        hm = make_float4(mxy.x, mxy.y, mzw.x, mzw.y);
       }
     }
     if (sumW >= 0.01f) {
@@ -365,8 +373,15 @@ __global__ void __launch_bounds__(KB_NT, 2)
   const int lbx = li % (KB_TW / 2), lby = li / (KB_TW / 2);
   const int px0 = blockIdx.x * KB_TW + 2 * lbx, py0 = blockIdx.y * KB_TH + 2 * lby;
   // phase 1: the first pixel's loads and gathers in flight with the tile loads
+  // the four pixels' motion first: each pixel's reprojection gathers then wait for one load round trip, not two
+  uint2 mvq[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int px = px0 + (q & 1), py = py0 + (q >> 1);
+    mvq[q] = (px < f.W && py < f.H) ? __ldg(f.mv + py * f.p_mv + px) : make_uint2(0, 0);
+  }
   PixLoads PL;
-  if (px0 < f.W && py0 < f.H) pixel_issue(f, px0, py0, PL);
+  if (px0 < f.W && py0 < f.H) pixel_issue(f, px0, py0, mvq[0], PL);
   const int ox = blockIdx.x * KB_TW - 1, oy = blockIdx.y * KB_TH - 1;
   constexpr int N = KB_SWL * KB_SH;
 #pragma unroll 1
@@ -413,7 +428,7 @@ __global__ void __launch_bounds__(KB_NT, 2)
   for (int q = 0; q < 4; q++) {
     const int px = px0 + (q & 1), py = py0 + (q >> 1);
     const bool pin = px < f.W && py < f.H;
-    if (q > 0 && pin) pixel_issue(f, px, py, PL);
+    if (q > 0 && pin) pixel_issue(f, px, py, mvq[q], PL);
     const PixOut p = pin ? temporal_pixel_fast(f, px, py, ParityTile{S.I, 2 * lby + (q >> 1) + 1, 2 * lbx + (q & 1) + 1}, PL)
                          : pix_none();
     okp[q] = p.Ns.w != 0.0f;
@@ -1147,10 +1162,14 @@ __global__ void __launch_bounds__(FT_W *FT_H, 3) k_fine_final_fused(const __grid
 }
 
 // TAA (hush.js:639-677) with a 32 x 8 tile. The pixel's motion, colour and the four history texels of its bilinear
-// footprint are loaded before the tile barrier, so the motion -> history dependency overlaps the tile loads.
+// footprint are loaded before the tile barrier, so the motion -> history dependency overlaps the tile loads. The
+// YCoCg tile is held as (Y, Co) pairs beside a Cg plane, so the 3x3 statistics, the history sum, the clip bounds and
+// the blend run (Y, Co) as one packed FP32x2 operation and Cg as a scalar one, lane by lane the same arithmetic
+// (40 registers: six CTAs per SM).
 __global__ void __launch_bounds__(FT_W *FT_H) k_taa_fused(const __grid_constant__ HushFrame f) {
   constexpr int SW = FT_W + 2, SH = FT_H + 2, NT = FT_W * FT_H, NIT = (SW * SH + NT - 1) / NT;
-  __shared__ float3 sX[SW * SH];
+  __shared__ float2 sXY[SW * SH];
+  __shared__ float sXZ[SW * SH];
   const int li = threadIdx.x;
   const int tx = li % FT_W, ty = li / FT_W;
   const int px = blockIdx.x * FT_W + tx, py = blockIdx.y * FT_H + ty;
@@ -1180,7 +1199,9 @@ __global__ void __launch_bounds__(FT_W *FT_H) k_taa_fused(const __grid_constant_
     const int i = li + it * NT;
     if (i >= SW * SH) continue;
     const float4 x = h4_to_f4(tl[it]);
-    sX[i] = to_ycocg(tmap(make_float3(x.x, x.y, x.z)));
+    const float3 y = to_ycocg(tmap(make_float3(x.x, x.y, x.z)));
+    sXY[i] = make_float2(y.x, y.y);
+    sXZ[i] = y.z;
   }
   __syncthreads();
   if (px >= f.W || py >= f.H) return;
@@ -1192,39 +1213,56 @@ __global__ void __launch_bounds__(FT_W *FT_H) k_taa_fused(const __grid_constant_
     r = itmap(cur);
   } else {
     const int ti = (ty + 1) * SW + tx + 1;
-    float3 m1 = make_float3(0.f, 0.f, 0.f);
+    auto c9 = [&](int j) {
+      const int t = ti + (j / 3 - 1) * SW + (j % 3 - 1);
+      const float2 a = sXY[t];
+      return make_float4(a.x, a.y, sXZ[t], 0.0f);
+    };
+    float2 s2 = f2(0.f, 0.f);
+    float s1 = 0.f;
 #pragma unroll
     for (int j = 0; j < 9; j++) {
-      const float3 c = sX[ti + (j / 3 - 1) * SW + (j % 3 - 1)];
-      m1.x += c.x; m1.y += c.y; m1.z += c.z;
+      const float4 c = c9(j);
+      s2 = add2(s2, lo2(c));
+      s1 += c.z;
     }
-    m1.x /= 9.0f; m1.y /= 9.0f; m1.z /= 9.0f;
-    float3 v3 = make_float3(0.f, 0.f, 0.f);
+    const float m1x = s2.x / 9.0f, m1y = s2.y / 9.0f, m1z = s1 / 9.0f;
+    const float2 nm = f2(-m1x, -m1y);
+    float2 v2 = f2(0.f, 0.f);
+    float v1 = 0.f;
 #pragma unroll
     for (int j = 0; j < 9; j++) {
-      const float3 c = sX[ti + (j / 3 - 1) * SW + (j % 3 - 1)];
-      const float dx = c.x - m1.x, dy = c.y - m1.y, dz = c.z - m1.z;
-      v3.x += dx * dx; v3.y += dy * dy; v3.z += dz * dz;
+      const float4 c = c9(j);
+      const float2 d = add2(lo2(c), nm);
+      const float dz = c.z - m1z;
+      v2 = fma2(d, d, v2);
+      v1 += dz * dz;
     }
-    const float sdx = sqrtf(fmaxf(v3.x / 9.0f, 1e-12f)), sdy = sqrtf(fmaxf(v3.y / 9.0f, 1e-12f)),
-                sdz = sqrtf(fmaxf(v3.z / 9.0f, 1e-12f));
+    const float sdx = sqrtf(fmaxf(v2.x / 9.0f, 1e-12f)), sdy = sqrtf(fmaxf(v2.y / 9.0f, 1e-12f)),
+                sdz = sqrtf(fmaxf(v1 / 9.0f, 1e-12f));
     float3 res = cur;
     if (uvx >= 0.0f && uvy >= 0.0f && uvx <= 1.0f && uvy <= 1.0f) {
       const float fx = ppx - bxf, fy = ppy - byf;
-      float3 hist = make_float3(0.f, 0.f, 0.f);
+      float2 h2 = f2(0.f, 0.f);
+      float h1 = 0.f;
 #pragma unroll
       for (int j = 0; j < 4; j++) {
         const int oxj = j & 1, oyj = j >> 1;
         const float wb = (oxj == 1 ? fx : 1.0f - fx) * (oyj == 1 ? fy : 1.0f - fy);
         const float4 t = h4_to_f4(hq[j]);
-        hist.x += wb * t.x; hist.y += wb * t.y; hist.z += wb * t.z;
+        h2 = fma2(bc2(wb), lo2(t), h2);
+        h1 += wb * t.z;
       }
-      float3 hh = to_ycocg(tmap(hist));
-      hh.x = fminf(fmaxf(hh.x, m1.x - 1.25f * sdx), m1.x + 1.25f * sdx);
-      hh.y = fminf(fmaxf(hh.y, m1.y - 1.25f * sdy), m1.y + 1.25f * sdy);
-      hh.z = fminf(fmaxf(hh.z, m1.z - 1.25f * sdz), m1.z + 1.25f * sdz);
+      float3 hh = to_ycocg(tmap(make_float3(h2.x, h2.y, h1)));
+      const float2 sd2 = f2(sdx, sdy), m12 = f2(m1x, m1y);
+      const float2 lo = fma2(bc2(-1.25f), sd2, m12), hi = fma2(bc2(1.25f), sd2, m12);
+      hh.x = fminf(fmaxf(hh.x, lo.x), hi.x);
+      hh.y = fminf(fmaxf(hh.y, lo.y), hi.y);
+      hh.z = fminf(fmaxf(hh.z, m1z - 1.25f * sdz), m1z + 1.25f * sdz);
       const float3 hr = from_ycocg(hh);
-      res = make_float3(hr.x + (cur.x - hr.x) * 0.1f, hr.y + (cur.y - hr.y) * 0.1f, hr.z + (cur.z - hr.z) * 0.1f);
+      const float2 hr2 = f2(hr.x, hr.y);
+      const float2 b2 = fma2(add2(f2(cur.x, cur.y), f2(-hr.x, -hr.y)), bc2(0.1f), hr2);
+      res = make_float3(b2.x, b2.y, hr.z + (cur.z - hr.z) * 0.1f);
     }
     r = itmap(res);
   }
