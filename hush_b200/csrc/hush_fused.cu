@@ -112,6 +112,54 @@ HD_INL void pixel_issue(const HushFrame &f, int px, int py, uint2 mvr, PixLoads 
   L.pq = __ldg(f.par0_prev + (clampi(cy, 0, H - 1) >> 1) * f.W2 + (clampi(cx, 0, W - 1) >> 1));
 }
 
+// The same loads as pixel_issue(), as cp.async copies into shared memory (no registers held while they fly): slot
+// entry k of this thread at g[k * stride]: 0 normalDepth, 1 material, 2 previous par0, 3-6 key, 7-10 colour history,
+// 11-14 moments of the bilinear footprint. The caller commits the group.
+HD_INL void cp_async8(const uint2 *dst_smem, const uint2 *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(umma::smem_u32(dst_smem)), "l"(src) : "memory");
+}
+HD_INL void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+HD_INL void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+template <int STRIDE>
+HD_INL void pixel_issue_async(const HushFrame &f, int px, int py, uint2 mvr, uint2 *g) {
+  const int W = f.W, H = f.H;
+  cp_async8(g, f.nd + py * f.p_nd + px);
+  cp_async8(g + STRIDE, f.mat + py * f.p_mat + px);
+  if (f.reset) return;
+  const float4 mv = h4_to_f4(mvr);
+  const float ppx = (float)px + mv.x, ppy = (float)py + mv.y;
+  const int bix = __float2int_rz(floorf(ppx)), biy = __float2int_rz(floorf(ppy));
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int q = clampi(biy + (i >> 1), 0, H - 1) * W + clampi(bix + (i & 1), 0, W - 1);
+    cp_async8(g + (3 + i) * STRIDE, f.key_prev + q);
+    cp_async8(g + (7 + i) * STRIDE, f.hist_prev + q);
+    cp_async8(g + (11 + i) * STRIDE, f.mom_prev + q);
+  }
+  const int cx = __float2int_rz(floorf(ppx + 0.5f)), cy = __float2int_rz(floorf(ppy + 0.5f));
+  cp_async8(g + 2 * STRIDE, f.par0_prev + (clampi(cy, 0, H - 1) >> 1) * f.W2 + (clampi(cx, 0, W - 1) >> 1));
+}
+template <int STRIDE>
+HD_INL PixLoads pixel_fetch(const uint2 *g, uint2 mvr, bool reset) {
+  PixLoads L;
+  L.nd = g[0];
+  L.mat = g[STRIDE];
+  L.mv = mvr;
+  if (!reset) {
+    L.pq = g[2 * STRIDE];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      L.k4[i] = g[(3 + i) * STRIDE];
+      L.c4[i] = g[(7 + i) * STRIDE];
+      L.m4[i] = g[(11 + i) * STRIDE];
+    }
+  }
+  return L;
+}
+
 // pixel() of hush.js:111-223 over the (r, g, b, L) tile from the preloaded texels; same arithmetic as
 // temporal_pixel(). Writes A0, mom, key and returns the pixel's inputs to block().
 template <class Tile>
@@ -274,17 +322,22 @@ HD_INL float4 ffma4(float s, float4 w, float4 a) {  // a + s * w as two packed F
 // One thread per 2x2 block: tile 64 x 16 pixels = 32 x 8 blocks, 256 threads. Each thread runs pixel() for its four
 // pixels in block order, accumulates block()'s sums in registers in the WGSL's order (hush.js:226-282), forms the 20
 // features once and runs the whole FP32 MLP (weights in the constant bank, a kernel parameter: each FMA takes its
-// weight as a broadcast operand), so after the tile barrier no thread waits for another. The tile is stored column-parity-split (even and odd columns in separate rows of 33
-// entries): neighbouring threads, two pixel columns apart, then read consecutive 16-byte entries. The tensor-core
+// weight as a broadcast operand), so after the tile barrier no thread waits for another. The tile is stored
+// column-parity-split (even and odd columns in separate rows of 33 entries): neighbouring threads, two pixel columns
+// apart, then read consecutive 16-byte entries. The per-pixel loads (G-buffer texels and the dependent reprojection
+// gathers) go by cp.async into two shared-memory slots per thread, one pixel ahead: pixel q + 2's gathers are in
+// flight while pixel q + 1 computes, without holding registers (the FP32 and f16 forms). The tensor-core
 // forms instead write each block's features as one operand row and run each layer as two tcgen05 MMAs (M = 128,
 // N = 16) over the CTA's 256 rows, FP32 accumulators in TMEM; bias, ReLU and the heads stay FP32.
 constexpr int KB_TW = 64, KB_TH = 16, KB_NT = (KB_TW / 2) * (KB_TH / 2);
 constexpr int KB_SWL = KB_TW + 2, KB_SH = KB_TH + 2, KB_HW = KB_SWL / 2;
 HD_INL int kb_tix(int r, int c) { return (2 * r + (c & 1)) * KB_HW + (c >> 1); }
 
+constexpr int KB_NTEX = 15;  // texels of one pixel's loads (pixel_issue_async)
 struct KbSmem {
   float4 I[2 * KB_HW * KB_SH];   // illumination (r, g, b) and L (luminance or L_INVALID), apron 1
   float2 Lq[2 * KB_HW * KB_SH];  // (E * qf16(L), 1) for valid entries, (0, 0) otherwise
+  uint2 G[2][KB_NTEX][KB_NT];    // two pixels' loads in flight per thread, thread-minor (conflict-free)
 };
 // Tensor-core forms: the same tile plus the MMA operands of the CTA's 256 rows (one per block) in the K-major
 // no-swizzle layout, each as a split-precision pair (hi, lo): A1 256 x 32 (features, zero padded), A2 256 x 16
@@ -372,16 +425,18 @@ __global__ void __launch_bounds__(KB_NT, 2)
   }
   const int lbx = li % (KB_TW / 2), lby = li / (KB_TW / 2);
   const int px0 = blockIdx.x * KB_TW + 2 * lbx, py0 = blockIdx.y * KB_TH + 2 * lby;
-  // phase 1: the first pixel's loads and gathers in flight with the tile loads
-  // the four pixels' motion first: each pixel's reprojection gathers then wait for one load round trip, not two
+  // phase 1: the four pixels' motion first (each pixel's reprojection gathers then wait for one load round trip, not
+  // two), then the first pixels' loads and gathers in flight with the tile loads
   uint2 mvq[4];
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     const int px = px0 + (q & 1), py = py0 + (q >> 1);
     mvq[q] = (px < f.W && py < f.H) ? __ldg(f.mv + py * f.p_mv + px) : make_uint2(0, 0);
   }
+  constexpr bool ASYNC = !TC;  // per-pixel loads by cp.async into two shared-memory slots per thread
   PixLoads PL;
-  if (px0 < f.W && py0 < f.H) pixel_issue(f, px0, py0, mvq[0], PL);
+  if constexpr (!ASYNC)
+    if (px0 < f.W && py0 < f.H) pixel_issue(f, px0, py0, mvq[0], PL);
   const int ox = blockIdx.x * KB_TW - 1, oy = blockIdx.y * KB_TH - 1;
   constexpr int N = KB_SWL * KB_SH;
 #pragma unroll 1
@@ -397,6 +452,16 @@ __global__ void __launch_bounds__(KB_NT, 2)
       tn[u] = __ldg(f.nd + cy * f.p_nd + cx);
       tr[u] = __ldg(f.rad + cy * f.p_rad + cx);
       tm[u] = __ldg(f.mat + cy * f.p_mat + cx);
+    }
+    if constexpr (ASYNC) {
+      if (i0 == 0) {  // the first two pixels' loads, behind the first tile loads
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+          const int px = px0 + (q & 1), py = py0 + (q >> 1);
+          if (px < f.W && py < f.H) pixel_issue_async<KB_NT>(f, px, py, mvq[q], &S.G[q][0][li]);
+          cp_async_commit();
+        }
+      }
     }
 #pragma unroll
     for (int u = 0; u < 2; u++) {
@@ -428,9 +493,22 @@ __global__ void __launch_bounds__(KB_NT, 2)
   for (int q = 0; q < 4; q++) {
     const int px = px0 + (q & 1), py = py0 + (q >> 1);
     const bool pin = px < f.W && py < f.H;
-    if (q > 0 && pin) pixel_issue(f, px, py, mvq[q], PL);
+    if constexpr (ASYNC) {
+      if (q < 3) cp_async_wait<1>();
+      else cp_async_wait<0>();
+      if (pin) PL = pixel_fetch<KB_NT>(&S.G[q & 1][0][li], mvq[q], f.reset);
+    } else {
+      if (q > 0 && pin) pixel_issue(f, px, py, mvq[q], PL);
+    }
     const PixOut p = pin ? temporal_pixel_fast(f, px, py, ParityTile{S.I, 2 * lby + (q >> 1) + 1, 2 * lbx + (q & 1) + 1}, PL)
                          : pix_none();
+    if constexpr (ASYNC) {
+      if (q < 2) {  // pixel q + 2 into the slot pixel q has finished reading
+        const int qx = px0 + (q & 1), qy = py0 + 1;
+        if (qx < f.W && qy < f.H) pixel_issue_async<KB_NT>(f, qx, qy, mvq[q + 2], &S.G[q & 1][0][li]);
+        cp_async_commit();
+      }
+    }
     okp[q] = p.Ns.w != 0.0f;
     la[q] = p.P0.x;
     zs[q] = p.P2.z;
@@ -979,14 +1057,18 @@ HD_INL void tile_mid_pair(const HushFrame &f, int tileX, int tileY, const uint2 
   }
 }
 
-// stage 1: mid1 tiles then coarse1 tiles; stage 2: mid2 tiles then coarse2 tiles; stage 3: mid3 tiles.
+// stage 1: mid1 and coarse1 tiles; stage 2: mid2 and coarse2 tiles; stage 3: mid3 tiles. Tiles t < nA are mid tiles,
+// the rest coarse tiles; the coarse tiles run on the first block indices.
 template <int STAGE>
 __global__ void __launch_bounds__(HT_W *HT_H) k_half_stage(const __grid_constant__ HushFrame f, int nAx, int nA,
                                                            int nBx, const __grid_constant__ HalfMaps M) {
   constexpr int SMAX = (HT_W + 8) * (HT_H + 8);
   __shared__ alignas(128) float4 sA[SMAX];
   __shared__ alignas(128) float4 sG[SMAX];
-  const int b = blockIdx.x;
+  // the coarse tiles (fewer, each several times longer) take the first block indices, so they start in the first
+  // wave and the short mid tiles fill in behind them instead of leaving a tail of coarse tiles at the end
+  const int nC = (int)gridDim.x - nA;
+  const int b = blockIdx.x >= nC ? blockIdx.x - nC : blockIdx.x + nA;
   if (b < nA) {
     const int tX = b % nAx, tY = b / nAx;
     if (STAGE == 1) tile_mid1(f, tX, tY, sA, sG, M.ok ? &M : nullptr);
@@ -999,13 +1081,14 @@ __global__ void __launch_bounds__(HT_W *HT_H) k_half_stage(const __grid_constant
   }
 }
 
-// stages 2 and 3 with the two-pixel mid tiles: 32 x 8 mid2 / mid3 tiles (blockIdx.x < nA), then stage 2's coarse2
+// stages 2 and 3 with the two-pixel mid tiles: 32 x 8 mid2 / mid3 tiles (tile index < nA), and stage 2's coarse2
 // tiles (16 x 8, quarter resolution). Dynamic shared memory: the pair tile, or coarse2's two float4 tiles.
 template <int STAGE>
 __global__ void __launch_bounds__(HT_W *HT_H) k_half_pair(const __grid_constant__ HushFrame f, int nAx, int nA,
                                                           int nBx, const __grid_constant__ HalfMaps M) {
   extern __shared__ __align__(128) float4 hp_smem[];  // 128-byte aligned: coarse2 stages its guide by TMA
-  const int b = blockIdx.x;
+  const int nC = (int)gridDim.x - nA;  // coarse tiles first, as in k_half_stage
+  const int b = blockIdx.x >= nC ? blockIdx.x - nC : blockIdx.x + nA;
   if (b < nA) {
     if (STAGE == 2) tile_mid_pair<2, 2>(f, b % nAx, b / nAx, f.Bh0, f.Bh1, hp_smem);
     else tile_mid_pair<4, 3>(f, b % nAx, b / nAx, f.Bh1, f.Bh0, hp_smem);
@@ -1391,24 +1474,19 @@ cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpConst &mc
       cudaGetDevice(&dev);
       if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
       const dim3 g((f.W + KB_TW - 1) / KB_TW, (f.H + KB_TH - 1) / KB_TH);
-      if (mlp_mode == 0) {
-        k_temporal_block<0><<<g, KB_NT, sizeof(KbSmem), st>>>(f, mc, blob);
-      } else if (mlp_mode == 3) {
-        k_temporal_block<3><<<g, KB_NT, sizeof(KbSmem), st>>>(f, mc, blob);
-      } else {
-        // the tensor-core forms need more than 48 KB of dynamic shared memory: opt in once per device
-        static bool opted[2][64] = {};
-        const int m = mlp_mode == 1 ? 0 : 1;
-        if (!opted[m][dev]) {
-          const cudaError_t e = cudaFuncSetAttribute(m == 0 ? k_temporal_block<1> : k_temporal_block<2>,
-                                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     (int)sizeof(KbTcSmem));
-          if (e != cudaSuccess) return e;
-          opted[m][dev] = true;
-        }
-        if (m == 0) k_temporal_block<1><<<g, KB_NT, sizeof(KbTcSmem), st>>>(f, mc, blob + MLP_BLOB_BF16 / 16);
-        else k_temporal_block<2><<<g, KB_NT, sizeof(KbTcSmem), st>>>(f, mc, blob + MLP_BLOB_F16 / 16);
+      // every form needs more than 48 KB of dynamic shared memory: opt in once per device and form
+      static bool opted[4][64] = {};
+      const int m = mlp_mode & 3;
+      void (*const kern[4])(HushFrame, MlpConst, const uint4 *) = {k_temporal_block<0>, k_temporal_block<1>,
+                                                                   k_temporal_block<2>, k_temporal_block<3>};
+      const int smem = (m == 1 || m == 2) ? (int)sizeof(KbTcSmem) : (int)sizeof(KbSmem);
+      if (!opted[m][dev]) {
+        const cudaError_t e = cudaFuncSetAttribute(kern[m], cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        opted[m][dev] = true;
       }
+      const uint4 *b = m == 1 ? blob + MLP_BLOB_BF16 / 16 : m == 2 ? blob + MLP_BLOB_F16 / 16 : blob;
+      kern[m]<<<g, KB_NT, smem, st>>>(f, mc, b);
       break;
     }
     case 1: k_half_stage<1><<<hx * hy + qx * qy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx, half_maps(f)); break;
