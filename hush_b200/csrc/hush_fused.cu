@@ -86,33 +86,12 @@ HD_INL PixOut pix_none() {
 }
 
 // The loads of one pixel's pixel(): its G-buffer texels and the reprojection gathers of the previous frame's key,
-// colour and moments (bilinear footprint) and par0. Issued before the tile arithmetic and the barrier so that the
-// dependent-load chain (motion -> footprint) overlaps them.
+// colour and moments (bilinear footprint) and par0, as temporal_pixel_fast() reads them.
 struct PixLoads {
   uint2 nd, mv, mat, k4[4], c4[4], m4[4], pq;
 };
 
-HD_INL void pixel_issue(const HushFrame &f, int px, int py, uint2 mvr, PixLoads &L) {
-  const int W = f.W, H = f.H;
-  L.nd = __ldg(f.nd + py * f.p_nd + px);
-  L.mv = mvr;
-  L.mat = __ldg(f.mat + py * f.p_mat + px);
-  if (f.reset) return;
-  const float4 mv = h4_to_f4(L.mv);
-  const float ppx = (float)px + mv.x, ppy = (float)py + mv.y;
-  const int bix = __float2int_rz(floorf(ppx)), biy = __float2int_rz(floorf(ppy));
-#pragma unroll
-  for (int i = 0; i < 4; i++) {
-    const int q = clampi(biy + (i >> 1), 0, H - 1) * W + clampi(bix + (i & 1), 0, W - 1);
-    L.k4[i] = __ldg(f.key_prev + q);
-    L.c4[i] = __ldg(f.hist_prev + q);
-    L.m4[i] = __ldg(f.mom_prev + q);
-  }
-  const int cx = __float2int_rz(floorf(ppx + 0.5f)), cy = __float2int_rz(floorf(ppy + 0.5f));
-  L.pq = __ldg(f.par0_prev + (clampi(cy, 0, H - 1) >> 1) * f.W2 + (clampi(cx, 0, W - 1) >> 1));
-}
-
-// The same loads as pixel_issue(), as cp.async copies into shared memory (no registers held while they fly): slot
+// A pixel's loads are issued as cp.async copies into a shared-memory slot (no registers held while they fly): slot
 // entry k of this thread at g[k * stride]: 0 normalDepth, 1 material, 2 previous par0, 3-6 key, 7-10 colour history,
 // 11-14 moments of the bilinear footprint. The caller commits the group.
 HD_INL void cp_async8(const uint2 *dst_smem, const uint2 *src) {
@@ -326,7 +305,7 @@ HD_INL float4 ffma4(float s, float4 w, float4 a) {  // a + s * w as two packed F
 // column-parity-split (even and odd columns in separate rows of 33 entries): neighbouring threads, two pixel columns
 // apart, then read consecutive 16-byte entries. The per-pixel loads (G-buffer texels and the dependent reprojection
 // gathers) go by cp.async into two shared-memory slots per thread, one pixel ahead: pixel q + 2's gathers are in
-// flight while pixel q + 1 computes, without holding registers (the FP32 and f16 forms). The tensor-core
+// flight while pixel q + 1 computes, without holding registers. The tensor-core
 // forms instead write each block's features as one operand row and run each layer as two tcgen05 MMAs (M = 128,
 // N = 16) over the CTA's 256 rows, FP32 accumulators in TMEM; bias, ReLU and the heads stay FP32.
 constexpr int KB_TW = 64, KB_TH = 16, KB_NT = (KB_TW / 2) * (KB_TH / 2);
@@ -342,13 +321,19 @@ struct KbSmem {
 // Tensor-core forms: the same tile plus the MMA operands of the CTA's 256 rows (one per block) in the K-major
 // no-swizzle layout, each as a split-precision pair (hi, lo): A1 256 x 32 (features, zero padded), A2 256 x 16
 // (hidden layers), then the weights B1 / B2 / B3 (hi, and for bf16 lo).
+// The per-pixel load slots (pixel phase) and the MMA operands (MLP phase, after a CTA barrier) share their space.
 struct KbTcSmem {
   float4 I[2 * KB_HW * KB_SH];
   float2 Lq[2 * KB_HW * KB_SH];
-  alignas(128) uint8_t a1[KB_NT * 32 * 2];
-  alignas(128) uint8_t a1lo[KB_NT * 32 * 2];
-  alignas(128) uint8_t a2[KB_NT * 16 * 2];
-  alignas(128) uint8_t a2lo[KB_NT * 16 * 2];
+  union {
+    uint2 G[2][KB_NTEX][KB_NT];
+    struct {
+      alignas(128) uint8_t a1[KB_NT * 32 * 2];
+      alignas(128) uint8_t a1lo[KB_NT * 32 * 2];
+      alignas(128) uint8_t a2[KB_NT * 16 * 2];
+      alignas(128) uint8_t a2lo[KB_NT * 16 * 2];
+    };
+  };
   alignas(128) uint8_t b[2 * MLP_TC_BLOB_BYTES];
   alignas(8) uint64_t mbar[2];  // one per 128-row group
   uint32_t tmem;
@@ -433,10 +418,7 @@ __global__ void __launch_bounds__(KB_NT, 2)
     const int px = px0 + (q & 1), py = py0 + (q >> 1);
     mvq[q] = (px < f.W && py < f.H) ? __ldg(f.mv + py * f.p_mv + px) : make_uint2(0, 0);
   }
-  constexpr bool ASYNC = !TC;  // per-pixel loads by cp.async into two shared-memory slots per thread
   PixLoads PL;
-  if constexpr (!ASYNC)
-    if (px0 < f.W && py0 < f.H) pixel_issue(f, px0, py0, mvq[0], PL);
   const int ox = blockIdx.x * KB_TW - 1, oy = blockIdx.y * KB_TH - 1;
   constexpr int N = KB_SWL * KB_SH;
 #pragma unroll 1
@@ -453,14 +435,12 @@ __global__ void __launch_bounds__(KB_NT, 2)
       tr[u] = __ldg(f.rad + cy * f.p_rad + cx);
       tm[u] = __ldg(f.mat + cy * f.p_mat + cx);
     }
-    if constexpr (ASYNC) {
-      if (i0 == 0) {  // the first two pixels' loads, behind the first tile loads
+    if (i0 == 0) {  // the first two pixels' loads (cp.async into their slots), behind the first tile loads
 #pragma unroll
-        for (int q = 0; q < 2; q++) {
-          const int px = px0 + (q & 1), py = py0 + (q >> 1);
-          if (px < f.W && py < f.H) pixel_issue_async<KB_NT>(f, px, py, mvq[q], &S.G[q][0][li]);
-          cp_async_commit();
-        }
+      for (int q = 0; q < 2; q++) {
+        const int px = px0 + (q & 1), py = py0 + (q >> 1);
+        if (px < f.W && py < f.H) pixel_issue_async<KB_NT>(f, px, py, mvq[q], &S.G[q][0][li]);
+        cp_async_commit();
       }
     }
 #pragma unroll
@@ -493,21 +473,15 @@ __global__ void __launch_bounds__(KB_NT, 2)
   for (int q = 0; q < 4; q++) {
     const int px = px0 + (q & 1), py = py0 + (q >> 1);
     const bool pin = px < f.W && py < f.H;
-    if constexpr (ASYNC) {
-      if (q < 3) cp_async_wait<1>();
-      else cp_async_wait<0>();
-      if (pin) PL = pixel_fetch<KB_NT>(&S.G[q & 1][0][li], mvq[q], f.reset);
-    } else {
-      if (q > 0 && pin) pixel_issue(f, px, py, mvq[q], PL);
-    }
+    if (q < 3) cp_async_wait<1>();  // this pixel's group has landed (the next pixel's may still fly)
+    else cp_async_wait<0>();
+    if (pin) PL = pixel_fetch<KB_NT>(&S.G[q & 1][0][li], mvq[q], f.reset);
     const PixOut p = pin ? temporal_pixel_fast(f, px, py, ParityTile{S.I, 2 * lby + (q >> 1) + 1, 2 * lbx + (q & 1) + 1}, PL)
                          : pix_none();
-    if constexpr (ASYNC) {
-      if (q < 2) {  // pixel q + 2 into the slot pixel q has finished reading
-        const int qx = px0 + (q & 1), qy = py0 + 1;
-        if (qx < f.W && qy < f.H) pixel_issue_async<KB_NT>(f, qx, qy, mvq[q + 2], &S.G[q & 1][0][li]);
-        cp_async_commit();
-      }
+    if (q < 2) {  // pixel q + 2 into the slot pixel q has finished reading
+      const int qx = px0 + (q & 1), qy = py0 + 1;
+      if (qx < f.W && qy < f.H) pixel_issue_async<KB_NT>(f, qx, qy, mvq[q + 2], &S.G[q & 1][0][li]);
+      cp_async_commit();
     }
     okp[q] = p.Ns.w != 0.0f;
     la[q] = p.P0.x;
@@ -592,6 +566,7 @@ __global__ void __launch_bounds__(KB_NT, 2)
   }
   const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
   if constexpr (TC) {
+    __syncthreads();  // every thread is done with its load slots, which the operand rows overwrite
     // phase 4 (tensor cores): every thread writes its block's operand row (zeros for blocks outside the image or
     // without valid pixels) and takes part in all three layers
     constexpr bool BF16 = MODE == 1;
