@@ -64,9 +64,50 @@ extern "C" void hush_required_limits(int *cc_major, int *cc_minor, size_t *share
 static void drop_graphs(hush_t *h) {
   for (int i = 0; i < 2; i++) {
     if (h->gexec[i]) cudaGraphExecDestroy(h->gexec[i]);
+    if (h->gtmpl[i]) cudaGraphDestroy(h->gtmpl[i]);
     h->gexec[i] = nullptr;
+    h->gtmpl[i] = nullptr;
+    h->gnodes[i].clear();
     h->gkey_reset[i] = -1;
   }
+}
+
+// The kernel nodes of a captured fused frame in launch order, or none if the graph holds anything the parameter
+// update below cannot rewrite (another node type, a kernel outside the fused schedule).
+static std::vector<cudaGraphNode_t> frame_kernel_nodes(cudaGraph_t g) {
+  size_t n = 0;
+  if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0 || n > 16) return {};
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return {};
+  for (cudaGraphNode_t nd : nodes) {
+    cudaGraphNodeType t;
+    cudaKernelNodeParams p;
+    if (cudaGraphNodeGetType(nd, &t) != cudaSuccess || t != cudaGraphNodeTypeKernel ||
+        cudaGraphKernelNodeGetParams(nd, &p) != cudaSuccess || hush::fused_kernel_param_count(p.func) == 0)
+      return {};
+  }
+  return nodes;
+}
+
+// A frame of the same parity, reset flag and exposure as the executable graph's, with other input buffers: every
+// fused kernel takes the frame as its first parameter, so the graph is brought up to date by setting that parameter
+// of each kernel node (the other parameters, which depend only on the instance's own buffers, are kept).
+static cudaError_t update_frame_params(hush_t *h, int cur, const hush::HushFrame &f) {
+  for (cudaGraphNode_t nd : h->gnodes[cur]) {
+    cudaKernelNodeParams p;
+    cudaError_t e = cudaGraphKernelNodeGetParams(nd, &p);
+    if (e != cudaSuccess) return e;
+    const int n = hush::fused_kernel_param_count(p.func);
+    if (n <= 0 || n > 8 || !p.kernelParams) return cudaErrorInvalidValue;
+    void *args[8];
+    args[0] = const_cast<hush::HushFrame *>(&f);
+    for (int i = 1; i < n; i++) args[i] = p.kernelParams[i];
+    p.kernelParams = args;
+    p.extra = nullptr;
+    e = cudaGraphExecKernelNodeSetParams(h->gexec[cur], nd, &p);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 static void free_host_staging(hush_t *h) {
@@ -385,6 +426,16 @@ extern "C" int hush_denoise(hush_t *h, const hush_inputs *in, void *stream, cons
     const void *key[5] = {in->radiance, in->normal_depth, in->motion, in->material, in->emission};
     bool hit = h->gexec[cur] && h->gkey_reset[cur] == f.reset && h->gkey_exposure[cur] == f.exposure &&
                std::memcmp(h->gkey[cur], key, sizeof(key)) == 0;
+    if (!hit && h->gexec[cur] && !h->gnodes[cur].empty() && h->gkey_reset[cur] == f.reset &&
+        h->gkey_exposure[cur] == f.exposure) {
+      // only the input buffers changed: rewrite the frame parameter of each kernel node
+      if (update_frame_params(h, cur, f) == cudaSuccess) {
+        std::memcpy(h->gkey[cur], key, sizeof(key));
+        hit = true;
+      } else {
+        cudaGetLastError();  // clear the failure; capture instead
+      }
+    }
     if (!hit) {
       // capture the frame again; an existing executable graph of the same parity is updated in place (same
       // kernels, new parameters), which is much cheaper than instantiating a new one
@@ -409,11 +460,24 @@ extern "C" int hush_denoise(hush_t *h, const hush_inputs *in, void *stream, cons
           h->gexec[cur] = nullptr;
         }
       }
-      if (!updated) e = cudaGraphInstantiate(&h->gexec[cur], g, 0);
-      cudaGraphDestroy(g);
-      if (e != cudaSuccess) {
-        h->gexec[cur] = nullptr;
-        return hush_cuda_fail(h, e, "cudaGraphInstantiate");
+      if (updated) {
+        // the executable graph keeps the node identities of the graph it was instantiated from (gtmpl)
+        cudaGraphDestroy(g);
+      } else {
+        e = cudaGraphInstantiate(&h->gexec[cur], g, 0);
+        if (h->gtmpl[cur]) cudaGraphDestroy(h->gtmpl[cur]);
+        h->gtmpl[cur] = nullptr;
+        h->gnodes[cur].clear();
+        if (e != cudaSuccess) {
+          cudaGraphDestroy(g);
+          h->gexec[cur] = nullptr;
+          return hush_cuda_fail(h, e, "cudaGraphInstantiate");
+        }
+        // keep the captured graph: its kernel nodes name the executable graph's nodes for parameter updates (their
+        // parameters other than the frame depend only on the instance's buffers, sizes, weights and MLP form, and
+        // any change of those drops the graphs)
+        h->gtmpl[cur] = g;
+        if (h->schedule == HUSH_SCHED_FUSED) h->gnodes[cur] = frame_kernel_nodes(g);
       }
       std::memcpy(h->gkey[cur], key, sizeof(key));
       h->gkey_reset[cur] = f.reset;

@@ -1483,4 +1483,17 @@ cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpConst &mc
 
 size_t fused_scratch_bytes(int, int) { return 0; }
 
+int fused_kernel_param_count(const void *func) {
+  const void *three[4] = {(const void *)k_temporal_block<0>, (const void *)k_temporal_block<1>,
+                          (const void *)k_temporal_block<2>, (const void *)k_temporal_block<3>};
+  for (const void *k : three)
+    if (func == k) return 3;  // (f, wp, blob)
+  if (func == (const void *)k_half_stage<1> || func == (const void *)k_half_pair<2> ||
+      func == (const void *)k_half_pair<3>)
+    return 5;  // (f, nAx, nA, nBx, M)
+  if (func == (const void *)k_fine_final_fused) return 2;  // (f, M)
+  if (func == (const void *)k_taa_fused) return 1;          // (f)
+  return 0;
+}
+
 }  // namespace hush

@@ -44,6 +44,10 @@ struct hush_s {
   int gkey_reset[2] = {-1, -1};
   float gkey_exposure[2] = {0, 0};
   cudaStream_t gstream[2] = {nullptr, nullptr};
+  // the captured graph each executable graph came from, and its kernel nodes in launch order: a frame whose input
+  // buffers differ only updates the nodes' HushFrame parameter instead of capturing the frame again
+  cudaGraph_t gtmpl[2] = {nullptr, nullptr};
+  std::vector<cudaGraphNode_t> gnodes[2];
   // host-buffer frames (hush_denoise_host): two device staging sets for the five inputs, a copy-in and a copy-out
   // stream, and the events that order them against the frames
   void *hin_pool = nullptr;

@@ -26,6 +26,8 @@ cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpConst &mc
 int fused_stage_count();
 const char *fused_stage_label(int stage);
 size_t fused_scratch_bytes(int W, int H);
+// Number of parameters of a fused-schedule kernel (its first parameter is the HushFrame), 0 for any other function.
+int fused_kernel_param_count(const void *func);
 
 // Tensor-core MLP weight operands for h = 16 in the UMMA K-major no-swizzle shared-memory layout: B1 (16 x 32, W1
 // zero-padded along K), B2 (16 x 16), B3 (16 x 16, W3 zero-padded along N), in bf16 or f16 (mlp_tc.cu). lo = 1
