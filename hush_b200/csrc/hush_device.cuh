@@ -267,25 +267,50 @@ HD_INL float4 filt_x(const float4 *sA, const float4 *sG, int lx, int ly, int qx,
   float sw = cw;
   float scx = center.x * cw, scy = center.y * cw, scz = center.z * cw;
   float sv = center.w * cw * cw;
+  // the taps in the WGSL's order (row-major, centre left out), two at a time: the pair's (n.n)^128 chains, weights
+  // and squared weights are packed FP32x2 operations (lane by lane the scalar arithmetic), the accumulation stays in
+  // tap order
+  constexpr int NTAP = (2 * R + 1) * (2 * R + 1) - 1;
 #pragma unroll
-  for (int dy = -R; dy <= R; dy++) {
+  for (int k = 0; k < NTAP; k += 2) {
+    int dxs[2], dys[2];
 #pragma unroll
-    for (int dx = -R; dx <= R; dx++) {
-      if (dx == 0 && dy == 0) continue;
-      const int o = dy * STEP * SW + dx * STEP;
-      const float4 gq = sG[ti + o];
-      const int tx = qx + dx * STEP, ty = qy + dy * STEP;
-      if ((!CHECK || (tx >= 0 && ty >= 0 && tx < w && ty < h)) && gq.w >= 0.0f) {
-        const float4 cq = sA[ti + o];
-        const float arg = fmaf(-fabsf(gq.w - gp.w), izl[dx * dx + dy * dy],
-                               fmaf(-sll, fabsf(lum(cq) - lc), lg_h(R, dx) + lg_h(R, dy)));
-        const float wt = pow128(fmaxf(dot3(gq, gp), 0.0f)) * ex2_approx(arg);
-        sw += wt;
-        scx += wt * cq.x;
-        scy += wt * cq.y;
-        scz += wt * cq.z;
-        sv += wt * wt * cq.w;
-      }
+    for (int u = 0; u < 2; u++) {
+      const int t = k + u < NTAP / 2 ? k + u : k + u + 1;  // skip the centre
+      dxs[u] = t % (2 * R + 1) - R;
+      dys[u] = t / (2 * R + 1) - R;
+    }
+    const int o0 = dys[0] * STEP * SW + dxs[0] * STEP, o1 = dys[1] * STEP * SW + dxs[1] * STEP;
+    const float4 g0 = sG[ti + o0], g1 = sG[ti + o1];
+    const float4 c0 = sA[ti + o0], c1 = sA[ti + o1];
+    bool ok0 = g0.w >= 0.0f, ok1 = g1.w >= 0.0f;
+    if (CHECK) {
+      const int x0 = qx + dxs[0] * STEP, y0 = qy + dys[0] * STEP, x1 = qx + dxs[1] * STEP, y1 = qy + dys[1] * STEP;
+      ok0 = ok0 && x0 >= 0 && y0 >= 0 && x0 < w && y0 < h;
+      ok1 = ok1 && x1 >= 0 && y1 >= 0 && x1 < w && y1 < h;
+    }
+    float2 pp = make_float2(fmaxf(dot3(g0, gp), 0.0f), fmaxf(dot3(g1, gp), 0.0f));
+#pragma unroll
+    for (int i = 0; i < 7; i++) pp = __fmul2_rn(pp, pp);  // (n.n)^128
+    const float a0 = fmaf(-fabsf(g0.w - gp.w), izl[dxs[0] * dxs[0] + dys[0] * dys[0]],
+                          fmaf(-sll, fabsf(lum(c0) - lc), lg_h(R, dxs[0]) + lg_h(R, dys[0])));
+    const float a1 = fmaf(-fabsf(g1.w - gp.w), izl[dxs[1] * dxs[1] + dys[1] * dys[1]],
+                          fmaf(-sll, fabsf(lum(c1) - lc), lg_h(R, dxs[1]) + lg_h(R, dys[1])));
+    const float2 wt = __fmul2_rn(pp, make_float2(ex2_approx(a0), ex2_approx(a1)));
+    const float2 ww = __fmul2_rn(wt, wt);
+    if (ok0) {
+      sw += wt.x;
+      scx += wt.x * c0.x;
+      scy += wt.x * c0.y;
+      scz += wt.x * c0.z;
+      sv += ww.x * c0.w;
+    }
+    if (ok1) {
+      sw += wt.y;
+      scx += wt.y * c1.x;
+      scy += wt.y * c1.y;
+      scz += wt.y * c1.z;
+      sv += ww.y * c1.w;
     }
   }
   return make_float4(scx / sw, scy / sw, scz / sw, sv / (sw * sw));

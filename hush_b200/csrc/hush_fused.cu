@@ -1084,7 +1084,7 @@ constexpr int FT_W = 32, FT_H = 8;
 // it instead of being fetched and decoded per tap.
 constexpr int FH_W = FT_W / 2 + 2, FH_H = FT_H / 2 + 2, FQ_W = FT_W / 4 + 2, FQ_H = FT_H / 4 + 2;
 constexpr int FB_W = FT_W + 4, FB_H = FT_H + 2;  // the TMA box of the A0 / key tiles
-__global__ void __launch_bounds__(FT_W *FT_H, 3) k_fine_final_fused(const __grid_constant__ HushFrame f,
+__global__ void __launch_bounds__(FT_W *FT_H, 4) k_fine_final_fused(const __grid_constant__ HushFrame f,
                                                                      const __grid_constant__ FineMaps M) {
   constexpr int AP = 1, SW = FT_W + 2, SH = FT_H + 2;
   constexpr int NH = FH_W * FH_H, NQ = FQ_W * FQ_H, NP = (FT_W / 2) * (FT_H / 2);
