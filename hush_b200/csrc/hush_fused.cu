@@ -1180,18 +1180,39 @@ __global__ void __launch_bounds__(FT_W *FT_H, 4) k_fine_final_fused(const __grid
   const int qsx = (f.W + 3) / 4, qsy = (f.H + 3) / 4;
   const float cposx = ((float)px + 0.5f) / 4.0f - 0.5f, cposy = ((float)py + 0.5f) / 4.0f - 0.5f;
   const float cbx = floorf(cposx), cby = floorf(cposy);
+  // jbw() of two taps at a time: the (n.n)^8 and weight products as packed FP32x2, the accumulation in tap order
+  auto jbw2 = [&](float2 wb, float4 n0, float4 n1) {
+    const float2 d = make_float2(fmaxf(dot3(n0, gp), 0.0f), fmaxf(dot3(n1, gp), 0.0f));
+    const float2 d2 = __fmul2_rn(d, d), d4 = __fmul2_rn(d2, d2);
+    const float2 e = make_float2(ex2_approx(-fabsf(n0.w - z) * rzl), ex2_approx(-fabsf(n1.w - z) * rzl));
+    return __fmul2_rn(__fmul2_rn(__fmul2_rn(wb, e), d4), d4);
+  };
+  auto wbx = [](float fx_, float fy_, int j) {
+    return ((j & 1) == 1 ? fx_ : 1.0f - fx_) * ((j >> 1) == 1 ? fy_ : 1.0f - fy_);
+  };
   float uBx = 0.f, uBy = 0.f, uBz = 0.f, uAx = 0.f, uAy = 0.f, uAz = 0.f, swh = 0.f;
+  const float hfx = hposx - hbx, hfy = hposy - hby;
 #pragma unroll
-  for (int j = 0; j < 4; j++) {
-    const int qx = (int)hbx + (j & 1), qy = (int)hby + (j >> 1);
-    const int t = (qy - hy0) * FH_W + (qx - hx0);
-    const float4 gh = sHG[t];
-    if (!(qx >= 0 && qy >= 0 && qx < hsx && qy < hsy) || gh.w < 0.0f) continue;
-    const float w = jbw_x(hposx - hbx, hposy - hby, j, gh, gh.w, gp, z, rzl);
-    const float4 a = sHA[t], m = sHB[t];
-    swh += w;
-    uBx += w * m.x; uBy += w * m.y; uBz += w * m.z;
-    uAx += w * a.x; uAy += w * a.y; uAz += w * a.z;
+  for (int j = 0; j < 4; j += 2) {
+    const int qy = (int)hby + (j >> 1);
+    const int qx0 = (int)hbx, qx1 = qx0 + 1;
+    const int t0 = (qy - hy0) * FH_W + (qx0 - hx0), t1 = t0 + 1;
+    const float4 g0 = sHG[t0], g1 = sHG[t1];
+    const bool iy = qy >= 0 && qy < hsy;
+    const bool ok0 = iy && qx0 >= 0 && qx0 < hsx && g0.w >= 0.0f, ok1 = iy && qx1 >= 0 && qx1 < hsx && g1.w >= 0.0f;
+    const float2 w = jbw2(make_float2(wbx(hfx, hfy, j), wbx(hfx, hfy, j + 1)), g0, g1);
+    if (ok0) {
+      const float4 a = sHA[t0], m = sHB[t0];
+      swh += w.x;
+      uBx += w.x * m.x; uBy += w.x * m.y; uBz += w.x * m.z;
+      uAx += w.x * a.x; uAy += w.x * a.y; uAz += w.x * a.z;
+    }
+    if (ok1) {
+      const float4 a = sHA[t1], m = sHB[t1];
+      swh += w.y;
+      uBx += w.y * m.x; uBy += w.y * m.y; uBz += w.y * m.z;
+      uAx += w.y * a.x; uAy += w.y * a.y; uAz += w.y * a.z;
+    }
   }
   float ix = fx, iy = fy, iz = fz;
   if (swh > 1e-4f) {
@@ -1200,16 +1221,26 @@ __global__ void __launch_bounds__(FT_W *FT_H, 4) k_fine_final_fused(const __grid
     iz = uBz / swh + pr.w * (fz - uAz / swh);
   }
   float uCx = 0.f, uCy = 0.f, uCz = 0.f, swq = 0.f;
+  const float cfx = cposx - cbx, cfy = cposy - cby;
 #pragma unroll
-  for (int j = 0; j < 4; j++) {
-    const int rx = (int)cbx + (j & 1), ry = (int)cby + (j >> 1);
-    const int t = (ry - qy0) * FQ_W + (rx - qx0);
-    const float4 cg = sQG[t];
-    if (!(rx >= 0 && ry >= 0 && rx < qsx && ry < qsy) || cg.w < 0.0f) continue;
-    const float w = jbw_x(cposx - cbx, cposy - cby, j, cg, cg.w, gp, z, rzl);
-    const float4 c = sQC[t];
-    swq += w;
-    uCx += w * c.x; uCy += w * c.y; uCz += w * c.z;
+  for (int j = 0; j < 4; j += 2) {
+    const int ry = (int)cby + (j >> 1);
+    const int rx0 = (int)cbx, rx1 = rx0 + 1;
+    const int t0 = (ry - qy0) * FQ_W + (rx0 - qx0), t1 = t0 + 1;
+    const float4 g0 = sQG[t0], g1 = sQG[t1];
+    const bool iy = ry >= 0 && ry < qsy;
+    const bool ok0 = iy && rx0 >= 0 && rx0 < qsx && g0.w >= 0.0f, ok1 = iy && rx1 >= 0 && rx1 < qsx && g1.w >= 0.0f;
+    const float2 w = jbw2(make_float2(wbx(cfx, cfy, j), wbx(cfx, cfy, j + 1)), g0, g1);
+    if (ok0) {
+      const float4 c = sQC[t0];
+      swq += w.x;
+      uCx += w.x * c.x; uCy += w.x * c.y; uCz += w.x * c.z;
+    }
+    if (ok1) {
+      const float4 c = sQC[t1];
+      swq += w.y;
+      uCx += w.y * c.x; uCy += w.y * c.y; uCz += w.y * c.z;
+    }
   }
   float upx = ix, upy = iy, upz = iz;
   if (swq > 1e-4f) { upx = uCx / swq; upy = uCy / swq; upz = uCz / swq; }
