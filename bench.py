@@ -330,6 +330,21 @@ def run_ours(args):
     e2e_ms = max_over_ranks(f0.elapsed_time(f1)) / e2e_steps
     h2d = sum(host[0][n].numel() * 2 for n in scene.NAMES)
     d2h = outs[0].numel() * 2
+    # the PCIe bound of e2e: the same five pinned input copies alone, back to back on one stream (CUDA events)
+    staging = {n: torch.empty_like(frames[0][n]) for n in scene.NAMES}
+    for _ in range(3):
+        for n in scene.NAMES:
+            staging[n].copy_(host[0][n], non_blocking=True)
+    torch.cuda.synchronize()
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record(stream)
+    for i in range(10):
+        for n in scene.NAMES:
+            staging[n].copy_(host[i % len(host)][n], non_blocking=True)
+    c1.record(stream)
+    torch.cuda.synchronize()
+    h2d_peak_gbs = h2d * 10 / (c0.elapsed_time(c1) * 1e-3) / 1e9
+    del staging
 
     # ---- the other MLP form on the same frames, device-resident inputs (BF16 tensor-core MLP vs FP32 plain MLP)
     alt = "bf16" if args.mlp != "bf16" else "fp32"
@@ -416,7 +431,9 @@ def run_ours(args):
         "stages": per_stage,
         "clocks": clocks,
         "e2e": {"value": round(e2e_ms / world, 4), "unit": "ms/frame", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
+                "d2h_bytes_per_step": d2h,
+                # host -> device rate of the timed e2e steps against the same copies timed alone
+                "h2d_gbs": round(h2d / (e2e_ms * 1e-3) / 1e9, 1), "h2d_copy_peak_gbs": round(h2d_peak_gbs, 1)},
         "gpu_launches": n_kernels * args.steps,
         "kernel_status": hush.kernel_status(),  # the error word of the bounded waits after the run (0 = none gave up)
         "mlp_forms": {args.mlp: {"ms_per_frame": round(ms_frame, 4)},
