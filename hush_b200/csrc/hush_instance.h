@@ -43,7 +43,6 @@ struct hush_s {
   const void *gkey[2][5] = {};
   int gkey_reset[2] = {-1, -1};
   float gkey_exposure[2] = {0, 0};
-  cudaStream_t gstream[2] = {nullptr, nullptr};
   // the captured graph each executable graph came from, and its kernel nodes in launch order: a frame whose input
   // buffers differ only updates the nodes' HushFrame parameter instead of capturing the frame again
   cudaGraph_t gtmpl[2] = {nullptr, nullptr};

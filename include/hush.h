@@ -115,7 +115,8 @@ const void *hush_output(const hush_t *h);
 int hush_timer_enable(hush_t *h, int mode);
 int hush_timer_read(hush_t *h, hush_timing *out, int max);
 
-/* CUDA-graph replay of whole frames (config-5 style): capture the frame once per input-pointer set and replay it. */
+/* CUDA-graph replay of whole frames (config-5 style), one executable graph per ping-pong parity: new input pointers
+ * rewrite the kernels' frame parameter in place; a change of the reset flag or the exposure captures the frame again. */
 int hush_set_graph(hush_t *h, int enable);
 
 /* The kernels' error word: a bounded wait that gave up (tensor-core MLP of stage 0: bit 0; the trainer's tensor-core
