@@ -62,9 +62,10 @@ class HushPostInputs(C.Structure):
 
 
 # the training twin's passes (hush_twin_pass) and buffers (hush_trainer_buf)
-TWIN_PASSES = ["mlp", "mid1", "mid2", "mid3", "fine", "taa", "loss", "temporal"]
+TWIN_PASSES = ["mlp", "mid1", "mid2", "mid3", "fine", "taa", "loss", "temporal", "coarse1", "coarse2"]
 TWIN_BUF_NAMES = ["THETA", "GRAD", "LOSS", "PAR", "DPAR", "B1", "B2", "B3", "DB1", "DB2", "DB3", "A1", "X", "DX", "OUT",
-                  "OUT_PREV", "DOUT", "DA0", "DA1", "DMOM", "DHIST", "DMOM_PREV", "DAG"]
+                  "OUT_PREV", "DOUT", "DA0", "DA1", "DMOM", "DHIST", "DMOM_PREV", "DAG", "AH", "DAH", "C1", "DC1", "C0",
+                  "DC0"]
 
 POST_LEVELS = 6
 POST_RGBA8, POST_BGRA8, POST_RGBA32F = 0, 1, 2

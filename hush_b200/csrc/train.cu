@@ -3,7 +3,8 @@
 // The twin runs the frame after TEMPORAL in FP32 without the f16 storage rounding (so finite differences see a
 // smooth function): the MLP on FP32 master weights (hush.js:683-704 / 357-362), the mid levels mid1-mid3 (hush.js:366,
 // 753-754), the fine level + recombination (hush.js:578-620) and TAA (hush.js:649-676). TEMPORAL and the coarse levels
-// run as the reference passes (their outputs do not depend on the weights within a frame). The loss is the relative L1
+// run as the reference passes in the frame (their outputs do not depend on the weights within a frame); each also has
+// its own forward / adjoint pair for the per-pass API and the window sweep. The loss is the relative L1
 // of the TAA output against the noise-free image (clipped at 1 per value) plus a temporal-gradient term.
 //
 // Gradients are exact for one frame with the temporal history held fixed (the history buffers are inputs of the
@@ -293,6 +294,186 @@ __global__ void __launch_bounds__(TW *TH) k_mid_bwd(const TwinFrame T) {
   float *dp1 = &T.dpar[3 * o + 1].x, *dp2 = &T.dpar[3 * o + 2].x;
   atomicAdd(dp1 + K, ds);
   atomicAdd(dp2 + K, dc);
+}
+
+// ------------------------------------------------------------------------------------------------ coarse levels
+// COARSE1 (hush.js:372-421: down() of the half-res block means, then the 5x5 a-trous with step 1) and coarse2
+// (hush.js:752: the 5x5 a-trous with step 2), both with the variance prefilter, s = COARSE_S and c = 1, in FP32
+// without the f16 storage rounding. Their only differentiable input is the colour + variance level they filter (the
+// guide is geometry), so each adjoint takes dL/d(output level) to dL/d(input level): the direct taps, the luminance
+// edge-stopping terms of every tap and of the centre, and the prefiltered variance through s / sd.
+template <int STEP, int SW>
+struct Filt2 {
+  static constexpr int NT = 24;
+  float4 gp, center;
+  float gv, lc, den, sl, cw, W;
+  float wq[NT], lq[NT];
+  bool ok[NT];
+  float3 S;
+  float V;
+  HD_INL static float hw(int d) { return d == 0 ? 0.375f : (d == 1 || d == -1) ? 0.25f : 0.0625f; }
+  HD_INL static int dx_of(int t) { const int k = t < NT / 2 ? t : t + 1; return k % 5 - 2; }
+  HD_INL static int dy_of(int t) { const int k = t < NT / 2 ? t : t + 1; return k / 5 - 2; }
+  HD_INL void run(const float4 *sA, const float4 *sG, int ti, int qx, int qy, int w, int h, float s, float c) {
+    gp = sG[ti];
+    center = sA[ti];
+    gv = 0.0625f * (sA[ti - SW - 1].w + sA[ti - SW + 1].w + sA[ti + SW - 1].w + sA[ti + SW + 1].w) +
+         0.125f * (sA[ti - SW].w + sA[ti - 1].w + sA[ti + 1].w + sA[ti + SW].w) + 0.25f * center.w;
+    lc = lum(center);
+    den = sqrtf(fmaxf(gv, 1e-12f)) + 1e-6f;
+    sl = s / den;
+    const float zl = sG[ti - 1].w, zr = sG[ti + 1].w, zu = sG[ti - SW].w, zd = sG[ti + SW].w;
+    const float gx = fminf(zr > 0.0f ? fabsf(zr - gp.w) : 1e9f, zl > 0.0f ? fabsf(zl - gp.w) : 1e9f);
+    const float gy = fminf(zd > 0.0f ? fabsf(zd - gp.w) : 1e9f, zu > 0.0f ? fabsf(zu - gp.w) : 1e9f);
+    const float zg = fminf(fmaxf(gx, gy), gp.w);
+    cw = (0.375f * 0.375f) * c;
+    W = cw;
+    S = make_float3(center.x * cw, center.y * cw, center.z * cw);
+    V = center.w * cw * cw;
+#pragma unroll
+    for (int t = 0; t < NT; t++) {
+      const int dx = dx_of(t), dy = dy_of(t);
+      const int off = dy * STEP * SW + dx * STEP;
+      const float4 gq = sG[ti + off];
+      const int tx = qx + dx * STEP, ty = qy + dy * STEP;
+      ok[t] = tx >= 0 && ty >= 0 && tx < w && ty < h && gq.w >= 0.0f;
+      wq[t] = 0.0f;
+      lq[t] = 0.0f;
+      if (ok[t]) {
+        const float4 cq = sA[ti + off];
+        lq[t] = lum(cq);
+        const float iz = 1.0f / (zg * (sqrtf((float)(dx * dx + dy * dy)) * STEP) + 1e-3f);
+        wq[t] = hw(dx) * hw(dy) * pow128(fmaxf(dot3(gq, gp), 0.0f)) *
+                expf(-fabsf(gq.w - gp.w) * iz - sl * fabsf(lq[t] - lc));
+        W += wq[t];
+        S.x += wq[t] * cq.x; S.y += wq[t] * cq.y; S.z += wq[t] * cq.z;
+        V += wq[t] * wq[t] * cq.w;
+      }
+    }
+  }
+  HD_INL float4 out() const { return make_float4(S.x / W, S.y / W, S.z / W, V / (W * W)); }
+
+  // Adjoint for the output gradient (g_rgb, g_v), added into dIn (image of row pitch `pitch`, size w x h): every
+  // tap at its image position; the centre and its 3x3 prefilter neighbours at their clamp-to-edge positions (qx, qy)
+  // is the centre's image position.
+  HD_INL void adjoint(const float4 *sA, int ti, float3 g, float g_v, float s, float4 *dIn, int qx, int qy, int w,
+                      int h) const {
+    const float o_r = S.x / W, o_g = S.y / W, o_b = S.z / W, ov = V / (W * W);
+    const float3 gS = make_float3(g.x / W, g.y / W, g.z / W);
+    const float gV = g_v / (W * W);
+    const float gW = -(g.x * o_r + g.y * o_g + g.z * o_b) / W - 2.0f * g_v * ov / W;
+    float dsl = 0.0f, dlp = 0.0f;
+#pragma unroll
+    for (int t = 0; t < NT; t++) {
+      if (!ok[t]) continue;
+      const int dx = dx_of(t), dy = dy_of(t);
+      const float4 cq = sA[ti + dy * STEP * SW + dx * STEP];
+      const float dw = gS.x * cq.x + gS.y * cq.y + gS.z * cq.z + gV * 2.0f * wq[t] * cq.w + gW;
+      const float de = dw * wq[t];
+      const float sg = sgn(lq[t] - lc);
+      dsl += de * (-fabsf(lq[t] - lc));
+      dlp += de * sl * sg;
+      const float dlq = -de * sl * sg;
+      atomic_add4(dIn + (qy + dy * STEP) * w + qx + dx * STEP,
+                  make_float4(gS.x * wq[t] + dlq * 0.2126f, gS.y * wq[t] + dlq * 0.7152f, gS.z * wq[t] + dlq * 0.0722f,
+                              gV * wq[t] * wq[t]));
+    }
+    const float dgv = gv > 1e-12f ? dsl * (-s / (den * den)) * (0.5f / sqrtf(gv)) : 0.0f;
+#pragma unroll
+    for (int dy = -1; dy <= 1; dy++) {
+#pragma unroll
+      for (int dx = -1; dx <= 1; dx++) {
+        const float k = (dx == 0 && dy == 0) ? 0.25f : (dx == 0 || dy == 0) ? 0.125f : 0.0625f;
+        const int o = clampi(qy + dy, 0, h - 1) * w + clampi(qx + dx, 0, w - 1);
+        if (dx == 0 && dy == 0)
+          atomic_add4(dIn + o, make_float4(gS.x * cw + dlp * 0.2126f, gS.y * cw + dlp * 0.7152f,
+                                           gS.z * cw + dlp * 0.0722f, gV * cw * cw + k * dgv));
+        else
+          atomicAdd(&dIn[o].w, k * dgv);
+      }
+    }
+  }
+};
+
+// down() (hush.js:385-402) of the twin's FP32 block means ah at quarter-res texel Q, without the f16 rounding; the
+// weights are the blocks' pixel counts (F3), N their sum (0: the texel has no surface and holds zeros).
+HD_INL float4 down_tw(const HushFrame &f, const float4 *ah, int Qx, int Qy, float *Nout) {
+  float N = 0.f, vr = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const int hx = Qx * 2 + (j & 1), hy = Qy * 2 + (j >> 1);
+    if (hx >= f.W2 || hy >= f.H2) continue;
+    const float w = unpack2(__ldg(f.F3 + hy * f.W2 + hx).y).y;
+    if (w <= 0.0f) continue;
+    const float4 a = ah[hy * f.W2 + hx];
+    N += w;
+    cx += w * a.x; cy += w * a.y; cz += w * a.z;
+    vr += w * a.w;
+  }
+  if (Nout) *Nout = N;
+  if (N == 0.0f) return make_float4(0.f, 0.f, 0.f, 0.f);
+  return make_float4(cx / N, cy / N, cz / N, vr / N / N);
+}
+
+// ah = the block means F2.zw as FP32 (COARSE1's input level in the per-pass pair)
+__global__ void k_ah_fill(const TwinFrame T, float4 *ah) {
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o < T.f.W2 * T.f.H2) ah[o] = f2_ac_tw(T.f.F2, o);
+}
+
+// LEVEL 1: src = down(ah), output c1; LEVEL 2: src = c1, output c0. The guide is the stored coarse guide CG.
+template <int LEVEL>
+__global__ void __launch_bounds__(TW *TH) k_coarse_tw(const TwinFrame T, const float4 *src, float4 *dst,
+                                                        const float4 *gout, float4 *gin) {
+  constexpr int STEP = LEVEL, AP = 2 * STEP, SW = TW + 2 * AP, SH = TH + 2 * AP;
+  __shared__ float4 sA[SW * SH], sG[SW * SH];
+  const HushFrame &f = T.f;
+  const int li = threadIdx.y * TW + threadIdx.x;
+  const int bx = blockIdx.x * TW, by = blockIdx.y * TH;
+  for (int i = li; i < SW * SH; i += TW * TH) {
+    const int qx = clampi(bx - AP + i % SW, 0, f.W4 - 1), qy = clampi(by - AP + i / SW, 0, f.H4 - 1);
+    const int q = qy * f.W4 + qx;
+    sA[i] = LEVEL == 1 ? down_tw(f, src, qx, qy, nullptr) : src[q];
+    float4 g = ldh(f.CG, q);
+    float4 n = oct_dec(g.x, g.y);
+    n.w = g.z;
+    sG[i] = n;
+  }
+  __syncthreads();
+  const int X = bx + threadIdx.x, Y = by + threadIdx.y;
+  if (X >= f.W4 || Y >= f.H4) return;
+  const int o = Y * f.W4 + X, ti = (threadIdx.y + AP) * SW + threadIdx.x + AP;
+  if (sG[ti].w < 0.0f) {  // no surface: the level holds zeros (and passes no gradient)
+    if (!gout) dst[o] = make_float4(0.f, 0.f, 0.f, 0.f);
+    return;
+  }
+  Filt2<STEP, SW> F;
+  F.run(sA, sG, ti, X, Y, f.W4, f.H4, COARSE_S, 1.0f);
+  if (!gout) {
+    dst[o] = F.out();
+    return;
+  }
+  const float4 g = gout[o];
+  F.adjoint(sA, ti, make_float3(g.x, g.y, g.z), g.w, COARSE_S, gin, X, Y, f.W4, f.H4);
+}
+
+// down()'s adjoint: dah (half-res) += the gradient of its quarter-res texel spread over the blocks by their weights
+// (colour: w / N; variance: w / N^2). A gather: every half-res texel reads its one quarter-res texel.
+__global__ void k_down_bwd(const TwinFrame T, const float4 *ah, const float4 *ddown, float4 *dah) {
+  const HushFrame &f = T.f;
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= f.W2 * f.H2) return;
+  const int hx = o % f.W2, hy = o / f.W2;
+  const float w = unpack2(__ldg(f.F3 + o).y).y;
+  if (w <= 0.0f) return;
+  float N = 0.0f;
+  down_tw(f, ah, hx >> 1, hy >> 1, &N);
+  const float4 g = ddown[(hy >> 1) * f.W4 + (hx >> 1)];
+  const float k = w / N;
+  float4 d = dah[o];
+  d.x += g.x * k; d.y += g.y * k; d.z += g.z * k;
+  d.w += g.w * k / N;
+  dah[o] = d;
 }
 
 // ------------------------------------------------------------------------------------------------ fine + final
@@ -1359,6 +1540,11 @@ struct hush_trainer_s {
   // dhist / dmomp (the previous frame's colour history and moments) and dag (its alpha, gamma per half-res pixel)
   float4 *dA0 = nullptr, *dA1 = nullptr, *dmom = nullptr, *dhist = nullptr, *dmomp = nullptr;
   float2 *dag = nullptr;
+  // the coarse levels' per-pass pairs: COARSE1's input ah (half-res block means) and its gradient, the levels c1 / c0
+  // (quarter-res) and their gradients, and down()'s quarter-res gradient (scratch of COARSE1's adjoint)
+  int W4 = 0, H4 = 0;
+  float4 *ah = nullptr, *dah = nullptr, *c1 = nullptr, *dc1 = nullptr, *c0 = nullptr, *dc0 = nullptr, *ddown = nullptr;
+  char *coarse_pool = nullptr;
   // hush_trainer_window_bptt: the window's per-frame state records and the carried gradients (ping-pong)
   struct Rec {
     uint2 *A0, *key, *mom, *hist, *taa, *par0, *C0, *C1, *CG;
@@ -1440,6 +1626,28 @@ extern "C" int hush_trainer_create(hush_t *h, const float *theta, hush_trainer_t
   return HUSH_OK;
 }
 
+// The coarse levels' buffers, made on first use (the per-pass API only; the frame and window paths never touch them).
+static cudaError_t ensure_coarse(hush_trainer_t *t) {
+  if (t->coarse_pool) return cudaSuccess;
+  t->W4 = t->h->W4;
+  t->H4 = t->h->H4;
+  const size_t half = (size_t)t->W2 * t->H2, quarter = (size_t)t->W4 * t->H4;
+  auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t bytes = al(half * 16) * 2 + al(quarter * 16) * 5;
+  cudaError_t e = cudaMalloc(&t->coarse_pool, bytes);
+  if (e != cudaSuccess) {
+    t->coarse_pool = nullptr;
+    return e;
+  }
+  e = cudaMemset(t->coarse_pool, 0, bytes);
+  size_t off = 0;
+  auto take = [&](size_t b) { char *p = t->coarse_pool + off; off += al(b); return (float4 *)p; };
+  t->ah = take(half * 16); t->dah = take(half * 16);
+  t->c1 = take(quarter * 16); t->dc1 = take(quarter * 16); t->c0 = take(quarter * 16); t->dc0 = take(quarter * 16);
+  t->ddown = take(quarter * 16);
+  return e;
+}
+
 extern "C" void hush_trainer_destroy(hush_trainer_t *t) {
   if (!t) return;
   cudaSetDevice(t->h->dev);
@@ -1456,6 +1664,7 @@ extern "C" void hush_trainer_destroy(hush_trainer_t *t) {
     if (g) cudaGraphExecDestroy(g);
   if (t->cap) cudaStreamDestroy(t->cap);
   cudaFree(t->pool);
+  cudaFree(t->coarse_pool);
   cudaFree(t->win_pool);
   cudaFree(t->rec_pool);
   cudaFree(t->carry_pool);
@@ -1878,6 +2087,12 @@ extern "C" int hush_trainer_begin(hush_trainer_t *t, const hush_inputs *in, cons
   cudaError_t e = launch_pass(PASS_TEMPORAL, t->T.f, t->h->w16, st);
   if (e == cudaSuccess) e = launch_pass(PASS_COARSE1, t->T.f, t->h->w16, st);
   if (e == cudaSuccess) e = launch_pass(PASS_COARSE2, t->T.f, t->h->w16, st);
+  if (e == cudaSuccess) e = ensure_coarse(t);
+  if (e == cudaSuccess) {
+    const int half = t->W2 * t->H2;
+    k_ah_fill<<<(half + 255) / 256, 256, 0, st>>>(t->T, t->ah);
+    e = cudaGetLastError();
+  }
   if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "trainer pass launch");
   t->begun = 1;
   return HUSH_OK;
@@ -1895,6 +2110,12 @@ extern "C" int hush_trainer_zero_adjoints(hush_trainer_t *t, void *stream) {
   float4 *tb[5] = {t->dA0, t->dA1, t->dmom, t->dhist, t->dmomp};
   for (int i = 0; i < 5 && e == cudaSuccess; i++) e = cudaMemsetAsync(tb[i], 0, full * 16, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(t->dag, 0, half * 8, st);
+  if (t->coarse_pool) {
+    const size_t quarter = (size_t)t->W4 * t->H4;
+    if (e == cudaSuccess) e = cudaMemsetAsync(t->dah, 0, half * 16, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(t->dc1, 0, quarter * 16, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(t->dc0, 0, quarter * 16, st);
+  }
   return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, "cudaMemsetAsync");
 }
 
@@ -1946,6 +2167,22 @@ static int run_twin_pass(hush_trainer_t *t, int pass, int backward, void *stream
         k_tm_bwd<<<(full + 255) / 256, 256, 0, st>>>(T, t->gT2, t->dX);
       }
       break;
+    case HUSH_TWIN_COARSE1:
+    case HUSH_TWIN_COARSE2: {
+      const dim3 gq((t->W4 + TW - 1) / TW, (t->H4 + TH - 1) / TH);
+      if (pass == HUSH_TWIN_COARSE2) {
+        if (backward) k_coarse_tw<2><<<gq, blk, 0, st>>>(T, t->c1, nullptr, t->dc0, t->dc1);
+        else k_coarse_tw<2><<<gq, blk, 0, st>>>(T, t->c1, t->c0, nullptr, nullptr);
+      } else if (!backward) {
+        k_coarse_tw<1><<<gq, blk, 0, st>>>(T, t->ah, t->c1, nullptr, nullptr);
+      } else {  // dc1 -> down()'s quarter-res gradient -> the block means
+        e = cudaMemsetAsync(t->ddown, 0, (size_t)t->W4 * t->H4 * 16, st);
+        if (e == cudaSuccess) k_coarse_tw<1><<<gq, blk, 0, st>>>(T, t->ah, nullptr, t->dc1, t->ddown);
+        const int half = t->W2 * t->H2;
+        if (e == cudaSuccess) k_down_bwd<<<(half + 255) / 256, 256, 0, st>>>(T, t->ah, t->ddown, t->dah);
+      }
+      break;
+    }
     default:  // HUSH_TWIN_LOSS
       k_loss<<<t->n_loss_ctas, 256, 0, st>>>(T, backward);
       k_reduce_f64<<<1, 256, 0, st>>>(t->loss_partials, t->n_loss_ctas, t->loss, nullptr);
@@ -1977,6 +2214,18 @@ extern "C" int hush_temporal_fwd(hush_trainer_t *t, void *stream) {
 }
 extern "C" int hush_temporal_bwd(hush_trainer_t *t, void *stream) {
   return run_twin_pass(t, HUSH_TWIN_TEMPORAL, 1, stream, "hush_temporal_bwd");
+}
+extern "C" int hush_coarse1_fwd(hush_trainer_t *t, void *stream) {
+  return run_twin_pass(t, HUSH_TWIN_COARSE1, 0, stream, "hush_coarse1_fwd");
+}
+extern "C" int hush_coarse1_bwd(hush_trainer_t *t, void *stream) {
+  return run_twin_pass(t, HUSH_TWIN_COARSE1, 1, stream, "hush_coarse1_bwd");
+}
+extern "C" int hush_coarse2_fwd(hush_trainer_t *t, void *stream) {
+  return run_twin_pass(t, HUSH_TWIN_COARSE2, 0, stream, "hush_coarse2_fwd");
+}
+extern "C" int hush_coarse2_bwd(hush_trainer_t *t, void *stream) {
+  return run_twin_pass(t, HUSH_TWIN_COARSE2, 1, stream, "hush_coarse2_bwd");
 }
 
 // ------------------------------------------------------------------------------------------------ window BPTT
@@ -2153,6 +2402,15 @@ extern "C" int hush_trainer_buffer(hush_trainer_t *t, int which, void **ptr, int
     case HUSH_TB_DHIST: p = t->dhist; break;
     case HUSH_TB_DMOM_PREV: p = t->dmomp; break;
     case HUSH_TB_DAG: p = t->dag; w = t->W2; h = t->H2; c = 2; break;
+    case HUSH_TB_AH: case HUSH_TB_DAH: case HUSH_TB_C1: case HUSH_TB_DC1: case HUSH_TB_C0: case HUSH_TB_DC0: {
+      const cudaError_t e = ensure_coarse(t);
+      if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "hush_trainer_buffer: coarse buffers");
+      float4 *q[6] = {t->ah, t->dah, t->c1, t->dc1, t->c0, t->dc0};
+      p = q[which - HUSH_TB_AH];
+      w = which <= HUSH_TB_DAH ? t->W2 : t->W4;
+      h = which <= HUSH_TB_DAH ? t->H2 : t->H4;
+      break;
+    }
     default: return tr_fail(t, "hush_trainer_buffer: unknown buffer");
   }
   *ptr = p;

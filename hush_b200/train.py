@@ -155,7 +155,8 @@ class Trainer:
                                                float(lambda_t), C.c_void_p(_stream_handle(stream))))
 
     def fwd(self, name: str, stream=None):
-        """Forward of one pass ("mlp", "mid1", "mid2", "mid3", "fine", "taa", "loss", "temporal")."""
+        """Forward of one pass ("mlp", "mid1", "mid2", "mid3", "fine", "taa", "loss", "temporal", "coarse1",
+        "coarse2")."""
         self._check(getattr(L.lib(), f"hush_{name}_fwd")(self._t, C.c_void_p(_stream_handle(stream))))
 
     def bwd(self, name: str, stream=None):
@@ -167,7 +168,8 @@ class Trainer:
 
     def buffer(self, name: str):
         """Torch view of a trainer buffer (hush_trainer_buf): THETA / GRAD (812,), LOSS (1,), PAR / DPAR (h, w, 12),
-        B1..B3 / DB1..DB3 (h, w, 4), A1 / X / DX / OUT / OUT_PREV / DOUT (H, W, 4)."""
+        B1..B3 / DB1..DB3 (h, w, 4), A1 / X / DX / OUT / OUT_PREV / DOUT (H, W, 4), AH / DAH (h, w, 4), C1 / DC1 /
+        C0 / DC0 (quarter resolution, 4 channels)."""
         import torch
 
         ptr, w, h, c = C.c_void_p(), C.c_int(), C.c_int(), C.c_int()

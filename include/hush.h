@@ -241,7 +241,9 @@ typedef enum {
   HUSH_TWIN_LOSS = 6, /* OUT, clean, clean_prev, OUT_PREV        -> LOSS     | 1    -> dOUT                     */
   HUSH_TWIN_TEMPORAL = 7, /* G-buffer, previous history (colour, moments, key, par0) -> A0, moments, key, features |
                            * dA0, dMOM -> dHIST, dMOM_PREV, dAG (the previous frame's colour, moments, alpha / gamma) */
-  HUSH_TWIN_PASSES = 8
+  HUSH_TWIN_COARSE1 = 8, /* AH (block means), counts (F3), coarse guide CG -> C1 | dC1 -> dAH                   */
+  HUSH_TWIN_COARSE2 = 9, /* C1, coarse guide CG                            -> C0 | dC0 -> dC1                   */
+  HUSH_TWIN_PASSES = 10
 } hush_twin_pass;
 
 /* The trainer's buffers (device memory owned by the trainer, valid until hush_trainer_destroy; OUT / OUT_PREV swap at
@@ -266,7 +268,13 @@ typedef enum {
   HUSH_TB_DHIST = 20,   /* W x H x 4: dL/d the previous frame's colour history (TEMPORAL adds into it) */
   HUSH_TB_DMOM_PREV = 21, /* W x H x 4: dL/d the previous frame's moments                             */
   HUSH_TB_DAG = 22,     /* W2 x H2 x 2: dL/d the previous frame's alpha, gamma per half-res pixel     */
-  HUSH_TB_COUNT = 23
+  HUSH_TB_AH = 23,      /* W2 x H2 x 4: COARSE1's input, the block means (F2.zw) as FP32              */
+  HUSH_TB_DAH = 24,     /* W2 x H2 x 4                                                               */
+  HUSH_TB_C1 = 25,      /* W4 x H4 x 4: coarse level 1 (COARSE1's output, coarse2's input), FP32      */
+  HUSH_TB_DC1 = 26,     /* W4 x H4 x 4                                                               */
+  HUSH_TB_C0 = 27,      /* W4 x H4 x 4: coarse level 2 (coarse2's output), FP32                       */
+  HUSH_TB_DC0 = 28,     /* W4 x H4 x 4                                                               */
+  HUSH_TB_COUNT = 29
 } hush_trainer_buf;
 
 /* TEMPORAL and the coarse levels for the frame's inputs, and the frame context for the pass calls (clean: dense f32
@@ -298,6 +306,16 @@ int hush_loss_bwd(hush_trainer_t *t, void *stream);
  * block features are not differentiated (the MLP's inputs are held fixed). */
 int hush_temporal_fwd(hush_trainer_t *t, void *stream);
 int hush_temporal_bwd(hush_trainer_t *t, void *stream);
+/* COARSE1 (hush.js:372-421: down() of the block means weighted by their pixel counts, then the 5x5 a-trous with
+ * step 1) and coarse2 (hush.js:752: the 5x5 a-trous with step 2), both with the variance prefilter, s = COARSE_S and
+ * c = 1, in FP32 over the trainer's AH / C1 / C0 (hush_trainer_begin fills AH from the frame's F2.zw). The levels have
+ * no learnable input; each adjoint ADDS dL/d(its input level) (dAH, dC1) from dL/d(its output level) (dC1, dC0):
+ * the direct taps, every tap's and the centre's luminance edge-stopping term, and the prefiltered variance through
+ * s / sd. The guide (the coarse guide CG, normals and depths) is geometry and carries no gradient. */
+int hush_coarse1_fwd(hush_trainer_t *t, void *stream);
+int hush_coarse1_bwd(hush_trainer_t *t, void *stream);
+int hush_coarse2_fwd(hush_trainer_t *t, void *stream);
+int hush_coarse2_bwd(hush_trainer_t *t, void *stream);
 
 /* Backpropagation through time over one window of n_frames frames (frames[] / cleans[] as in hush_train_step): the
  * window starts without history, every frame runs forward with its state kept, then the frames run backward from the

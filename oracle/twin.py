@@ -46,9 +46,13 @@ def gather(img, yy, xx):
     return img[yy.clamp(0, img.shape[0] - 1), xx.clamp(0, img.shape[1] - 1)]
 
 
-def filt(A, G, s, c, step, pref):
-    """atrousFn with R = 1 at every pixel of a (H, W) level; A (H, W, 4) colour + variance, G (H, W, 4) normal +
-    depth, s / c (H, W). Clamp-to-edge tiles, taps outside the image or on sky skipped."""
+H3, H5 = (0.25, 0.5, 0.25), (1 / 16, 1 / 4, 3 / 8, 1 / 4, 1 / 16)  # the B-spline tap weights of atrousFn (R = 1, 2)
+
+
+def filt(A, G, s, c, step, pref, R=1):
+    """atrousFn (hush.js:431-476) with radius R at every pixel of a (H, W) level; A (H, W, 4) colour + variance, G
+    (H, W, 4) normal + depth, s / c (H, W) or scalars. Clamp-to-edge tiles, taps outside the image or on sky
+    skipped."""
     H, W = A.shape[:2]
     ys, xs = torch.meshgrid(torch.arange(H), torch.arange(W), indexing="ij")
     gp, cen = G, A
@@ -70,15 +74,16 @@ def filt(A, G, s, c, step, pref):
     # sky centres are discarded by the caller; a positive depth keeps their weights finite (an infinite weight in a
     # discarded torch.where branch still turns the zero gradient into NaN)
     zg = torch.where(gp[..., 3] >= 0, zg, torch.ones_like(zg))
-    cw = 0.25 * c
+    hw = H3 if R == 1 else H5
+    cw = (hw[R] * hw[R]) * torch.as_tensor(c, dtype=torch.float64) * torch.ones_like(lc)
     Wt = cw
     S = cen[..., :3] * cw[..., None]
     V = cen[..., 3] * cw * cw
-    for dy in (-1, 0, 1):
-        for dx in (-1, 0, 1):
+    for dy in range(-R, R + 1):
+        for dx in range(-R, R + 1):
             if dx == 0 and dy == 0:
                 continue
-            hh = (0.5 if dx == 0 else 0.25) * (0.5 if dy == 0 else 0.25)
+            hh = hw[dx + R] * hw[dy + R]
             tx, ty = xs + dx * step, ys + dy * step
             gq, cq = gather(G, ty, tx), gather(A, ty, tx)
             ok = (tx >= 0) & (ty >= 0) & (tx < W) & (ty < H) & (gq[..., 3] >= 0)
@@ -90,6 +95,50 @@ def filt(A, G, s, c, step, pref):
             S = S + wq[..., None] * cq[..., :3]
             V = V + wq * wq * cq[..., 3]
     return torch.cat([S / Wt[..., None], (V / (Wt * Wt))[..., None]], -1)
+
+
+COARSE_S = 0.25  # hush.js:26
+
+
+def coarse_guide(CG):
+    """The coarse guide as the coarse passes read it: (qh, qw, 4) rgba16float (oct normal, depth) -> decoded normal +
+    depth."""
+    g = _t(np.asarray(CG, np.float16).astype(np.float64))
+    return torch.cat([oct_dec(g[..., 0], g[..., 1]), g[..., 2:3]], -1)
+
+
+def down(Ah, cnt):
+    """down() of hush.js:385-402 over the whole quarter-res grid without the f16 rounding: the block means Ah
+    (h, w, 4) weighted by the blocks' pixel counts cnt (h, w) over each 2x2 group -> (col / N, var / N / N), zeros
+    where no block has a surface."""
+    h, w = Ah.shape[:2]
+    qh, qw = (h + 1) // 2, (w + 1) // 2
+    pad_h, pad_w = 2 * qh - h, 2 * qw - w
+    A = torch.nn.functional.pad(Ah.permute(2, 0, 1), (0, pad_w, 0, pad_h)).permute(1, 2, 0)
+    n = torch.nn.functional.pad(torch.clamp(cnt, min=0.0), (0, pad_w, 0, pad_h))
+    A = A.reshape(qh, 2, qw, 2, 4)
+    n = n.reshape(qh, 2, qw, 2)
+    N = n.sum((1, 3))
+    col = (n[..., None] * A[..., :3]).sum((1, 3))
+    vr = (n * A[..., 3]).sum((1, 3))
+    Ns = torch.where(N > 0, N, torch.ones_like(N))
+    out = torch.cat([col / Ns[..., None], (vr / Ns / Ns)[..., None]], -1)
+    return torch.where((N > 0)[..., None], out, torch.zeros_like(out))
+
+
+def coarse1(Ah, cnt, Gq):
+    """COARSE1 (hush.js:372-421): the 5x5 a-trous (step 1, variance prefilter, s = COARSE_S, c = 1) of down(Ah);
+    zeros where the coarse guide has no surface."""
+    sky = Gq[..., 3] < 0
+    y = filt(down(Ah, cnt), Gq, COARSE_S, 1.0, 1, True, R=2)
+    return torch.where(sky[..., None], torch.zeros_like(y), y)
+
+
+def coarse2(C1, Gq):
+    """coarse2 (hush.js:752): the 5x5 a-trous (step 2, variance prefilter, s = COARSE_S, c = 1) of C1."""
+    sky = Gq[..., 3] < 0
+    y = filt(C1, Gq, COARSE_S, 1.0, 2, True, R=2)
+    return torch.where(sky[..., None], torch.zeros_like(y), y)
 
 
 def jbw(frx, fry, j, nq, zq, n, z):

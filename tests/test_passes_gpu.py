@@ -1,7 +1,8 @@
-"""Each pass of the training twin as a forward / adjoint pair through the C ABI (hush_<pass>_fwd / hush_<pass>_bwd) on
-a B200: the forward against the FP64 restatement of the same pass (oracle/twin.py) at the pass's own inputs, the
-adjoint against that restatement's FP64 autograd vector-Jacobian product and against central finite differences
-(h = 1e-3) of the CUDA forward, and the chain of adjoints against the fused frame's gradient."""
+"""Each pass of the training twin, the coarse levels included, as a forward / adjoint pair through the C ABI
+(hush_<pass>_fwd / hush_<pass>_bwd) on a B200: the forward against the FP64 restatement of the same pass
+(oracle/twin.py) at the pass's own inputs, the adjoint against that restatement's FP64 autograd vector-Jacobian
+product and against central finite differences (h = 1e-3) of the CUDA forward, and the chain of adjoints against the
+fused frame's gradient."""
 import ctypes as C
 
 import numpy as np
@@ -17,7 +18,12 @@ torch = pytest.importorskip("torch")
 from oracle import twin  # noqa: E402
 
 ORDER = ["mlp", "mid1", "mid2", "mid3", "fine", "taa", "loss"]
+COARSE = ["coarse1", "coarse2"]  # the coarse levels: no learnable input; their adjoints carry the input-level gradient
 H_FD = 1e-3
+# COARSE1's input (the block means) enters through down()'s 2x2 weighted means, so its gradients are a fraction of
+# the level's and the FP32 rounding of the forward over +-1e-3 dominates its differences: the coarse passes take a
+# step of 1e-2 for the differences of the CUDA forward (the FP64 differences keep 1e-3)
+H_FD_CUDA = {"coarse1": 1e-2, "coarse2": 1e-2}
 
 
 def _dev(f):
@@ -39,7 +45,7 @@ class Frame:
             self.tr.end_frame()
         self.inputs = _dev(self.host[2])
         self.tr.begin(self.inputs, self.cleans[2], self.cleans[1], lam)
-        for p in ORDER:
+        for p in ORDER + COARSE:
             self.tr.fwd(p)
         torch.cuda.synchronize()
         c = self.g.frame & 1
@@ -54,6 +60,8 @@ class Frame:
         st["reset"] = False
         self.st = st
         self.feats, self.Gh, self.sky_h, self.Ah = twin.half_inputs(st)
+        self.cnt_h = twin.unpack_half(st["F3"])[..., 3]  # the blocks' pixel counts (down()'s weights)
+        self.Gq = twin.coarse_guide(st["CG"])
 
     def b(self, name):
         return self.tr.buffer(name)
@@ -72,6 +80,8 @@ SPEC = {
     "fine": ("X", "DX", 3, {"B3": "DB3", "PAR": "DPAR"}),
     "taa": ("OUT", "DOUT", 3, {"X": "DX"}),
     "loss": ("LOSS", None, 1, {"OUT": "DOUT"}),
+    "coarse1": ("C1", "DC1", 4, {"AH": "DAH"}),
+    "coarse2": ("C0", "DC0", 4, {"C1": "DC1"}),
 }
 # PAR components each pass reads (alpha gamma beta kappa | s0..s3 | c0..c3)
 PAR_USED = {"mid1": (5, 9), "mid2": (6, 10), "mid3": (7, 11), "fine": (2, 3, 4, 8)}
@@ -121,6 +131,14 @@ def _reference(fr, name, seed):
         par, b3 = fr.f64("PAR"), fr.f64("B3")
         _, y = twin.fine(fr.st, par, b3, fr.Gh, fr.sky_h, fr.Ah)
         ins = {"B3": b3, "PAR": par}
+    elif name == "coarse1":
+        ah = fr.f64("AH")
+        y = twin.coarse1(ah, fr.cnt_h, fr.Gq)
+        ins = {"AH": ah}
+    elif name == "coarse2":
+        c1 = fr.f64("C1")
+        y = twin.coarse2(c1, fr.Gq)
+        ins = {"C1": c1}
     elif name == "taa":
         x = fr.f64("X", rgb=True)
         y = twin.taa(fr.st, x)
@@ -148,7 +166,7 @@ def frame():
     return Frame()
 
 
-@pytest.mark.parametrize("name", ORDER)
+@pytest.mark.parametrize("name", ORDER + COARSE)
 def test_pass_forward_matches_fp64(frame, name):
     seed = _seed(frame, name, torch.Generator().manual_seed(1))
     frame.tr.fwd(name)
@@ -162,7 +180,7 @@ def test_pass_forward_matches_fp64(frame, name):
     assert err.max().item() <= 1e-4 * max(scale, 1e-6), (name, err.max().item(), scale)
 
 
-@pytest.mark.parametrize("name", ORDER)
+@pytest.mark.parametrize("name", ORDER + COARSE)
 def test_pass_adjoint_matches_fp64_vjp(frame, name):
     seed = _seed(frame, name, torch.Generator().manual_seed(2))
     got = _run_bwd(frame, name, seed)
@@ -183,7 +201,7 @@ def test_pass_adjoint_matches_fp64_vjp(frame, name):
         assert err.max().item() <= 1e-3 * scale, (name, inp, err.max().item() / scale)
 
 
-@pytest.mark.parametrize("name", ORDER)
+@pytest.mark.parametrize("name", ORDER + COARSE)
 def test_pass_adjoint_matches_central_differences(frame, name):
     seed = _seed(frame, name, torch.Generator().manual_seed(3))
     got = _run_bwd(frame, name, seed)
@@ -205,13 +223,14 @@ def test_pass_adjoint_matches_central_differences(frame, name):
         nz = torch.nonzero(g.abs() > 1e-3 * g.abs().max()).view(-1).numpy()
         pick = np.unique(np.concatenate([top, rng.choice(nz, size=min(16, nz.size), replace=False)]))
         buf = frame.b(inp).view(-1)
+        h_fd = H_FD_CUDA.get(name, H_FD)
         for i in pick:
             v0 = buf[i].item()
-            buf[i] = v0 + H_FD
+            buf[i] = v0 + h_fd
             vp = buf[i].item()  # the FP32 value actually stored
             frame.tr.fwd(name)
             sp = _objective(frame, name, seed)
-            buf[i] = v0 - H_FD
+            buf[i] = v0 - h_fd
             vm = buf[i].item()
             frame.tr.fwd(name)
             sm = _objective(frame, name, seed)
@@ -307,7 +326,7 @@ def test_train_step_is_the_training_loop():
     assert not np.array_equal(a.theta, theta)
 
 
-@pytest.mark.parametrize("name", ORDER)
+@pytest.mark.parametrize("name", ORDER + COARSE)
 def test_pass_adjoint_matches_fp64_central_differences(frame, name):
     """The CUDA adjoint of each pass against central differences (h = 1e-3) of the same pass evaluated in FP64 at the
     CUDA pass's inputs: free of the FP32 rounding of the forward. Every entry whose +-h interval is smooth agrees to
@@ -329,6 +348,10 @@ def test_pass_adjoint_matches_fp64_central_differences(frame, name):
                 _, y = twin.fine(frame.st, inputs["PAR"], inputs["B3"], frame.Gh, frame.sky_h, frame.Ah)
             elif name == "taa":
                 y = twin.taa(frame.st, inputs["X"][..., :3])
+            elif name == "coarse1":
+                y = twin.coarse1(inputs["AH"], frame.cnt_h, frame.Gq)
+            elif name == "coarse2":
+                y = twin.coarse2(inputs["C1"], frame.Gq)
             else:
                 y = twin.loss_of(frame.st, inputs["OUT"][..., :3], frame.lam)
             return y.sum().item() if sd is None else (sd[..., :y.shape[-1]] * y).sum().item()

@@ -107,3 +107,25 @@ def test_temporal_restatement_gradient_matches_central_differences():
             assert abs(fd - ga) <= 1e-5 * max(abs(fd), flat.max().item()), (k, i, fd, ga)
             checked += 1
     assert checked >= 20
+
+
+def test_coarse_restatement_tracks_the_oracle_passes():
+    """oracle/twin.coarse1 / coarse2 (float64, the references of the coarse adjoints: down() without the f16 rounding,
+    then the 5x5 a-trous of steps 1 and 2) against the oracle's f32 COARSE1 and coarse2 passes on the same frame: equal
+    to the f16 rounding of down() and of the stored levels."""
+    cfg = scene.SceneConfig(64, 48, 3, n_moving=2, seed=8)
+    frames = [scene.frame_host(cfg, i, clean=True) for i in range(3)]
+    o = oracle.OracleHush(cfg.width, cfg.height, builtin_weights())
+    for f in frames[:2]:
+        o.denoise(f)
+    f = frames[2]
+    for p in ("temporal", "infer", "coarse1", "coarse2"):
+        o.run_pass(p, f)
+    F2, F3 = twin.unpack_half(o.buffer("F2")), twin.unpack_half(o.buffer("F3"))
+    Gq = twin.coarse_guide(o.buffer("CG"))
+    c1 = twin.coarse1(F2[..., 4:8], F3[..., 3], Gq)
+    c0 = twin.coarse2(c1, Gq)
+    for got, name in ((c1, "C1"), (c0, "C0")):
+        ref = o.buffer(name).astype(np.float64)
+        rel = np.abs(got.numpy() - ref) / np.maximum(np.abs(ref), 1e-2 * np.abs(ref).mean())
+        assert np.mean(rel <= 2e-3) > 0.995, (name, np.mean(rel <= 2e-3))
