@@ -4,8 +4,9 @@
 // smooth function): the MLP on FP32 master weights (hush.js:683-704 / 357-362), the mid levels mid1-mid3 (hush.js:366,
 // 753-754), the fine level + recombination (hush.js:578-620) and TAA (hush.js:649-676). TEMPORAL and the coarse levels
 // run as the reference passes in the frame (their outputs do not depend on the weights within a frame); each also has
-// its own forward / adjoint pair for the per-pass API and the window sweep. The loss is the relative L1
-// of the TAA output against the noise-free image (clipped at 1 per value) plus a temporal-gradient term.
+// its own forward / adjoint pair in the per-pass API, and TEMPORAL's adjoint drives the window sweep through time. The
+// loss is the relative L1 of the TAA output against the noise-free image (clipped at 1 per value) plus a
+// temporal-gradient term.
 //
 // Gradients are exact for one frame with the temporal history held fixed (the history buffers are inputs of the
 // frame); over a window the per-frame gradients are summed (truncated backpropagation through time: the alpha / gamma
