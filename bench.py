@@ -521,13 +521,13 @@ def _extras_ms(frames, stream, n=32, warmup=4):
 
 def _train_step_ms(local, stream, barrier, max_over_ranks, warmup=2, steps=5, mlp="bf16", bptt=False):
     """Device time of one training step: 16 windows x 8 frames of 384x384 generated on the device, the twin's
-    forward + adjoint per frame (MLP as bf16 tensor-core GEMM tiles, or FP32), the gradient / loss all-reduce across
-    ranks (N > 1) and the Adam step."""
+    forward + adjoint per frame (MLP as bf16 tensor-core GEMM tiles, or FP32) or, with bptt, each window forward and
+    backward through time, the gradient / loss all-reduce across ranks (N > 1) and the Adam step."""
     import torch
 
     from hush_b200 import Hush
     from hush_b200.dp import DataParallel, finish_step
-    from hush_b200.train import TrainConfig, Trainer, window, window_scene, xavier_init
+    from hush_b200.train import TrainConfig, Trainer, window_scene, xavier_init
 
     cfg = TrainConfig(mlp=mlp, bptt=bptt)
     dp = DataParallel()
@@ -537,13 +537,10 @@ def _train_step_ms(local, stream, barrier, max_over_ranks, warmup=2, steps=5, ml
     rng = dp.seed_rng(cfg.init_seed + 1)
     sc = window_scene(cfg)
 
-    buf = window(cfg, 0) if bptt else None
-
     def one():
         seeds = [dp.window_seed(rng, cfg.seeds) for _ in range(cfg.batch)]
         if bptt:
-            for s in seeds:
-                tr.window_bptt(window(cfg, s, buf), cfg.lambda_t, stream=stream)
+            tr.windows_bptt(sc, seeds, cfg.frames, cfg.lambda_t, stream=stream)
         else:
             tr.windows(sc, seeds, cfg.frames, cfg.lambda_t, stream=stream)
         return finish_step(tr, dp, cfg.batch * cfg.frames, cfg.lr, cfg.clip)

@@ -126,6 +126,8 @@ _SIGS = {
                                        C.c_float, _P]),
     "hush_trainer_window_bptt": (C.c_int, [_P, C.POINTER(HushInputs), C.POINTER(C.c_void_p), C.c_int, C.c_float,
                                            _P]),
+    "hush_trainer_windows_bptt": (C.c_int, [_P, C.POINTER(HushScene), C.POINTER(C.c_uint32), C.c_int, C.c_int,
+                                            C.c_float, _P]),
     "hush_trainer_begin": (C.c_int, [_P, C.POINTER(HushInputs), C.c_void_p, C.c_void_p, C.c_float, _P]),
     "hush_trainer_zero_adjoints": (C.c_int, [_P, _P]),
     "hush_trainer_buffer": (C.c_int, [_P, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int), C.POINTER(C.c_int),

@@ -1571,6 +1571,11 @@ struct hush_trainer_s {
   cudaGraphExec_t win_graph[4] = {};
   int wg_frames = 0, wg_mode = -1;
   float wg_lambda = 0.f, wg_exposure = 0.f;
+  // hush_trainer_windows_bptt replays a window's forward + reverse sweep as one CUDA graph: its kernel arguments are
+  // fixed by the trainer's buffers, records and win_pool, the frame count, lambda, the exposure and the MLP form
+  cudaGraphExec_t bptt_graph = nullptr;
+  int bg_frames = 0, bg_mode = -1;
+  float bg_lambda = 0.f, bg_exposure = 0.f;
   cudaStream_t cap = nullptr;
   // hush_trainer_windows runs windows concurrently on lanes: lane 0 is this trainer, lanes 1.. are helper trainers on
   // private Hush instances of the same size (their own history), reading this trainer's weights and accumulating
@@ -1663,6 +1668,7 @@ extern "C" void hush_trainer_destroy(hush_trainer_t *t) {
   if (t->fork_ev) cudaEventDestroy(t->fork_ev);
   for (cudaGraphExec_t &g : t->win_graph)
     if (g) cudaGraphExecDestroy(g);
+  if (t->bptt_graph) cudaGraphExecDestroy(t->bptt_graph);
   if (t->cap) cudaStreamDestroy(t->cap);
   cudaFree(t->pool);
   cudaFree(t->coarse_pool);
@@ -1900,12 +1906,19 @@ static void drop_window_graphs(hush_trainer_t *t) {
 // state (frame counter, history flags) advances exactly as the direct calls advance it. The generation runs outside
 // the graph because its scene parameters change with the seed.
 // The windows seeds[0], seeds[stride], ... in order on one trainer and stream.
-static int windows_serial(hush_trainer_t *t, const hush_scene *sc, const uint32_t *seeds, int n_windows, int stride,
-                          int n_frames, float lambda_t, cudaStream_t st) {
-  const size_t full = (size_t)t->W * t->H, img = (full * 8 + 255) & ~(size_t)255,
-               cl = (full * 12 + 255) & ~(size_t)255, per = 5 * img + cl;
+static void drop_bptt_graph(hush_trainer_t *t) {
+  if (t->bptt_graph) { cudaGraphExecDestroy(t->bptt_graph); t->bptt_graph = nullptr; }
+}
+
+// win_pool for n_frames generated frames (each: the five G-buffer images, img bytes apart, then the noise-free image;
+// per bytes a frame). Reallocating it drops the graphs that captured its addresses.
+static int ensure_win_pool(hush_trainer_t *t, int n_frames, size_t &img, size_t &per) {
+  const size_t full = (size_t)t->W * t->H, cl = (full * 12 + 255) & ~(size_t)255;
+  img = (full * 8 + 255) & ~(size_t)255;
+  per = 5 * img + cl;
   if (t->win_frames < n_frames) {
     drop_window_graphs(t);
+    drop_bptt_graph(t);
     cudaFree(t->win_pool);
     t->win_pool = nullptr;
     t->win_frames = 0;
@@ -1913,6 +1926,27 @@ static int windows_serial(hush_trainer_t *t, const hush_scene *sc, const uint32_
     if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "cudaMalloc of the window buffers");
     t->win_frames = n_frames;
   }
+  return HUSH_OK;
+}
+
+// The frames of window seed `seed` generated into win_pool on `st`.
+static int generate_window(hush_trainer_t *t, const hush_scene *sc, uint32_t seed, int n_frames, size_t img,
+                           size_t per, cudaStream_t st) {
+  hush_scene w = *sc;
+  w.seed = seed;
+  for (int i = 0; i < n_frames; i++) {
+    char *b = t->win_pool + per * i;
+    const int rc = hush_scene_frame_device(&w, i, b, b + img, b + 2 * img, b + 3 * img, b + 4 * img, b + 5 * img, st);
+    if (rc != HUSH_OK) return hush_fail(t->h, rc, "training windows: scene generation failed");
+  }
+  return HUSH_OK;
+}
+
+static int windows_serial(hush_trainer_t *t, const hush_scene *sc, const uint32_t *seeds, int n_windows, int stride,
+                          int n_frames, float lambda_t, cudaStream_t st) {
+  size_t img = 0, per = 0;
+  const int prc = ensure_win_pool(t, n_frames, img, per);
+  if (prc != HUSH_OK) return prc;
   if (t->wg_frames != n_frames || t->wg_lambda != lambda_t || t->wg_exposure != t->h->exposure ||
       t->wg_mode != t->mlp_mode) {
     drop_window_graphs(t);
@@ -1925,14 +1959,9 @@ static int windows_serial(hush_trainer_t *t, const hush_scene *sc, const uint32_
     cudaError_t e = cudaStreamCreateWithFlags(&t->cap, cudaStreamNonBlocking);
     if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "cudaStreamCreate");
   }
-  hush_scene w = *sc;
   for (int k = 0; k < n_windows; k += stride) {
-    w.seed = seeds[k];
-    for (int i = 0; i < n_frames; i++) {
-      char *b = t->win_pool + per * i;
-      const int rc = hush_scene_frame_device(&w, i, b, b + img, b + 2 * img, b + 3 * img, b + 4 * img, b + 5 * img, st);
-      if (rc != HUSH_OK) return hush_fail(t->h, rc, "hush_trainer_windows: scene generation failed");
-    }
+    const int grc = generate_window(t, sc, seeds[k], n_frames, img, per, st);
+    if (grc != HUSH_OK) return grc;
     cudaGraphExec_t &g = t->win_graph[((t->h->frame & 1) << 1) | (t->cur & 1)];
     if (g) {  // replay, then advance the host state as the frames would
       cudaError_t e = cudaGraphLaunch(g, st);
@@ -2015,23 +2044,31 @@ static int make_lanes(hush_trainer_t *t, int n) {
   return HUSH_OK;
 }
 
-// Windows of the analytic scene generator, trained in place: for each seed, the window's frames are generated on the
-// device and run forward + backward as hush_train_step runs them. Up to TRAIN_LANES windows run concurrently, window
-// k on lane k % lanes (each lane its own stream, history and accumulators, the lanes forked from and joined back to
-// `stream`); the lanes' gradients and losses are then added into this trainer's in lane order.
-extern "C" int hush_trainer_windows(hush_trainer_t *t, const hush_scene *sc, const uint32_t *seeds, int n_windows,
-                                    int n_frames, float lambda_t, void *stream) {
-  if (!t || !sc || !seeds) return hush_fail(t ? t->h : nullptr, HUSH_ERR_ARG, "hush_trainer_windows: NULL argument");
-  if (n_windows < 1 || n_frames < 1) return tr_fail(t, "hush_trainer_windows: empty batch");
-  if (sc->width != t->W || sc->height != t->H)
-    return tr_fail(t, "hush_trainer_windows: the scene size differs from the trainer's");
+static int windows_serial_bptt(hush_trainer_t *t, const hush_scene *sc, const uint32_t *seeds, int n_windows,
+                               int stride, int n_frames, float lambda_t, cudaStream_t st);
+
+// Windows of the analytic scene generator, trained in place (hush_trainer_windows: per-frame gradient by
+// windows_serial; hush_trainer_windows_bptt: through time by windows_serial_bptt): for each seed, the window's frames
+// are generated on the device and run forward + backward. Up to TRAIN_LANES windows run concurrently, window k on
+// lane k % lanes (each lane its own stream, history, records and accumulators, the lanes forked from and joined back
+// to `stream`); the lanes' gradients and losses are then added into this trainer's in lane order.
+static int run_windows(hush_trainer_t *t, const hush_scene *sc, const uint32_t *seeds, int n_windows, int n_frames,
+                       float lambda_t, void *stream, bool bptt, const char *name) {
+  const std::string nm(name);
+  if (!t || !sc || !seeds) return hush_fail(t ? t->h : nullptr, HUSH_ERR_ARG, nm + ": NULL argument");
+  if (n_windows < 1 || n_frames < 1) return tr_fail(t, nm + ": empty batch");
+  if (sc->width != t->W || sc->height != t->H) return tr_fail(t, nm + ": the scene size differs from the trainer's");
   if (t->W != t->h->W || t->H != t->h->H)
-    return tr_fail(t, "hush_trainer_windows: the denoiser was resized after the trainer was created");
-  if (t->is_lane) return tr_fail(t, "hush_trainer_windows: called on a helper lane");
+    return tr_fail(t, nm + ": the denoiser was resized after the trainer was created");
+  if (t->is_lane) return tr_fail(t, nm + ": called on a helper lane");
   cudaSetDevice(t->h->dev);
   cudaStream_t st = (cudaStream_t)stream;
+  auto serial = [&](hush_trainer_t *lt, const uint32_t *s, int nw, int stride, cudaStream_t ls) {
+    return bptt ? windows_serial_bptt(lt, sc, s, nw, stride, n_frames, lambda_t, ls)
+                : windows_serial(lt, sc, s, nw, stride, n_frames, lambda_t, ls);
+  };
   const int n = n_windows < TRAIN_LANES ? n_windows : TRAIN_LANES;
-  if (n == 1) return windows_serial(t, sc, seeds, n_windows, 1, n_frames, lambda_t, st);
+  if (n == 1) return serial(t, seeds, n_windows, 1, st);
   int rc = make_lanes(t, n);
   if (rc != HUSH_OK) return rc;
   cudaError_t e = cudaEventRecord(t->fork_ev, st);
@@ -2042,10 +2079,10 @@ extern "C" int hush_trainer_windows(hush_trainer_t *t, const hush_scene *sc, con
     if (l > 0) {
       hush_set_exposure(lt->h, t->h->exposure);
       lt->mlp_mode = t->mlp_mode;
-      rc = windows_serial(lt, sc, seeds + l, n_windows - l, n, n_frames, lambda_t, t->lane_st[l]);
+      rc = serial(lt, seeds + l, n_windows - l, n, t->lane_st[l]);
       if (rc != HUSH_OK) rc = hush_fail(t->h, rc, std::string("training lane: ") + hush_last_error(lt->h));
     } else {
-      rc = windows_serial(t, sc, seeds, n_windows, n, n_frames, lambda_t, t->lane_st[0]);
+      rc = serial(t, seeds, n_windows, n, t->lane_st[0]);
     }
   }
   // join every lane that was forked, whatever happened above
@@ -2059,6 +2096,11 @@ extern "C" int hush_trainer_windows(hush_trainer_t *t, const hush_scene *sc, con
   k_sum_lanes<<<(NW + 255) / 256, 256, 0, st>>>(t->grad, t->loss_acc, la);
   e = cudaGetLastError();
   return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, "summing the training lanes");
+}
+
+extern "C" int hush_trainer_windows(hush_trainer_t *t, const hush_scene *sc, const uint32_t *seeds, int n_windows,
+                                    int n_frames, float lambda_t, void *stream) {
+  return run_windows(t, sc, seeds, n_windows, n_frames, lambda_t, stream, false, "hush_trainer_windows");
 }
 
 extern "C" int hush_trainer_set_mlp(hush_trainer_t *t, int mode) {
@@ -2248,6 +2290,7 @@ static int ensure_records(hush_trainer_t *t, int n) {
   const size_t quarter = (size_t)((t->W2 + 1) / 2) * ((t->H2 + 1) / 2);
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
   const size_t per = al(full * 8) * 5 + al(half * 8) + al(half * 16) * 4 + al(quarter * 8) * 3 + al(full * 16);
+  drop_bptt_graph(t);  // it captured the old records' addresses
   cudaFree(t->rec_pool);
   t->rec.clear();
   cudaError_t e = cudaMalloc(&t->rec_pool, per * n);
@@ -2299,6 +2342,8 @@ static TwinFrame rec_twin(hush_trainer_t *t, const hush_inputs *in, const float 
 // with the gradient the next frame sent to this frame's colour history, and giving dL/dA0), mid3..mid1, the MLP
 // (whose alpha / gamma seeds are the gradient the next frame sent to this frame's par0), then TEMPORAL's adjoint,
 // which sends this frame's gradient to the previous frame's colour history, moments and alpha / gamma.
+static cudaError_t bptt_launches(hush_trainer_t *t, const hush_inputs *frames, const float *const *cleans,
+                                 int n_frames, float lambda_t, cudaStream_t st);
 extern "C" int hush_trainer_window_bptt(hush_trainer_t *t, const hush_inputs *frames, const float *const *cleans,
                                         int n_frames, float lambda_t, void *stream) {
   if (!t || !frames || !cleans)
@@ -2314,7 +2359,15 @@ extern "C" int hush_trainer_window_bptt(hush_trainer_t *t, const hush_inputs *fr
   cudaSetDevice(t->h->dev);
   int rc = ensure_records(t, n_frames);
   if (rc != HUSH_OK) return rc;
-  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = bptt_launches(t, frames, cleans, n_frames, lambda_t, (cudaStream_t)stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, "hush_trainer_window_bptt");
+}
+
+// The launches of one window through time on `st` (inputs checked, records allocated); no host state changes, so a
+// capture of them replays for every window whose inputs sit at the same addresses.
+static cudaError_t bptt_launches(hush_trainer_t *t, const hush_inputs *frames, const float *const *cleans,
+                                 int n_frames, float lambda_t, cudaStream_t st) {
   const int W = t->W, H = t->H, W2 = t->W2, H2 = t->H2;
   const size_t full = (size_t)W * H, half = (size_t)W2 * H2;
   const dim3 blk(TW, TH), gh((W2 + TW - 1) / TW, (H2 + TH - 1) / TH), gf((W + TW - 1) / TW, (H + TH - 1) / TH);
@@ -2373,8 +2426,72 @@ extern "C" int hush_trainer_window_bptt(hush_trainer_t *t, const hush_inputs *fr
       c = n;
     }
   }
-  if (e == cudaSuccess) e = cudaGetLastError();
-  return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, "hush_trainer_window_bptt");
+  return e;
+}
+
+// The windows seeds[0], seeds[stride], ... through time, in order on one trainer and stream: each window generated
+// into win_pool on `st`, then its forward + reverse sweep (bptt_launches) replayed as one CUDA graph, captured at the
+// first window and kept while the frame count, lambda, the exposure and the MLP form stay the same (the buffers it
+// names are the trainer's and stay put; reallocating them drops it). Where capture is not possible the launches run
+// directly.
+static int windows_serial_bptt(hush_trainer_t *t, const hush_scene *sc, const uint32_t *seeds, int n_windows,
+                               int stride, int n_frames, float lambda_t, cudaStream_t st) {
+  size_t img = 0, per = 0;
+  int rc = ensure_win_pool(t, n_frames, img, per);
+  if (rc == HUSH_OK) rc = ensure_records(t, n_frames);
+  if (rc != HUSH_OK) return rc;
+  if (t->bg_frames != n_frames || t->bg_lambda != lambda_t || t->bg_exposure != t->h->exposure ||
+      t->bg_mode != t->mlp_mode) {
+    drop_bptt_graph(t);
+    t->bg_frames = n_frames;
+    t->bg_lambda = lambda_t;
+    t->bg_exposure = t->h->exposure;
+    t->bg_mode = t->mlp_mode;
+  }
+  if (!t->cap) {
+    cudaError_t e = cudaStreamCreateWithFlags(&t->cap, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "cudaStreamCreate");
+  }
+  std::vector<hush_inputs> in(n_frames);
+  std::vector<const float *> cl(n_frames);
+  for (int i = 0; i < n_frames; i++) {
+    char *b = t->win_pool + per * i;
+    std::memset(&in[i], 0, sizeof(hush_inputs));
+    in[i].radiance = b; in[i].normal_depth = b + img; in[i].motion = b + 2 * img; in[i].material = b + 3 * img;
+    in[i].emission = b + 4 * img;
+    cl[i] = (const float *)(b + 5 * img);
+  }
+  for (int k = 0; k < n_windows; k += stride) {
+    rc = generate_window(t, sc, seeds[k], n_frames, img, per, st);
+    if (rc != HUSH_OK) return rc;
+    if (!t->bptt_graph) {  // capture on the trainer's own stream (the caller's may be the legacy default stream)
+      cudaGraph_t graph = nullptr;
+      cudaError_t e = cudaStreamBeginCapture(t->cap, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        const cudaError_t el = bptt_launches(t, in.data(), cl.data(), n_frames, lambda_t, t->cap);
+        e = cudaStreamEndCapture(t->cap, &graph);
+        if (e == cudaSuccess && el != cudaSuccess) e = el;
+      }
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&t->bptt_graph, graph, 0);
+      if (graph) cudaGraphDestroy(graph);
+      if (e != cudaSuccess) {  // capture not possible here: run the launches directly
+        cudaGetLastError();
+        drop_bptt_graph(t);
+        e = bptt_launches(t, in.data(), cl.data(), n_frames, lambda_t, st);
+        if (e == cudaSuccess) e = cudaGetLastError();
+        if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "hush_trainer_windows_bptt");
+        continue;
+      }
+    }
+    const cudaError_t e = cudaGraphLaunch(t->bptt_graph, st);
+    if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "cudaGraphLaunch of a window through time");
+  }
+  return HUSH_OK;
+}
+
+extern "C" int hush_trainer_windows_bptt(hush_trainer_t *t, const hush_scene *sc, const uint32_t *seeds,
+                                         int n_windows, int n_frames, float lambda_t, void *stream) {
+  return run_windows(t, sc, seeds, n_windows, n_frames, lambda_t, stream, true, "hush_trainer_windows_bptt");
 }
 
 extern "C" int hush_trainer_buffer(hush_trainer_t *t, int which, void **ptr, int *width, int *height, int *channels) {

@@ -79,6 +79,15 @@ class Trainer:
         self._check(L.lib().hush_trainer_windows(self._t, C.byref(sc), arr, len(seeds), int(n_frames),
                                                  float(lambda_t), C.c_void_p(_stream_handle(stream))))
 
+    def windows_bptt(self, scene_cfg: SceneConfig, seeds, n_frames: int, lambda_t: float = 0.0, stream=None):
+        """hush_trainer_windows_bptt: for each seed, the n_frames frames of scene_cfg with that seed generated on the
+        device and run forward and backward through time (window_bptt) on concurrent lanes, each window replayed as a
+        CUDA graph; gradient and loss accumulate, no step."""
+        sc = scene_cfg.c()
+        arr = (C.c_uint32 * len(seeds))(*[int(x) & 0xFFFFFFFF for x in seeds])
+        self._check(L.lib().hush_trainer_windows_bptt(self._t, C.byref(sc), arr, len(seeds), int(n_frames),
+                                                      float(lambda_t), C.c_void_p(_stream_handle(stream))))
+
     def loss_sum(self, stream=None) -> float:
         """Sum of the frame losses since the previous call."""
         v = C.c_double()
@@ -272,14 +281,12 @@ def train(cfg: TrainConfig, log_every: int = 100, on_log=None, time_budget_s: fl
     rng = dp.seed_rng(cfg.init_seed + 1)
     sc = window_scene(cfg)
     hist = []
-    buf = window(cfg, 0) if cfg.bptt else None  # device buffers of one window, reused
     t0 = time.time()
     for step in range(cfg.steps):
         ts = time.perf_counter()
         seeds = [dp.window_seed(rng, cfg.seeds) for _ in range(cfg.batch)]
-        if cfg.bptt:  # each window generated on the device, then forward and backward through time
-            for s in seeds:
-                tr.window_bptt(window(cfg, s, buf), cfg.lambda_t)
+        if cfg.bptt:  # generation + forward + backward through time of every window
+            tr.windows_bptt(sc, seeds, cfg.frames, cfg.lambda_t)
         else:
             tr.windows(sc, seeds, cfg.frames, cfg.lambda_t)  # generation + forward + adjoint of every frame
         loss, gn = finish_step(tr, dp, cfg.batch * cfg.frames, cfg.lr, cfg.clip)

@@ -328,6 +328,15 @@ int hush_coarse2_bwd(hush_trainer_t *t, void *stream);
 int hush_trainer_window_bptt(hush_trainer_t *t, const hush_inputs *frames, const float *const *cleans, int n_frames,
                              float lambda_t, void *stream);
 
+/* hush_trainer_window_bptt over the training windows of the analytic scene generator, as hush_trainer_windows runs
+ * them: for each of n_windows seeds the n_frames frames of *sc are generated on the device into trainer-owned buffers
+ * and the window runs forward and backward through time. Up to eight windows run concurrently on the same lanes
+ * (each lane its own records), summed into this trainer's accumulators in lane order; each window's forward + reverse
+ * sweep replays as a cached CUDA graph. No optimiser step; sc's size must be the trainer's. The trainer's own Hush
+ * history is not touched. */
+int hush_trainer_windows_bptt(hush_trainer_t *t, const struct hush_scene_s *sc, const uint32_t *seeds, int n_windows,
+                              int n_frames, float lambda_t, void *stream);
+
 /* Weight gradient of the parameter MLP (812 doubles in dtheta, overwritten) from a half-resolution image of rows:
  * packed features F0..F3 (16-byte texels, width2 x height2, as hush_buffer returns them), dL/dpar (12 floats per
  * row, as hush_trainer_par lays them out, all 12 channels honoured) and FP32 weights theta (812). The same

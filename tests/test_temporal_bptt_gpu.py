@@ -178,3 +178,41 @@ def test_window_bptt_matches_the_fp64_window_gradient():
     assert not np.allclose(got, truncated)
     tr.destroy()
     g.destroy()
+
+
+def test_native_windows_through_time_match_the_window_calls():
+    """hush_trainer_windows_bptt (generation on the device, windows on concurrent lanes, each window's forward and
+    reverse sweep replayed as a CUDA graph) accumulates the same loss and gradient as hush_trainer_window_bptt called
+    window by window on the same generated windows, in both MLP forms (the loss to 1e-12, the gradient to 1e-6 of its
+    largest value). Batches of three windows of three frames: the
+    first batch captures each lane's graph, the next ones replay it; a one-window batch runs on the caller's stream.
+    The alpha / gamma heads get their gradient through time on this path too."""
+    from hush_b200.train import TrainConfig, window, window_scene
+
+    cfg = TrainConfig(size=64, frames=3)
+    theta = xavier_init(9)
+    a = Trainer(Hush(0, {"width": 64, "height": 64, "schedule": "passes"}), theta)
+    b = Trainer(Hush(0, {"width": 64, "height": 64, "schedule": "passes"}), theta)
+
+    def calls(seeds):
+        b.zero_grad()
+        b.loss_sum()
+        for s in seeds:
+            b.window_bptt(window(cfg, s), 0.5)
+        return b.loss_sum(), b.grad()
+
+    for mlp in ("fp32", "bf16"):
+        a.set_mlp(mlp)
+        b.set_mlp(mlp)
+        for seeds in ([11, 12, 13], [14, 15, 16], [17, 18, 19], [20]):
+            a.zero_grad()
+            a.loss_sum()
+            a.windows_bptt(window_scene(cfg), seeds, cfg.frames, 0.5)
+            la, ga = a.loss_sum(), a.grad()
+            lb, gb = calls(seeds)
+            assert la == pytest.approx(lb, rel=1e-12), (mlp, seeds)
+            # the adjoints' FP32 atomics add in a different order: differences at FP32 rounding level
+            assert np.abs(ga - gb).max() <= 1e-6 * np.abs(gb).max(), (mlp, seeds)
+            assert np.abs(ga[AG_IDX]).max() > 1e-6 * np.abs(ga).max(), (mlp, seeds)
+    a.destroy()
+    b.destroy()
