@@ -49,6 +49,8 @@ struct TwinFrame {
   float4 *dB1, *dB2, *dB3;  // half: level gradients
   const float4 *gA1;        // full: dL/d fine level through the colour history (the next frame's TEMPORAL), or NULL
   float4 *dA0;              // full: dL/d TEMPORAL's colour + variance A0 (the fine level's input), or NULL
+  float4 *dAh;              // half: dL/d block means (F2.zw) from mid1 and the recombination, or NULL
+  float4 *dC0;              // quarter: dL/d coarse level C0 from the recombination, or NULL
   float4 *dpar;           // half: 3 float4 per row
   float *partials;        // per-CTA weight-gradient partials (NW floats each)
   double *loss_partials;  // per-CTA loss partials
@@ -271,7 +273,7 @@ __global__ void __launch_bounds__(TW *TH) k_mid_bwd(const TwinFrame T) {
   const HushFrame &f = T.f;
   const float4 *src = K == 2 ? T.B1 : T.B2;
   const float4 *gout = K == 1 ? T.dB1 : (K == 2 ? T.dB2 : T.dB3);
-  float4 *gin = K == 1 ? nullptr : (K == 2 ? T.dB1 : T.dB2);
+  float4 *gin = K == 1 ? T.dAh : (K == 2 ? T.dB1 : T.dB2);  // level 1 reads the block means
   const int li = threadIdx.y * TW + threadIdx.x;
   const int bx = blockIdx.x * TW, by = blockIdx.y * TH;
   for (int i = li; i < SW * SH; i += TW * TH) {
@@ -289,8 +291,16 @@ __global__ void __launch_bounds__(TW *TH) k_mid_bwd(const TwinFrame T) {
   Filt1<STEP, K == 1, SW> F;
   F.run(sA, sG, ti, X, Y, f.W2, f.H2, s, c);
   const float4 g = gout[o];
-  float ds, dc;
-  F.adjoint(sA, ti, make_float3(g.x, g.y, g.z), g.w, s, ds, dc, gin, o, f.W2);
+  float ds, dc, dgv = 0.0f;
+  F.adjoint(sA, ti, make_float3(g.x, g.y, g.z), g.w, s, ds, dc, gin, o, f.W2, K == 1 ? &dgv : nullptr);
+  if (K == 1 && gin && dgv != 0.0f) {  // level 1's 3x3 variance prefilter (clamp-to-edge taps)
+#pragma unroll
+    for (int j = 0; j < 9; j++) {
+      const int dx = j % 3 - 1, dy = j / 3 - 1;
+      const float k = (dx == 0 && dy == 0) ? 0.25f : ((dx == 0 || dy == 0) ? 0.125f : 0.0625f);
+      atomicAdd(&gin[clampi(Y + dy, 0, f.H2 - 1) * f.W2 + clampi(X + dx, 0, f.W2 - 1)].w, k * dgv);
+    }
+  }
   // s_k / c_k live in components k of par1 / par2
   float *dp1 = &T.dpar[3 * o + 1].x, *dp2 = &T.dpar[3 * o + 2].x;
   atomicAdd(dp1 + K, ds);
@@ -477,11 +487,36 @@ __global__ void k_down_bwd(const TwinFrame T, const float4 *ah, const float4 *dd
   dah[o] = d;
 }
 
+// c1 = the stored coarse level C1 as FP32 (coarse2's input in the window sweep, straight through the f16 storage)
+__global__ void k_c1_fill(const TwinFrame T, float4 *c1) {
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o < T.f.W4 * T.f.H4) c1[o] = ldh(T.f.C1, o);
+}
+
+// The block means' adjoint into TEMPORAL's output: block() forms Ah as the mean of the f16-quantised A0 over the
+// block's surface pixels (hush.js:241-244, 280), so every surface pixel gets dL/dAh / nv (the quantisation counts as
+// the identity).
+__global__ void k_ah_to_a0(const TwinFrame T, const float4 *dah, float4 *dA0) {
+  const HushFrame &f = T.f;
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= f.W * f.H) return;
+  const int px = o % f.W, py = o / f.W;
+  if (ldh(f.key, o).z < 0.0f) return;  // sky: not in the block's mean
+  const int hp = (py >> 1) * f.W2 + (px >> 1);
+  const float nv = unpack2(__ldg(f.F3 + hp).y).y;
+  if (nv <= 0.0f) return;
+  const float4 g = dah[hp];
+  const float k = 1.0f / nv;
+  float4 d = dA0[o];
+  d.x += g.x * k; d.y += g.y * k; d.z += g.z * k; d.w += g.w * k;
+  dA0[o] = d;
+}
+
 // ------------------------------------------------------------------------------------------------ fine + final
 struct Recomb {
   float fx, fy, fz, swh, swq, uBx, uBy, uBz, uAx, uAy, uAz, uCx, uCy, uCz;
   float wh[4], wqq[4];
-  int qh[4];
+  int qh[4], qq[4];
   bool vh[4], vq[4];
 };
 
@@ -517,12 +552,18 @@ HD_INL void recomb_fwd(const TwinFrame &T, int px, int py, float4 A1, float4 gp,
   R.uCx = R.uCy = R.uCz = R.swq = 0.f;
   for (int j = 0; j < 4; j++) {
     const int qx = (int)cbx + (j & 1), qy = (int)cby + (j >> 1);
+    R.vq[j] = false;
+    R.wqq[j] = 0.f;
+    R.qq[j] = 0;
     if (qx < 0 || qy < 0 || qx >= qsx || qy >= qsy) continue;
     const int q = qy * f.W4 + qx;
     const float4 cg = ldh(f.CG, q);
     if (cg.z < 0.0f) continue;
     const float w = jbw(cposx - cbx, cposy - cby, j, oct_dec(cg.x, cg.y), cg.z, gp, z);
     const float4 c = ldh(f.C0, q);
+    R.vq[j] = true;
+    R.wqq[j] = w;
+    R.qq[j] = q;
     R.swq += w;
     R.uCx += w * c.x; R.uCy += w * c.y; R.uCz += w * c.z;
   }
@@ -869,6 +910,16 @@ __global__ void __launch_bounds__(TW *TH) k_fine_bwd(const TwinFrame T, const fl
       const float upx = R.uCx / R.swq, upy = R.uCy / R.swq, upz = R.uCz / R.swq;
       gbeta = g2.x * (upx - ix) + g2.y * (upy - iy) + g2.z * (upz - iz);
       gill = make_float3(g2.x * (1.0f - p0.z), g2.y * (1.0f - p0.z), g2.z * (1.0f - p0.z));
+      if (T.dC0) {  // up = sum w C0 / sum w: each coarse tap's colour (its variance gets no gradient here)
+        for (int j = 0; j < 4; j++) {
+          if (!R.vq[j]) continue;
+          const float k = p0.z * R.wqq[j] / R.swq;
+          float *d = &T.dC0[R.qq[j]].x;
+          atomicAdd(d, g2.x * k);
+          atomicAdd(d + 1, g2.y * k);
+          atomicAdd(d + 2, g2.z * k);
+        }
+      }
     }
     float3 gf = gill;
     float gkappa = 0.0f;
@@ -882,6 +933,13 @@ __global__ void __launch_bounds__(TW *TH) k_fine_bwd(const TwinFrame T, const fl
         atomicAdd(d, gill.x * w);
         atomicAdd(d + 1, gill.y * w);
         atomicAdd(d + 2, gill.z * w);
+        if (T.dAh) {  // ill = uB / sw + kappa (f - uA / sw): the block means' colour
+          const float k = -p0.w * w;
+          float *a = &T.dAh[R.qh[j]].x;
+          atomicAdd(a, gill.x * k);
+          atomicAdd(a + 1, gill.y * k);
+          atomicAdd(a + 2, gill.z * k);
+        }
       }
     }
     float gv1 = 0.0f;  // the fine level's variance reaches X through nothing; only the history may seed it
@@ -2359,7 +2417,9 @@ extern "C" int hush_trainer_window_bptt(hush_trainer_t *t, const hush_inputs *fr
   cudaSetDevice(t->h->dev);
   int rc = ensure_records(t, n_frames);
   if (rc != HUSH_OK) return rc;
-  cudaError_t e = bptt_launches(t, frames, cleans, n_frames, lambda_t, (cudaStream_t)stream);
+  cudaError_t e = ensure_coarse(t);  // the coarse levels' adjoint buffers
+  if (e != cudaSuccess) return hush_cuda_fail(t->h, e, "cudaMalloc of the coarse-level buffers");
+  e = bptt_launches(t, frames, cleans, n_frames, lambda_t, (cudaStream_t)stream);
   if (e == cudaSuccess) e = cudaGetLastError();
   return e == cudaSuccess ? HUSH_OK : hush_cuda_fail(t->h, e, "hush_trainer_window_bptt");
 }
@@ -2369,8 +2429,9 @@ extern "C" int hush_trainer_window_bptt(hush_trainer_t *t, const hush_inputs *fr
 static cudaError_t bptt_launches(hush_trainer_t *t, const hush_inputs *frames, const float *const *cleans,
                                  int n_frames, float lambda_t, cudaStream_t st) {
   const int W = t->W, H = t->H, W2 = t->W2, H2 = t->H2;
-  const size_t full = (size_t)W * H, half = (size_t)W2 * H2;
+  const size_t full = (size_t)W * H, half = (size_t)W2 * H2, quarter = (size_t)t->W4 * t->H4;
   const dim3 blk(TW, TH), gh((W2 + TW - 1) / TW, (H2 + TH - 1) / TH), gf((W + TW - 1) / TW, (H + TH - 1) / TH);
+  const dim3 gq((t->W4 + TW - 1) / TW, (t->H4 + TH - 1) / TH);
   auto twin = [&](int i) {
     return rec_twin(t, frames + i, cleans[i], i ? cleans[i - 1] : nullptr, i, lambda_t);
   };
@@ -2408,15 +2469,31 @@ static cudaError_t bptt_launches(hush_trainer_t *t, const hush_inputs *frames, c
     k_taa_bwd_coef<<<gf, blk, 0, st>>>(T, t->gT, t->tcoef);
     k_taa_bwd_gather<<<gf, blk, 0, st>>>(T, t->tcoef, t->gT2);
     e = cudaMemsetAsync(t->dA0, 0, full * 16, st);
+    if (e == cudaSuccess && i > 0) e = cudaMemsetAsync(t->dah, 0, half * 16, st);
+    if (e == cudaSuccess && i > 0) e = cudaMemsetAsync(t->dc0, 0, quarter * 16, st);
     if (e != cudaSuccess) break;
     T.gA1 = t->c_hist[c];
     T.dA0 = t->dA0;
+    if (i > 0) {  // A0 reaches the loss also through the block means (mid1, the recombination, the coarse levels)
+      T.dAh = t->dah;
+      T.dC0 = t->dc0;
+    }
     k_fine_bwd<true><<<gf, blk, 0, st>>>(T, t->gT2);
     k_mid_bwd<3><<<gh, blk, 0, st>>>(T);
     k_mid_bwd<2><<<gh, blk, 0, st>>>(T);
     k_mid_bwd<1><<<gh, blk, 0, st>>>(T);
     launch_mlp_bwd(t, T, st);
     if (i > 0) {
+      // the coarse levels' adjoints (C0 -> C1 -> down() -> block means), then the block means into A0
+      k_ah_fill<<<(unsigned)((half + 255) / 256), 256, 0, st>>>(T, t->ah);
+      k_c1_fill<<<(unsigned)((quarter + 255) / 256), 256, 0, st>>>(T, t->c1);
+      e = cudaMemsetAsync(t->dc1, 0, quarter * 16, st);
+      if (e == cudaSuccess) e = cudaMemsetAsync(t->ddown, 0, quarter * 16, st);
+      if (e != cudaSuccess) break;
+      k_coarse_tw<2><<<gq, blk, 0, st>>>(T, t->c1, nullptr, t->dc0, t->dc1);
+      k_coarse_tw<1><<<gq, blk, 0, st>>>(T, t->ah, nullptr, t->dc1, t->ddown);
+      k_down_bwd<<<(unsigned)((half + 255) / 256), 256, 0, st>>>(T, t->ah, t->ddown, t->dah);
+      k_ah_to_a0<<<(unsigned)((full + 255) / 256), 256, 0, st>>>(T, t->dah, t->dA0);
       const int n = c ^ 1;
       e = cudaMemsetAsync(t->c_hist[n], 0, full * 16, st);
       if (e == cudaSuccess) e = cudaMemsetAsync(t->c_mom[n], 0, full * 16, st);
@@ -2440,6 +2517,8 @@ static int windows_serial_bptt(hush_trainer_t *t, const hush_scene *sc, const ui
   int rc = ensure_win_pool(t, n_frames, img, per);
   if (rc == HUSH_OK) rc = ensure_records(t, n_frames);
   if (rc != HUSH_OK) return rc;
+  const cudaError_t ec = ensure_coarse(t);  // the coarse levels' adjoint buffers
+  if (ec != cudaSuccess) return hush_cuda_fail(t->h, ec, "cudaMalloc of the coarse-level buffers");
   if (t->bg_frames != n_frames || t->bg_lambda != lambda_t || t->bg_exposure != t->h->exposure ||
       t->bg_mode != t->mlp_mode) {
     drop_bptt_graph(t);

@@ -210,9 +210,9 @@ def mid(k: int, src, Gh, sky_h, par):
     return torch.where(sky_h[..., None], z4, filt(src, Gh, pf[..., 4 + k], pf[..., 8 + k], step, k == 1))
 
 
-def fine(st: dict, par, B3, Gh, sky_h, Ah, A0=None):
+def fine(st: dict, par, B3, Gh, sky_h, Ah, A0=None, C0=None):
     """Fine level and recombination (hush.js:578-620): (A1, X), (H, W, 4) and (H, W, 3). A0: TEMPORAL's colour +
-    variance as a tensor (to differentiate through it), else st["A0"]."""
+    variance as a tensor (to differentiate through it), else st["A0"]; C0 likewise for the coarse level."""
     par_f = _par_f(par, sky_h)
     A0 = _t(st["A0"]) if A0 is None else A0
     key = _t(st["key"])
@@ -246,7 +246,7 @@ def fine(st: dict, par, B3, Gh, sky_h, Ah, A0=None):
     kappa, beta = p_full[..., 3], p_full[..., 2]
     swh_s = torch.where(mid_ok, swh, torch.ones_like(swh))
     ill = torch.where(mid_ok[..., None], uB / swh_s[..., None] + kappa[..., None] * (f - uA / swh_s[..., None]), f)
-    C0, CG = _t(st["C0"]), _t(st["CG"])
+    C0, CG = (_t(st["C0"]) if C0 is None else C0), _t(st["CG"])
     CGd = torch.cat([oct_dec(CG[..., 0], CG[..., 1]), CG[..., 2:3]], -1)
     cposx, cposy = (xs.double() + 0.5) / 4.0 - 0.5, (ys.double() + 0.5) / 4.0 - 0.5
     cbx, cby = torch.floor(cposx), torch.floor(cposy)
@@ -416,11 +416,28 @@ def _st_value(x64, stored):
     return x64 + (_t(np.asarray(stored, np.float32)) - x64).detach()
 
 
+def block_means(A0, surf):
+    """block()'s mean of A0 (H, W, 4) over each 2x2 block's surface pixels surf (H, W) (hush.js:241-244): (h, w, 4),
+    zeros for blocks without a surface."""
+    H, W = A0.shape[:2]
+    h, w = (H + 1) // 2, (W + 1) // 2
+    A = torch.nn.functional.pad(A0.permute(2, 0, 1), (0, 2 * w - W, 0, 2 * h - H)).permute(1, 2, 0)
+    m = torch.nn.functional.pad(surf.double(), (0, 2 * w - W, 0, 2 * h - H))
+    A = A.reshape(h, 2, w, 2, 4)
+    m = m.reshape(h, 2, w, 2)
+    nv = m.sum((1, 3))
+    s = (m[..., None] * A).sum((1, 3))
+    return torch.where((nv > 0)[..., None], s / torch.clamp(nv, min=1.0)[..., None], torch.zeros_like(s))
+
+
 def window_loss(states, theta, lambda_t=0.0):
     """The summed loss of a window with the gradient through time of hush_trainer_window_bptt: states[i] is frame i's
     st (twin_loss's keys, plus the frame's stored mom / hist / par0 and the G-buffer, and key_prev), frame 0 a reset.
     TEMPORAL runs in float64 on the previous frame's history, each stored value (A0, moments, colour history, par0)
-    entering with the straight-through gradient; the features, coarse levels and TAA history are constants."""
+    entering with the straight-through gradient; from the second frame on A0 also reaches the loss through the block
+    means (block(), then mid1, the recombination and the coarse levels COARSE1 / coarse2, the stored block means,
+    C1 and C0 entering straight through; states[i] then also holds C1). The features and the TAA history are
+    constants."""
     total = 0.0
     hist_prev = mom_prev = par0_prev = None
     for i, st in enumerate(states):
@@ -431,11 +448,18 @@ def window_loss(states, theta, lambda_t=0.0):
             A0_64, mom_64 = temporal(st, hist_prev, mom_prev, par0_prev)
             A0, mom = _st_value(A0_64, st["A0"]), _st_value(mom_64, st["mom"])
         feats, Gh, sky_h, Ah = half_inputs(st)
+        C0 = None
+        if i > 0:
+            surf = _t(np.asarray(st["key"], np.float32))[..., 2] >= 0
+            Ah = _st_value(block_means(A0, surf), Ah.numpy())
+            Gq = coarse_guide(st["CG"])
+            C1 = _st_value(coarse1(Ah, unpack_half(st["F3"])[..., 3], Gq), st["C1"])
+            C0 = _st_value(coarse2(C1, Gq), st["C0"])
         _, par = mlp(feats, theta, sky_h)
         B1 = mid(1, Ah, Gh, sky_h, par)
         B2 = mid(2, B1, Gh, sky_h, par)
         B3 = mid(3, B2, Gh, sky_h, par)
-        A1, X = fine(st, par, B3, Gh, sky_h, Ah, A0=A0)
+        A1, X = fine(st, par, B3, Gh, sky_h, Ah, A0=A0, C0=C0)
         total = total + loss_of(st, taa(st, X), lambda_t)
         sky = _t(np.asarray(st["key"], np.float32))[..., 2] < 0
         A1 = torch.where(sky[..., None], torch.zeros_like(A1), A1)  # sky pixels store no history
