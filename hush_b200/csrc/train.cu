@@ -2397,9 +2397,11 @@ static TwinFrame rec_twin(hush_trainer_t *t, const hush_inputs *in, const float 
 
 // Backpropagation through time over one window (see include/hush.h): forward over the frames, keeping each frame's
 // state, then the reverse sweep, frame by frame from the last: the twin's forward again, the loss, TAA, fine (seeded
-// with the gradient the next frame sent to this frame's colour history, and giving dL/dA0), mid3..mid1, the MLP
-// (whose alpha / gamma seeds are the gradient the next frame sent to this frame's par0), then TEMPORAL's adjoint,
-// which sends this frame's gradient to the previous frame's colour history, moments and alpha / gamma.
+// with the gradient the next frame sent to this frame's colour history, and giving dL/dA0 and, from the second frame
+// on, dL/d block means and dL/dC0), mid3..mid1 (mid1 adding into dL/d block means), the MLP (whose alpha / gamma
+// seeds are the gradient the next frame sent to this frame's par0), the coarse levels' adjoints (C0 -> C1 -> down()
+// -> block means) and the block means into A0, then TEMPORAL's adjoint, which sends this frame's gradient to the
+// previous frame's colour history, moments and alpha / gamma.
 static cudaError_t bptt_launches(hush_trainer_t *t, const hush_inputs *frames, const float *const *cleans,
                                  int n_frames, float lambda_t, cudaStream_t st);
 extern "C" int hush_trainer_window_bptt(hush_trainer_t *t, const hush_inputs *frames, const float *const *cleans,

@@ -321,8 +321,10 @@ int hush_coarse2_bwd(hush_trainer_t *t, void *stream);
  * window starts without history, every frame runs forward with its state kept, then the frames run backward from the
  * last one. Besides each frame's own loss gradient (what hush_trainer_frame takes), the gradient flows across frames
  * through TEMPORAL (hush_temporal_bwd): from a frame's colour + variance A0 and moments into the previous frame's
- * colour history (its fine level), moments and alpha / gamma, so the alpha and gamma heads of the MLP train. The
- * block features and the TAA history are held fixed (truncated there). Adds into the gradient and loss accumulators,
+ * colour history (its fine level), moments and alpha / gamma, so the alpha and gamma heads of the MLP train. A0
+ * reaches the loss directly (the fine level) and through the block means (block(), hush.js:241-244), which feed mid1,
+ * the recombination and the coarse levels COARSE1 / coarse2; both paths are followed. The block features and the TAA
+ * history are held fixed (truncated there). Adds into the gradient and loss accumulators,
  * like hush_trainer_windows; allocates the window's per-frame records (about 11 MB per frame at 384 x 384) on first
  * use. The trainer's own Hush history is not touched. */
 int hush_trainer_window_bptt(hush_trainer_t *t, const hush_inputs *frames, const float *const *cleans, int n_frames,
