@@ -516,7 +516,7 @@ __global__ void k_ah_to_a0(const TwinFrame T, const float4 *dah, float4 *dA0) {
 struct Recomb {
   float fx, fy, fz, swh, swq, uBx, uBy, uBz, uAx, uAy, uAz, uCx, uCy, uCz;
   float wh[4], wqq[4];
-  int qh[4], qq[4];
+  int qh[4];
   bool vh[4], vq[4];
 };
 
@@ -552,18 +552,12 @@ HD_INL void recomb_fwd(const TwinFrame &T, int px, int py, float4 A1, float4 gp,
   R.uCx = R.uCy = R.uCz = R.swq = 0.f;
   for (int j = 0; j < 4; j++) {
     const int qx = (int)cbx + (j & 1), qy = (int)cby + (j >> 1);
-    R.vq[j] = false;
-    R.wqq[j] = 0.f;
-    R.qq[j] = 0;
     if (qx < 0 || qy < 0 || qx >= qsx || qy >= qsy) continue;
     const int q = qy * f.W4 + qx;
     const float4 cg = ldh(f.CG, q);
     if (cg.z < 0.0f) continue;
     const float w = jbw(cposx - cbx, cposy - cby, j, oct_dec(cg.x, cg.y), cg.z, gp, z);
     const float4 c = ldh(f.C0, q);
-    R.vq[j] = true;
-    R.wqq[j] = w;
-    R.qq[j] = q;
     R.swq += w;
     R.uCx += w * c.x; R.uCy += w * c.y; R.uCz += w * c.z;
   }
@@ -862,6 +856,28 @@ __global__ void k_tm_bwd(const TwinFrame T, const float4 *gtm, float4 *dX) {
 // gradients.
 // SEED_TM: the seed is the gradient w.r.t. the tone-mapped colour tm(X) (the fused frame); else w.r.t. X itself (the
 // per-pass pair, whose TAA adjoint has already applied the tm adjoint).
+// dL/dC0 of the recombination's coarse term (window sweep only): up = sum w C0 / sum w, ill2 = ill + (up - ill) beta,
+// so each quarter-res tap's colour gets g2 beta w / sum w (its variance none). The taps' weights are recomputed as
+// recomb_fwd() forms them, so the per-frame adjoint keeps no per-tap state.
+HD_INL void recomb_coarse_adj(const TwinFrame &T, int px, int py, float4 gp, float swq, float beta, float3 g2) {
+  const HushFrame &f = T.f;
+  const int qsx = (f.W + 3) / 4, qsy = (f.H + 3) / 4;
+  const float cposx = ((float)px + 0.5f) / 4.0f - 0.5f, cposy = ((float)py + 0.5f) / 4.0f - 0.5f;
+  const float cbx = floorf(cposx), cby = floorf(cposy);
+  for (int j = 0; j < 4; j++) {
+    const int qx = (int)cbx + (j & 1), qy = (int)cby + (j >> 1);
+    if (qx < 0 || qy < 0 || qx >= qsx || qy >= qsy) continue;
+    const int q = qy * f.W4 + qx;
+    const float4 cg = ldh(f.CG, q);
+    if (cg.z < 0.0f) continue;
+    const float k = beta * jbw(cposx - cbx, cposy - cby, j, oct_dec(cg.x, cg.y), cg.z, gp, gp.w) / swq;
+    float *d = &T.dC0[q].x;
+    atomicAdd(d, g2.x * k);
+    atomicAdd(d + 1, g2.y * k);
+    atomicAdd(d + 2, g2.z * k);
+  }
+}
+
 template <bool SEED_TM>
 __global__ void __launch_bounds__(TW *TH) k_fine_bwd(const TwinFrame T, const float4 *gT) {
   constexpr int AP = 1, SW = TW + 2, SH = TH + 2;
@@ -910,16 +926,6 @@ __global__ void __launch_bounds__(TW *TH) k_fine_bwd(const TwinFrame T, const fl
       const float upx = R.uCx / R.swq, upy = R.uCy / R.swq, upz = R.uCz / R.swq;
       gbeta = g2.x * (upx - ix) + g2.y * (upy - iy) + g2.z * (upz - iz);
       gill = make_float3(g2.x * (1.0f - p0.z), g2.y * (1.0f - p0.z), g2.z * (1.0f - p0.z));
-      if (T.dC0) {  // up = sum w C0 / sum w: each coarse tap's colour (its variance gets no gradient here)
-        for (int j = 0; j < 4; j++) {
-          if (!R.vq[j]) continue;
-          const float k = p0.z * R.wqq[j] / R.swq;
-          float *d = &T.dC0[R.qq[j]].x;
-          atomicAdd(d, g2.x * k);
-          atomicAdd(d + 1, g2.y * k);
-          atomicAdd(d + 2, g2.z * k);
-        }
-      }
     }
     float3 gf = gill;
     float gkappa = 0.0f;
@@ -933,13 +939,6 @@ __global__ void __launch_bounds__(TW *TH) k_fine_bwd(const TwinFrame T, const fl
         atomicAdd(d, gill.x * w);
         atomicAdd(d + 1, gill.y * w);
         atomicAdd(d + 2, gill.z * w);
-        if (T.dAh) {  // ill = uB / sw + kappa (f - uA / sw): the block means' colour
-          const float k = -p0.w * w;
-          float *a = &T.dAh[R.qh[j]].x;
-          atomicAdd(a, gill.x * k);
-          atomicAdd(a + 1, gill.y * k);
-          atomicAdd(a + 2, gill.z * k);
-        }
       }
     }
     float gv1 = 0.0f;  // the fine level's variance reaches X through nothing; only the history may seed it
@@ -974,6 +973,45 @@ __global__ void __launch_bounds__(TW *TH) k_fine_bwd(const TwinFrame T, const fl
     atomicAdd(d0 + 3, q4[1]);
     atomicAdd(d1 + 0, q4[2]);
     atomicAdd(d2 + 0, q4[3]);
+  }
+}
+
+// The recombination's adjoint into the block means and the coarse level (window sweep only; k_fine_bwd does the
+// rest): ill = uB / sum_h w + kappa (f - uA / sum_h w) and ill2 = ill + (up - ill) beta, up = sum_q w C0 / sum_q w, so
+// each half-res tap's block-mean colour gets -kappa w / sum_h w dL/d ill and each quarter-res tap's colour
+// beta w / sum_q w dL/d ill2 (X = ill2 albedo + emission). The tap weights do not depend on the levels, so nothing
+// of the fine level is recomputed.
+template <bool SEED_TM>
+__global__ void __launch_bounds__(TW *TH) k_fine_pyr_bwd(const TwinFrame T, const float4 *gT) {
+  const HushFrame &f = T.f;
+  const int px = blockIdx.x * TW + threadIdx.x, py = blockIdx.y * TH + threadIdx.y;
+  if (px >= f.W || py >= f.H) return;
+  const int o = py * f.W + px;
+  const float4 key = ldh(f.key, o);
+  if (key.z < 0.0f) return;  // sky: X = emission
+  float4 gp = oct_dec(key.x, key.y);
+  gp.w = key.z;
+  const int hp = (py >> 1) * f.W2 + (px >> 1);
+  const float4 gt = gT[o];
+  const float3 gX = SEED_TM ? tm_adjoint(T.X[o], gt) : make_float3(gt.x, gt.y, gt.z);
+  const float4 alb = ldh(f.mat, py * f.p_mat + px), p0 = T.par[3 * hp];
+  const float3 g2 = make_float3(gX.x * alb.x, gX.y * alb.y, gX.z * alb.z);
+  Recomb R;
+  recomb_fwd(T, px, py, make_float4(0.f, 0.f, 0.f, 0.f), gp, R);
+  float3 gill = g2;
+  if (R.swq > 1e-4f) {
+    gill = make_float3(g2.x * (1.0f - p0.z), g2.y * (1.0f - p0.z), g2.z * (1.0f - p0.z));
+    recomb_coarse_adj(T, px, py, gp, R.swq, p0.z, g2);
+  }
+  if (R.swh > 1e-4f) {
+    for (int j = 0; j < 4; j++) {
+      if (!R.vh[j]) continue;
+      const float k = -p0.w * R.wh[j] / R.swh;
+      float *a = &T.dAh[R.qh[j]].x;
+      atomicAdd(a, gill.x * k);
+      atomicAdd(a + 1, gill.y * k);
+      atomicAdd(a + 2, gill.z * k);
+    }
   }
 }
 
@@ -2481,6 +2519,7 @@ static cudaError_t bptt_launches(hush_trainer_t *t, const hush_inputs *frames, c
       T.dC0 = t->dc0;
     }
     k_fine_bwd<true><<<gf, blk, 0, st>>>(T, t->gT2);
+    if (i > 0) k_fine_pyr_bwd<true><<<gf, blk, 0, st>>>(T, t->gT2);
     k_mid_bwd<3><<<gh, blk, 0, st>>>(T);
     k_mid_bwd<2><<<gh, blk, 0, st>>>(T);
     k_mid_bwd<1><<<gh, blk, 0, st>>>(T);
