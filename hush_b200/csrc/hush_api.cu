@@ -247,6 +247,12 @@ extern "C" int hush_create(const hush_desc *desc, hush_t **out) {
       if (e != cudaSuccess) rc = hush_cuda_fail(h, e, "cudaEventCreate");
     }
   }
+  if (rc == HUSH_OK) {  // the fused frame's coarse branch
+    e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming);
+    if (e != cudaSuccess) rc = hush_cuda_fail(h, e, "creating the coarse-level stream");
+  }
   if (rc != HUSH_OK) {
     g_err = h->last_error;
     hush_destroy(h);
@@ -269,6 +275,9 @@ extern "C" void hush_destroy(hush_t *h) {
       if (e) cudaEventDestroy(e);
   if (h->h2d) cudaStreamDestroy(h->h2d);
   if (h->d2h) cudaStreamDestroy(h->d2h);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
+  if (h->side) cudaStreamDestroy(h->side);
   delete h;
 }
 
@@ -398,10 +407,28 @@ static int encode_frame(hush_t *h, const HushFrame &f, cudaStream_t st, bool tim
       e = launch_pass(p, f, h->w16, st);
     }
   } else {
+    // The coarse chain (the coarse tiles of stages 1 and 2: COARSE1, then coarse2) needs only stage 0's outputs and
+    // feeds only FINE_FINAL (stage 4). Untimed, it runs on the instance's side stream beside the mid chain (mid1 ->
+    // mid2 -> mid3), forked after stage 0 and joined before stage 4 (a captured frame holds them as two parallel
+    // branches), so its tiles fill the issue slots the latency-bound mid kernels leave and each kernel keeps its own
+    // register count. Timed frames keep one stream and each stage's mid and coarse tiles in one launch, so that the
+    // stage times add up to the frame.
+    const bool fork = !timed && h->side;
+    const MlpConst &mc = h->mconst[h->mlp_mode];
     const int ns = fused_stage_count();
     for (int s = 0; s < ns && e == cudaSuccess; s++) {
       mark(fused_stage_label(s));
-      e = launch_fused_stage(s, f, h->mconst[h->mlp_mode], h->mlp_mode, h->tc_blob_dev, st);
+      if (fork && s == 1) {
+        e = cudaEventRecord(h->ev_fork, st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(h->side, h->ev_fork, 0);
+        for (int c = 1; c <= 2 && e == cudaSuccess; c++)
+          e = launch_fused_stage(c, HP_COARSE, f, mc, h->mlp_mode, h->tc_blob_dev, h->side);
+        if (e == cudaSuccess) e = cudaEventRecord(h->ev_join, h->side);
+      }
+      if (fork && s == 4 && e == cudaSuccess) e = cudaStreamWaitEvent(st, h->ev_join, 0);
+      if (e != cudaSuccess) break;
+      const int part = (s == 1 || s == 2) && fork ? HP_MID : HP_BOTH;
+      e = launch_fused_stage(s, part, f, mc, h->mlp_mode, h->tc_blob_dev, st);
     }
   }
   if (timed) {

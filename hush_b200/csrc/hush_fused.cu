@@ -1032,45 +1032,43 @@ HD_INL void tile_mid_pair(const HushFrame &f, int tileX, int tileY, const uint2 
   }
 }
 
-// stage 1: mid1 and coarse1 tiles; stage 2: mid2 and coarse2 tiles; stage 3: mid3 tiles. Tiles t < nA are mid tiles,
-// the rest coarse tiles; the coarse tiles run on the first block indices.
-template <int STAGE>
+// The half-res levels, one kind of tile per launch (PART, a HalfPart): stage 1 mid1 (HP_MID) or COARSE1 (HP_COARSE)
+// tiles, stage 2 mid2 or coarse2 tiles, stage 3 mid3 tiles; block b is mid tile b (nA of them, nAx per row) or
+// coarse tile b (nBx per row).
+template <int STAGE, int PART>
 __global__ void __launch_bounds__(HT_W *HT_H) k_half_stage(const __grid_constant__ HushFrame f, int nAx, int nA,
                                                            int nBx, const __grid_constant__ HalfMaps M) {
   constexpr int SMAX = (HT_W + 8) * (HT_H + 8);
   __shared__ alignas(128) float4 sA[SMAX];
   __shared__ alignas(128) float4 sG[SMAX];
-  // the coarse tiles (fewer, each several times longer) take the first block indices, so they start in the first
-  // wave and the short mid tiles fill in behind them instead of leaving a tail of coarse tiles at the end
-  const int nC = (int)gridDim.x - nA;
-  const int b = blockIdx.x >= nC ? blockIdx.x - nC : blockIdx.x + nA;
-  if (b < nA) {
+  const int b = (int)blockIdx.x;
+  if (PART == HP_MID) {
+    if (b >= nA) return;
     const int tX = b % nAx, tY = b / nAx;
     if (STAGE == 1) tile_mid1(f, tX, tY, sA, sG, M.ok ? &M : nullptr);
     else if (STAGE == 2) tile_mid<2, 2>(f, tX, tY, f.Bh0, f.Bh1, sA, sG, M.ok ? &M.gd2 : nullptr, &M.bh0);
     else tile_mid<4, 3>(f, tX, tY, f.Bh1, f.Bh0, sA, sG, M.ok ? &M.gd4 : nullptr, &M.bh1);
   } else {
-    const int t = b - nA, tX = t % nBx, tY = t / nBx;
+    const int tX = b % nBx, tY = b / nBx;
     if (STAGE == 1) tile_coarse1(f, tX, tY, sA, sG);
     else if (STAGE == 2) tile_coarse2(f, tX, tY, sA, sG, M.qok ? &M : nullptr);
   }
 }
 
-// stages 2 and 3 with the two-pixel mid tiles: 32 x 8 mid2 / mid3 tiles (tile index < nA), and stage 2's coarse2
-// tiles (16 x 8, quarter resolution). Dynamic shared memory: the pair tile, or coarse2's two float4 tiles.
-template <int STAGE>
+// stages 2 and 3 with the two-pixel mid tiles: 32 x 8 mid2 / mid3 tiles (HP_MID), or stage 2's coarse2 tiles (16 x 8,
+// quarter resolution; HP_COARSE). Dynamic shared memory: the pair tile, or coarse2's two float4 tiles.
+template <int STAGE, int PART>
 __global__ void __launch_bounds__(HT_W *HT_H) k_half_pair(const __grid_constant__ HushFrame f, int nAx, int nA,
                                                           int nBx, const __grid_constant__ HalfMaps M) {
   extern __shared__ __align__(128) float4 hp_smem[];  // 128-byte aligned: coarse2 stages its guide by TMA
-  const int nC = (int)gridDim.x - nA;  // coarse tiles first, as in k_half_stage
-  const int b = blockIdx.x >= nC ? blockIdx.x - nC : blockIdx.x + nA;
-  if (b < nA) {
+  const int b = (int)blockIdx.x;
+  if (PART == HP_MID) {
+    if (b >= nA) return;
     if (STAGE == 2) tile_mid_pair<2, 2>(f, b % nAx, b / nAx, f.Bh0, f.Bh1, hp_smem);
     else tile_mid_pair<4, 3>(f, b % nAx, b / nAx, f.Bh1, f.Bh0, hp_smem);
   } else if (STAGE == 2) {
     constexpr int SMAX = (HT_W + 8) * (HT_H + 8);
-    const int t = b - nA;
-    tile_coarse2(f, t % nBx, t / nBx, hp_smem, hp_smem + SMAX, M.qok ? &M : nullptr);
+    tile_coarse2(f, b % nBx, b / nBx, hp_smem, hp_smem + SMAX, M.qok ? &M : nullptr);
   }
 }
 
@@ -1467,8 +1465,8 @@ static const FineMaps &fine_maps(const HushFrame &f) {
   return e.m;
 }
 
-cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpConst &mc, int mlp_mode, const void *mlp_tc,
-                               cudaStream_t st) {
+cudaError_t launch_fused_stage(int stage, int part, const HushFrame &f, const MlpConst &mc, int mlp_mode,
+                               const void *mlp_tc, cudaStream_t st) {
   const int hx = (f.W2 + HT_W - 1) / HT_W, hy = (f.H2 + HT_H - 1) / HT_H;
   const int qx = (f.W4 + HT_W - 1) / HT_W, qy = (f.H4 + HT_H - 1) / HT_H;
   const int hpx = (f.W2 + MP_W - 1) / MP_W;  // two-pixel mid tiles per row
@@ -1495,14 +1493,26 @@ cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpConst &mc
       kern[m]<<<g, KB_NT, smem, st>>>(f, mc, b);
       break;
     }
-    case 1: k_half_stage<1><<<hx * hy + qx * qy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx, half_maps(f)); break;
+    // stages 1 and 2: the mid tiles and the coarse tiles are separate kernels (each with its own register count);
+    // both parts run them one after the other on `st`
+    case 1:
+      if (part != HP_COARSE)
+        k_half_stage<1, HP_MID><<<hx * hy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx, half_maps(f));
+      if (part != HP_MID)
+        k_half_stage<1, HP_COARSE><<<qx * qy, HT_W * HT_H, 0, st>>>(f, hx, hx * hy, qx, half_maps(f));
+      break;
     case 2: {
-      constexpr int sm = mid_pair_smem<2>() > 2 * (HT_W + 8) * (HT_H + 8) * 16 ? mid_pair_smem<2>()
-                                                                               : 2 * (HT_W + 8) * (HT_H + 8) * 16;
-      k_half_pair<2><<<hpx * hy + qx * qy, HT_W * HT_H, sm, st>>>(f, hpx, hpx * hy, qx, half_maps(f));
+      constexpr int smc = 2 * (HT_W + 8) * (HT_H + 8) * 16;  // coarse2's two float4 tiles
+      if (part != HP_COARSE)
+        k_half_pair<2, HP_MID><<<hpx * hy, HT_W * HT_H, mid_pair_smem<2>(), st>>>(f, hpx, hpx * hy, qx, half_maps(f));
+      if (part != HP_MID)
+        k_half_pair<2, HP_COARSE><<<qx * qy, HT_W * HT_H, smc, st>>>(f, hpx, hpx * hy, qx, half_maps(f));
       break;
     }
-    case 3: k_half_pair<3><<<hpx * hy, HT_W * HT_H, mid_pair_smem<4>(), st>>>(f, hpx, hpx * hy, qx, half_maps(f)); break;
+    case 3:
+      if (part == HP_COARSE) break;  // no coarse level in stage 3
+      k_half_pair<3, HP_MID><<<hpx * hy, HT_W * HT_H, mid_pair_smem<4>(), st>>>(f, hpx, hpx * hy, qx, half_maps(f));
+      break;
     case 4:
       k_fine_final_fused<<<dim3((f.W + FT_W - 1) / FT_W, (f.H + FT_H - 1) / FT_H), FT_W * FT_H, 0, st>>>(f, fine_maps(f));
       break;
@@ -1519,9 +1529,11 @@ int fused_kernel_param_count(const void *func) {
                           (const void *)k_temporal_block<2>, (const void *)k_temporal_block<3>};
   for (const void *k : three)
     if (func == k) return 3;  // (f, wp, blob)
-  if (func == (const void *)k_half_stage<1> || func == (const void *)k_half_pair<2> ||
-      func == (const void *)k_half_pair<3>)
-    return 5;  // (f, nAx, nA, nBx, M)
+  const void *half[5] = {(const void *)k_half_stage<1, HP_MID>, (const void *)k_half_stage<1, HP_COARSE>,
+                         (const void *)k_half_pair<2, HP_MID>, (const void *)k_half_pair<2, HP_COARSE>,
+                         (const void *)k_half_pair<3, HP_MID>};
+  for (const void *k : half)
+    if (func == k) return 5;  // (f, nAx, nA, nBx, M)
   if (func == (const void *)k_fine_final_fused) return 2;  // (f, M)
   if (func == (const void *)k_taa_fused) return 1;          // (f)
   return 0;

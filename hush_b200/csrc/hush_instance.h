@@ -53,6 +53,9 @@ struct hush_s {
   uint2 *hin[2][5] = {};
   cudaStream_t h2d = nullptr, d2h = nullptr;
   cudaEvent_t ev_in[2] = {}, ev_used[2] = {}, ev_out[2] = {};
+  // the fused frame's coarse branch (COARSE1 -> coarse2 beside mid1 -> mid3): its stream and the fork / join events
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 // helpers of hush_api.cu

@@ -21,8 +21,14 @@ struct FusedPlan {
   const char *labels[8];
 };
 struct MlpConst;
-cudaError_t launch_fused_stage(int stage, const HushFrame &f, const MlpConst &mc, int mlp_mode, const void *mlp_tc,
-                               cudaStream_t st);
+// Which tiles of a half-res stage a launch runs. The mid tiles and the coarse tiles are separate kernels, so that the
+// coarse chain (COARSE1 -> coarse2) can run beside the mid chain (mid1 -> mid2 -> mid3) on another stream and each
+// kernel keeps its own register count; HP_BOTH runs the stage's two kernels one after the other.
+enum HalfPart { HP_BOTH = 0, HP_MID = 1, HP_COARSE = 2 };
+// One stage of the fused frame on `st`; part (a HalfPart) selects the tiles of stages 1 and 2, the half-res levels
+// with a coarse level beside them (stage 3 has no coarse tiles, the other stages ignore it).
+cudaError_t launch_fused_stage(int stage, int part, const HushFrame &f, const MlpConst &mc, int mlp_mode,
+                               const void *mlp_tc, cudaStream_t st);
 int fused_stage_count();
 const char *fused_stage_label(int stage);
 size_t fused_scratch_bytes(int W, int H);
