@@ -411,8 +411,8 @@ static int encode_frame(hush_t *h, const HushFrame &f, cudaStream_t st, bool tim
     // feeds only FINE_FINAL (stage 4). Untimed, it runs on the instance's side stream beside the mid chain (mid1 ->
     // mid2 -> mid3), forked after stage 0 and joined before stage 4 (a captured frame holds them as two parallel
     // branches), so its tiles fill the issue slots the latency-bound mid kernels leave and each kernel keeps its own
-    // register count. Timed frames keep one stream and each stage's mid and coarse tiles in one launch, so that the
-    // stage times add up to the frame.
+    // register count. Timed frames keep one stream and run each stage's mid and coarse kernels one after the other,
+    // so that the stage times add up to the frame.
     const bool fork = !timed && h->side;
     const MlpConst &mc = h->mconst[h->mlp_mode];
     const int ns = fused_stage_count();

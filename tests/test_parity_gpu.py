@@ -282,7 +282,7 @@ FORM_FRAC = 1e-3
 @pytest.mark.parametrize("mlp", ["fp32", "f16", "bf16"])
 @pytest.mark.parametrize("cfg,n", [(scene.CONFIG_360P, 4), (scene.CONFIG_1080P, 3)], ids=["360p", "1080p"])
 def test_tensor_core_mlp_forms(mlp, cfg, n):
-    """The MLP forms against the f32 oracle at the north-star bound of 2e-3: each tcgen05 layer runs on split-
+    """The MLP forms against the f32 oracle at the parity bound of 2e-3: each tcgen05 layer runs on split-
     precision operands (hi + lo, the residual of the rounding in a second operand) with FP32 accumulation in TMEM,
     so the features and weights (f16 values) are exact and the hidden activations carry 16 (bf16) or 22 (f16)
     bits; the forms are held to the FP32 form's fraction."""
