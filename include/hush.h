@@ -95,7 +95,9 @@ int hush_get_frame(const hush_t *h);
 
 /* denoise(encoder, inputs, timer) (hush.js:813-822, encode 835-874): enqueues one frame on `stream` and returns
  * (in *out) the instance-owned output image (rgba16float, dense, linear HDR, alpha 1). Two images alternate from
- * frame to frame: the pointer stays valid until the next-but-one call (hush.js:796-798). */
+ * frame to frame: the pointer stays valid until the next-but-one call (hush.js:796-798). In the fused schedule part
+ * of the frame (the coarse levels) runs on a stream the instance owns, forked from `stream` and joined back into it
+ * within the frame by events, so the frame as a whole stays ordered on `stream` (also inside a stream capture). */
 int hush_denoise(hush_t *h, const hush_inputs *in, void *stream, const void **out);
 /* denoise with the G-buffer in host memory (a CPU renderer, a replayed capture): the five inputs (rgba16float,
  * `pitch` in bytes, pinned host memory for truly asynchronous copies) are copied into one of two instance-owned
