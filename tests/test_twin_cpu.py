@@ -129,3 +129,26 @@ def test_coarse_restatement_tracks_the_oracle_passes():
         ref = o.buffer(name).astype(np.float64)
         rel = np.abs(got.numpy() - ref) / np.maximum(np.abs(ref), 1e-2 * np.abs(ref).mean())
         assert np.mean(rel <= 2e-3) > 0.995, (name, np.mean(rel <= 2e-3))
+
+
+def test_block_means_restatement_tracks_the_oracle():
+    """oracle/twin.block_means (float64, the window gradient's path from TEMPORAL's A0 into the block means) against
+    the block means the oracle's TEMPORAL pass stores (F2.zw: the mean of the f16 A0 over a block's surface pixels,
+    then stored as f16 rounded toward zero): equal to that rounding, zero on blocks without a surface."""
+    cfg = scene.SceneConfig(64, 48, 3, n_moving=2, seed=9)
+    frames = [scene.frame_host(cfg, i, clean=True) for i in range(3)]
+    o = oracle.OracleHush(cfg.width, cfg.height, builtin_weights())
+    for f in frames[:2]:
+        o.denoise(f)
+    f = frames[2]
+    o.run_pass("temporal", f)
+    c = o.frame & 1
+    A0 = torch.tensor(o.buffer("A0").astype(np.float64))
+    surf = torch.tensor(o.buffer(f"KEY{c}").astype(np.float64)[..., 2] >= 0)
+    got = twin.block_means(A0, surf).numpy()
+    ref = twin.unpack_half(o.buffer("F2"))[..., 4:8].numpy()
+    none = twin.unpack_half(o.buffer("F3"))[..., 3].numpy() <= 0
+    assert none.any() and (~none).any()
+    assert np.all(got[none] == 0.0) and np.all(ref[none] == 0.0)
+    rel = np.abs(got[~none] - ref[~none]) / np.maximum(np.abs(ref[~none]), 1e-2 * np.abs(ref[~none]).mean())
+    assert rel.max() <= 2 ** -9, rel.max()
